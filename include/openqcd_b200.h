@@ -1,0 +1,153 @@
+/*
+ * openqcd_b200.h -- C interface of the B200 (sm_100a) implementation of
+ * openQCD-2.4.2's Wilson-Dirac operator and SAP+GCR solver path.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Drop-in replacements with the reference's names, prototypes and
+ *     argument meaning (include/dirac.h, include/sw_term.h, include/sap.h,
+ *     include/linsolv.h of the reference).  Spinor arguments are arrays in the
+ *     reference's storage order (ipt order, even sites first, VOLUME
+ *     elements); they may live in host memory (pageable or pinned) or in
+ *     device memory.  The calls are synchronous.  The gauge and SW fields
+ *     these operators use are the library's device copies, loaded with
+ *     b200_upload_ud()/b200_upload_swd() or generated on the device; they play
+ *     the role of the reference's udfld()/swdfld() module globals.
+ *
+ *  2. b200_* management calls (geometry, parameters, field upload) and
+ *     b200_dev_* calls on fields that stay on the device in the library's own
+ *     block-major layout (used by solvers, tests and benchmarks).
+ *
+ * Error behaviour: the reference aborts the program on fatal errors
+ * (modules/utils/error.c:119-200 error(), error_root()).  By default this
+ * library does the same (message on stderr, exit(1)); after
+ * b200_set_fatal(0) a failing call records the message, readable with
+ * b200_last_error(), and returns (status -1 where the prototype returns int).
+ * Recoverable solver failures use the reference's ifail/status codes.
+ */
+#ifndef OPENQCD_B200_H
+#define OPENQCD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Types with the memory layout of the reference's include/su3.h:32-112,
+ * defined here only when su3.h has not been included first. */
+#ifndef SU3_H
+typedef struct { float re, im; } complex;
+typedef struct { double re, im; } complex_dble;
+typedef struct { complex c1, c2, c3; } su3_vector;
+typedef struct { complex_dble c1, c2, c3; } su3_vector_dble;
+typedef struct { su3_vector c1, c2, c3, c4; } spinor;
+typedef struct { su3_vector_dble c1, c2, c3, c4; } spinor_dble;
+typedef struct { complex c11, c12, c13, c21, c22, c23, c31, c32, c33; } su3;
+typedef struct { complex_dble c11, c12, c13, c21, c22, c23, c31, c32, c33; } su3_dble;
+typedef struct { float u[36]; } pauli;
+typedef struct { double u[36]; } pauli_dble;
+#endif
+#ifndef SW_TERM_H
+typedef struct b200_pauli_wsp pauli_wsp_t;   /* unused here; kept for the prototype */
+#endif
+
+/* ------------------------------------------------------------------ state */
+
+/* Lattice geometry.  L[4] lattice sizes (x0 = time), bs[4] the SAP block
+ * size, which is also the tile of the device layout.  ipt (may be NULL) is
+ * the reference's ipt[VOLUME] table (main/README.global:128-131); without it
+ * only the b200_dev_* calls are available.  Replaces geometry()
+ * (modules/lattice/geometry.c:273) for this library. */
+int b200_geometry(const int L[4], const int bs[4], const int *ipt);
+
+/* Parameter data base: the values the reference reads from
+ * set_lat_parms (modules/flags/lat_parms.c:216, csw), set_bc_parms (:516,
+ * only type 3 = periodic gauge / antiperiodic quark fields is supported),
+ * set_sw_parms (:920, m0), set_tm_parms (:963, eoflg) and set_sap_parms
+ * (modules/flags/sap_parms.c:112). */
+int b200_set_lat_parms(double csw);
+int b200_set_bc_parms(int type);
+int b200_set_sw_parms(double m0);
+int b200_set_tm_parms(int eoflg);
+int b200_set_sap_parms(const int bs[4], int isolv, int nmr, int ncy);
+
+/* Gauge field in the reference's layout (udfld(), 4*VOLUME su3_dble, 8 links
+ * per odd site, boundary phase already applied: modules/uflds/uflds.c:150,
+ * :338).  Upload refreshes the FP32 copy (assign_ud2u, uflds.c:479). */
+int b200_upload_ud(const su3_dble *ud);
+int b200_download_ud(su3_dble *ud);
+
+/* SW field in the reference's layout (swdfld(), 2*VOLUME pauli_dble, NOT
+ * inverted, i.e. after sw_term(NO_PTS)).  Upload also forms the inverses
+ * and FP32 copies (sw_term(ODD_PTS)/assign_swd2sw equivalents).  Returns 0,
+ * or a bit mask of unsafe inversions (1 even, 2 odd sites; the reference's
+ * Frobenius-condition criterion, pauli_dble.c:55-59). */
+int b200_upload_swd(const pauli_dble *swd);
+/* which = 0: the SW field, 1: its inverse on all sites (mu = 0). */
+int b200_download_swd(pauli_dble *swd, int which);
+
+/* sw_term(NO_PTS) (modules/sw_term/sw_term.c:399) on the device, from the
+ * device gauge field; same return value as b200_upload_swd(). */
+int b200_sw_term(void);
+
+/* Test gauge field on the device: U = exp(eps X) per link, X drawn like the
+ * reference's random_alg() (modules/linalg/liealg.c:289), antiperiodic
+ * time boundary sign applied as set_ud_phase() does. */
+int b200_random_ud(double eps, unsigned long long seed);
+
+const char *b200_last_error(void);
+void b200_set_fatal(int on);
+int b200_sync(void);
+int b200_volume(void);
+
+/* --------------------------------------- drop-in operators (dirac.h:24-52) */
+/* Dw_dble.c:1377 */ void Dw_dble(double mu, spinor_dble *s, spinor_dble *r);
+/* Dw_dble.c:1507 */ void Dwee_dble(double mu, spinor_dble *s, spinor_dble *r);
+/* Dw_dble.c:1565 */ void Dwoo_dble(double mu, spinor_dble *s, spinor_dble *r);
+/* Dw_dble.c:1627 */ void Dwoe_dble(spinor_dble *s, spinor_dble *r);
+/* Dw_dble.c:1705 */ void Dweo_dble(spinor_dble *s, spinor_dble *r);
+/* Dw_dble.c:1792 */ void Dwhat_dble(double mu, spinor_dble *s, spinor_dble *r);
+/* Dw.c:973  */ void Dw(float mu, spinor *s, spinor *r);
+/* Dw.c:1101 */ void Dwee(float mu, spinor *s, spinor *r);
+/* Dw.c:1155 */ void Dwoo(float mu, spinor *s, spinor *r);
+/* Dw.c:1213 */ void Dwoe(spinor *s, spinor *r);
+/* Dw.c:1291 */ void Dweo(spinor *s, spinor *r);
+/* Dw.c:1378 */ void Dwhat(float mu, spinor *s, spinor *r);
+
+/* ------------------------------------ drop-in SW term (sw_term.h:37-56) */
+/* pauli_dble.c:1840 */ void apply_sw_dble(int vol, double mu, pauli_dble *m, spinor_dble *s, spinor_dble *r);
+/* pauli.c:1107      */ void apply_sw(int vol, float mu, pauli *m, spinor *s, spinor *r);
+/* pauli_dble.c:1860 */ int apply_swinv_dble(int vol, double mu, pauli_dble *m, spinor_dble *s,
+                                              pauli_wsp_t *pwsp, spinor_dble *r);
+
+/* ------------------------------------------ drop-in solvers (sap.h:23-34) */
+/* sap.c:720: one SAP cycle on single-precision fields psi, rho */
+void sap(float mu, int isolv, int nmr, spinor *psi, spinor *rho);
+/* sap_gcr.c:140: SAP-preconditioned flexible GCR; same ifail/status codes */
+double sap_gcr(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi,
+               int *ifail, int *status);
+
+/* ------------------------------------ device-resident fields (own layout) */
+/* prec = 64 (spinor_dble) or 32 (spinor).  Operator codes for
+ * b200_dev_dirac: 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo, 5 Dwhat. */
+void *b200_dev_alloc_spinor(int prec);
+void b200_dev_free(void *p);
+int b200_dev_random_spinor(int prec, void *f, double sigma, unsigned long long seed);
+int b200_dev_from_ref(int prec, const void *q, void *f);
+int b200_dev_to_ref(int prec, const void *f, void *q);
+int b200_dev_dirac(int prec, int op, double mu, const void *s, void *r);
+int b200_dev_sap(float mu, int isolv, int nmr, int ncy, void *psi, void *rho);
+double b200_dev_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                        int *ifail, int *status);
+double b200_dev_norm2(int prec, const void *f);
+/* Device time of n back-to-back operator applications, measured with CUDA
+ * events on the library's stream; returns total milliseconds in *ms. */
+int b200_dev_time_dirac(int prec, int op, double mu, const void *s, void *r, int n, float *ms);
+/* Same, for Dw_dble through the drop-in entry point with host arrays in the
+ * reference layout (host->device copy, layout conversion, operator,
+ * conversion back, device->host copy), timed with events around each call. */
+int b200_time_Dw_dble_host(double mu, spinor_dble *s, spinor_dble *r, int n, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,428 @@
+// The C ABI: library context, error handling, and every extern "C" entry
+// point declared in include/openqcd_b200.h.
+#include "lib.h"
+#include "../../include/openqcd_b200.h"
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+namespace qcd {
+
+double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                   int *ifail, int *status);
+
+static Ctx g_ctx;
+static thread_local std::string g_err;
+static bool g_fatal = true;
+
+Ctx &ctx() { return g_ctx; }
+void set_error(const std::string &m) { g_err = m; }
+
+int fail(const std::string &msg) {
+  g_err = msg;
+  if (g_fatal) {
+    fprintf(stderr, "\nError in openqcd_b200: %s\nProgram aborted\n", msg.c_str());
+    fflush(stderr);
+    exit(1);
+  }
+  return -1;
+}
+
+static int need(bool ok, const char *what) { return ok ? 0 : fail(what); }
+
+static int ensure_stage(Ctx &c, size_t bytes) {
+  if (c.stage_bytes >= bytes) return 0;
+  cudaFree(c.stage);
+  c.stage = nullptr;
+  c.stage_bytes = 0;
+  if (cudaMalloc(&c.stage, bytes) != cudaSuccess) return fail("out of device memory (staging buffer)");
+  c.stage_bytes = bytes;
+  return 0;
+}
+
+static int ensure_tmp(Ctx &c) {
+  if (!c.tmp64 && cudaMalloc(&c.tmp64, spinor_bytes(c, 64)) != cudaSuccess) return fail("out of device memory");
+  if (!c.tmp32 && cudaMalloc(&c.tmp32, spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory");
+  return 0;
+}
+
+static int check_ready(const Ctx &c) { return need(c.ready, "geometry not set (call b200_geometry first)"); }
+static int check_fields(const Ctx &c) {
+  if (check_ready(c)) return -1;
+  if (!c.have_ud) return fail("no gauge field on the device (b200_upload_ud or b200_random_ud)");
+  if (!c.have_sw) return fail("no SW field on the device (b200_upload_swd or b200_sw_term)");
+  return 0;
+}
+
+// Run a device-layout operator on reference-layout arrays (host or device):
+// copy in, convert, apply, convert back, copy out.  The output array is read
+// first because the even/odd pieces leave one parity of r unchanged.
+template <typename R>
+static void ref_layout_op(int op, R mu, const void *s, void *r) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return;
+  const int prec = sizeof(R) == 8 ? 64 : 32;
+  const size_t nb = spinor_bytes(c, prec);
+  if (ensure_stage(c, 2 * nb)) return;
+  while (c.ws64.size() < 2 || c.ws32.size() < 2) {
+    void *p;
+    bool d = c.ws64.size() < 2;
+    if (cudaMalloc(&p, spinor_bytes(c, d ? 64 : 32)) != cudaSuccess) { fail("out of device memory"); return; }
+    (d ? c.ws64 : c.ws32).push_back(p);
+  }
+  void *fs = prec == 64 ? c.ws64[0] : c.ws32[0];
+  void *fr = prec == 64 ? c.ws64[1] : c.ws32[1];
+  char *st_in = (char *)c.stage, *st_out = (char *)c.stage + nb;
+  cudaStream_t st = c.stream;
+  cudaMemcpyAsync(st_in, s, nb, cudaMemcpyDefault, st);
+  spinor_from_ref(c, prec, st_in, fs, st);
+  if (op != 0) {
+    cudaMemcpyAsync(st_out, r, nb, cudaMemcpyDefault, st);
+    spinor_from_ref(c, prec, st_out, fr, st);
+  }
+  dirac_op<R>(c, op, mu, fs, fr, prec == 64 ? c.tmp64 : c.tmp32, st);
+  spinor_to_ref(c, prec, fr, st_out, st);
+  cudaMemcpyAsync(r, st_out, nb, cudaMemcpyDefault, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) fail(std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+}
+
+}  // namespace qcd
+
+using qcd::Ctx;
+using qcd::ctx;
+using qcd::fail;
+using qcd::g_err;
+using qcd::g_fatal;
+using qcd::check_ready;
+using qcd::check_fields;
+using qcd::ensure_stage;
+using qcd::ensure_tmp;
+using qcd::need;
+using qcd::ref_layout_op;
+using qcd::spinor_bytes;
+using qcd::spinor_from_ref;
+using qcd::spinor_to_ref;
+using qcd::dirac_op;
+using qcd::sap_prepare;
+using qcd::sap_cycle;
+using qcd::sap_gcr_dev;
+using qcd::la_norm2;
+using qcd::PAR_ALL;
+using qcd::apply_sw_ref_layout;
+using qcd::apply_swinv_ref_layout;
+
+extern "C" {
+
+const char *b200_last_error(void) { return g_err.c_str(); }
+void b200_set_fatal(int on) { g_fatal = on != 0; }
+int b200_sync(void) { return cudaStreamSynchronize(ctx().stream) == cudaSuccess ? 0 : fail("CUDA error"); }
+int b200_volume(void) { return ctx().ready ? ctx().g.vol : 0; }
+
+int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
+  Ctx &c = ctx();
+  if (!c.stream && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail("no CUDA device available");
+  // a new geometry invalidates every resident field
+  void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage};
+  for (void *p : bufs) cudaFree(p);
+  for (void *p : c.ws32) cudaFree(p);
+  for (void *p : c.ws64) cudaFree(p);
+  c.ws32.clear(); c.ws64.clear();
+  c.ud = nullptr; c.u32 = nullptr; c.swd = c.swd_inv = nullptr; c.sw32 = c.sw32_inv = nullptr;
+  c.tmp64 = c.tmp32 = c.stage = nullptr; c.stage_bytes = 0;
+  c.have_ud = c.have_sw = false;
+  c.ready = false;
+  if (geometry_init(c, L, bs, ipt)) return -1;
+  c.ready = true;
+  return 0;
+}
+
+int b200_set_lat_parms(double csw) { ctx().csw = csw; ctx().have_sw = false; return 0; }
+int b200_set_bc_parms(int type) {
+  if (type != 3) return fail("set_bc_parms: only boundary condition type 3 is supported");
+  ctx().bc = type;
+  return 0;
+}
+int b200_set_sw_parms(double m0) { ctx().m0 = m0; ctx().have_sw = false; return 0; }
+int b200_set_tm_parms(int eoflg) { ctx().eoflg = eoflg != 0; return 0; }
+
+int b200_set_sap_parms(const int bs[4], int isolv, int nmr, int ncy) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  for (int mu = 0; mu < 4; mu++)
+    if (bs[mu] != c.g.bs[mu]) return fail("set_sap_parms: the SAP block size must equal the geometry block size");
+  if (isolv < 0 || isolv > 1 || nmr < 1 || ncy < 1) return fail("set_sap_parms: parameters are out of range");
+  c.isolv = isolv; c.nmr = nmr; c.ncy = ncy;
+  c.sap_set = true;
+  return 0;
+}
+
+int b200_upload_ud(const su3_dble *ud) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  size_t n = (size_t)c.g.vol * 36 * sizeof(double2);
+  if (!c.ud && cudaMalloc(&c.ud, n) != cudaSuccess) return fail("out of device memory (gauge field)");
+  if (ensure_stage(c, n)) return -1;
+  cudaMemcpyAsync(c.stage, ud, 4 * (size_t)c.g.vol * sizeof(su3_dble), cudaMemcpyDefault, c.stream);
+  if (links_from_ref(c, c.stage, c.stream)) return -1;
+  c.have_ud = true;
+  if (links_refresh_f32(c, c.stream)) return -1;
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("upload_ud: CUDA error");
+}
+
+int b200_download_ud(su3_dble *ud) {
+  Ctx &c = ctx();
+  if (check_ready(c) || need(c.have_ud, "no gauge field on the device")) return -1;
+  size_t n = 4 * (size_t)c.g.vol * sizeof(su3_dble);
+  if (ensure_stage(c, n)) return -1;
+  if (links_to_ref(c, c.stage, c.stream)) return -1;
+  cudaMemcpyAsync(ud, c.stage, n, cudaMemcpyDefault, c.stream);
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("download_ud: CUDA error");
+}
+
+int b200_upload_swd(const pauli_dble *swd) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  size_t n = 2 * (size_t)c.g.vol * sizeof(pauli_dble);
+  if (!c.swd && cudaMalloc(&c.swd, n) != cudaSuccess) return fail("out of device memory (SW field)");
+  if (ensure_stage(c, n)) return -1;
+  cudaMemcpyAsync(c.stage, swd, n, cudaMemcpyDefault, c.stream);
+  if (pauli_from_ref(c, c.stage, c.stream)) return -1;
+  if (sw_refresh_derived(c, c.stream)) return -1;
+  return c.sw_inv_fail;
+}
+
+int b200_download_swd(pauli_dble *swd, int which) {
+  Ctx &c = ctx();
+  if (check_ready(c) || need(c.have_sw, "no SW field on the device")) return -1;
+  size_t n = 2 * (size_t)c.g.vol * sizeof(pauli_dble);
+  if (ensure_stage(c, n)) return -1;
+  if (pauli_to_ref(c, which, c.stage, c.stream)) return -1;
+  cudaMemcpyAsync(swd, c.stage, n, cudaMemcpyDefault, c.stream);
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("download_swd: CUDA error");
+}
+
+int b200_sw_term(void) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  if (sw_compute(c, c.stream)) return -1;
+  return c.sw_inv_fail;
+}
+
+int b200_random_ud(double eps, unsigned long long seed) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  if (gen_links(c, eps, seed, c.stream)) return -1;
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("random_ud: CUDA error");
+}
+
+// ------------------------------------------------------- drop-in operators
+void Dw_dble(double mu, spinor_dble *s, spinor_dble *r) { ref_layout_op<double>(0, mu, s, r); }
+void Dwee_dble(double mu, spinor_dble *s, spinor_dble *r) { ref_layout_op<double>(1, mu, s, r); }
+void Dwoo_dble(double mu, spinor_dble *s, spinor_dble *r) { ref_layout_op<double>(2, mu, s, r); }
+void Dwoe_dble(spinor_dble *s, spinor_dble *r) { ref_layout_op<double>(3, 0.0, s, r); }
+void Dweo_dble(spinor_dble *s, spinor_dble *r) { ref_layout_op<double>(4, 0.0, s, r); }
+void Dwhat_dble(double mu, spinor_dble *s, spinor_dble *r) { ref_layout_op<double>(5, mu, s, r); }
+void Dw(float mu, spinor *s, spinor *r) { ref_layout_op<float>(0, mu, s, r); }
+void Dwee(float mu, spinor *s, spinor *r) { ref_layout_op<float>(1, mu, s, r); }
+void Dwoo(float mu, spinor *s, spinor *r) { ref_layout_op<float>(2, mu, s, r); }
+void Dwoe(spinor *s, spinor *r) { ref_layout_op<float>(3, 0.0f, s, r); }
+void Dweo(spinor *s, spinor *r) { ref_layout_op<float>(4, 0.0f, s, r); }
+void Dwhat(float mu, spinor *s, spinor *r) { ref_layout_op<float>(5, mu, s, r); }
+
+// Site-local SW term on arbitrary arrays of vol sites.
+static void sw_local(int prec, int vol, double mu, const void *m, const void *s, void *r, bool inverse, int *ifail) {
+  Ctx &c = ctx();
+  if (!c.stream && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) {
+    fail("no CUDA device available");
+    return;
+  }
+  if (vol <= 0) return;
+  size_t es = prec == 64 ? 8 : 4;
+  size_t nm = (size_t)vol * 72 * es, ns = (size_t)vol * 24 * es;
+  if (ensure_stage(c, nm + 2 * ns + 64)) return;
+  char *dm = (char *)c.stage, *ds = dm + nm, *dr = ds + ns;
+  int *df = (int *)(dr + ns);
+  cudaStream_t st = c.stream;
+  cudaMemcpyAsync(dm, m, nm, cudaMemcpyDefault, st);
+  cudaMemcpyAsync(ds, s, ns, cudaMemcpyDefault, st);
+  if (inverse) {
+    cudaMemsetAsync(df, 0, sizeof(int), st);
+    apply_swinv_ref_layout(vol, mu, dm, ds, dr, df, st);
+  } else {
+    apply_sw_ref_layout(prec, vol, mu, dm, ds, dr, st);
+  }
+  cudaMemcpyAsync(r, dr, ns, cudaMemcpyDefault, st);
+  int hf = 0;
+  if (inverse) cudaMemcpyAsync(&hf, df, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) fail("apply_sw: CUDA error");
+  if (ifail) *ifail = hf;
+}
+
+void apply_sw_dble(int vol, double mu, pauli_dble *m, spinor_dble *s, spinor_dble *r) {
+  sw_local(64, vol, mu, m, s, r, false, nullptr);
+}
+void apply_sw(int vol, float mu, pauli *m, spinor *s, spinor *r) { sw_local(32, vol, mu, m, s, r, false, nullptr); }
+int apply_swinv_dble(int vol, double mu, pauli_dble *m, spinor_dble *s, pauli_wsp_t *pwsp, spinor_dble *r) {
+  (void)pwsp;
+  int f = 0;
+  sw_local(64, vol, mu, m, s, r, true, &f);
+  return f;
+}
+
+// ---------------------------------------------------------- drop-in solvers
+void sap(float mu, int isolv, int nmr, spinor *psi, spinor *rho) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return;
+  if (isolv == 1 && (c.sw_inv_fail & 2)) { fail("sap: the SW term on the odd sites is not safely invertible"); return; }
+  if (sap_prepare(c, c.stream)) return;
+  size_t nb = spinor_bytes(c, 32);
+  if (ensure_stage(c, 2 * nb)) return;
+  void *fp = b200_dev_alloc_spinor(32), *fr = b200_dev_alloc_spinor(32), *fb = b200_dev_alloc_spinor(32);
+  if (!fp || !fr || !fb) return;
+  char *s0 = (char *)c.stage, *s1 = s0 + nb;
+  cudaStream_t st = c.stream;
+  cudaMemcpyAsync(s0, psi, nb, cudaMemcpyDefault, st);
+  cudaMemcpyAsync(s1, rho, nb, cudaMemcpyDefault, st);
+  spinor_from_ref(c, 32, s0, fp, st);
+  spinor_from_ref(c, 32, s1, fr, st);
+  sap_cycle(c, mu, isolv, nmr, fp, fr, fb, st);
+  spinor_to_ref(c, 32, fp, s0, st);
+  spinor_to_ref(c, 32, fr, s1, st);
+  cudaMemcpyAsync(psi, s0, nb, cudaMemcpyDefault, st);
+  cudaMemcpyAsync(rho, s1, nb, cudaMemcpyDefault, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) fail("sap: CUDA error");
+  cudaFree(fp); cudaFree(fr); cudaFree(fb);
+}
+
+double sap_gcr(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi, int *ifail,
+               int *status) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1.0;
+  size_t nb = spinor_bytes(c, 64);
+  if (ensure_stage(c, nb)) return -1.0;
+  void *fe = b200_dev_alloc_spinor(64), *fp = b200_dev_alloc_spinor(64);
+  if (!fe || !fp) return -1.0;
+  cudaStream_t st = c.stream;
+  cudaMemcpyAsync(c.stage, eta, nb, cudaMemcpyDefault, st);
+  spinor_from_ref(c, 64, c.stage, fe, st);
+  double rho = sap_gcr_dev(c, nkv, nmx, istop, res, mu, fe, fp, ifail, status);
+  spinor_to_ref(c, 64, fp, c.stage, st);
+  cudaMemcpyAsync(psi, c.stage, nb, cudaMemcpyDefault, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) fail("sap_gcr: CUDA error");
+  cudaFree(fe); cudaFree(fp);
+  return rho;
+}
+
+// ------------------------------------------------------- device-resident API
+void *b200_dev_alloc_spinor(int prec) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return nullptr;
+  void *p = nullptr;
+  if (cudaMalloc(&p, spinor_bytes(c, prec)) != cudaSuccess) { fail("out of device memory"); return nullptr; }
+  cudaMemset(p, 0, spinor_bytes(c, prec));
+  return p;
+}
+void b200_dev_free(void *p) { cudaFree(p); }
+
+int b200_dev_random_spinor(int prec, void *f, double sigma, unsigned long long seed) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  if (gen_spinor(c, prec, f, sigma, seed, c.stream)) return -1;
+  return b200_sync();
+}
+
+int b200_dev_from_ref(int prec, const void *q, void *f) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  size_t nb = spinor_bytes(c, prec);
+  if (ensure_stage(c, nb)) return -1;
+  cudaMemcpyAsync(c.stage, q, nb, cudaMemcpyDefault, c.stream);
+  if (spinor_from_ref(c, prec, c.stage, f, c.stream)) return -1;
+  return b200_sync();
+}
+
+int b200_dev_to_ref(int prec, const void *f, void *q) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  size_t nb = spinor_bytes(c, prec);
+  if (ensure_stage(c, nb)) return -1;
+  if (spinor_to_ref(c, prec, f, c.stage, c.stream)) return -1;
+  cudaMemcpyAsync(q, c.stage, nb, cudaMemcpyDefault, c.stream);
+  return b200_sync();
+}
+
+int b200_dev_dirac(int prec, int op, double mu, const void *s, void *r) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return -1;
+  int rc = prec == 64 ? dirac_op<double>(c, op, mu, s, r, c.tmp64, c.stream)
+                      : dirac_op<float>(c, op, (float)mu, s, r, c.tmp32, c.stream);
+  if (rc) return fail("dirac: bad operator code or launch failure");
+  return b200_sync();
+}
+
+int b200_dev_sap(float mu, int isolv, int nmr, int ncy, void *psi, void *rho) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return -1;
+  if (isolv == 1 && (c.sw_inv_fail & 2)) return fail("sap: the SW term on the odd sites is not safely invertible");
+  if (sap_prepare(c, c.stream)) return -1;
+  for (int n = 0; n < ncy; n++)
+    if (sap_cycle(c, mu, isolv, nmr, psi, rho, c.tmp32, c.stream)) return -1;
+  return b200_sync();
+}
+
+double b200_dev_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
+                        int *status) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return -1.0;
+  return sap_gcr_dev(c, nkv, nmx, istop, res, mu, eta, psi, ifail, status);
+}
+
+double b200_dev_norm2(int prec, const void *f) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1.0;
+  double r[2];
+  if (la_norm2(c, prec, f, PAR_ALL, r)) return -1.0;
+  return r[0] + r[1];
+}
+
+int b200_dev_time_dirac(int prec, int op, double mu, const void *s, void *r, int n, float *ms) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaStreamSynchronize(c.stream);
+  cudaEventRecord(e0, c.stream);
+  for (int i = 0; i < n; i++) {
+    if (prec == 64) dirac_op<double>(c, op, mu, s, r, c.tmp64, c.stream);
+    else dirac_op<float>(c, op, (float)mu, s, r, c.tmp32, c.stream);
+  }
+  cudaEventRecord(e1, c.stream);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("time_dirac: CUDA error");
+}
+
+int b200_time_Dw_dble_host(double mu, spinor_dble *s, spinor_dble *r, int n, float *ms) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaStreamSynchronize(c.stream);
+  cudaEventRecord(e0, c.stream);
+  for (int i = 0; i < n; i++) Dw_dble(mu, s, r);
+  cudaEventRecord(e1, c.stream);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("time_Dw_dble_host: CUDA error");
+}
+
+}  // extern "C"

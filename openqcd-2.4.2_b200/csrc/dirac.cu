@@ -1,0 +1,131 @@
+// Wilson-Dirac operator kernels (full, even/odd pieces, Dwhat) in FP64 and
+// FP32 on the block-major layout of qcd.cuh.
+//
+// One templated kernel covers every operator of the reference's
+// modules/dirac/Dw_dble.c and modules/dirac/Dw.c.  Per site x of the selected
+// parity it forms
+//     acc  = (A(x) + i mu_x gamma5) s(x)                    if OP_SW
+//     h    = -1/2 sum_mu [hop terms of t around x]          if OP_HOP/OP_HOPSUB
+//     h    = A(x)^-1 h                                      if OP_INV
+//     acc += h  (OP_HOP)   or   acc -= h  (OP_HOPSUB)
+//     r(x) = acc  or  r(x) += acc (OP_ACC)
+// which gives
+//     Dw    : all sites, SW|HOP            (Dw_dble.c:1377)
+//     Dwee  : even,      SW                (Dw_dble.c:1507)
+//     Dwoo  : odd,       SW                (Dw_dble.c:1565)
+//     Dwoe  : odd,       HOP               (Dw_dble.c:1627)
+//     Dweo  : even,      HOPSUB|ACC        (Dw_dble.c:1705, subtracts from r)
+//     Dwhat : odd HOP|INV into a scratch field, then even SW|HOPSUB
+//                                          (Dw_dble.c:1792)
+// It is a pure gather: each thread reads the spinors of its 8 neighbours and
+// the 8 links that touch its site, and writes only its own site.
+#include "lib.h"
+
+namespace qcd {
+
+enum { OP_SW = 1, OP_HOP = 2, OP_HOPSUB = 4, OP_INV = 8, OP_ACC = 16 };
+
+template <typename R, int OPS, int PAR>
+__global__ void __launch_bounds__(128) dirac_kernel(Geom g, const void *__restrict__ s, const void *__restrict__ t,
+                                                    void *r, const void *__restrict__ u,
+                                                    const void *__restrict__ sw, const void *__restrict__ swinv,
+                                                    R mu_e, R mu_o, const int *__restrict__ sched) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int p, blk, si;
+  if (PAR == 2) {
+    if (i >= g.vol) return;
+    int b = i / g.vb;
+    int rr = i - b * g.vb;
+    p = rr >= g.vbh;
+    si = rr - p * g.vbh;
+    blk = sched ? __ldg(sched + b) : b;
+  } else {
+    if (i >= g.volh) return;
+    p = PAR;
+    blk = i / g.vbh;
+    si = i - blk * g.vbh;
+    if (sched) blk = __ldg(sched + blk);
+  }
+  Site x;
+  site_decode(g, p, blk, si, x);
+  const int chunk = p * g.nbl + blk;
+
+  spinor<R> acc;
+  if (OPS & OP_SW) {
+    spinor<R> in = Store<R>::load_spinor(s, chunk, si, g.vbh);
+    acc = apply_sw_site<R>(sw, chunk, si, g.vbh, p == 0 ? mu_e : mu_o, in);
+  } else {
+    szero(acc);
+  }
+
+  if (OPS & (OP_HOP | OP_HOPSUB)) {
+    spinor<R> h;
+    szero(h);
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      int c2, s2;
+      site_nbr(g, x, mu, +1, c2, s2);
+      {
+        spinor<R> sp = Store<R>::load_spinor(t, c2, s2, g.vbh);
+        su3<R> uu = Store<R>::load_link(u, chunk, mu, si, g.vbh);
+        hop_fwd<R>(mu, uu, sp, h);
+      }
+      site_nbr(g, x, mu, -1, c2, s2);
+      {
+        spinor<R> sm = Store<R>::load_spinor(t, c2, s2, g.vbh);
+        su3<R> uu = Store<R>::load_link(u, c2, mu, s2, g.vbh);
+        hop_bwd<R>(mu, uu, sm, h);
+      }
+    }
+    sscale<R>(h, (R)-0.5);
+    if (OPS & OP_INV) h = apply_sw_site<R>(swinv, chunk, si, g.vbh, (R)0, h);
+    if (OPS & OP_HOP) sadd(acc, h);
+    else ssub(acc, h);
+  }
+
+  if (OPS & OP_ACC) {
+    spinor<R> old = Store<R>::load_spinor_rw(r, chunk, si, g.vbh);
+    sadd(old, acc);
+    Store<R>::store_spinor(r, chunk, si, g.vbh, old);
+  } else {
+    Store<R>::store_spinor(r, chunk, si, g.vbh, acc);
+  }
+}
+
+template <typename R, int OPS, int PAR>
+static void launch(const Ctx &c, const void *s, const void *t, void *r, R mu_e, R mu_o, bool inv,
+                   cudaStream_t st) {
+  const void *u = sizeof(R) == 8 ? (const void *)c.ud : (const void *)c.u32;
+  const void *sw = sizeof(R) == 8 ? (const void *)c.swd : (const void *)c.sw32;
+  const void *swinv = sizeof(R) == 8 ? (const void *)c.swd_inv : (const void *)c.sw32_inv;
+  (void)inv;
+  int n = PAR == 2 ? c.g.vol : c.g.volh;
+  int threads = 128;
+  dirac_kernel<R, OPS, PAR><<<(n + threads - 1) / threads, threads, 0, st>>>(c.g, s, t, r, u, sw, swinv, mu_e, mu_o,
+                                                                           PAR == 2 ? c.sched : nullptr);
+}
+
+// op: 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo, 5 Dwhat.  tmp: a scratch field
+// (same precision) used by Dwhat for its odd intermediate.
+template <typename R>
+int dirac_op(const Ctx &c, int op, R mu, const void *s, void *r, void *tmp, cudaStream_t st) {
+  R muo = c.eoflg ? (R)0 : mu;
+  switch (op) {
+    case 0: launch<R, OP_SW | OP_HOP, 2>(c, s, s, r, mu, muo, false, st); break;
+    case 1: launch<R, OP_SW, 0>(c, s, s, r, mu, mu, false, st); break;
+    case 2: launch<R, OP_SW, 1>(c, s, s, r, muo, muo, false, st); break;
+    case 3: launch<R, OP_HOP, 1>(c, s, s, r, mu, mu, false, st); break;
+    case 4: launch<R, OP_HOPSUB | OP_ACC, 0>(c, s, s, r, mu, mu, false, st); break;
+    case 5:
+      launch<R, OP_HOP | OP_INV, 1>(c, s, s, tmp, (R)0, (R)0, true, st);
+      launch<R, OP_SW | OP_HOPSUB, 0>(c, s, tmp, r, mu, mu, false, st);
+      break;
+    default: return -1;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template int dirac_op<double>(const Ctx &, int, double, const void *, void *, void *, cudaStream_t);
+template int dirac_op<float>(const Ctx &, int, float, const void *, void *, void *, cudaStream_t);
+
+}  // namespace qcd

@@ -1,0 +1,216 @@
+// Geometry tables and conversion between the reference's storage order and
+// the device layout of qcd.cuh.
+//
+// The reference labels sites by ix = ipt[x3 + L3*x2 + L2*L3*x1 + L1*L2*L3*x0]
+// with the even sites first (main/README.global:128-160).  Its spinor fields
+// are arrays of 24 doubles (spinor_dble) or 24 floats (spinor) in that order,
+// its gauge field stores 8 links per odd site, U(x,mu) at ud[8*(ix-V/2)+2mu]
+// and U(x-mu,mu) at ud[8*(ix-V/2)+2mu+1] (main/README.global:229-262), and its
+// SW field stores the upper/lower Pauli matrix of site ix at swd[2ix] and
+// swd[2ix+1] (modules/sw_term/sw_term.c:42-44).  The tables built here map
+// every device site to those positions; the conversion kernels are plain
+// gathers.
+#include "lib.h"
+#include <cstring>
+
+namespace qcd {
+
+static int pack4(const int a[4]) { return a[0] | (a[1] << 8) | (a[2] << 16) | (a[3] << 24); }
+
+int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
+  Geom &g = c.g;
+  for (int mu = 0; mu < 4; mu++) {
+    if (L[mu] < 2 || bs[mu] < 2 || (bs[mu] % 2) || (L[mu] % bs[mu]))
+      return fail("geometry: block sizes must be even and divide the lattice sizes");
+    if ((L[mu] / bs[mu]) % 2) return fail("geometry: the number of blocks along every axis must be even");
+    if (L[mu] > 4096 || bs[mu] > 255 || L[mu] / bs[mu] > 255) return fail("geometry: sizes out of range");
+    g.L[mu] = L[mu]; g.bs[mu] = bs[mu]; g.nb[mu] = L[mu] / bs[mu];
+  }
+  g.vol = L[0] * L[1] * L[2] * L[3];
+  g.volh = g.vol / 2;
+  g.nbl = g.nb[0] * g.nb[1] * g.nb[2] * g.nb[3];
+  g.vb = bs[0] * bs[1] * bs[2] * bs[3];
+  g.vbh = g.vb / 2;
+  g.lstr[3] = 1; g.lstr[2] = bs[3]; g.lstr[1] = bs[3] * bs[2]; g.lstr[0] = bs[3] * bs[2] * bs[1];
+  g.bstr[3] = 1; g.bstr[2] = g.nb[3]; g.bstr[1] = g.nb[3] * g.nb[2]; g.bstr[0] = g.nb[3] * g.nb[2] * g.nb[1];
+
+  std::vector<int> bco(g.nbl), lco(g.vb), sch(g.nbl);
+  for (int b = 0; b < g.nbl; b++) {
+    int n[4], r = b;
+    for (int mu = 3; mu >= 0; mu--) { n[mu] = r % g.nb[mu]; r /= g.nb[mu]; }
+    bco[b] = pack4(n);
+    sch[b] = b;
+  }
+  for (int l = 0; l < g.vb; l++) {
+    int y[4], r = l;
+    for (int mu = 3; mu >= 0; mu--) { y[mu] = r % bs[mu]; r /= bs[mu]; }
+    int p = (y[0] + y[1] + y[2] + y[3]) & 1;
+    lco[p * g.vbh + l / 2] = pack4(y);
+  }
+  cudaFree(c.d_bcoord); cudaFree(c.d_lcoord); cudaFree(c.sched);
+  if (cudaMalloc(&c.d_bcoord, g.nbl * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c.d_lcoord, g.vb * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c.sched, g.nbl * sizeof(int)) != cudaSuccess)
+    return fail("geometry: device allocation failed");
+  cudaMemcpy(c.d_bcoord, bco.data(), g.nbl * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(c.d_lcoord, lco.data(), g.vb * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemcpy(c.sched, sch.data(), g.nbl * sizeof(int), cudaMemcpyHostToDevice);
+  g.bcoord = c.d_bcoord;
+  g.lcoord = c.d_lcoord;
+
+  cudaFree(c.d_dev2q); cudaFree(c.d_link2q);
+  c.d_dev2q = c.d_link2q = nullptr;
+  c.have_ipt = false;
+  if (ipt) {
+    std::vector<int> d2q(g.vol), l2q(4 * (size_t)g.vol), seen(g.vol, 0);
+    auto lex = [&](const int x[4]) { return x[3] + L[3] * (x[2] + L[2] * (x[1] + L[1] * x[0])); };
+    for (int p = 0; p < 2; p++)
+      for (int b = 0; b < g.nbl; b++)
+        for (int s = 0; s < g.vbh; s++) {
+          int n[4], y[4], x[4];
+          for (int mu = 0; mu < 4; mu++) {
+            n[mu] = (bco[b] >> (8 * mu)) & 255;
+            y[mu] = (lco[p * g.vbh + s] >> (8 * mu)) & 255;
+            x[mu] = n[mu] * bs[mu] + y[mu];
+          }
+          size_t d = (size_t)(p * g.nbl + b) * g.vbh + s;
+          int ix = ipt[lex(x)];
+          if (ix < 0 || ix >= g.vol || seen[ix] || ((ix >= g.volh) != (p == 1)))
+            return fail("geometry: ipt[] is not an even-first permutation of the lattice sites");
+          seen[ix] = 1;
+          d2q[d] = ix;
+          for (int mu = 0; mu < 4; mu++) {
+            if (p == 1) {
+              l2q[4 * d + mu] = 8 * (ix - g.volh) + 2 * mu;
+            } else {
+              int xu[4] = {x[0], x[1], x[2], x[3]};
+              xu[mu] = (xu[mu] + 1) % L[mu];
+              int iy = ipt[lex(xu)];
+              l2q[4 * d + mu] = 8 * (iy - g.volh) + 2 * mu + 1;
+            }
+          }
+        }
+    if (cudaMalloc(&c.d_dev2q, g.vol * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c.d_link2q, 4 * (size_t)g.vol * sizeof(int)) != cudaSuccess)
+      return fail("geometry: device allocation failed");
+    cudaMemcpy(c.d_dev2q, d2q.data(), g.vol * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(c.d_link2q, l2q.data(), 4 * (size_t)g.vol * sizeof(int), cudaMemcpyHostToDevice);
+    c.h_dev2q = d2q;
+    c.have_ipt = true;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("geometry: CUDA error");
+}
+
+// ------------------------------------------------------------------ spinors
+template <typename R>
+__global__ void k_spinor_from_ref(Geom g, const int *__restrict__ d2q, const R *__restrict__ q, void *dev) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= g.vol) return;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  const R *src = q + (size_t)__ldg(d2q + d) * 24;
+  spinor<R> v;
+#pragma unroll
+  for (int k = 0; k < 12; k++) v.c[k / 3].c[k % 3] = mk<R>(src[2 * k], src[2 * k + 1]);
+  Store<R>::store_spinor(dev, chunk, s, g.vbh, v);
+}
+
+template <typename R>
+__global__ void k_spinor_to_ref(Geom g, const int *__restrict__ d2q, const void *dev, R *q) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= g.vol) return;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  R *dst = q + (size_t)__ldg(d2q + d) * 24;
+  spinor<R> v = Store<R>::load_spinor_rw(dev, chunk, s, g.vbh);
+#pragma unroll
+  for (int k = 0; k < 12; k++) { dst[2 * k] = v.c[k / 3].c[k % 3].re; dst[2 * k + 1] = v.c[k / 3].c[k % 3].im; }
+}
+
+int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st) {
+  if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
+  int n = c.g.vol, t = 128;
+  if (prec == 64) k_spinor_from_ref<double><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const double *)q, dev);
+  else k_spinor_from_ref<float><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const float *)q, dev);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("spinor_from_ref: launch failed");
+}
+
+int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st) {
+  if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
+  int n = c.g.vol, t = 128;
+  if (prec == 64) k_spinor_to_ref<double><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, dev, (double *)q);
+  else k_spinor_to_ref<float><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, dev, (float *)q);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("spinor_to_ref: launch failed");
+}
+
+// -------------------------------------------------------------------- links
+__global__ void k_links_from_ref(Geom g, const int *__restrict__ l2q, const double *__restrict__ q, double2 *ud) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 4 * g.vol) return;
+  int d = i >> 2, mu = i & 3;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  const double *src = q + (size_t)__ldg(l2q + i) * 18;
+  double2 *dst = ud + ((size_t)chunk * 4 + mu) * 9 * g.vbh + s;
+#pragma unroll
+  for (int k = 0; k < 9; k++) dst[(size_t)k * g.vbh] = make_double2(src[2 * k], src[2 * k + 1]);
+}
+
+__global__ void k_links_to_ref(Geom g, const int *__restrict__ l2q, const double2 *__restrict__ ud, double *q) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 4 * g.vol) return;
+  int d = i >> 2, mu = i & 3;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  double *dst = q + (size_t)__ldg(l2q + i) * 18;
+  const double2 *src = ud + ((size_t)chunk * 4 + mu) * 9 * g.vbh + s;
+#pragma unroll
+  for (int k = 0; k < 9; k++) { double2 v = src[(size_t)k * g.vbh]; dst[2 * k] = v.x; dst[2 * k + 1] = v.y; }
+}
+
+int links_from_ref(Ctx &c, const void *qud, cudaStream_t st) {
+  if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
+  int n = 4 * c.g.vol, t = 128;
+  k_links_from_ref<<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_link2q, (const double *)qud, c.ud);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("links_from_ref: launch failed");
+}
+
+int links_to_ref(const Ctx &c, void *qud, cudaStream_t st) {
+  if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
+  int n = 4 * c.g.vol, t = 128;
+  k_links_to_ref<<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_link2q, c.ud, (double *)qud);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("links_to_ref: launch failed");
+}
+
+// -------------------------------------------------------------------- pauli
+__global__ void k_pauli_from_ref(Geom g, const int *__restrict__ d2q, const double *__restrict__ q, double2 *sw) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= g.vol) return;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  const double *src = q + (size_t)__ldg(d2q + d) * 72;
+  double2 *dst = sw + (size_t)chunk * 36 * g.vbh + s;
+#pragma unroll 4
+  for (int k = 0; k < 36; k++) dst[(size_t)k * g.vbh] = make_double2(src[2 * k], src[2 * k + 1]);
+}
+
+__global__ void k_pauli_to_ref(Geom g, const int *__restrict__ d2q, const double2 *__restrict__ sw, double *q) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= g.vol) return;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  double *dst = q + (size_t)__ldg(d2q + d) * 72;
+  const double2 *src = sw + (size_t)chunk * 36 * g.vbh + s;
+#pragma unroll 4
+  for (int k = 0; k < 36; k++) { double2 v = src[(size_t)k * g.vbh]; dst[2 * k] = v.x; dst[2 * k + 1] = v.y; }
+}
+
+int pauli_from_ref(Ctx &c, const void *qsw, cudaStream_t st) {
+  if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
+  int n = c.g.vol, t = 128;
+  k_pauli_from_ref<<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const double *)qsw, c.swd);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("pauli_from_ref: launch failed");
+}
+
+int pauli_to_ref(const Ctx &c, int which, void *qsw, cudaStream_t st) {
+  if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
+  int n = c.g.vol, t = 128;
+  k_pauli_to_ref<<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, which ? c.swd_inv : c.swd, (double *)qsw);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("pauli_to_ref: launch failed");
+}
+
+}  // namespace qcd

@@ -1,0 +1,109 @@
+// Internal host-side declarations: the library context (geometry, resident
+// fields, parameters) and the launchers each .cu file provides.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "qcd.cuh"
+
+namespace qcd {
+
+// Everything the reference keeps in module-global state for this path:
+// geometry (lattice/geometry.c), the gauge field (uflds/uflds.c udfld/ufld),
+// the SW field (sw_term/swflds.c swdfld/swfld) and the parameter data base
+// (flags/lat_parms.c, flags/sap_parms.c).
+struct Ctx {
+  bool ready = false;
+  int dev = 0;
+  Geom g{};                     // device pointers inside point to the tables below
+  int *d_bcoord = nullptr, *d_lcoord = nullptr;
+  int *sched = nullptr;         // block traversal order for full-lattice kernels
+  // reference (openQCD) storage order, when the caller supplied its ipt[]
+  bool have_ipt = false;
+  int *d_dev2q = nullptr;       // [vol] device site (chunk*vbh+s) -> reference index ix
+  int *d_link2q = nullptr;      // [4*vol] (device site, mu) -> slot in the reference ud[4V]
+  std::vector<int> h_dev2q;
+
+  // parameters
+  double csw = 0.0, m0 = 0.0;
+  int bc = 3, eoflg = 0;
+  int isolv = 1, nmr = 4, ncy = 5;
+  bool sap_set = false;
+
+  // resident fields
+  double2 *ud = nullptr;        // FP64 forward links
+  float2 *u32 = nullptr;        // FP32 copy (assign_ud2u)
+  double2 *swd = nullptr;       // FP64 SW term, not inverted
+  double2 *swd_inv = nullptr;   // FP64 inverse (mu = 0) on all sites
+  float4 *sw32 = nullptr;       // FP32 copies (assign_swd2sw)
+  float4 *sw32_inv = nullptr;
+  bool have_ud = false, have_sw = false, sw_inv_ok = false;
+  int sw_inv_fail = 0;
+
+  // scratch
+  void *tmp64 = nullptr;        // one FP64 spinor field
+  void *tmp32 = nullptr;        // one FP32 spinor field
+  void *stage = nullptr;        // staging buffer for reference-layout transfers
+  size_t stage_bytes = 0;
+  double *red = nullptr;        // reduction partials
+  double *red_out = nullptr;    // reduction results (device)
+  double *h_red = nullptr;      // pinned host mirror of red_out
+  int red_blocks = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<void *> ws32, ws64;   // solver workspaces (reserve_ws / reserve_wsd)
+};
+
+Ctx &ctx();
+void set_error(const std::string &msg);
+int fail(const std::string &msg);   // records msg, returns -1 (or aborts in fatal mode)
+
+size_t spinor_bytes(const Ctx &c, int prec);   // prec 64 or 32
+
+// dirac.cu
+template <typename R>
+int dirac_op(const Ctx &c, int op, R mu, const void *s, void *r, void *tmp, cudaStream_t st);
+
+// layout.cu
+int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt);
+int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st);   // q: reference AoS on device
+int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st);
+int links_from_ref(Ctx &c, const void *qud, cudaStream_t st);                           // qud on device
+int links_to_ref(const Ctx &c, void *qud, cudaStream_t st);
+int pauli_from_ref(Ctx &c, const void *qsw, cudaStream_t st);                           // qsw on device
+int pauli_to_ref(const Ctx &c, int which, void *qsw, cudaStream_t st);
+
+// sw.cu
+int sw_refresh_derived(Ctx &c, cudaStream_t st);     // inverses + FP32 copies from swd
+int sw_compute(Ctx &c, cudaStream_t st);             // SW term from the links (sw_term)
+int links_refresh_f32(Ctx &c, cudaStream_t st);      // u32 from ud
+int apply_sw_ref_layout(int prec, int vol, double mu, const void *m, const void *s, void *r, cudaStream_t st);
+int apply_swinv_ref_layout(int vol, double mu, const void *m, const void *s, void *r, int *d_fail,
+                           cudaStream_t st);
+
+// fields.cu
+int gen_links(Ctx &c, double eps, uint64_t seed, cudaStream_t st);
+int gen_spinor(const Ctx &c, int prec, void *dev, double sigma, uint64_t seed, cudaStream_t st);
+
+// linalg.cu : BLAS-1 on device-layout spinor fields.  "n" = number of sites
+// counted from the start of the field (vol for full fields, volh for even).
+// Reductions accumulate in double per thread and in double-double across
+// blocks, deterministically.
+enum { PAR_ALL = 2, PAR_EVEN = 0, PAR_ODD = 1 };
+int la_norm2(Ctx &c, int prec, const void *x, int par, double *res_dd);                 // |x|^2 -> (hi,lo)
+int la_dot(Ctx &c, int prec, const void *x, const void *y, int par, double *res);       // (x,y) -> re,im (dd each)
+int la_unorm(Ctx &c, int prec, const void *x, int par, double *res);                    // max site norm
+void la_zero(const Ctx &c, int prec, void *x, int par, cudaStream_t st);
+void la_copy(const Ctx &c, int prec_in, const void *x, int prec_out, void *y, int par, cudaStream_t st);
+void la_scale(const Ctx &c, int prec, void *x, double a, int par, cudaStream_t st);
+void la_axpy(const Ctx &c, int prec, void *y, double are, double aim, const void *x, int par, cudaStream_t st);  // y += a x
+void la_diff(const Ctx &c, int prec, const void *x, void *y, int par, cudaStream_t st);  // y = x - y
+void la_add_s2sd(const Ctx &c, const void *s32, void *sd, int par, cudaStream_t st);    // sd += s
+void la_diff_sd2s(const Ctx &c, const void *ad, const void *bd, void *r32, int par, cudaStream_t st);  // r = a - b
+
+// sap.cu
+int sap_prepare(Ctx &c, cudaStream_t st);
+int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
+
+}  // namespace qcd

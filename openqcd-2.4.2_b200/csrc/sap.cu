@@ -1,0 +1,475 @@
+// Schwarz alternating procedure (SAP) on the device, FP32.
+//
+// One cycle of the reference's sap() (modules/sap/sap.c:720) visits the
+// blocks of colour 0 and then those of colour 1.  For every block of the
+// current colour it solves the block Dirac equation with Dirichlet (zero)
+// exterior by nmr minimal-residual steps, adds the block solution phi to psi,
+// replaces rho on the block by the block residual, and then subtracts the hop
+// of phi out of the block from rho on the neighbouring blocks
+// (Dw_bnd + sap_com, modules/dirac/Dw_bnd.c:801, modules/sap/sap_com.c:465).
+// Blocks of one colour never touch each other, so they run as independent
+// CTAs; the exterior update is a separate gather kernel over the sites of the
+// other colour.
+//
+// k_sap_blocks_eo restates the even-odd preconditioned block solve of the
+// reference (isolv=1: Dwoo_blk, Dweo_blk, blk_eo_mres, Dwoe_blk, Dwoo_blk,
+// update_flds1/2; sap.c:740-767, blk_solv.c:1153, sap.c:618-716);
+// k_sap_blocks_plain the plain one (isolv=0: blk_mres, update_flds0;
+// blk_solv.c:1117, sap.c:592).  One CTA owns one block: the fields that
+// neighbouring sites read (the current even residual, the odd intermediate,
+// the even solution) live in shared memory as 24 planes of vbh floats, the
+// Dhat image of the residual stays in registers, links and SW matrices come
+// through the L1 cache.
+#include "lib.h"
+
+namespace qcd {
+
+struct SapArgs {
+  Geom g;
+  int colour;
+  float mu;
+  int nmr;
+  int eoflg;
+  float4 *psi, *rho, *phi;
+  const float2 *u;
+  const float4 *sw, *swinv;
+};
+
+// block of the given colour with in-colour index h (block lex index of the
+// pair 2h, 2h+1 that has the requested parity of sum(n))
+__device__ __forceinline__ int block_of_colour(const Geom &g, int h, int colour) {
+  int q = 2 * h;
+  int n[4];
+  unpack4(__ldg(g.bcoord + q), n);
+  return q + (((n[0] + n[1] + n[2] + n[3]) & 1) != colour);
+}
+
+// shared-memory spinor planes: plane k (0..23 reals) at sm[k*ld + s]
+__device__ __forceinline__ spinor<float> sm_load(const float *sm, int ld, int s) {
+  spinor<float> r;
+#pragma unroll
+  for (int k = 0; k < 12; k++) r.c[k / 3].c[k % 3] = mk<float>(sm[(2 * k) * ld + s], sm[(2 * k + 1) * ld + s]);
+  return r;
+}
+__device__ __forceinline__ void sm_store(float *sm, int ld, int s, const spinor<float> &v) {
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    sm[(2 * k) * ld + s] = v.c[k / 3].c[k % 3].re;
+    sm[(2 * k + 1) * ld + s] = v.c[k / 3].c[k % 3].im;
+  }
+}
+
+// -1/2 * H restricted to the block (Dirichlet exterior): hop terms of the
+// field in shared memory (parity 1-p) around site (p, s) of block blk.
+__device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int blk, int s, const float *src,
+                                                   int ld) {
+  const Geom &g = a.g;
+  int y[4];
+  unpack4(__ldg(g.lcoord + p * g.vbh + s), y);
+  int l = y[0] * g.lstr[0] + y[1] * g.lstr[1] + y[2] * g.lstr[2] + y[3] * g.lstr[3];
+  const int chunk = p * g.nbl + blk, ochunk = (1 - p) * g.nbl + blk;
+  spinor<float> h;
+  szero(h);
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    if (y[mu] + 1 < g.bs[mu]) {
+      int s2 = (l + g.lstr[mu]) >> 1;
+      spinor<float> sp = sm_load(src, ld, s2);
+      su3<float> uu = Store<float>::load_link(a.u, chunk, mu, s, g.vbh);
+      hop_fwd<float>(mu, uu, sp, h);
+    }
+    if (y[mu] > 0) {
+      int s2 = (l - g.lstr[mu]) >> 1;
+      spinor<float> sm = sm_load(src, ld, s2);
+      su3<float> uu = Store<float>::load_link(a.u, ochunk, mu, s2, g.vbh);
+      hop_bwd<float>(mu, uu, sm, h);
+    }
+  }
+  sscale<float>(h, -0.5f);
+  return h;
+}
+
+template <int NC>
+__device__ __forceinline__ void block_allreduce(double v[NC], double *red) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  }
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NC; k++) red[k * 32 + w] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NC; k++) {
+    double t = 0.0;
+    for (int j = 0; j < nw; j++) t += red[k * 32 + j];
+    v[k] = t;
+  }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
+  extern __shared__ float smem[];
+  const Geom &g = a.g;
+  const int ld = g.vbh;
+  float *S1 = smem, *W = smem + 24 * ld, *S0 = smem + 48 * ld;
+  __shared__ double red[3 * 32];
+  __shared__ float zsh[2];
+  __shared__ int stop;
+  const int blk = block_of_colour(g, blockIdx.x, a.colour);
+  const int ce = blk, co = g.nbl + blk;
+  const int T = blockDim.x;
+
+  // v_o = A_o^-1 rho_o  -> W
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    int s = threadIdx.x + k * T;
+    if (s < g.vbh) {
+      spinor<float> r = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
+      sm_store(W, ld, s, apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, r));
+    }
+  }
+  __syncthreads();
+  // s1_e = rho_e - D_eo v_o ; s0_e = 0
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    int s = threadIdx.x + k * T;
+    if (s < g.vbh) {
+      spinor<float> r = Store<float>::load_spinor_rw(a.rho, ce, s, g.vbh);
+      ssub(r, block_hop(a, 0, blk, s, W, ld));
+      sm_store(S1, ld, s, r);
+      spinor<float> z;
+      szero(z);
+      sm_store(S0, ld, s, z);
+    }
+  }
+  if (threadIdx.x == 0) stop = 0;
+  __syncthreads();
+
+  // nmr minimal-residual steps on Dhat (blk_solv.c:1153-1188)
+  for (int imr = 0; imr < a.nmr; imr++) {
+    // w_o = A_o^-1 D_oe s1_e
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      int s = threadIdx.x + k * T;
+      if (s < g.vbh) {
+        spinor<float> h = block_hop(a, 1, blk, s, S1, ld);
+        sm_store(W, ld, s, apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h));
+      }
+    }
+    __syncthreads();
+    // s2_e = (A_e + i mu g5) s1_e - D_eo w_o ; r = |s2|^2, z = (s2, s1)
+    spinor<float> s2[NS];
+    double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      int s = threadIdx.x + k * T;
+      if (s < g.vbh) {
+        spinor<float> s1 = sm_load(S1, ld, s);
+        s2[k] = apply_sw_site<float>(a.sw, ce, s, g.vbh, a.mu, s1);
+        ssub(s2[k], block_hop(a, 0, blk, s, W, ld));
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) {
+            const cpx<float> x2 = s2[k].c[c].c[j], x1 = s1.c[c].c[j];
+            v[0] += (double)x2.re * x2.re + (double)x2.im * x2.im;
+            v[1] += (double)x2.re * x1.re + (double)x2.im * x1.im;
+            v[2] += (double)x2.re * x1.im - (double)x2.im * x1.re;
+          }
+      }
+    }
+    block_allreduce<3>(v, red);
+    if (threadIdx.x == 0) {
+      float r = (float)v[0];
+      if (r < 2.0f * 1.17549435e-38f) {
+        stop = 1;
+      } else {
+        float ri = 1.0f / r;
+        zsh[0] = (float)v[1] * ri;
+        zsh[1] = (float)v[2] * ri;
+      }
+    }
+    __syncthreads();
+    if (stop) break;
+    const float zr = zsh[0], zi = zsh[1];
+    // s0 += z s1 ; s1 -= z s2
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      int s = threadIdx.x + k * T;
+      if (s < g.vbh) {
+        spinor<float> s1 = sm_load(S1, ld, s), s0 = sm_load(S0, ld, s);
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) {
+            cpx<float> x1 = s1.c[c].c[j], x2 = s2[k].c[c].c[j];
+            s0.c[c].c[j].re += zr * x1.re - zi * x1.im;
+            s0.c[c].c[j].im += zr * x1.im + zi * x1.re;
+            s1.c[c].c[j].re -= zr * x2.re - zi * x2.im;
+            s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
+          }
+        sm_store(S0, ld, s, s0);
+        sm_store(S1, ld, s, s1);
+      }
+    }
+    __syncthreads();
+  }
+
+  // odd part of the block solution: phi_o = A_o^-1 rho_o - A_o^-1 D_oe phi_e,
+  // then psi += phi, rho_o = -i mu g5 phi_o (or 0 with the eo flag), rho_e = s1_e
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    int s = threadIdx.x + k * T;
+    if (s < g.vbh) {
+      spinor<float> h = block_hop(a, 1, blk, s, S0, ld);
+      spinor<float> t = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h);
+      spinor<float> r = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
+      spinor<float> ph = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, r);
+      ssub(ph, t);
+      spinor<float> ps = Store<float>::load_spinor_rw(a.psi, co, s, g.vbh);
+      sadd(ps, ph);
+      Store<float>::store_spinor(a.psi, co, s, g.vbh, ps);
+      Store<float>::store_spinor(a.phi, co, s, g.vbh, ph);
+      spinor<float> ro;
+      if (a.eoflg) {
+        szero(ro);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          const float m = c < 2 ? -a.mu : a.mu;   // r = i m phi
+#pragma unroll
+          for (int j = 0; j < 3; j++) ro.c[c].c[j] = mk<float>(-m * ph.c[c].c[j].im, m * ph.c[c].c[j].re);
+        }
+      }
+      Store<float>::store_spinor(a.rho, co, s, g.vbh, ro);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NS; k++) {
+    int s = threadIdx.x + k * T;
+    if (s < g.vbh) {
+      spinor<float> s0 = sm_load(S0, ld, s);
+      spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ce, s, g.vbh);
+      sadd(ps, s0);
+      Store<float>::store_spinor(a.psi, ce, s, g.vbh, ps);
+      Store<float>::store_spinor(a.phi, ce, s, g.vbh, s0);
+      Store<float>::store_spinor(a.rho, ce, s, g.vbh, sm_load(S1, ld, s));
+    }
+  }
+}
+
+// Plain MR on the block Dirac operator Dw_blk + i mu g5 (twisted mass off on
+// odd sites with the eo flag): all sites, s0/s1 in shared memory, Dw s1 in
+// registers.  Sites are handled as (parity, s) pairs.
+template <int NS>
+__global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
+  extern __shared__ float smem[];
+  const Geom &g = a.g;
+  const int ld = g.vbh;
+  // planes: S1 even, S1 odd, S0 even, S0 odd
+  float *S1[2] = {smem, smem + 24 * ld};
+  float *S0[2] = {smem + 48 * ld, smem + 72 * ld};
+  __shared__ double red[3 * 32];
+  __shared__ float zsh[2];
+  __shared__ int stop;
+  const int blk = block_of_colour(g, blockIdx.x, a.colour);
+  const int T = blockDim.x;
+  const float muo = a.eoflg ? 0.0f : a.mu;
+
+  for (int p = 0; p < 2; p++)
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      int s = threadIdx.x + k * T;
+      if (s < g.vbh) {
+        sm_store(S1[p], ld, s, Store<float>::load_spinor_rw(a.rho, p * g.nbl + blk, s, g.vbh));
+        spinor<float> z;
+        szero(z);
+        sm_store(S0[p], ld, s, z);
+      }
+    }
+  if (threadIdx.x == 0) stop = 0;
+  __syncthreads();
+
+  for (int imr = 0; imr < a.nmr; imr++) {
+    spinor<float> s2[2][NS];
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int p = 0; p < 2; p++)
+#pragma unroll
+      for (int k = 0; k < NS; k++) {
+        int s = threadIdx.x + k * T;
+        if (s < g.vbh) {
+          spinor<float> s1 = sm_load(S1[p], ld, s);
+          s2[p][k] = apply_sw_site<float>(a.sw, p * g.nbl + blk, s, g.vbh, p ? muo : a.mu, s1);
+          sadd(s2[p][k], block_hop(a, p, blk, s, S1[1 - p], ld));
+#pragma unroll
+          for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+              const cpx<float> x2 = s2[p][k].c[c].c[j], x1 = s1.c[c].c[j];
+              v[0] += (double)x2.re * x2.re + (double)x2.im * x2.im;
+              v[1] += (double)x2.re * x1.re + (double)x2.im * x1.im;
+              v[2] += (double)x2.re * x1.im - (double)x2.im * x1.re;
+            }
+        }
+      }
+    block_allreduce<3>(v, red);
+    if (threadIdx.x == 0) {
+      float r = (float)v[0];
+      if (r < 2.0f * 1.17549435e-38f) stop = 1;
+      else {
+        float ri = 1.0f / r;
+        zsh[0] = (float)v[1] * ri;
+        zsh[1] = (float)v[2] * ri;
+      }
+    }
+    __syncthreads();
+    if (stop) break;
+    const float zr = zsh[0], zi = zsh[1];
+    for (int p = 0; p < 2; p++)
+#pragma unroll
+      for (int k = 0; k < NS; k++) {
+        int s = threadIdx.x + k * T;
+        if (s < g.vbh) {
+          spinor<float> s1 = sm_load(S1[p], ld, s), s0 = sm_load(S0[p], ld, s);
+#pragma unroll
+          for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+              cpx<float> x1 = s1.c[c].c[j], x2 = s2[p][k].c[c].c[j];
+              s0.c[c].c[j].re += zr * x1.re - zi * x1.im;
+              s0.c[c].c[j].im += zr * x1.im + zi * x1.re;
+              s1.c[c].c[j].re -= zr * x2.re - zi * x2.im;
+              s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
+            }
+          sm_store(S0[p], ld, s, s0);
+          sm_store(S1[p], ld, s, s1);
+        }
+      }
+    __syncthreads();
+  }
+  for (int p = 0; p < 2; p++)
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+      int s = threadIdx.x + k * T;
+      if (s < g.vbh) {
+        int ch = p * g.nbl + blk;
+        spinor<float> s0 = sm_load(S0[p], ld, s);
+        spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ch, s, g.vbh);
+        sadd(ps, s0);
+        Store<float>::store_spinor(a.psi, ch, s, g.vbh, ps);
+        Store<float>::store_spinor(a.phi, ch, s, g.vbh, s0);
+        Store<float>::store_spinor(a.rho, ch, s, g.vbh, sm_load(S1[p], ld, s));
+      }
+    }
+}
+
+// rho(y) -= D_{y,x} phi(x) for every site y of a block of colour 1-c and every
+// neighbour x of y in a (colour c) block: the block-boundary hop of the
+// reference's Dw_bnd/sap_com, as a gather.
+__global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
+  const Geom &g = a.g;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= (size_t)(g.nbl / 2) * g.vb) return;
+  int h = (int)(i / g.vb), r = (int)(i % g.vb);
+  int p = r >= g.vbh, s = r - p * g.vbh;
+  int blk = block_of_colour(g, h, 1 - a.colour);
+  Site x;
+  site_decode(g, p, blk, s, x);
+  const int chunk = p * g.nbl + blk;
+  spinor<float> hsum;
+  szero(hsum);
+  bool any = false;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    if (crosses_block(g, x, mu, +1)) {
+      int c2, s2;
+      site_nbr(g, x, mu, +1, c2, s2);
+      spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
+      su3<float> uu = Store<float>::load_link(a.u, chunk, mu, s, g.vbh);
+      hop_fwd<float>(mu, uu, sp, hsum);
+      any = true;
+    }
+    if (crosses_block(g, x, mu, -1)) {
+      int c2, s2;
+      site_nbr(g, x, mu, -1, c2, s2);
+      spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
+      su3<float> uu = Store<float>::load_link(a.u, c2, mu, s2, g.vbh);
+      hop_bwd<float>(mu, uu, sm, hsum);
+      any = true;
+    }
+  }
+  if (!any) return;
+  sscale<float>(hsum, 0.5f);   // rho -= (-1/2) H phi
+  spinor<float> rr = Store<float>::load_spinor_rw(a.rho, chunk, s, g.vbh);
+  sadd(rr, hsum);
+  Store<float>::store_spinor(a.rho, chunk, s, g.vbh, rr);
+}
+
+static int pick_threads(int vbh, int &ns) {
+  for (ns = 1; ns <= 3; ns++) {
+    int t = ((vbh + ns - 1) / ns + 31) / 32 * 32;
+    if (t <= 256) return t;
+  }
+  ns = 0;
+  return 0;
+}
+
+int sap_prepare(Ctx &c, cudaStream_t st) {
+  (void)st;
+  int ns;
+  int t = pick_threads(c.g.vbh, ns);
+  if (!t) return fail("sap: block volume too large (at most 1536 sites)");
+  size_t eo = (size_t)72 * c.g.vbh * sizeof(float), pl = (size_t)96 * c.g.vbh * sizeof(float);
+  if (eo > 200 * 1024 || pl > 200 * 1024) {
+    if (pl > 200 * 1024 && c.isolv == 0) return fail("sap: block too large for the plain MR solver");
+  }
+  cudaFuncSetAttribute(k_sap_blocks_eo<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sap_blocks_eo<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sap_blocks_eo<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sap_blocks_plain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sap_blocks_plain<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_sap_blocks_plain<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return 0;
+}
+
+// One SAP cycle sap(mu, isolv, nmr, psi, rho) on FP32 device fields.
+// phi_blk is a scratch FP32 field.
+int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st) {
+  int ns;
+  int t = pick_threads(c.g.vbh, ns);
+  SapArgs a;
+  a.g = c.g;
+  a.mu = mu;
+  a.nmr = nmr;
+  a.eoflg = c.eoflg;
+  a.psi = (float4 *)psi;
+  a.rho = (float4 *)rho;
+  a.phi = (float4 *)phi_blk;
+  a.u = c.u32;
+  a.sw = c.sw32;
+  a.swinv = c.sw32_inv;
+  size_t shm = (size_t)(isolv ? 72 : 96) * c.g.vbh * sizeof(float);
+  if (shm > 200 * 1024) return fail("sap: block too large for shared memory");
+  int nbh = c.g.nbl / 2;
+  size_t nb_sites = (size_t)nbh * c.g.vb;
+  for (int ic = 0; ic < 2; ic++) {
+    a.colour = ic;
+    if (isolv) {
+      if (ns == 1) k_sap_blocks_eo<1><<<nbh, t, shm, st>>>(a);
+      else if (ns == 2) k_sap_blocks_eo<2><<<nbh, t, shm, st>>>(a);
+      else k_sap_blocks_eo<3><<<nbh, t, shm, st>>>(a);
+    } else {
+      if (ns == 1) k_sap_blocks_plain<1><<<nbh, t, shm, st>>>(a);
+      else if (ns == 2) k_sap_blocks_plain<2><<<nbh, t, shm, st>>>(a);
+      else k_sap_blocks_plain<3><<<nbh, t, shm, st>>>(a);
+    }
+    k_sap_bnd<<<(unsigned)((nb_sites + 127) / 128), 128, 0, st>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+}
+
+}  // namespace qcd

@@ -1,0 +1,175 @@
+// Flexible GCR and the SAP+GCR solver on device-resident fields.
+//
+// fgcr_dev restates the reference's fgcr (modules/linsolv/fgcr.c:215-299,
+// gcr_step :157, update_psi :181, get_res :128): Krylov vectors in FP32,
+// Gram-Schmidt products accumulated in double, the small scalar arrays a, b,
+// c in single precision on the host, the true residual recomputed in FP64 at
+// every restart, and the restart rule rn < PRECISION_LIMIT * rn_old with
+// PRECISION_LIMIT = 100 * FLT_EPSILON.  sap_gcr_dev restates
+// modules/sap/sap_gcr.c:140-250 with Mop = ncy SAP cycles (sap_gcr.c:126).
+#include "lib.h"
+#include <cfloat>
+#include <cmath>
+#include <functional>
+
+namespace qcd {
+
+size_t spinor_bytes(const Ctx &c, int prec) { return (size_t)c.g.vol * 12 * (prec == 64 ? 16 : 8); }
+
+static int reserve(Ctx &c, std::vector<void *> &ws, size_t n, int prec) {
+  while (ws.size() < n) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, spinor_bytes(c, prec)) != cudaSuccess) return fail("out of device memory (workspace)");
+    ws.push_back(p);
+  }
+  return 0;
+}
+
+struct cplxf { float re, im; };
+
+using DopFn = std::function<void(const void *s64, void *r64)>;
+using MopFn = std::function<void(int k, const void *rho32, void *phi32, void *chi32)>;
+
+static double get_res(Ctx &c, int istop, const void *rho) {
+  double r[4];
+  if (istop) {
+    la_unorm(c, 32, rho, PAR_ALL, r);
+    return (double)(float)r[0];
+  }
+  la_norm2(c, 32, rho, PAR_ALL, r);
+  return sqrt((double)(float)(r[0] + r[1]));
+}
+
+static cplxf sprod(Ctx &c, const void *x, const void *y) {
+  double r[4];
+  la_dot(c, 32, x, y, PAR_ALL, r);
+  return {(float)(r[0] + r[1]), (float)(r[2] + r[3])};
+}
+
+static float normalize(Ctx &c, void *x) {
+  double r[2];
+  la_norm2(c, 32, x, PAR_ALL, r);
+  float n = (float)(r[0] + r[1]);
+  n = (float)sqrt((double)n);
+  if (n != 0.0f) la_scale(c, 32, x, 1.0f / n, PAR_ALL, c.stream);
+  return n;
+}
+
+double fgcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, const void *eta, void *psi, int *status,
+                const DopFn &Dop, const MopFn &Mop) {
+  if (nkv < 1 || nmx < 1 || res <= DBL_EPSILON || istop < 0 || istop > 1) {
+    fail("fgcr: parameters are out of range");
+    return -1.0;
+  }
+  if (reserve(c, c.ws32, 2 * nkv + 1, 32) || reserve(c, c.ws64, 2, 64)) return -1.0;
+  std::vector<void *> phi(c.ws32.begin(), c.ws32.begin() + nkv), chi(c.ws32.begin() + nkv + 1, c.ws32.begin() + 2 * nkv + 1);
+  void *rho = c.ws32[nkv];
+  void *wrk = c.ws64[0];
+  std::vector<cplxf> a((size_t)nkv * nkv), cc(nkv);
+  std::vector<float> b(nkv);
+  const double PRECISION_LIMIT = (double)(100.0f * FLT_EPSILON);
+  cudaStream_t st = c.stream;
+
+  la_zero(c, 64, psi, PAR_ALL, st);
+  la_copy(c, 64, eta, 32, rho, PAR_ALL, st);
+  double rn = get_res(c, istop, rho);
+  double tol = res * rn;
+  status[0] = 0;
+
+  while (rn > tol) {
+    double rn_old = rn;
+    int k;
+    for (k = 0;; k++) {
+      // gcr_step
+      Mop(k, rho, phi[k], chi[k]);
+      for (int l = 0; l < k; l++) {
+        cplxf z = sprod(c, chi[l], chi[k]);
+        a[(size_t)nkv * l + k] = z;
+        la_axpy(c, 32, chi[k], -z.re, -z.im, chi[l], PAR_ALL, st);
+      }
+      b[k] = normalize(c, chi[k]);
+      cc[k] = sprod(c, chi[k], rho);
+      la_axpy(c, 32, rho, -cc[k].re, -cc[k].im, chi[k], PAR_ALL, st);
+      rn = get_res(c, istop, rho);
+      status[0] += 1;
+      if (rn <= tol || rn < PRECISION_LIMIT * rn_old || k == nkv - 1 || status[0] >= nmx) break;
+    }
+    // update_psi
+    for (int l = k; l >= 0; l--) {
+      cplxf z = cc[l];
+      for (int i = l + 1; i <= k; i++) {
+        cplxf al = a[(size_t)l * nkv + i];
+        z.re -= al.re * cc[i].re - al.im * cc[i].im;
+        z.im -= al.re * cc[i].im + al.im * cc[i].re;
+      }
+      float r = 1.0f / b[l];
+      cc[l].re = z.re * r;
+      cc[l].im = z.im * r;
+    }
+    la_zero(c, 32, rho, PAR_ALL, st);
+    for (int l = k; l >= 0; l--) la_axpy(c, 32, rho, cc[l].re, cc[l].im, phi[l], PAR_ALL, st);
+    la_add_s2sd(c, rho, psi, PAR_ALL, st);
+    Dop(psi, wrk);
+    la_diff_sd2s(c, eta, wrk, rho, PAR_ALL, st);
+    rn = get_res(c, istop, rho);
+    if (status[0] >= nmx && rn > tol) {
+      status[0] = -1;
+      return rn;
+    }
+  }
+  return rn;
+}
+
+// Device twin of sap_gcr(): eta, psi FP64 device fields (psi may equal eta).
+double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                   int *ifail, int *status) {
+  ifail[0] = 0;
+  status[0] = 0;
+  if (!c.sap_set) { fail("sap_gcr: SAP parameters are not set"); return -1.0; }
+  if (!c.have_ud || !c.have_sw) { fail("sap_gcr: gauge or SW field missing on the device"); return -1.0; }
+  if (sap_prepare(c, c.stream)) return -1.0;
+  double rho = 0.0;
+  if (c.isolv == 1 && (c.sw_inv_fail & 2)) {
+    ifail[0] = -3;
+  } else {
+    double u[2];
+    la_unorm(c, 64, eta, PAR_ALL, u);
+    double rho0 = u[0];
+    if (rho0 != 0.0) {
+      if (reserve(c, c.ws64, 3, 64) || reserve(c, c.ws32, 2 * nkv + 2, 32)) return -1.0;
+      void *rsd = c.ws64[1];
+      void *phib = c.ws32[2 * nkv + 1];
+      la_copy(c, 64, eta, 64, rsd, PAR_ALL, c.stream);
+      la_scale(c, 64, rsd, 1.0 / rho0, PAR_ALL, c.stream);
+      const float muf = (float)mu;
+      const int isolv = c.isolv, nmr = c.nmr, ncy = c.ncy;
+      DopFn Dop = [&](const void *s, void *r) { dirac_op<double>(c, 0, mu, s, r, c.tmp64, c.stream); };
+      MopFn Mop = [&](int, const void *rh, void *ph, void *ch) {
+        la_zero(c, 32, ph, PAR_ALL, c.stream);
+        la_copy(c, 32, rh, 32, ch, PAR_ALL, c.stream);
+        for (int n = 0; n < ncy; n++) sap_cycle(c, muf, isolv, nmr, ph, ch, phib, c.stream);
+        la_diff(c, 32, rh, ch, PAR_ALL, c.stream);
+      };
+      // psi may alias eta: fgcr only reads rsd from here on
+      rho = fgcr_dev(c, nkv, nmx, istop, res, rsd, psi, status, Dop, Mop);
+      la_scale(c, 64, psi, rho0, PAR_ALL, c.stream);
+      rho *= rho0;
+      if (status[0] < 0) {
+        ifail[0] = -1;
+        status[0] = nmx;
+      }
+    } else {
+      la_zero(c, 64, psi, PAR_ALL, c.stream);
+    }
+  }
+  if (ifail[0] <= -2) {
+    if (psi != eta) la_zero(c, 64, psi, PAR_ALL, c.stream);
+    double r[2];
+    if (istop) { la_unorm(c, 64, eta, PAR_ALL, r); rho = r[0]; }
+    else { la_norm2(c, 64, eta, PAR_ALL, r); rho = sqrt(r[0]); }
+  }
+  cudaStreamSynchronize(c.stream);
+  return rho;
+}
+
+}  // namespace qcd

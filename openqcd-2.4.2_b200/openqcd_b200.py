@@ -1,0 +1,286 @@
+"""Python host binding of libopenqcd_b200.so (ctypes).
+
+Mirrors the C interface in include/openqcd_b200.h: the reference-named
+drop-in calls (Dw_dble, Dw, Dwee_dble, ..., apply_sw_dble, sap, sap_gcr) take
+numpy arrays in the reference's storage order; the b200_dev_* calls take
+device pointers (ints) to fields in the library's own layout.
+
+The library must have been built (build.py); importing this module on a
+machine without it raises, there is no fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libopenqcd_b200.so")
+
+_lib = None
+
+DIRAC_OPS = {"Dw": 0, "Dwee": 1, "Dwoo": 2, "Dwoe": 3, "Dweo": 4, "Dwhat": 5}
+
+_SIGS = {
+    "b200_geometry": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_set_lat_parms": (C.c_int, [C.c_double]),
+    "b200_set_bc_parms": (C.c_int, [C.c_int]),
+    "b200_set_sw_parms": (C.c_int, [C.c_double]),
+    "b200_set_tm_parms": (C.c_int, [C.c_int]),
+    "b200_set_sap_parms": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "b200_upload_ud": (C.c_int, [C.c_void_p]),
+    "b200_download_ud": (C.c_int, [C.c_void_p]),
+    "b200_upload_swd": (C.c_int, [C.c_void_p]),
+    "b200_download_swd": (C.c_int, [C.c_void_p, C.c_int]),
+    "b200_sw_term": (C.c_int, []),
+    "b200_random_ud": (C.c_int, [C.c_double, C.c_ulonglong]),
+    "b200_last_error": (C.c_char_p, []),
+    "b200_set_fatal": (None, [C.c_int]),
+    "b200_sync": (C.c_int, []),
+    "b200_volume": (C.c_int, []),
+    "Dw_dble": (None, [C.c_double, C.c_void_p, C.c_void_p]),
+    "Dwee_dble": (None, [C.c_double, C.c_void_p, C.c_void_p]),
+    "Dwoo_dble": (None, [C.c_double, C.c_void_p, C.c_void_p]),
+    "Dwoe_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Dweo_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Dwhat_dble": (None, [C.c_double, C.c_void_p, C.c_void_p]),
+    "Dw": (None, [C.c_float, C.c_void_p, C.c_void_p]),
+    "Dwee": (None, [C.c_float, C.c_void_p, C.c_void_p]),
+    "Dwoo": (None, [C.c_float, C.c_void_p, C.c_void_p]),
+    "Dwoe": (None, [C.c_void_p, C.c_void_p]),
+    "Dweo": (None, [C.c_void_p, C.c_void_p]),
+    "Dwhat": (None, [C.c_float, C.c_void_p, C.c_void_p]),
+    "apply_sw_dble": (None, [C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "apply_sw": (None, [C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "apply_swinv_dble": (C.c_int, [C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sap": (None, [C.c_float, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "sap_gcr": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_void_p]),
+    "b200_dev_alloc_spinor": (C.c_void_p, [C.c_int]),
+    "b200_dev_free": (None, [C.c_void_p]),
+    "b200_dev_random_spinor": (C.c_int, [C.c_int, C.c_void_p, C.c_double, C.c_ulonglong]),
+    "b200_dev_from_ref": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_dev_to_ref": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_dev_dirac": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
+    "b200_dev_sap": (C.c_int, [C.c_float, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_dev_sap_gcr": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]),
+    "b200_dev_norm2": (C.c_double, [C.c_int, C.c_void_p]),
+    "b200_dev_time_dirac": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+}
+
+EXPORTED = list(_SIGS)
+
+
+def lib():
+    """Load the shared library (once) and declare the prototypes."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libopenqcd_b200.so is not built (run openqcd-2.4.2_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        L.b200_set_fatal(0)
+        _lib = L
+    return _lib
+
+
+class B200Error(RuntimeError):
+    pass
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if isinstance(a, np.ndarray) else a
+
+
+def check(rc):
+    if rc is not None and rc < 0:
+        raise B200Error(lib().b200_last_error().decode())
+    return rc
+
+
+def geometry(L, bs, ipt=None):
+    Lc = np.ascontiguousarray(L, dtype=np.int32)
+    bc = np.ascontiguousarray(bs, dtype=np.int32)
+    ip = None if ipt is None else np.ascontiguousarray(ipt, dtype=np.int32)
+    return check(lib().b200_geometry(_ptr(Lc), _ptr(bc), None if ip is None else _ptr(ip)))
+
+
+def set_parms(csw, m0, eoflg=0, bc=3):
+    L = lib()
+    check(L.b200_set_lat_parms(csw))
+    check(L.b200_set_bc_parms(bc))
+    check(L.b200_set_sw_parms(m0))
+    check(L.b200_set_tm_parms(eoflg))
+
+
+def set_sap_parms(bs, isolv, nmr, ncy):
+    b = np.ascontiguousarray(bs, dtype=np.int32)
+    return check(lib().b200_set_sap_parms(_ptr(b), isolv, nmr, ncy))
+
+
+def upload_ud(ud):
+    return check(lib().b200_upload_ud(_ptr(np.ascontiguousarray(ud, dtype=np.float64))))
+
+
+def download_ud(vol):
+    out = np.zeros(4 * vol * 18)
+    check(lib().b200_download_ud(_ptr(out)))
+    return out
+
+
+def upload_swd(swd):
+    return check(lib().b200_upload_swd(_ptr(np.ascontiguousarray(swd, dtype=np.float64))))
+
+
+def download_swd(vol, which=0):
+    out = np.zeros(2 * vol * 36)
+    check(lib().b200_download_swd(_ptr(out), which))
+    return out
+
+
+def sw_term():
+    return check(lib().b200_sw_term())
+
+
+def random_ud(eps, seed):
+    return check(lib().b200_random_ud(eps, seed))
+
+
+def _err_after():
+    e = lib().b200_last_error()
+    return e.decode() if e else ""
+
+
+def dirac_ref(op, prec, mu, s, r=None):
+    """Apply a reference-named operator to reference-layout numpy arrays."""
+    L = lib()
+    dt = np.float64 if prec == 64 else np.float32
+    s = np.ascontiguousarray(s, dtype=dt)
+    r = np.zeros_like(s) if r is None else np.array(r, dtype=dt, copy=True)
+    name = op + ("_dble" if prec == 64 else "")
+    f = getattr(L, name)
+    before = _err_after()
+    if op in ("Dwoe", "Dweo"):
+        f(_ptr(s), _ptr(r))
+    else:
+        f(mu, _ptr(s), _ptr(r))
+    after = _err_after()
+    if after and after != before:
+        raise B200Error(after)
+    return r
+
+
+class DevField:
+    """A spinor field resident on the device in the library's layout."""
+
+    def __init__(self, prec):
+        self.prec = prec
+        self.ptr = lib().b200_dev_alloc_spinor(prec)
+        if not self.ptr:
+            raise B200Error(_err_after())
+
+    def free(self):
+        if self.ptr:
+            lib().b200_dev_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def from_ref(self, q):
+        dt = np.float64 if self.prec == 64 else np.float32
+        q = np.ascontiguousarray(q, dtype=dt)
+        check(lib().b200_dev_from_ref(self.prec, _ptr(q), self.ptr))
+        return self
+
+    def to_ref(self, vol):
+        dt = np.float64 if self.prec == 64 else np.float32
+        out = np.zeros(vol * 24, dtype=dt)
+        check(lib().b200_dev_to_ref(self.prec, self.ptr, _ptr(out)))
+        return out
+
+    def random(self, sigma, seed):
+        check(lib().b200_dev_random_spinor(self.prec, self.ptr, sigma, seed))
+        return self
+
+    def norm2(self):
+        return lib().b200_dev_norm2(self.prec, self.ptr)
+
+
+def dev_dirac(op, mu, s, r):
+    return check(lib().b200_dev_dirac(s.prec, DIRAC_OPS[op], mu, s.ptr, r.ptr))
+
+
+def dev_sap(mu, isolv, nmr, ncy, psi, rho):
+    return check(lib().b200_dev_sap(mu, isolv, nmr, ncy, psi.ptr, rho.ptr))
+
+
+def dev_sap_gcr(nkv, nmx, istop, res, mu, eta, psi):
+    ifail = C.c_int(0)
+    status = C.c_int(0)
+    rho = lib().b200_dev_sap_gcr(nkv, nmx, istop, res, mu, eta.ptr, psi.ptr, C.byref(ifail), C.byref(status))
+    if rho < 0:
+        raise B200Error(_err_after())
+    return rho, ifail.value, status.value
+
+
+def sap_gcr(nkv, nmx, istop, res, mu, eta):
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    psi = np.zeros_like(eta)
+    ifail = C.c_int(0)
+    status = C.c_int(0)
+    rho = lib().sap_gcr(nkv, nmx, istop, res, mu, _ptr(eta), _ptr(psi), C.byref(ifail), C.byref(status))
+    if rho < 0:
+        raise B200Error(_err_after())
+    return psi, rho, ifail.value, status.value
+
+
+def sap_ref(mu, isolv, nmr, psi, rho):
+    psi = np.array(psi, dtype=np.float32, copy=True)
+    rho = np.array(rho, dtype=np.float32, copy=True)
+    before = _err_after()
+    lib().sap(mu, isolv, nmr, _ptr(psi), _ptr(rho))
+    after = _err_after()
+    if after and after != before:
+        raise B200Error(after)
+    return psi, rho
+
+
+def apply_sw_dble(vol, mu, m, s):
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    r = np.zeros_like(s)
+    lib().apply_sw_dble(vol, mu, _ptr(np.ascontiguousarray(m, dtype=np.float64)), _ptr(s), _ptr(r))
+    return r
+
+
+def apply_sw(vol, mu, m, s):
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    r = np.zeros_like(s)
+    lib().apply_sw(vol, mu, _ptr(np.ascontiguousarray(m, dtype=np.float32)), _ptr(s), _ptr(r))
+    return r
+
+
+def apply_swinv_dble(vol, mu, m, s):
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    r = np.zeros_like(s)
+    f = lib().apply_swinv_dble(vol, mu, _ptr(np.ascontiguousarray(m, dtype=np.float64)), _ptr(s), None, _ptr(r))
+    return r, f
+
+
+def time_dirac(prec, op, mu, s, r, n):
+    ms = C.c_float(0.0)
+    check(lib().b200_dev_time_dirac(prec, DIRAC_OPS[op], mu, s.ptr, r.ptr, n, C.byref(ms)))
+    return ms.value
+
+
+def time_Dw_dble_host(mu, s, r, n):
+    ms = C.c_float(0.0)
+    check(lib().b200_time_Dw_dble_host(mu, _ptr(s), _ptr(r), n, C.byref(ms)))
+    return ms.value

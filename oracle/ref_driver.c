@@ -1,0 +1,345 @@
+/*
+ * Test-infrastructure driver around the REFERENCE library (the reference's
+ * own modules compiled in place by oracle/build_ref.py).  It is the oracle:
+ * only tests/, the smoke check and bench.py's CPU-baseline leg load it.
+ *
+ * It exposes flat C entry points (prefix ref_) that Python reaches through
+ * ctypes.  Spinor, gauge and SW arrays cross this boundary as plain doubles or
+ * floats in the reference's own storage order:
+ *   spinor_dble[VOLUME]   ipt order, even sites first (main/README.global)
+ *   su3_dble[4*VOLUME]    8 links per odd site (main/README.global:229-262)
+ *   pauli_dble[2*VOLUME]  upper/lower 6x6 at sw[2ix], sw[2ix+1]
+ *                         (modules/sw_term/sw_term.c:42-44)
+ *
+ * Field generation follows the workload recipe: every link is exp(eps*X)
+ * with X drawn by random_alg() (modules/linalg/liealg.c:289) and the SU(3)
+ * exponential expXsu3() (modules/su3fcts/chexp.c:878); then set_bc() and
+ * set_ud_phase() (modules/uflds/uflds.c:338) apply the boundary conditions.
+ */
+#define MAIN_PROGRAM
+
+#include <stdlib.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+#include <omp.h>
+#include "mpi.h"
+#include "su3.h"
+#include "flags.h"
+#include "random.h"
+#include "su3fcts.h"
+#include "utils.h"
+#include "lattice.h"
+#include "uflds.h"
+#include "sflds.h"
+#include "linalg.h"
+#include "sw_term.h"
+#include "block.h"
+#include "dirac.h"
+#include "sap.h"
+#include "linsolv.h"
+#include "global.h"
+
+static int initialised = 0;
+static int nws = 0, nwsd = 0;
+
+/* The OpenMP runtime is shared by every copy of the reference loaded into a
+ * process, while each copy assumes exactly NTHREAD threads
+ * (modules/utils/utils.c:195), so every entry point pins the team size. */
+#define ENTER() omp_set_num_threads(NTHREAD)
+
+int ref_volume(void) { ENTER(); return VOLUME; }
+int ref_nthread(void) { ENTER(); return NTHREAD; }
+
+void ref_dims(int *L)
+{
+   ENTER();
+   L[0] = L0; L[1] = L1; L[2] = L2; L[3] = L3;
+}
+
+static void need_ws(int n, int nd)
+{
+   if (n > nws) { alloc_ws(n); nws = n; }
+   if (nd > nwsd) { alloc_wsd(nd); nwsd = nd; }
+}
+
+/* Geometry, parameter data base and random-number generator.  Must be called
+ * once per process before any other ref_ function. */
+void ref_init(int bc, int seed, double csw, double m0, int eoflg)
+{
+   ENTER();
+   int provided;
+   double phi[2] = {0.0, 0.0}, phip[2] = {0.0, 0.0}, theta[3] = {0.0, 0.0, 0.0};
+
+   if (!initialised)
+   {
+      MPI_Init_thread(NULL, NULL, MPI_THREAD_FUNNELED, &provided);
+      omp_set_num_threads(NTHREAD);
+      omp_set_dynamic(0);
+      set_lat_parms(6.0, 1.0, 0, NULL, 0, csw);
+      set_bc_parms(bc, 1.0, 1.0, 1.0, 1.0, phi, phip, theta);
+      start_ranlux(0, seed);
+      geometry();
+      chexp_init();
+      initialised = 1;
+   }
+   set_sw_parms(m0);
+   set_tm_parms(eoflg);
+   need_ws(40, 8);
+}
+
+void ref_set_sw_parms(double m0) { ENTER(); set_sw_parms(m0); set_flags(ERASED_SWD); }
+void ref_set_tm_parms(int eoflg) { ENTER(); set_tm_parms(eoflg); }
+
+void ref_set_sap_parms(int b0, int b1, int b2, int b3, int isolv, int nmr, int ncy)
+{
+   ENTER();
+   int bs[4];
+   bs[0] = b0; bs[1] = b1; bs[2] = b2; bs[3] = b3;
+   set_sap_parms(bs, isolv, nmr, ncy);
+}
+
+/* Links U = exp(eps*X)*1 on all 4*VOLUME link slots, then boundary
+ * conditions and phase.  Reseeds the generator first. */
+void ref_gen_links(double eps, int seed)
+{
+   ENTER();
+   int i;
+   su3_dble *ud;
+   su3_alg_dble X __attribute__((aligned(64)));
+
+   start_ranlux(0, seed);
+   ud = udfld();
+   for (i = 0; i < 4 * VOLUME; i++)
+   {
+      memset(ud + i, 0, sizeof(su3_dble));
+      ud[i].c11.re = 1.0;
+      ud[i].c22.re = 1.0;
+      ud[i].c33.re = 1.0;
+      random_alg(1, 0, &X);
+      expXsu3(eps, &X, ud + i);
+   }
+   set_flags(UPDATED_UD);
+   set_flags(UNSET_UD_PHASE);
+   set_bc();
+   set_ud_phase();
+}
+
+void ref_random_ud(int seed)
+{
+   ENTER();
+   start_ranlux(0, seed);
+   random_ud();
+   set_ud_phase();
+}
+
+void ref_get_ipt(int *out)
+{
+   ENTER();
+   memcpy(out, ipt, VOLUME * sizeof(int));
+}
+
+void ref_get_ud(double *out) { ENTER(); memcpy(out, udfld(), 4 * VOLUME * sizeof(su3_dble)); }
+
+void ref_set_ud(const double *in)
+{
+   ENTER();
+   memcpy(udfld(), in, 4 * VOLUME * sizeof(su3_dble));
+   set_flags(UPDATED_UD);
+}
+
+/* sw_term(set) with set = 0 (NO_PTS), 1 (EVEN_PTS), 2 (ODD_PTS),
+ * 3 (ALL_PTS): compute the SW field and invert it on the given points
+ * (modules/sw_term/sw_term.c:399).  Returns the reference's ifail. */
+int ref_sw_term(int set)
+{
+   ENTER();
+   ptset_t s = NO_PTS;
+   if (set == 1) s = EVEN_PTS;
+   else if (set == 2) s = ODD_PTS;
+   else if (set == 3) s = ALL_PTS;
+   return sw_term(s);
+}
+
+void ref_get_swd(double *out) { ENTER(); memcpy(out, swdfld(), 2 * VOLUME * sizeof(pauli_dble)); }
+
+void ref_random_sd(int seed, double sigma, double *out)
+{
+   ENTER();
+   spinor_dble **wsd;
+   start_ranlux(0, seed);
+   wsd = reserve_wsd(1);
+   random_sd(VOLUME_TRD, 2, wsd[0], sigma);
+   memcpy(out, wsd[0], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+}
+
+/* Double-precision operators: op = 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo,
+ * 5 Dwhat (modules/dirac/Dw_dble.c:1377-1889).  r is both read (Dweo
+ * subtracts from it) and written. */
+void ref_dirac_dble(int op, double mu, const double *s, double *r)
+{
+   ENTER();
+   spinor_dble **wsd;
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], s, VOLUME * sizeof(spinor_dble));
+   memcpy(wsd[1], r, VOLUME * sizeof(spinor_dble));
+   switch (op)
+   {
+   case 0: Dw_dble(mu, wsd[0], wsd[1]); break;
+   case 1: Dwee_dble(mu, wsd[0], wsd[1]); break;
+   case 2: Dwoo_dble(mu, wsd[0], wsd[1]); break;
+   case 3: Dwoe_dble(wsd[0], wsd[1]); break;
+   case 4: Dweo_dble(wsd[0], wsd[1]); break;
+   case 5: Dwhat_dble(mu, wsd[0], wsd[1]); break;
+   default: break;
+   }
+   memcpy(r, wsd[1], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+}
+
+/* Single-precision twins (modules/dirac/Dw.c:973-1473).  The single-
+ * precision gauge and SW fields are refreshed from the double-precision
+ * ones first (assign_ud2u, assign_swd2sw). */
+void ref_dirac(int op, float mu, const float *s, float *r)
+{
+   ENTER();
+   spinor **ws;
+   assign_ud2u();
+   assign_swd2sw();
+   ws = reserve_ws(2);
+   memcpy(ws[0], s, VOLUME * sizeof(spinor));
+   memcpy(ws[1], r, VOLUME * sizeof(spinor));
+   switch (op)
+   {
+   case 0: Dw(mu, ws[0], ws[1]); break;
+   case 1: Dwee(mu, ws[0], ws[1]); break;
+   case 2: Dwoo(mu, ws[0], ws[1]); break;
+   case 3: Dwoe(ws[0], ws[1]); break;
+   case 4: Dweo(ws[0], ws[1]); break;
+   case 5: Dwhat(mu, ws[0], ws[1]); break;
+   default: break;
+   }
+   memcpy(r, ws[1], VOLUME * sizeof(spinor));
+   release_ws();
+}
+
+/* One or more SAP cycles sap(mu,isolv,nmr,psi,rho) on single-precision
+ * fields (modules/sap/sap.c:720), after the block-grid set-up sap_gcr()
+ * performs (modules/sap/sap_gcr.c:150-200). */
+int ref_sap(float mu, int isolv, int nmr, int ncy, float *psi, float *rho)
+{
+   ENTER();
+   int nb, isw, n, ifail = 0;
+   spinor **ws;
+
+   blk_list(SAP_BLOCKS, &nb, &isw);
+   if (nb == 0)
+      alloc_bgr(SAP_BLOCKS);
+   assign_ud2ubgr(SAP_BLOCKS);
+   if (query_flags(SWD_UP2DATE) != 1 || query_flags(SWD_E_INVERTED) == 1 ||
+       query_flags(SWD_O_INVERTED) == 1)
+      sw_term(NO_PTS);
+   ifail = assign_swd2swbgr(SAP_BLOCKS, isolv ? ODD_PTS : NO_PTS);
+
+   ws = reserve_ws(2);
+   memcpy(ws[0], psi, VOLUME * sizeof(spinor));
+   memcpy(ws[1], rho, VOLUME * sizeof(spinor));
+   for (n = 0; n < ncy; n++)
+      sap(mu, isolv, nmr, ws[0], ws[1]);
+   memcpy(psi, ws[0], VOLUME * sizeof(spinor));
+   memcpy(rho, ws[1], VOLUME * sizeof(spinor));
+   release_ws();
+   return ifail;
+}
+
+/* The reference SAP+GCR solver (modules/sap/sap_gcr.c:140).  The SW term is
+ * brought into the non-inverted state first, as the main programs do. */
+double ref_sap_gcr(int nkv, int nmx, int istop, double res, double mu,
+                   const double *eta, double *psi, int *ifail, int *status)
+{
+   ENTER();
+   double rho;
+   spinor_dble **wsd;
+
+   need_ws(2 * nkv + 1 + 4, 8);
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], eta, VOLUME * sizeof(spinor_dble));
+   rho = sap_gcr(nkv, nmx, istop, res, mu, wsd[0], wsd[1], ifail, status);
+   memcpy(psi, wsd[1], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+   return rho;
+}
+
+/* Wall-clock seconds for n applications of Dw_dble (op 0) or Dw (op 1) on a
+ * Gaussian field, timed with the reference's MPI_Wtime. */
+double ref_time_dirac(int op, double mu, int n)
+{
+   ENTER();
+   int i;
+   double t0, t1;
+   spinor_dble **wsd;
+   spinor **ws;
+
+   if (op == 0)
+   {
+      wsd = reserve_wsd(2);
+      random_sd(VOLUME_TRD, 2, wsd[0], 1.0);
+      Dw_dble(mu, wsd[0], wsd[1]);
+      t0 = MPI_Wtime();
+      for (i = 0; i < n; i++)
+         Dw_dble(mu, wsd[0], wsd[1]);
+      t1 = MPI_Wtime();
+      release_wsd();
+   }
+   else
+   {
+      assign_ud2u();
+      assign_swd2sw();
+      ws = reserve_ws(2);
+      random_s(VOLUME_TRD, 2, ws[0], 1.0f);
+      Dw((float)mu, ws[0], ws[1]);
+      t0 = MPI_Wtime();
+      for (i = 0; i < n; i++)
+         Dw((float)mu, ws[0], ws[1]);
+      t1 = MPI_Wtime();
+      release_ws();
+   }
+   return t1 - t0;
+}
+
+/* Site-local SW term of the reference on caller arrays
+ * (modules/sw_term/pauli_dble.c:1840, :1860; pauli.c:1107). */
+void ref_apply_sw_dble(int vol, double mu, const double *m, const double *s, double *r)
+{
+   ENTER();
+   apply_sw_dble(vol, mu, (pauli_dble *)m, (spinor_dble *)s, (spinor_dble *)r);
+}
+
+void ref_apply_sw(int vol, float mu, const float *m, const float *s, float *r)
+{
+   ENTER();
+   apply_sw(vol, mu, (pauli *)m, (spinor *)s, (spinor *)r);
+}
+
+int ref_apply_swinv_dble(int vol, double mu, const double *m, const double *s, double *r)
+{
+   ENTER();
+   int ifail;
+   pauli_wsp_t *pwsp;
+   pwsp = alloc_pauli_wsp();
+   ifail = apply_swinv_dble(vol, mu, (pauli_dble *)m, (spinor_dble *)s, pwsp, (spinor_dble *)r);
+   free_pauli_wsp(pwsp);
+   return ifail;
+}
+
+int ref_inv_pauli_dble(double mu, const double *m, double *im)
+{
+   ENTER();
+   int ifail;
+   pauli_wsp_t *pwsp;
+   pwsp = alloc_pauli_wsp();
+   ifail = inv_pauli_dble(mu, (pauli_dble *)m, pwsp, (pauli_dble *)im);
+   free_pauli_wsp(pwsp);
+   return ifail;
+}

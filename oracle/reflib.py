@@ -1,0 +1,188 @@
+"""ctypes binding of the reference CPU oracle (oracle/_ref/<tag>/libref.so).
+
+Test infrastructure: imported only by tests/, the smoke check and the CPU
+baseline of bench.py.  One library per lattice geometry; a process can load
+several (each has its own copy of the reference's module state).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# lattice -> thread-local lattice (the reference's Lx_TRD), NTHREAD = V / V_TRD
+GEOMETRIES = {
+    (8, 8, 8, 8): (4, 4, 4, 8),          # 8 threads
+    (8, 8, 8, 16): (4, 4, 4, 8),         # 16 threads
+    (16, 8, 8, 8): (4, 4, 4, 8),         # 16 threads
+    (16, 16, 16, 16): (8, 8, 8, 8),      # 16 threads
+    (64, 32, 32, 32): (32, 16, 16, 32),  # 8 threads
+}
+
+
+def tag(L, T, portable=False):
+    vol = L[0] * L[1] * L[2] * L[3]
+    return "%dx%dx%dx%d_t%d%s" % (L[0], L[1], L[2], L[3], vol // (T[0] * T[1] * T[2] * T[3]),
+                                 "_c" if portable else "")
+
+
+def lib_path(L, T=None, portable=False):
+    T = T or GEOMETRIES[tuple(L)]
+    return os.path.join(HERE, "_ref", tag(L, T, portable), "libref.so")
+
+
+def available(L, T=None, portable=False):
+    return os.path.exists(lib_path(L, T, portable))
+
+
+def ensure_built(L, T=None, ref="/root/reference", portable=False):
+    """Build the library for this geometry if it is missing and the reference
+    sources are present (they are not on the GPU machines).  portable=True
+    selects the reference's plain-C code paths (no AVX inline assembly)."""
+    T = T or GEOMETRIES[tuple(L)]
+    p = lib_path(L, T, portable)
+    if not os.path.exists(p) and os.path.isdir(ref):
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("build_ref", os.path.join(HERE, "build_ref.py"))
+        m = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(m)
+        m.build(list(L), list(T), ref, verbose=False, portable=portable)
+    return os.path.exists(p)
+
+
+class RefLib:
+    def __init__(self, L, T=None, portable=False):
+        T = T or GEOMETRIES[tuple(L)]
+        self.L = tuple(L)
+        self.portable = portable
+        path = lib_path(L, T, portable)
+        if not os.path.exists(path):
+            raise RuntimeError("reference oracle not built: " + path)
+        self.lib = C.CDLL(path)
+        l = self.lib
+        l.ref_init.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]
+        l.ref_set_sw_parms.argtypes = [C.c_double]
+        l.ref_set_tm_parms.argtypes = [C.c_int]
+        l.ref_set_sap_parms.argtypes = [C.c_int] * 7
+        l.ref_gen_links.argtypes = [C.c_double, C.c_int]
+        l.ref_random_ud.argtypes = [C.c_int]
+        l.ref_sw_term.argtypes = [C.c_int]
+        l.ref_random_sd.argtypes = [C.c_int, C.c_double, C.c_void_p]
+        l.ref_dirac_dble.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        l.ref_dirac.argtypes = [C.c_int, C.c_float, C.c_void_p, C.c_void_p]
+        l.ref_sap.argtypes = [C.c_float, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        l.ref_sap_gcr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]
+        l.ref_sap_gcr.restype = C.c_double
+        l.ref_time_dirac.argtypes = [C.c_int, C.c_double, C.c_int]
+        l.ref_time_dirac.restype = C.c_double
+        self.vol = l.ref_volume()
+        self.nthread = l.ref_nthread()
+
+    @staticmethod
+    def _p(a):
+        return a.ctypes.data_as(C.c_void_p)
+
+    def init(self, bc=3, seed=1234, csw=1.5, m0=0.0, eoflg=0):
+        self.lib.ref_init(bc, seed, csw, m0, eoflg)
+
+    def set_sw_parms(self, m0):
+        self.lib.ref_set_sw_parms(m0)
+
+    def set_tm_parms(self, eoflg):
+        self.lib.ref_set_tm_parms(eoflg)
+
+    def set_sap_parms(self, bs, isolv, nmr, ncy):
+        self.lib.ref_set_sap_parms(bs[0], bs[1], bs[2], bs[3], isolv, nmr, ncy)
+
+    def gen_links(self, eps, seed):
+        self.lib.ref_gen_links(eps, seed)
+
+    def sw_term(self, which=0):
+        return self.lib.ref_sw_term(which)
+
+    def ipt(self):
+        out = np.zeros(self.vol, dtype=np.int32)
+        self.lib.ref_get_ipt(self._p(out))
+        return out
+
+    def ud(self):
+        out = np.zeros(4 * self.vol * 18)
+        self.lib.ref_get_ud(self._p(out))
+        return out
+
+    def set_ud(self, ud):
+        ud = np.ascontiguousarray(ud, dtype=np.float64)
+        self.lib.ref_set_ud(self._p(ud))
+
+    def swd(self):
+        out = np.zeros(2 * self.vol * 36)
+        self.lib.ref_get_swd(self._p(out))
+        return out
+
+    def random_sd(self, seed, sigma=1.0):
+        out = np.zeros(self.vol * 24)
+        self.lib.ref_random_sd(seed, sigma, self._p(out))
+        return out
+
+    def dirac_dble(self, op, mu, s, r=None):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        r = np.zeros_like(s) if r is None else np.array(r, dtype=np.float64, copy=True)
+        self.lib.ref_dirac_dble(op, mu, self._p(s), self._p(r))
+        return r
+
+    def dirac(self, op, mu, s, r=None):
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        r = np.zeros_like(s) if r is None else np.array(r, dtype=np.float32, copy=True)
+        self.lib.ref_dirac(op, mu, self._p(s), self._p(r))
+        return r
+
+    def sap(self, mu, isolv, nmr, ncy, psi, rho):
+        psi = np.array(psi, dtype=np.float32, copy=True)
+        rho = np.array(rho, dtype=np.float32, copy=True)
+        f = self.lib.ref_sap(mu, isolv, nmr, ncy, self._p(psi), self._p(rho))
+        return psi, rho, f
+
+    def sap_gcr(self, nkv, nmx, istop, res, mu, eta):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        psi = np.zeros_like(eta)
+        ifail = C.c_int(0)
+        status = C.c_int(0)
+        rho = self.lib.ref_sap_gcr(nkv, nmx, istop, res, mu, self._p(eta), self._p(psi), C.byref(ifail),
+                                   C.byref(status))
+        return psi, rho, ifail.value, status.value
+
+    def time_dirac(self, op, mu, n):
+        return self.lib.ref_time_dirac(op, mu, n)
+
+    def apply_sw_dble(self, vol, mu, m, s):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        r = np.zeros_like(s)
+        self.lib.ref_apply_sw_dble.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.ref_apply_sw_dble(vol, mu, self._p(m), self._p(s), self._p(r))
+        return r
+
+    def apply_sw(self, vol, mu, m, s):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        r = np.zeros_like(s)
+        self.lib.ref_apply_sw.argtypes = [C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.ref_apply_sw(vol, mu, self._p(m), self._p(s), self._p(r))
+        return r
+
+    def apply_swinv_dble(self, vol, mu, m, s):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        r = np.zeros_like(s)
+        self.lib.ref_apply_swinv_dble.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        f = self.lib.ref_apply_swinv_dble(vol, mu, self._p(m), self._p(s), self._p(r))
+        return r, f
+
+    def inv_pauli_dble(self, mu, m):
+        m = np.ascontiguousarray(m, dtype=np.float64)
+        im = np.zeros(36)
+        self.lib.ref_inv_pauli_dble.argtypes = [C.c_double, C.c_void_p, C.c_void_p]
+        f = self.lib.ref_inv_pauli_dble(mu, self._p(m), self._p(im))
+        return im, f

@@ -1,0 +1,51 @@
+"""Shared set-up for the parity tests: reference fields from the CPU oracle,
+loaded into the device library through its C interface."""
+import numpy as np
+
+import openqcd_b200 as qb
+import reflib
+
+OPS = ["Dw", "Dwee", "Dwoo", "Dwoe", "Dweo", "Dwhat"]
+
+
+def site_rel_err(a, b, vol):
+    """max over sites of |a(x)-b(x)| / |b(x)| (24 reals per site)."""
+    a = np.asarray(a, dtype=np.float64).reshape(vol, 24)
+    b = np.asarray(b, dtype=np.float64).reshape(vol, 24)
+    d = np.linalg.norm(a - b, axis=1)
+    n = np.linalg.norm(b, axis=1)
+    mask = n > 0
+    if not mask.any():
+        return float(d.max())
+    return float((d[mask] / n[mask]).max()) if mask.all() else max(float((d[mask] / n[mask]).max()), float(d[~mask].max()))
+
+
+def rel_norm_err(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+class Setup:
+    """Reference fields on lattice L (links exp(eps X), SW term), and the
+    device library loaded with the same fields."""
+
+    def __init__(self, L, bs=(4, 4, 4, 4), eps=0.4, csw=1.5, m0=0.0, seed=1234, eoflg=0, portable=False):
+        assert reflib.ensure_built(L, portable=portable), "reference oracle library missing for %s" % (L,)
+        self.ref = reflib.RefLib(L, portable=portable)
+        self.ref.init(bc=3, seed=seed, csw=csw, m0=m0, eoflg=eoflg)
+        self.ref.gen_links(eps, seed)
+        assert self.ref.sw_term(0) == 0
+        self.L = tuple(L)
+        self.bs = tuple(bs)
+        self.vol = self.ref.vol
+        self.ipt = self.ref.ipt()
+        self.ud = self.ref.ud()
+        self.swd = self.ref.swd()
+        qb.geometry(L, bs, self.ipt)
+        qb.set_parms(csw, m0, eoflg)
+        qb.upload_ud(self.ud)
+        self.sw_fail = qb.upload_swd(self.swd)
+
+    def source(self, seed):
+        return self.ref.random_sd(seed)
