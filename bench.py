@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the Dirac-operator hot path on B200.
+
+One step = one application of the FP64 O(a)-improved Wilson-Dirac operator
+Dw_dble (modules/dirac/Dw_dble.c:1377 in the reference) to a 32^3x64 lattice
+(V = 2,097,152 sites; links exp(0.3 X), m0 = -0.05, csw = 1.7, bs = 4^4),
+the single-operator bandwidth workload.  The metric is the algorithmic HBM
+throughput, 1536 bytes per site (spinor in 192 + out 192 + 4 links 576 + SW
+576), in GB/s; every application moves 3.2 GB, far more than the 126 MB L2,
+so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value   : device-resident fields, K back-to-back launches timed with CUDA
+          events on the library's stream, max over ranks.
+e2e     : the drop-in C entry point Dw_dble(mu, s, r) on page-locked host
+          arrays in the reference layout (host->device copy, layout
+          conversion, operator, conversion back, device->host copy).
+Extra keys report the FP32 operator and the plain GPU SAP+GCR solve
+(seconds per right-hand side to FP64 relative residual 1e-10).
+
+With N GPUs (torchrun) every rank holds its own lattice (independent
+replicas, weak scaling); the only collective is the max-over-ranks of the
+timings.  --impl reference times the reference's own CPU Dw_dble (built from
+its sources, OpenMP on the host cores) on the same workload, on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "openqcd-2.4.2_b200"))
+
+import numpy as np  # noqa: E402
+
+LATTICE = (64, 32, 32, 32)
+BS = (4, 4, 4, 4)
+EPS, M0, CSW, MU = 0.3, -0.05, 1.7, 0.0
+BYTES_PER_SITE = {64: 1536, 32: 768}
+WORKLOAD = "Dw_dble on 32^3x64 (links exp(0.3 X), m0=-0.05, csw=1.7, periodic gauge / antiperiodic fermion bc)"
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, dev):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[3 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+class Dist:
+    def __init__(self):
+        self.rank = env_int("RANK", 0)
+        self.world = env_int("WORLD_SIZE", 1)
+        self.local = env_int("LOCAL_RANK", 0)
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            self.torch, self.dist = torch, dist
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.dist.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+def ref_lattice_threads():
+    """Thread-local lattice for the reference build: as many OpenMP threads as
+    host cores allow (NTHREAD = V / V_TRD, a power of two up to 64)."""
+    n = os.cpu_count() or 8
+    for nt, T in ((64, (16, 16, 16, 8)), (32, (16, 16, 16, 16)), (16, (32, 16, 16, 16)), (8, (32, 16, 16, 32))):
+        if nt <= n:
+            return nt, T
+    return 8, (32, 16, 16, 32)
+
+
+def reference_lib(L):
+    """The reference oracle library for the bench lattice (CPU baseline only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import reflib
+    nt, T = ref_lattice_threads()
+    while True:
+        if reflib.available(L, T) or reflib.ensure_built(L, T):
+            return reflib.RefLib(L, T), nt
+        # fall back to fewer threads if that build is not present
+        if nt == 8:
+            return None, 0
+        nt //= 2
+        T = {32: (16, 16, 16, 16), 16: (32, 16, 16, 16), 8: (32, 16, 16, 32)}[nt]
+
+
+def cpu_reference_timing(L, mu, seconds=12.0, warm=1, ud_ref=None):
+    """Time the reference's Dw_dble (its own CPU code, OpenMP) on the bench
+    lattice.  Returns (GB/s, threads, sample description)."""
+    ref, nt = reference_lib(L)
+    if ref is None:
+        return None
+    ref.init(bc=3, seed=4321, csw=CSW, m0=M0, eoflg=0)
+    if ud_ref is not None:
+        ref.set_ud(ud_ref)
+    else:
+        ref.lib.ref_random_ud(4321)
+    ref.sw_term(0)
+    ref.time_dirac(0, mu, warm)
+    t1 = ref.time_dirac(0, mu, 1)
+    n = max(2, int(seconds / max(t1, 1e-3)))
+    t = ref.time_dirac(0, mu, n)
+    vol = ref.vol
+    gbs = BYTES_PER_SITE[64] * vol * n / t / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": nt, "kind": "reference",
+            "sample": "%d applications of the reference Dw_dble (AVX/FMA3 build, NPROC=1, NTHREAD=%d) on 32^3x64, %.1f s"
+                      % (n, nt, t)}
+
+
+def run_reference(args, d):
+    if d.rank != 0:
+        return 0
+    ref, nt = reference_lib(LATTICE)
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference oracle library for 32^3x64 is not built"}))
+        return 0
+    ref.init(bc=3, seed=4321, csw=CSW, m0=M0, eoflg=0)
+    ref.gen_links(EPS, 4321)
+    ref.sw_term(0)
+    ref.time_dirac(0, MU, max(1, args.warmup))
+    times = [ref.time_dirac(0, MU, 1) for _ in range(args.steps)]
+    tot = sum(times)
+    vol = ref.vol
+    gbs = BYTES_PER_SITE[64] * vol * args.steps / tot / 1e9
+    out = {
+        "impl": "reference", "metric": "Dw_dble GB/s", "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD + " -- reference CPU implementation", "lattice": list(LATTICE),
+                   "l2": "inputs larger than L2 (3.2 GB per application)"},
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": nt, "kind": "reference",
+                         "sample": "%d single applications of the reference Dw_dble, NTHREAD=%d" % (args.steps, nt)},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--lattice", default=None, help="L0,L1,L2,L3 (profiling runs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solver", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    d = Dist()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, d)
+        return run_b200(args, d)
+    finally:
+        d.close()
+
+
+def run_b200(args, d):
+    import openqcd_b200 as qb
+    L = tuple(int(x) for x in args.lattice.split(",")) if args.lattice else LATTICE
+    qb.set_device(d.local)
+    ipt = qb.even_first_ipt(L)
+    qb.geometry(L, BS, ipt)
+    qb.set_parms(CSW, M0, 0)
+    qb.random_ud(EPS, 20251203 + d.rank)
+    qb.sw_term()
+    vol = qb.lib().b200_volume()
+    s = qb.DevField(64).random(1.0, 7 + d.rank)
+    r = qb.DevField(64)
+
+    for _ in range(args.warmup):
+        qb.time_dirac(64, "Dw", MU, s, r, 1)
+    d.barrier()
+    qb.lib().b200_sync()
+    clk = Clocks(d.local)
+    ms = qb.time_dirac(64, "Dw", MU, s, r, args.steps)
+    clocks = clk.stop()
+    qb.lib().b200_sync()
+    d.barrier()
+    ms_max = d.max(ms)
+    bytes_step = BYTES_PER_SITE[64] * vol
+    value = d.world * bytes_step * args.steps / (ms_max / 1e3) / 1e9
+    per_launch_ms = ms / args.steps
+    peak, peak_kind = peaks()
+    achieved = bytes_step / (per_launch_ms / 1e3) / 1e9
+
+    extra = {}
+    # FP32 operator (Dw, modules/dirac/Dw.c:973)
+    s32 = qb.DevField(32).random(1.0, 8)
+    r32 = qb.DevField(32)
+    qb.time_dirac(32, "Dw", MU, s32, r32, 3)
+    ms32 = qb.time_dirac(32, "Dw", MU, s32, r32, args.steps) / args.steps
+    extra["dw_f32"] = {"ms": ms32, "GBs": BYTES_PER_SITE[32] * vol / (ms32 / 1e3) / 1e9,
+                       "frac_of_peak": BYTES_PER_SITE[32] * vol / (ms32 / 1e3) / 1e9 / peak}
+    for op, bps in (("Dwhat", 1344), ):
+        qb.time_dirac(64, op, MU, s, r, 3)
+        m = qb.time_dirac(64, op, MU, s, r, args.steps) / args.steps
+        extra["dwhat_f64"] = {"ms": m, "GBs": bps * vol / (m / 1e3) / 1e9}
+    s32.free(); r32.free()
+
+    e2e = None
+    if not args.no_e2e:
+        sh = qb.HostArray(vol * 24)
+        rh = qb.HostArray(vol * 24)
+        qb.check(qb.lib().b200_dev_to_ref(64, s.ptr, sh.a.ctypes.data))
+        qb.time_Dw_dble_host(MU, sh.a, rh.a, 2)
+        n_e2e = max(3, min(args.steps, 10))
+        d.barrier()
+        ms_e = qb.time_Dw_dble_host(MU, sh.a, rh.a, n_e2e)
+        ms_e = d.max(ms_e)
+        e2e = {"value": d.world * bytes_step * n_e2e / (ms_e / 1e3) / 1e9, "unit": "GB/s",
+               "h2d_bytes_per_step": vol * 192, "d2h_bytes_per_step": vol * 192,
+               "ms_per_step": ms_e / n_e2e}
+        sh.free(); rh.free()
+
+    if not args.no_solver:
+        qb.set_sap_parms(BS, 1, 4, 5)
+        eta = qb.DevField(64).random(1.0, 9)
+        psi = qb.DevField(64)
+        qb.dev_sap_gcr(16, 256, 0, 1e-10, MU, eta, psi)   # warm-up
+        qb.lib().b200_sync()
+        t0 = time.time()
+        rho, ifail, st = qb.dev_sap_gcr(16, 256, 0, 1e-10, MU, eta, psi)
+        dt = time.time() - t0
+        chk = qb.DevField(64)
+        qb.dev_dirac("Dw", MU, psi, chk)
+        extra["sap_gcr"] = {"s_per_rhs": dt, "status": st, "ifail": ifail,
+                            "rel_residual": rho / np.sqrt(eta.norm2()), "nkv": 16, "isolv": 1, "nmr": 4, "ncy": 5,
+                            "bs": list(BS), "res": 1e-10,
+                            "solver": "plain GPU sap_gcr: FP64 outer residual, FP32 SAP and Krylov space"}
+
+    cpu = None
+    if not args.no_cpu_baseline and d.rank == 0 and d.world == 1 and L == LATTICE:
+        try:
+            cpu = cpu_reference_timing(L, MU)
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"unavailable": str(e)[:200]}
+
+    traffic = None
+    pf = os.path.join(ROOT, "profiles", "dw_dble_traffic.json")
+    if os.path.exists(pf):
+        try:
+            traffic = json.load(open(pf)).get("bytes_per_launch_full_lattice")
+        except Exception:
+            traffic = None
+
+    if d.rank == 0:
+        out = {
+            "metric": "Dw_dble GB/s", "value": value, "unit": "GB/s", "n_gpus": d.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (device-generated links exp(0.3 X), Gaussian source)",
+            "config": {"workload": WORKLOAD, "lattice": list(L), "block": list(BS), "global_batch": 1,
+                       "parallelism": "replicas%d" % d.world if d.world > 1 else "single",
+                       "l2": "inputs larger than L2 (3.2 GB per application), no flush"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_step},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+        }
+        out.update(extra)
+        print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

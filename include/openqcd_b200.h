@@ -28,6 +28,8 @@
 #ifndef OPENQCD_B200_H
 #define OPENQCD_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -45,12 +47,18 @@ typedef struct { complex c11, c12, c13, c21, c22, c23, c31, c32, c33; } su3;
 typedef struct { complex_dble c11, c12, c13, c21, c22, c23, c31, c32, c33; } su3_dble;
 typedef struct { float u[36]; } pauli;
 typedef struct { double u[36]; } pauli_dble;
+typedef struct { double q[2]; } qflt;
+typedef struct { qflt re, im; } complex_qflt;
 #endif
 #ifndef SW_TERM_H
 typedef struct b200_pauli_wsp pauli_wsp_t;   /* unused here; kept for the prototype */
 #endif
 
 /* ------------------------------------------------------------------ state */
+
+/* Select the CUDA device the library uses (default 0); call before
+ * b200_geometry().  One process per GPU. */
+int b200_set_device(int dev);
 
 /* Lattice geometry.  L[4] lattice sizes (x0 = time), bs[4] the SAP block
  * size, which is also the tile of the device layout.  ipt (may be NULL) is
@@ -94,6 +102,15 @@ int b200_sw_term(void);
  * time boundary sign applied as set_ud_phase() does. */
 int b200_random_ud(double eps, unsigned long long seed);
 
+/* Page-locked host memory for reference-layout arrays (fast host<->device
+ * transfers in the drop-in calls). */
+void *b200_host_alloc(size_t bytes);
+void b200_host_free(void *p);
+/* Device-memory buffer of the given size, and a copy between any two
+ * host/device addresses (cudaMemcpyDefault semantics). */
+void *b200_dev_alloc(size_t bytes);
+int b200_memcpy(void *dst, const void *src, size_t bytes);
+
 const char *b200_last_error(void);
 void b200_set_fatal(int on);
 int b200_sync(void);
@@ -125,6 +142,34 @@ void sap(float mu, int isolv, int nmr, spinor *psi, spinor *rho);
 /* sap_gcr.c:140: SAP-preconditioned flexible GCR; same ifail/status codes */
 double sap_gcr(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi,
                int *ifail, int *status);
+
+/* ------------------------------- drop-in BLAS-1 (linalg.h, salg*.c) */
+/* vol sites; with icom & 0x2 the fields span vol sites per thread of the
+ * caller's NTHREAD threads (b200_set_nthread, default 1); icom & 0x1 (MPI
+ * sum) is a no-op here.  Arrays in host or device memory. */
+int b200_set_nthread(int n);
+/* salg_dble.c:2611 */ complex_qflt spinor_prod_dble(int vol, int icom, spinor_dble *s, spinor_dble *r);
+/* salg_dble.c      */ qflt spinor_prod_re_dble(int vol, int icom, spinor_dble *s, spinor_dble *r);
+/* salg_dble.c:2729 */ qflt norm_square_dble(int vol, int icom, spinor_dble *s);
+/* salg_dble.c      */ void mulc_spinor_add_dble(int vol, int icom, spinor_dble *s, spinor_dble *r, complex_dble z);
+/* salg_dble.c      */ void mulr_spinor_add_dble(int vol, int icom, spinor_dble *s, spinor_dble *r, double c);
+/* salg_dble.c      */ void scale_dble(int vol, int icom, double c, spinor_dble *s);
+/* salg_dble.c      */ double normalize_dble(int vol, int icom, spinor_dble *s);
+/* salg.c:1223 */ complex spinor_prod(int vol, int icom, spinor *s, spinor *r);
+/* salg.c      */ float spinor_prod_re(int vol, int icom, spinor *s, spinor *r);
+/* salg.c:1289 */ float norm_square(int vol, int icom, spinor *s);
+/* salg.c:1319 */ void mulc_spinor_add(int vol, int icom, spinor *s, spinor *r, complex z);
+/* salg.c      */ void mulr_spinor_add(int vol, int icom, spinor *s, spinor *r, float c);
+/* salg.c      */ void scale(int vol, int icom, float c, spinor *s);
+/* salg.c:1415 */ float normalize(int vol, int icom, spinor *s);
+
+/* fgcr.c:215: flexible GCR with the caller's operator Dop and
+ * preconditioner Mop (called back with the caller's own arrays, which Dop
+ * and Mop must be able to act on).  vol and the workspaces ws[2*nkv+1],
+ * wsd[1] as in the reference (vol per thread, see b200_set_nthread). */
+double fgcr(int vol, void (*Dop)(spinor_dble *s, spinor_dble *r), void (*Mop)(int k, spinor *rho, spinor *phi, spinor *chi),
+            spinor **ws, spinor_dble **wsd, int nkv, int nmx, int istop, double res, spinor_dble *eta,
+            spinor_dble *psi, int *status);
 
 /* ------------------------------------ device-resident fields (own layout) */
 /* prec = 64 (spinor_dble) or 32 (spinor).  Operator codes for

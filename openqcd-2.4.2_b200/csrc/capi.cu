@@ -116,9 +116,34 @@ using qcd::apply_swinv_ref_layout;
 extern "C" {
 
 const char *b200_last_error(void) { return g_err.c_str(); }
+
+void *b200_host_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) { fail("page-locked host allocation failed"); return nullptr; }
+  return p;
+}
+void b200_host_free(void *p) { cudaFreeHost(p); }
+
+void *b200_dev_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) { fail("device allocation failed"); return nullptr; }
+  return p;
+}
+
+int b200_memcpy(void *dst, const void *src, size_t bytes) {
+  return cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) == cudaSuccess ? 0 : fail("memcpy failed");
+}
 void b200_set_fatal(int on) { g_fatal = on != 0; }
 int b200_sync(void) { return cudaStreamSynchronize(ctx().stream) == cudaSuccess ? 0 : fail("CUDA error"); }
 int b200_volume(void) { return ctx().ready ? ctx().g.vol : 0; }
+
+int b200_set_device(int dev) {
+  Ctx &c = ctx();
+  if (c.stream) return fail("set_device: must be called before the first geometry call");
+  if (cudaSetDevice(dev) != cudaSuccess) return fail("set_device: no such CUDA device");
+  c.dev = dev;
+  return 0;
+}
 
 int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   Ctx &c = ctx();

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(128) dirac_kernel(Geom g, const void *__restri
   }
 }
 
+
 template <typename R, int OPS, int PAR>
 static void launch(const Ctx &c, const void *s, const void *t, void *r, R mu_e, R mu_o, bool inv,
                    cudaStream_t st) {

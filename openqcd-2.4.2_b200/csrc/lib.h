@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
+#include <functional>
 #include <string>
 #include <vector>
 #include "qcd.cuh"
@@ -52,6 +53,9 @@ struct Ctx {
   double *h_red = nullptr;      // pinned host mirror of red_out
   int red_blocks = 0;
   cudaStream_t stream = nullptr;
+  int nthread = 1;              // the caller's NTHREAD, for icom & 0x2 in the BLAS drop-ins
+  void *fstage[3] = {nullptr, nullptr, nullptr};   // staging of host operands
+  size_t fstage_bytes[3] = {0, 0, 0};
   std::vector<void *> ws32, ws64;   // solver workspaces (reserve_ws / reserve_wsd)
 };
 
@@ -101,6 +105,40 @@ void la_axpy(const Ctx &c, int prec, void *y, double are, double aim, const void
 void la_diff(const Ctx &c, int prec, const void *x, void *y, int par, cudaStream_t st);  // y = x - y
 void la_add_s2sd(const Ctx &c, const void *s32, void *sd, int par, cudaStream_t st);    // sd += s
 void la_diff_sd2s(const Ctx &c, const void *ad, const void *bd, void *r32, int par, cudaStream_t st);  // r = a - b
+
+// blas.cu: layout-agnostic BLAS-1 on device-accessible arrays of nsite
+// sites in the reference's order (24 reals per site)
+int flat_scratch(Ctx &c, double **scratch, double **out);
+int flat_dot(Ctx &c, int prec, const void *x, const void *y, size_t nsite, double *res_dd, double *scratch,
+             double *out_dev);
+int flat_norm2(Ctx &c, int prec, const void *x, size_t nsite, double *res_dd, double *scratch, double *out_dev);
+int flat_umax(Ctx &c, int prec, const void *x, size_t nsite, double *res, double *scratch, double *out_dev);
+void flat_axpy(Ctx &c, int prec, void *y, const void *x, size_t nsite, double ar, double ai);
+void flat_scale(Ctx &c, int prec, void *y, size_t nsite, double a);
+void flat_zero(Ctx &c, int prec, void *y, size_t nsite);
+void flat_copy(Ctx &c, int pin, const void *x, int pout, void *y, size_t nsite);
+void flat_add_s2sd(Ctx &c, const void *s, void *sd, size_t nsite);
+void flat_diff_sd2s(Ctx &c, const void *a, const void *b, void *r, size_t nsite);
+void flat_diff(Ctx &c, int prec, const void *x, void *y, size_t nsite);
+
+// solver.cu: the GCR recursion over an abstract set of FP32/FP64 field
+// operations, so the same code serves device-layout fields (sap_gcr) and
+// caller arrays (the generic fgcr drop-in).
+struct cplxf { float re, im; };
+struct KrylovOps {
+  std::function<double(const void *, int)> res32;                 // get_res (fgcr.c:128)
+  std::function<cplxf(const void *, const void *)> dot32;         // spinor_prod
+  std::function<float(void *)> normalize32;                        // normalize
+  std::function<void(void *, float, float, const void *)> axpy32;  // mulc_spinor_add
+  std::function<void(void *)> zero32, zero64;
+  std::function<void(const void *, void *)> copy64to32;            // assign_sd2s
+  std::function<void(const void *, void *)> add32to64;             // add_s2sd
+  std::function<void(const void *, const void *, void *)> diff64to32;  // diff_sd2s
+};
+double fgcr_core(const KrylovOps &o, int nkv, int nmx, int istop, double res, const void *eta, void *psi,
+                 int *status, const std::function<void(const void *, void *)> &Dop,
+                 const std::function<void(int, const void *, void *, void *)> &Mop,
+                 const std::vector<void *> &phi, const std::vector<void *> &chi, void *rho, void *wrk);
 
 // sap.cu
 int sap_prepare(Ctx &c, cudaStream_t st);

@@ -25,54 +25,23 @@ static int reserve(Ctx &c, std::vector<void *> &ws, size_t n, int prec) {
   return 0;
 }
 
-struct cplxf { float re, im; };
-
 using DopFn = std::function<void(const void *s64, void *r64)>;
 using MopFn = std::function<void(int k, const void *rho32, void *phi32, void *chi32)>;
 
-static double get_res(Ctx &c, int istop, const void *rho) {
-  double r[4];
-  if (istop) {
-    la_unorm(c, 32, rho, PAR_ALL, r);
-    return (double)(float)r[0];
-  }
-  la_norm2(c, 32, rho, PAR_ALL, r);
-  return sqrt((double)(float)(r[0] + r[1]));
-}
-
-static cplxf sprod(Ctx &c, const void *x, const void *y) {
-  double r[4];
-  la_dot(c, 32, x, y, PAR_ALL, r);
-  return {(float)(r[0] + r[1]), (float)(r[2] + r[3])};
-}
-
-static float normalize(Ctx &c, void *x) {
-  double r[2];
-  la_norm2(c, 32, x, PAR_ALL, r);
-  float n = (float)(r[0] + r[1]);
-  n = (float)sqrt((double)n);
-  if (n != 0.0f) la_scale(c, 32, x, 1.0f / n, PAR_ALL, c.stream);
-  return n;
-}
-
-double fgcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, const void *eta, void *psi, int *status,
-                const DopFn &Dop, const MopFn &Mop) {
+double fgcr_core(const KrylovOps &o, int nkv, int nmx, int istop, double res, const void *eta, void *psi,
+                 int *status, const DopFn &Dop, const MopFn &Mop, const std::vector<void *> &phi,
+                 const std::vector<void *> &chi, void *rho, void *wrk) {
   if (nkv < 1 || nmx < 1 || res <= DBL_EPSILON || istop < 0 || istop > 1) {
     fail("fgcr: parameters are out of range");
     return -1.0;
   }
-  if (reserve(c, c.ws32, 2 * nkv + 1, 32) || reserve(c, c.ws64, 2, 64)) return -1.0;
-  std::vector<void *> phi(c.ws32.begin(), c.ws32.begin() + nkv), chi(c.ws32.begin() + nkv + 1, c.ws32.begin() + 2 * nkv + 1);
-  void *rho = c.ws32[nkv];
-  void *wrk = c.ws64[0];
   std::vector<cplxf> a((size_t)nkv * nkv), cc(nkv);
   std::vector<float> b(nkv);
   const double PRECISION_LIMIT = (double)(100.0f * FLT_EPSILON);
-  cudaStream_t st = c.stream;
 
-  la_zero(c, 64, psi, PAR_ALL, st);
-  la_copy(c, 64, eta, 32, rho, PAR_ALL, st);
-  double rn = get_res(c, istop, rho);
+  o.zero64(psi);
+  o.copy64to32(eta, rho);
+  double rn = o.res32(rho, istop);
   double tol = res * rn;
   status[0] = 0;
 
@@ -80,21 +49,21 @@ double fgcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, const void *eta
     double rn_old = rn;
     int k;
     for (k = 0;; k++) {
-      // gcr_step
+      // gcr_step (fgcr.c:157)
       Mop(k, rho, phi[k], chi[k]);
       for (int l = 0; l < k; l++) {
-        cplxf z = sprod(c, chi[l], chi[k]);
+        cplxf z = o.dot32(chi[l], chi[k]);
         a[(size_t)nkv * l + k] = z;
-        la_axpy(c, 32, chi[k], -z.re, -z.im, chi[l], PAR_ALL, st);
+        o.axpy32(chi[k], -z.re, -z.im, chi[l]);
       }
-      b[k] = normalize(c, chi[k]);
-      cc[k] = sprod(c, chi[k], rho);
-      la_axpy(c, 32, rho, -cc[k].re, -cc[k].im, chi[k], PAR_ALL, st);
-      rn = get_res(c, istop, rho);
+      b[k] = o.normalize32(chi[k]);
+      cc[k] = o.dot32(chi[k], rho);
+      o.axpy32(rho, -cc[k].re, -cc[k].im, chi[k]);
+      rn = o.res32(rho, istop);
       status[0] += 1;
       if (rn <= tol || rn < PRECISION_LIMIT * rn_old || k == nkv - 1 || status[0] >= nmx) break;
     }
-    // update_psi
+    // update_psi (fgcr.c:181)
     for (int l = k; l >= 0; l--) {
       cplxf z = cc[l];
       for (int i = l + 1; i <= k; i++) {
@@ -106,18 +75,60 @@ double fgcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, const void *eta
       cc[l].re = z.re * r;
       cc[l].im = z.im * r;
     }
-    la_zero(c, 32, rho, PAR_ALL, st);
-    for (int l = k; l >= 0; l--) la_axpy(c, 32, rho, cc[l].re, cc[l].im, phi[l], PAR_ALL, st);
-    la_add_s2sd(c, rho, psi, PAR_ALL, st);
+    o.zero32(rho);
+    for (int l = k; l >= 0; l--) o.axpy32(rho, cc[l].re, cc[l].im, phi[l]);
+    o.add32to64(rho, psi);
     Dop(psi, wrk);
-    la_diff_sd2s(c, eta, wrk, rho, PAR_ALL, st);
-    rn = get_res(c, istop, rho);
+    o.diff64to32(eta, wrk, rho);
+    rn = o.res32(rho, istop);
     if (status[0] >= nmx && rn > tol) {
       status[0] = -1;
       return rn;
     }
   }
   return rn;
+}
+
+// Vector operations on fields in the device layout (la_* of linalg.cu).
+static KrylovOps dev_ops(Ctx &c) {
+  KrylovOps o;
+  cudaStream_t st = c.stream;
+  o.res32 = [&c](const void *x, int istop) {
+    double r[4];
+    if (istop) {
+      la_unorm(c, 32, x, PAR_ALL, r);
+      return (double)(float)r[0];
+    }
+    la_norm2(c, 32, x, PAR_ALL, r);
+    return sqrt((double)(float)(r[0] + r[1]));
+  };
+  o.dot32 = [&c](const void *x, const void *y) {
+    double r[4];
+    la_dot(c, 32, x, y, PAR_ALL, r);
+    return cplxf{(float)(r[0] + r[1]), (float)(r[2] + r[3])};
+  };
+  o.normalize32 = [&c, st](void *x) {
+    double r[2];
+    la_norm2(c, 32, x, PAR_ALL, r);
+    float n = (float)sqrt((double)(float)(r[0] + r[1]));
+    if (n != 0.0f) la_scale(c, 32, x, 1.0f / n, PAR_ALL, st);
+    return n;
+  };
+  o.axpy32 = [&c, st](void *y, float ar, float ai, const void *x) { la_axpy(c, 32, y, ar, ai, x, PAR_ALL, st); };
+  o.zero32 = [&c, st](void *x) { la_zero(c, 32, x, PAR_ALL, st); };
+  o.zero64 = [&c, st](void *x) { la_zero(c, 64, x, PAR_ALL, st); };
+  o.copy64to32 = [&c, st](const void *x, void *y) { la_copy(c, 64, x, 32, y, PAR_ALL, st); };
+  o.add32to64 = [&c, st](const void *s, void *d) { la_add_s2sd(c, s, d, PAR_ALL, st); };
+  o.diff64to32 = [&c, st](const void *a, const void *b, void *r) { la_diff_sd2s(c, a, b, r, PAR_ALL, st); };
+  return o;
+}
+
+double fgcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, const void *eta, void *psi, int *status,
+                const DopFn &Dop, const MopFn &Mop) {
+  if (reserve(c, c.ws32, 2 * nkv + 1, 32) || reserve(c, c.ws64, 2, 64)) return -1.0;
+  std::vector<void *> phi(c.ws32.begin(), c.ws32.begin() + nkv),
+      chi(c.ws32.begin() + nkv + 1, c.ws32.begin() + 2 * nkv + 1);
+  return fgcr_core(dev_ops(c), nkv, nmx, istop, res, eta, psi, status, Dop, Mop, phi, chi, c.ws32[nkv], c.ws64[0]);
 }
 
 // Device twin of sap_gcr(): eta, psi FP64 device fields (psi may equal eta).

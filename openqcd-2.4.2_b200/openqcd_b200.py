@@ -18,9 +18,30 @@ LIB_PATH = os.path.join(HERE, "libopenqcd_b200.so")
 
 _lib = None
 
+
+class Qflt(C.Structure):
+    _fields_ = [("q", C.c_double * 2)]
+
+
+class ComplexQflt(C.Structure):
+    _fields_ = [("re", Qflt), ("im", Qflt)]
+
+
+class ComplexF(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+class ComplexD(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+DOP_T = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p)
+MOP_T = C.CFUNCTYPE(None, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
+
 DIRAC_OPS = {"Dw": 0, "Dwee": 1, "Dwoo": 2, "Dwoe": 3, "Dweo": 4, "Dwhat": 5}
 
 _SIGS = {
+    "b200_set_device": (C.c_int, [C.c_int]),
     "b200_geometry": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_set_lat_parms": (C.c_int, [C.c_double]),
     "b200_set_bc_parms": (C.c_int, [C.c_int]),
@@ -33,6 +54,10 @@ _SIGS = {
     "b200_download_swd": (C.c_int, [C.c_void_p, C.c_int]),
     "b200_sw_term": (C.c_int, []),
     "b200_random_ud": (C.c_int, [C.c_double, C.c_ulonglong]),
+    "b200_host_alloc": (C.c_void_p, [C.c_size_t]),
+    "b200_host_free": (None, [C.c_void_p]),
+    "b200_dev_alloc": (C.c_void_p, [C.c_size_t]),
+    "b200_memcpy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "b200_last_error": (C.c_char_p, []),
     "b200_set_fatal": (None, [C.c_int]),
     "b200_sync": (C.c_int, []),
@@ -55,6 +80,23 @@ _SIGS = {
     "sap": (None, [C.c_float, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "sap_gcr": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.c_void_p]),
+    "b200_set_nthread": (C.c_int, [C.c_int]),
+    "spinor_prod_dble": (ComplexQflt, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "spinor_prod_re_dble": (Qflt, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "norm_square_dble": (Qflt, [C.c_int, C.c_int, C.c_void_p]),
+    "mulc_spinor_add_dble": (None, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ComplexD]),
+    "mulr_spinor_add_dble": (None, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double]),
+    "scale_dble": (None, [C.c_int, C.c_int, C.c_double, C.c_void_p]),
+    "normalize_dble": (C.c_double, [C.c_int, C.c_int, C.c_void_p]),
+    "spinor_prod": (ComplexF, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "spinor_prod_re": (C.c_float, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "norm_square": (C.c_float, [C.c_int, C.c_int, C.c_void_p]),
+    "mulc_spinor_add": (None, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, ComplexF]),
+    "mulr_spinor_add": (None, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_float]),
+    "scale": (None, [C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "normalize": (C.c_float, [C.c_int, C.c_int, C.c_void_p]),
+    "fgcr": (C.c_double, [C.c_int, DOP_T, MOP_T, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_dev_alloc_spinor": (C.c_void_p, [C.c_int]),
     "b200_dev_free": (None, [C.c_void_p]),
     "b200_dev_random_spinor": (C.c_int, [C.c_int, C.c_void_p, C.c_double, C.c_ulonglong]),
@@ -100,6 +142,23 @@ def check(rc):
     if rc is not None and rc < 0:
         raise B200Error(lib().b200_last_error().decode())
     return rc
+
+
+def set_device(dev):
+    return check(lib().b200_set_device(dev))
+
+
+def even_first_ipt(L):
+    """An ipt[] table in the reference's convention (ipt[lexicographic index]
+    = storage index, even sites first), ordering each parity
+    lexicographically."""
+    L = tuple(L)
+    x = np.indices(L).reshape(4, -1)
+    par = x.sum(axis=0) & 1
+    order = np.argsort(par, kind="stable")
+    ipt = np.empty(order.size, dtype=np.int32)
+    ipt[order] = np.arange(order.size, dtype=np.int32)
+    return ipt
 
 
 def geometry(L, bs, ipt=None):
@@ -272,6 +331,24 @@ def apply_swinv_dble(vol, mu, m, s):
     r = np.zeros_like(s)
     f = lib().apply_swinv_dble(vol, mu, _ptr(np.ascontiguousarray(m, dtype=np.float64)), _ptr(s), None, _ptr(r))
     return r, f
+
+
+class HostArray:
+    """Page-locked host buffer exposed as a numpy array."""
+
+    def __init__(self, n, dtype=np.float64):
+        dt = np.dtype(dtype)
+        self.ptr = lib().b200_host_alloc(n * dt.itemsize)
+        if not self.ptr:
+            raise B200Error(_err_after())
+        buf = (C.c_char * (n * dt.itemsize)).from_address(self.ptr)
+        self.a = np.frombuffer(buf, dtype=dt, count=n)
+
+    def free(self):
+        if self.ptr:
+            self.a = None
+            lib().b200_host_free(self.ptr)
+            self.ptr = None
 
 
 def time_dirac(prec, op, mu, s, r, n):

@@ -309,17 +309,35 @@ double ref_time_dirac(int op, double mu, int n)
 }
 
 /* Site-local SW term of the reference on caller arrays
- * (modules/sw_term/pauli_dble.c:1840, :1860; pauli.c:1107). */
+ * (modules/sw_term/pauli_dble.c:1840, :1860; pauli.c:1107).  The reference's
+ * AVX code needs 32-byte aligned matrices and spinors, so the caller's arrays
+ * are copied into aligned buffers first. */
+static void *aligned_copy(const void *p, size_t n)
+{
+   void *q = aligned_alloc(64, (n + 63) / 64 * 64);
+   if (q != NULL && p != NULL)
+      memcpy(q, p, n);
+   return q;
+}
+
 void ref_apply_sw_dble(int vol, double mu, const double *m, const double *s, double *r)
 {
    ENTER();
-   apply_sw_dble(vol, mu, (pauli_dble *)m, (spinor_dble *)s, (spinor_dble *)r);
+   size_t nm = (size_t)vol * 2 * sizeof(pauli_dble), ns = (size_t)vol * sizeof(spinor_dble);
+   void *am = aligned_copy(m, nm), *as = aligned_copy(s, ns), *ar = aligned_copy(NULL, ns);
+   apply_sw_dble(vol, mu, (pauli_dble *)am, (spinor_dble *)as, (spinor_dble *)ar);
+   memcpy(r, ar, ns);
+   free(am); free(as); free(ar);
 }
 
 void ref_apply_sw(int vol, float mu, const float *m, const float *s, float *r)
 {
    ENTER();
-   apply_sw(vol, mu, (pauli *)m, (spinor *)s, (spinor *)r);
+   size_t nm = (size_t)vol * 2 * sizeof(pauli), ns = (size_t)vol * sizeof(spinor);
+   void *am = aligned_copy(m, nm), *as = aligned_copy(s, ns), *ar = aligned_copy(NULL, ns);
+   apply_sw(vol, mu, (pauli *)am, (spinor *)as, (spinor *)ar);
+   memcpy(r, ar, ns);
+   free(am); free(as); free(ar);
 }
 
 int ref_apply_swinv_dble(int vol, double mu, const double *m, const double *s, double *r)
@@ -327,9 +345,13 @@ int ref_apply_swinv_dble(int vol, double mu, const double *m, const double *s, d
    ENTER();
    int ifail;
    pauli_wsp_t *pwsp;
+   size_t nm = (size_t)vol * 2 * sizeof(pauli_dble), ns = (size_t)vol * sizeof(spinor_dble);
+   void *am = aligned_copy(m, nm), *as = aligned_copy(s, ns), *ar = aligned_copy(NULL, ns);
    pwsp = alloc_pauli_wsp();
-   ifail = apply_swinv_dble(vol, mu, (pauli_dble *)m, (spinor_dble *)s, pwsp, (spinor_dble *)r);
+   ifail = apply_swinv_dble(vol, mu, (pauli_dble *)am, (spinor_dble *)as, pwsp, (spinor_dble *)ar);
    free_pauli_wsp(pwsp);
+   memcpy(r, ar, ns);
+   free(am); free(as); free(ar);
    return ifail;
 }
 
@@ -338,8 +360,60 @@ int ref_inv_pauli_dble(double mu, const double *m, double *im)
    ENTER();
    int ifail;
    pauli_wsp_t *pwsp;
+   void *am = aligned_copy(m, sizeof(pauli_dble)), *ai = aligned_copy(NULL, sizeof(pauli_dble));
    pwsp = alloc_pauli_wsp();
-   ifail = inv_pauli_dble(mu, (pauli_dble *)m, pwsp, (pauli_dble *)im);
+   ifail = inv_pauli_dble(mu, (pauli_dble *)am, pwsp, (pauli_dble *)ai);
    free_pauli_wsp(pwsp);
+   memcpy(im, ai, sizeof(pauli_dble));
+   free(am); free(ai);
    return ifail;
+}
+
+/* Reference BLAS-1 on caller arrays of VOLUME sites (modules/linalg/
+ * salg_dble.c:2611, :2729; salg.c:1223, :1289), called as the reference's
+ * solvers do (vol = VOLUME_TRD, icom = 3). */
+void ref_spinor_prod_dble(const double *s, const double *r, double *out)
+{
+   ENTER();
+   complex_qflt z;
+   spinor_dble **wsd = reserve_wsd(2);
+   memcpy(wsd[0], s, VOLUME * sizeof(spinor_dble));
+   memcpy(wsd[1], r, VOLUME * sizeof(spinor_dble));
+   z = spinor_prod_dble(VOLUME_TRD, 3, wsd[0], wsd[1]);
+   out[0] = z.re.q[0]; out[1] = z.re.q[1]; out[2] = z.im.q[0]; out[3] = z.im.q[1];
+   release_wsd();
+}
+
+void ref_norm_square_dble(const double *s, double *out)
+{
+   ENTER();
+   qflt q;
+   spinor_dble **wsd = reserve_wsd(1);
+   memcpy(wsd[0], s, VOLUME * sizeof(spinor_dble));
+   q = norm_square_dble(VOLUME_TRD, 3, wsd[0]);
+   out[0] = q.q[0]; out[1] = q.q[1];
+   release_wsd();
+}
+
+void ref_spinor_prod(const float *s, const float *r, float *out)
+{
+   ENTER();
+   complex z;
+   spinor **ws = reserve_ws(2);
+   memcpy(ws[0], s, VOLUME * sizeof(spinor));
+   memcpy(ws[1], r, VOLUME * sizeof(spinor));
+   z = spinor_prod(VOLUME_TRD, 3, ws[0], ws[1]);
+   out[0] = z.re; out[1] = z.im;
+   release_ws();
+}
+
+float ref_norm_square(const float *s)
+{
+   ENTER();
+   float n;
+   spinor **ws = reserve_ws(1);
+   memcpy(ws[0], s, VOLUME * sizeof(spinor));
+   n = norm_square(VOLUME_TRD, 3, ws[0]);
+   release_ws();
+   return n;
 }

@@ -186,3 +186,32 @@ class RefLib:
         self.lib.ref_inv_pauli_dble.argtypes = [C.c_double, C.c_void_p, C.c_void_p]
         f = self.lib.ref_inv_pauli_dble(mu, self._p(m), self._p(im))
         return im, f
+
+    def spinor_prod_dble(self, s, r):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        out = np.zeros(4)
+        self.lib.ref_spinor_prod_dble.argtypes = [C.c_void_p] * 3
+        self.lib.ref_spinor_prod_dble(self._p(s), self._p(r), self._p(out))
+        return out
+
+    def norm_square_dble(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        out = np.zeros(2)
+        self.lib.ref_norm_square_dble.argtypes = [C.c_void_p] * 2
+        self.lib.ref_norm_square_dble(self._p(s), self._p(out))
+        return out
+
+    def spinor_prod(self, s, r):
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        r = np.ascontiguousarray(r, dtype=np.float32)
+        out = np.zeros(2, dtype=np.float32)
+        self.lib.ref_spinor_prod.argtypes = [C.c_void_p] * 3
+        self.lib.ref_spinor_prod(self._p(s), self._p(r), self._p(out))
+        return out
+
+    def norm_square(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        self.lib.ref_norm_square.argtypes = [C.c_void_p]
+        self.lib.ref_norm_square.restype = C.c_float
+        return self.lib.ref_norm_square(self._p(s))
