@@ -184,6 +184,19 @@ int b200_dev_sap(float mu, int isolv, int nmr, int ncy, void *psi, void *rho);
 double b200_dev_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
                         int *ifail, int *status);
 double b200_dev_norm2(int prec, const void *f);
+
+/* No counterpart in the reference.  Dwhat_dble (even-odd preconditioned FP64
+ * operator, as b200_dev_dirac(64, 5, ...)) on device-resident fields in the
+ * library's layout, without allocating anything: for callers that cannot let
+ * a library call cudaMalloc -- during CUDA graph capture, with a device memory
+ * pool that already holds all memory, or in loops that must avoid
+ * cudaMalloc's implicit synchronisation.  The odd-site intermediate lives in
+ * a static device array of 12 MiB (held by every GPU that loads the library
+ * until exit), so lattices larger than 131072 sites are rejected with an
+ * error.  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams or host threads) race. */
+int b200_dev_Dwhat_dble_noalloc(double mu, const void *s, void *r);
 /* Device time of n back-to-back operator applications, measured with CUDA
  * events on the library's stream; returns total milliseconds in *ms. */
 int b200_dev_time_dirac(int prec, int op, double mu, const void *s, void *r, int n, float *ms);

@@ -25,7 +25,9 @@ namespace qcd {
 
 enum { OP_SW = 1, OP_HOP = 2, OP_HOPSUB = 4, OP_INV = 8, OP_ACC = 16 };
 
-template <typename R, int OPS, int PAR>
+// RHALF / THALF = 1: the output r / the hop field t is a half-field holding
+// only the odd chunks (chunk index counted from the first odd chunk).
+template <typename R, int OPS, int PAR, int RHALF = 0, int THALF = 0>
 __global__ void __launch_bounds__(128) dirac_kernel(Geom g, const void *__restrict__ s, const void *__restrict__ t,
                                                     void *r, const void *__restrict__ u,
                                                     const void *__restrict__ sw, const void *__restrict__ swinv,
@@ -66,13 +68,13 @@ __global__ void __launch_bounds__(128) dirac_kernel(Geom g, const void *__restri
       int c2, s2;
       site_nbr(g, x, mu, +1, c2, s2);
       {
-        spinor<R> sp = Store<R>::load_spinor(t, c2, s2, g.vbh);
+        spinor<R> sp = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
         su3<R> uu = Store<R>::load_link(u, chunk, mu, si, g.vbh);
         hop_fwd<R>(mu, uu, sp, h);
       }
       site_nbr(g, x, mu, -1, c2, s2);
       {
-        spinor<R> sm = Store<R>::load_spinor(t, c2, s2, g.vbh);
+        spinor<R> sm = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
         su3<R> uu = Store<R>::load_link(u, c2, mu, s2, g.vbh);
         hop_bwd<R>(mu, uu, sm, h);
       }
@@ -83,12 +85,13 @@ __global__ void __launch_bounds__(128) dirac_kernel(Geom g, const void *__restri
     else ssub(acc, h);
   }
 
+  const int rchunk = RHALF ? chunk - g.nbl : chunk;
   if (OPS & OP_ACC) {
-    spinor<R> old = Store<R>::load_spinor_rw(r, chunk, si, g.vbh);
+    spinor<R> old = Store<R>::load_spinor_rw(r, rchunk, si, g.vbh);
     sadd(old, acc);
-    Store<R>::store_spinor(r, chunk, si, g.vbh, old);
+    Store<R>::store_spinor(r, rchunk, si, g.vbh, old);
   } else {
-    Store<R>::store_spinor(r, chunk, si, g.vbh, acc);
+    Store<R>::store_spinor(r, rchunk, si, g.vbh, acc);
   }
 }
 
@@ -123,6 +126,18 @@ int dirac_op(const Ctx &c, int op, R mu, const void *s, void *r, void *tmp, cuda
       break;
     default: return -1;
   }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// Dwhat_dble with the odd intermediate in a caller-provided half-field
+// (odd chunks only, volh sites); used by the allocation-free entry point.
+int dwhat_dble_halfscratch(const Ctx &c, double mu, const void *s, void *r, void *odd_scratch, cudaStream_t st) {
+  const int threads = 128;
+  const unsigned nb = (unsigned)((c.g.volh + threads - 1) / threads);
+  dirac_kernel<double, OP_HOP | OP_INV, 1, 1, 0><<<nb, threads, 0, st>>>(c.g, s, s, odd_scratch, c.ud, c.swd,
+                                                                          c.swd_inv, 0.0, 0.0, nullptr);
+  dirac_kernel<double, OP_SW | OP_HOPSUB, 0, 0, 1><<<nb, threads, 0, st>>>(c.g, s, odd_scratch, r, c.ud, c.swd,
+                                                                           c.swd_inv, mu, mu, nullptr);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

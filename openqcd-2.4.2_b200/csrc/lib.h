@@ -69,6 +69,8 @@ size_t spinor_bytes(const Ctx &c, int prec);   // prec 64 or 32
 template <typename R>
 int dirac_op(const Ctx &c, int op, R mu, const void *s, void *r, void *tmp, cudaStream_t st);
 
+int dwhat_dble_halfscratch(const Ctx &c, double mu, const void *s, void *r, void *odd_scratch, cudaStream_t st);
+
 // layout.cu
 int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt);
 int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st);   // q: reference AoS on device

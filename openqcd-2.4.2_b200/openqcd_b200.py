@@ -107,6 +107,7 @@ _SIGS = {
     "b200_dev_sap_gcr": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p]),
     "b200_dev_norm2": (C.c_double, [C.c_int, C.c_void_p]),
+    "b200_dev_Dwhat_dble_noalloc": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p]),
     "b200_dev_time_dirac": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 }
