@@ -200,6 +200,8 @@ int b200_dev_Dwhat_dble_noalloc(double mu, const void *s, void *r);
 /* Device time of n back-to-back operator applications, measured with CUDA
  * events on the library's stream; returns total milliseconds in *ms. */
 int b200_dev_time_dirac(int prec, int op, double mu, const void *s, void *r, int n, float *ms);
+/* Device time of n repetitions of ncy SAP cycles on FP32 device fields. */
+int b200_dev_time_sap(float mu, int isolv, int nmr, int ncy, void *psi, void *rho, int n, float *ms);
 /* Same, for Dw_dble through the drop-in entry point with host arrays in the
  * reference layout (host->device copy, layout conversion, operator,
  * conversion back, device->host copy), timed with events around each call. */

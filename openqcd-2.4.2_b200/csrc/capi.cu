@@ -433,6 +433,25 @@ int b200_dev_time_dirac(int prec, int op, double mu, const void *s, void *r, int
   return cudaGetLastError() == cudaSuccess ? 0 : fail("time_dirac: CUDA error");
 }
 
+int b200_dev_time_sap(float mu, int isolv, int nmr, int ncy, void *psi, void *rho, int n, float *ms) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return -1;
+  if (sap_prepare(c, c.stream)) return -1;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaStreamSynchronize(c.stream);
+  cudaEventRecord(e0, c.stream);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < ncy; k++) sap_cycle(c, mu, isolv, nmr, psi, rho, c.tmp32, c.stream);
+  cudaEventRecord(e1, c.stream);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("time_sap: CUDA error");
+}
+
 int b200_time_Dw_dble_host(double mu, spinor_dble *s, spinor_dble *r, int n, float *ms) {
   Ctx &c = ctx();
   if (check_fields(c)) return -1;

@@ -110,78 +110,120 @@ __device__ __forceinline__ void block_allreduce(double v[NC], double *red) {
   }
 }
 
+// The kernel runs as one loop over phases so that each heavy routine (the
+// odd-site hop, the even-site hop, the two SW products) has a single call
+// site; with separate set-up, MR and reconstruction code the kernel
+// overflowed the instruction cache.
+//   step 0         : V = W = A_o^-1 rho_o ;  S1 = rho_e - D_eo W ; S0 = 0
+//   step 1..nmr    : W = A_o^-1 D_oe S1 ;  s2 = (A_e + i mu g5) S1 - D_eo W ;
+//                    z = (s2,S1)/|s2|^2 ; S0 += z S1 ; S1 -= z s2
+//   step nmr+1     : phi_o = V - A_o^-1 D_oe S0 ; phi_e = S0 ; psi += phi ;
+//                    rho_e = S1 ; rho_o = -i mu g5 phi_o (0 with the eo flag)
 template <int NS>
 __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
   extern __shared__ float smem[];
   const Geom &g = a.g;
   const int ld = g.vbh;
-  float *S1 = smem, *W = smem + 24 * ld, *S0 = smem + 48 * ld;
+  float *S1 = smem, *W = smem + 24 * ld, *S0 = smem + 48 * ld, *V = smem + 72 * ld;
   __shared__ double red[3 * 32];
   __shared__ float zsh[2];
   __shared__ int stop;
   const int blk = block_of_colour(g, blockIdx.x, a.colour);
   const int ce = blk, co = g.nbl + blk;
   const int T = blockDim.x;
-
-  // v_o = A_o^-1 rho_o  -> W
-#pragma unroll
-  for (int k = 0; k < NS; k++) {
-    int s = threadIdx.x + k * T;
-    if (s < g.vbh) {
-      spinor<float> r = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
-      sm_store(W, ld, s, apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, r));
-    }
-  }
-  __syncthreads();
-  // s1_e = rho_e - D_eo v_o ; s0_e = 0
-#pragma unroll
-  for (int k = 0; k < NS; k++) {
-    int s = threadIdx.x + k * T;
-    if (s < g.vbh) {
-      spinor<float> r = Store<float>::load_spinor_rw(a.rho, ce, s, g.vbh);
-      ssub(r, block_hop(a, 0, blk, s, W, ld));
-      sm_store(S1, ld, s, r);
-      spinor<float> z;
-      szero(z);
-      sm_store(S0, ld, s, z);
-    }
-  }
+  const int nmr = a.nmr;
   if (threadIdx.x == 0) stop = 0;
-  __syncthreads();
 
-  // nmr minimal-residual steps on Dhat (blk_solv.c:1153-1188)
-  for (int imr = 0; imr < a.nmr; imr++) {
-    // w_o = A_o^-1 D_oe s1_e
+  for (int step = 0; step <= nmr + 1; step++) {
+    const bool last = step == nmr + 1;
+    // ---- odd sites
 #pragma unroll
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T;
       if (s < g.vbh) {
-        spinor<float> h = block_hop(a, 1, blk, s, S1, ld);
-        sm_store(W, ld, s, apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h));
+        spinor<float> h;
+        if (step == 0) h = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
+        else h = block_hop(a, 1, blk, s, last ? S0 : S1, ld);
+        spinor<float> t = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h);
+        if (step == 0) {
+          sm_store(V, ld, s, t);
+          sm_store(W, ld, s, t);
+        } else if (!last) {
+          sm_store(W, ld, s, t);
+        } else {
+          spinor<float> ph = sm_load(V, ld, s);
+          ssub(ph, t);
+          spinor<float> ps = Store<float>::load_spinor_rw(a.psi, co, s, g.vbh);
+          sadd(ps, ph);
+          Store<float>::store_spinor(a.psi, co, s, g.vbh, ps);
+          Store<float>::store_spinor(a.phi, co, s, g.vbh, ph);
+          spinor<float> ro;
+          if (a.eoflg) {
+            szero(ro);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+              const float m = c < 2 ? -a.mu : a.mu;   // rho_o = i m phi_o
+#pragma unroll
+              for (int j = 0; j < 3; j++) ro.c[c].c[j] = mk<float>(-m * ph.c[c].c[j].im, m * ph.c[c].c[j].re);
+            }
+          }
+          Store<float>::store_spinor(a.rho, co, s, g.vbh, ro);
+        }
       }
     }
     __syncthreads();
-    // s2_e = (A_e + i mu g5) s1_e - D_eo w_o ; r = |s2|^2, z = (s2, s1)
+    // ---- even sites
+    if (last) {
+#pragma unroll
+      for (int k = 0; k < NS; k++) {
+        int s = threadIdx.x + k * T;
+        if (s < g.vbh) {
+          spinor<float> s0 = sm_load(S0, ld, s);
+          spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ce, s, g.vbh);
+          sadd(ps, s0);
+          Store<float>::store_spinor(a.psi, ce, s, g.vbh, ps);
+          Store<float>::store_spinor(a.phi, ce, s, g.vbh, s0);
+          Store<float>::store_spinor(a.rho, ce, s, g.vbh, sm_load(S1, ld, s));
+        }
+      }
+      break;
+    }
     spinor<float> s2[NS];
     double v[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T;
       if (s < g.vbh) {
-        spinor<float> s1 = sm_load(S1, ld, s);
-        s2[k] = apply_sw_site<float>(a.sw, ce, s, g.vbh, a.mu, s1);
-        ssub(s2[k], block_hop(a, 0, blk, s, W, ld));
+        spinor<float> hw = block_hop(a, 0, blk, s, W, ld);
+        if (step == 0) {
+          spinor<float> r = Store<float>::load_spinor_rw(a.rho, ce, s, g.vbh);
+          ssub(r, hw);
+          sm_store(S1, ld, s, r);
+          spinor<float> z;
+          szero(z);
+          sm_store(S0, ld, s, z);
+        } else {
+          spinor<float> s1 = sm_load(S1, ld, s);
+          s2[k] = apply_sw_site<float>(a.sw, ce, s, g.vbh, a.mu, s1);
+          ssub(s2[k], hw);
 #pragma unroll
-        for (int c = 0; c < 4; c++)
+          for (int c = 0; c < 4; c++)
 #pragma unroll
-          for (int j = 0; j < 3; j++) {
-            const cpx<float> x2 = s2[k].c[c].c[j], x1 = s1.c[c].c[j];
-            v[0] += (double)x2.re * x2.re + (double)x2.im * x2.im;
-            v[1] += (double)x2.re * x1.re + (double)x2.im * x1.im;
-            v[2] += (double)x2.re * x1.im - (double)x2.im * x1.re;
-          }
+            for (int j = 0; j < 3; j++) {
+              const cpx<float> x2 = s2[k].c[c].c[j], x1 = s1.c[c].c[j];
+              v[0] += (double)x2.re * x2.re + (double)x2.im * x2.im;
+              v[1] += (double)x2.re * x1.re + (double)x2.im * x1.im;
+              v[2] += (double)x2.re * x1.im - (double)x2.im * x1.re;
+            }
+        }
       }
     }
+    if (step == 0) {
+      __syncthreads();
+      continue;
+    }
+    // MR coefficient (blk_solv.c:1153-1188): stop if |s2|^2 < 2 FLT_MIN
     block_allreduce<3>(v, red);
     if (threadIdx.x == 0) {
       float r = (float)v[0];
@@ -194,9 +236,11 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
       }
     }
     __syncthreads();
-    if (stop) break;
+    if (stop) {
+      step = nmr;   // go to the reconstruction step
+      continue;
+    }
     const float zr = zsh[0], zi = zsh[1];
-    // s0 += z s1 ; s1 -= z s2
 #pragma unroll
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T;
@@ -217,48 +261,6 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
       }
     }
     __syncthreads();
-  }
-
-  // odd part of the block solution: phi_o = A_o^-1 rho_o - A_o^-1 D_oe phi_e,
-  // then psi += phi, rho_o = -i mu g5 phi_o (or 0 with the eo flag), rho_e = s1_e
-#pragma unroll
-  for (int k = 0; k < NS; k++) {
-    int s = threadIdx.x + k * T;
-    if (s < g.vbh) {
-      spinor<float> h = block_hop(a, 1, blk, s, S0, ld);
-      spinor<float> t = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h);
-      spinor<float> r = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
-      spinor<float> ph = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, r);
-      ssub(ph, t);
-      spinor<float> ps = Store<float>::load_spinor_rw(a.psi, co, s, g.vbh);
-      sadd(ps, ph);
-      Store<float>::store_spinor(a.psi, co, s, g.vbh, ps);
-      Store<float>::store_spinor(a.phi, co, s, g.vbh, ph);
-      spinor<float> ro;
-      if (a.eoflg) {
-        szero(ro);
-      } else {
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-          const float m = c < 2 ? -a.mu : a.mu;   // r = i m phi
-#pragma unroll
-          for (int j = 0; j < 3; j++) ro.c[c].c[j] = mk<float>(-m * ph.c[c].c[j].im, m * ph.c[c].c[j].re);
-        }
-      }
-      Store<float>::store_spinor(a.rho, co, s, g.vbh, ro);
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < NS; k++) {
-    int s = threadIdx.x + k * T;
-    if (s < g.vbh) {
-      spinor<float> s0 = sm_load(S0, ld, s);
-      spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ce, s, g.vbh);
-      sadd(ps, s0);
-      Store<float>::store_spinor(a.psi, ce, s, g.vbh, ps);
-      Store<float>::store_spinor(a.phi, ce, s, g.vbh, s0);
-      Store<float>::store_spinor(a.rho, ce, s, g.vbh, sm_load(S1, ld, s));
-    }
   }
 }
 
@@ -423,7 +425,7 @@ int sap_prepare(Ctx &c, cudaStream_t st) {
   int ns;
   int t = pick_threads(c.g.vbh, ns);
   if (!t) return fail("sap: block volume too large (at most 1536 sites)");
-  size_t eo = (size_t)72 * c.g.vbh * sizeof(float), pl = (size_t)96 * c.g.vbh * sizeof(float);
+  size_t eo = (size_t)96 * c.g.vbh * sizeof(float), pl = (size_t)96 * c.g.vbh * sizeof(float);
   if (eo > 200 * 1024 || pl > 200 * 1024) {
     if (pl > 200 * 1024 && c.isolv == 0) return fail("sap: block too large for the plain MR solver");
   }
@@ -452,7 +454,7 @@ int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *
   a.u = c.u32;
   a.sw = c.sw32;
   a.swinv = c.sw32_inv;
-  size_t shm = (size_t)(isolv ? 72 : 96) * c.g.vbh * sizeof(float);
+  size_t shm = (size_t)96 * c.g.vbh * sizeof(float);
   if (shm > 200 * 1024) return fail("sap: block too large for shared memory");
   int nbh = c.g.nbl / 2;
   size_t nb_sites = (size_t)nbh * c.g.vb;

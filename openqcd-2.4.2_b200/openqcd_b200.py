@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libopenqcd_b200.so")
+LIB_PATH = os.environ.get("B200_LIB", os.path.join(HERE, "libopenqcd_b200.so"))
 
 _lib = None
 
@@ -109,6 +109,8 @@ _SIGS = {
     "b200_dev_norm2": (C.c_double, [C.c_int, C.c_void_p]),
     "b200_dev_Dwhat_dble_noalloc": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p]),
     "b200_dev_time_dirac": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "b200_dev_time_sap": (C.c_int, [C.c_float, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                    C.c_void_p]),
     "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 }
 
@@ -355,6 +357,12 @@ class HostArray:
 def time_dirac(prec, op, mu, s, r, n):
     ms = C.c_float(0.0)
     check(lib().b200_dev_time_dirac(prec, DIRAC_OPS[op], mu, s.ptr, r.ptr, n, C.byref(ms)))
+    return ms.value
+
+
+def time_sap(mu, isolv, nmr, ncy, psi, rho, n):
+    ms = C.c_float(0.0)
+    check(lib().b200_dev_time_sap(mu, isolv, nmr, ncy, psi.ptr, rho.ptr, n, C.byref(ms)))
     return ms.value
 
 
