@@ -112,6 +112,9 @@ void *b200_dev_alloc(size_t bytes);
 int b200_memcpy(void *dst, const void *src, size_t bytes);
 
 const char *b200_last_error(void);
+/* Forget the recorded message (calls of void prototypes are checked by
+ * clearing it before and reading it after). */
+void b200_clear_error(void);
 void b200_set_fatal(int on);
 int b200_sync(void);
 int b200_volume(void);
@@ -170,6 +173,35 @@ int b200_set_nthread(int n);
 double fgcr(int vol, void (*Dop)(spinor_dble *s, spinor_dble *r), void (*Mop)(int k, spinor *rho, spinor *phi, spinor *chi),
             spinor **ws, spinor_dble **wsd, int nkv, int nmx, int istop, double res, spinor_dble *eta,
             spinor_dble *psi, int *status);
+
+/* ------------------------------------------- deflation (dfl.h, little.h) */
+/* Parameters of set_dfl_parms (modules/flags/dfl_parms.c:209; the DFL block
+ * size must equal the geometry block size), set_dfl_pro_parms (:286) and
+ * set_dfl_gen_parms (:360). */
+int b200_set_dfl_parms(const int bs[4], int Ns);
+int b200_set_dfl_pro_parms(int nkv, int nmx, double res, int nmx_gcr, double res_gcr);
+int b200_set_dfl_gen_parms(double kappa, double mu, int ninv, int nmr, int ncy);
+/* Ns * (number of DFL blocks): the length of a little vector. */
+int b200_dfl_nv(void);
+/* Basis vector l of every block as one global FP32 field, reference layout. */
+int b200_dfl_set_basis(int l, const spinor *field);
+int b200_dfl_get_basis(int l, spinor *field);
+/* dfl_modes.c:423 */ void dfl_modes(int *ifail, int *status);
+int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status);
+/* dfl_subspace.c:171 */ void dfl_subspace(spinor **mds);
+/* dfl_subspace.c:83  */ void dfl_s2vd(spinor *s, complex_dble *vd);
+/* dfl_subspace.c:126 */ void dfl_vd2s(complex_dble *vd, spinor *s);
+/* Aw_ops.c:186 */ void set_Aw(double mu);
+/* Aw_ops.c:223 */ int set_Awhat(double mu);
+/* Aw_dble.c:122 */ void Aw_dble(complex_dble *v, complex_dble *w);
+/* Aw_dble.c:361 */ void Awhat_dble(complex_dble *v, complex_dble *w);
+/* ltl_gcr.c:155 */ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int *status);
+/* dfl_sap_gcr.c:353 */ double dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta,
+                                           spinor_dble *psi, int *ifail, int *status);
+/* dfl_sap_gcr.c:383 */ double dfl_sap_gcr2(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta,
+                                            spinor_dble *psi, int *ifail, int *status);
+double b200_dev_dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                            int *ifail, int *status);
 
 /* ------------------------------------ device-resident fields (own layout) */
 /* prec = 64 (spinor_dble) or 32 (spinor).  Operator codes for

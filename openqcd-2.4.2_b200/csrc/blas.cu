@@ -234,6 +234,23 @@ void flat_diff(Ctx &c, int prec, const void *x, void *y, size_t nsite) {
   else k_fdiff<float><<<g256(n), 256, 0, c.stream>>>((const float *)x, (float *)y, n);
 }
 
+// FP64 complex arrays of n entries (little vectors)
+int flat_cdot(Ctx &c, const double2 *x, const double2 *y, size_t n, double *res_dd, double *scratch, double *out_dev) {
+  int nb = nblocks(n);
+  k_fdot<double, 0><<<nb, FT, 0, c.stream>>>((const double *)x, (const double *)y, n, scratch);
+  k_fsum_dd<2><<<1, 32, 0, c.stream>>>(scratch, nb, out_dev);
+  cudaMemcpyAsync(c.h_red, out_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess) return fail("reduction: CUDA error");
+  for (int k = 0; k < 4; k++) res_dd[k] = c.h_red[k];
+  return 0;
+}
+void flat_caxpy(Ctx &c, double2 *y, const double2 *x, size_t n, double ar, double ai) {
+  k_faxpy<double><<<g256(n), 256, 0, c.stream>>>((double *)y, (const double *)x, n, ar, ai);
+}
+void flat_cscale(Ctx &c, double2 *y, size_t n, double a) {
+  k_fscale<double><<<g256(2 * n), 256, 0, c.stream>>>((double *)y, 2 * n, a);
+}
+
 int flat_scratch(Ctx &c, double **scratch, double **out) {
   if (!c.red) {
     if (cudaMalloc(&c.red, (size_t)FB * 4 * sizeof(double)) != cudaSuccess ||

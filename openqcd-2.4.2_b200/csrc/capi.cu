@@ -116,6 +116,7 @@ using qcd::apply_swinv_ref_layout;
 extern "C" {
 
 const char *b200_last_error(void) { return g_err.c_str(); }
+void b200_clear_error(void) { g_err.clear(); }
 
 void *b200_host_alloc(size_t bytes) {
   void *p = nullptr;
@@ -158,6 +159,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   c.ud = nullptr; c.u32 = nullptr; c.swd = c.swd_inv = nullptr; c.sw32 = c.sw32_inv = nullptr;
   c.tmp64 = c.tmp32 = c.stage = nullptr; c.stage_bytes = 0;
   c.have_ud = c.have_sw = false;
+  qcd::dfl_release(c);
   c.ready = false;
   if (geometry_init(c, L, bs, ipt)) return -1;
   c.ready = true;

@@ -1,0 +1,263 @@
+// C entry points of the deflation part: the reference's names from
+// include/dfl.h and include/little.h, plus the b200_* parameter setters and
+// device-layout variants.  Little vectors (Ns complex_dble per DFL block, in
+// the reference's block order) and spinor fields (reference layout) may be
+// in host or device memory.
+#include "lib.h"
+#include "../../include/openqcd_b200.h"
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+namespace qcd {
+
+static int dfl_ready(Ctx &c) {
+  if (!c.ready) return fail("geometry not set (call b200_geometry first)");
+  if (!c.dfl.ready) return fail("deflation parameters are not set (b200_set_dfl_parms)");
+  return 0;
+}
+
+static int fields_ready(Ctx &c) {
+  if (!c.have_ud || !c.have_sw) return fail("gauge or SW field missing on the device");
+  if (!c.tmp32 && cudaMalloc(&c.tmp32, spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory");
+  if (!c.tmp64 && cudaMalloc(&c.tmp64, spinor_bytes(c, 64)) != cudaSuccess) return fail("out of device memory");
+  return 0;
+}
+
+// little-vector staging: two device buffers of nv complex doubles
+static double2 *lbuf(Ctx &c, int k) {
+  DflState &d = c.dfl;
+  while ((int)d.lvd.size() < 4) {
+    double2 *p = nullptr;
+    if (cudaMalloc(&p, (size_t)d.nv * sizeof(double2)) != cudaSuccess) { fail("out of device memory"); return nullptr; }
+    d.lvd.push_back(p);
+  }
+  return d.lvd[k];
+}
+
+static void *spinor_stage(Ctx &c, int prec, int k) {
+  std::vector<void *> &v = prec == 64 ? c.ws64 : c.ws32;
+  while ((int)v.size() <= k) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, spinor_bytes(c, prec)) != cudaSuccess) { fail("out of device memory"); return nullptr; }
+    v.push_back(p);
+  }
+  return v[k];
+}
+
+static int stage_bytes_ok(Ctx &c, size_t n) {
+  if (c.stage_bytes >= n) return 0;
+  cudaFree(c.stage);
+  c.stage = nullptr;
+  c.stage_bytes = 0;
+  if (cudaMalloc(&c.stage, n) != cudaSuccess) return fail("out of device memory (staging)");
+  c.stage_bytes = n;
+  return 0;
+}
+
+// reference-layout FP32 field (host or device) -> device-layout field
+static int ref32_in(Ctx &c, const void *q, void *dev) {
+  size_t nb = spinor_bytes(c, 32);
+  if (stage_bytes_ok(c, nb)) return -1;
+  cudaMemcpyAsync(c.stage, q, nb, cudaMemcpyDefault, c.stream);
+  return spinor_from_ref(c, 32, c.stage, dev, c.stream);
+}
+
+static int ref32_out(Ctx &c, const void *dev, void *q) {
+  size_t nb = spinor_bytes(c, 32);
+  if (stage_bytes_ok(c, nb)) return -1;
+  if (spinor_to_ref(c, 32, dev, c.stage, c.stream)) return -1;
+  cudaMemcpyAsync(q, c.stage, nb, cudaMemcpyDefault, c.stream);
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("CUDA error");
+}
+
+}  // namespace qcd
+
+using qcd::Ctx;
+using qcd::ctx;
+using qcd::fail;
+
+extern "C" {
+
+int b200_set_dfl_parms(const int bs[4], int Ns) {
+  Ctx &c = ctx();
+  if (!c.ready) return fail("geometry not set (call b200_geometry first)");
+  return qcd::dfl_set_parms(c, bs, Ns);
+}
+
+int b200_set_dfl_pro_parms(int nkv, int nmx, double res, int nmx_gcr, double res_gcr) {
+  // modules/flags/dfl_parms.c:300-302
+  if (nkv < 2 || nmx < 1 || res <= DBL_EPSILON || nmx_gcr < 2 || res_gcr <= FLT_EPSILON)
+    return fail("set_dfl_pro_parms: improper parameter values");
+  qcd::DflState &d = ctx().dfl;
+  d.nkv = nkv; d.nmx = nmx; d.res = res; d.nmx_gcr = nmx_gcr; d.res_gcr = res_gcr;
+  return 0;
+}
+
+int b200_set_dfl_gen_parms(double kappa, double mu, int ninv, int nmr, int ncy) {
+  // modules/flags/dfl_parms.c:379-380
+  if (ninv < 4 || nmr < 1 || ncy < 1 || kappa < 0.0) return fail("set_dfl_gen_parms: parameters are out of range");
+  qcd::DflState &d = ctx().dfl;
+  d.gen_kappa = kappa; d.gen_mu = mu; d.gen_ninv = ninv; d.gen_nmr = nmr; d.gen_ncy = ncy;
+  d.gen_set = true;
+  return 0;
+}
+
+int b200_dfl_nv(void) { return ctx().dfl.ready ? ctx().dfl.nv : 0; }
+
+// Load basis vector l of every block from a global field in the reference
+// layout (host or device).  The blocks' vectors are used as given.
+int b200_dfl_set_basis(int l, const spinor *field) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return -1;
+  if (l < 0 || l >= c.dfl.Ns) return fail("dfl_set_basis: index out of range");
+  if (qcd::ref32_in(c, field, c.dfl.basis[l])) return -1;
+  c.dfl.have_basis = true;
+  c.dfl.aw_valid = c.dfl.awhat_valid = false;
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("CUDA error");
+}
+
+int b200_dfl_get_basis(int l, spinor *field) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return -1;
+  if (l < 0 || l >= c.dfl.Ns) return fail("dfl_get_basis: index out of range");
+  return qcd::ref32_out(c, c.dfl.basis[l], field);
+}
+
+// dfl_subspace.c:171: the basis from Ns global fields (reference layout)
+void dfl_subspace(spinor **mds) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return;
+  std::vector<void *> modes;
+  for (int l = 0; l < c.dfl.Ns; l++) {
+    void *f = qcd::spinor_stage(c, 32, l);
+    if (!f || qcd::ref32_in(c, mds[l], f)) return;
+    modes.push_back(f);
+  }
+  qcd::dfl_subspace_dev(c, modes, c.stream);
+}
+
+void dfl_s2vd(spinor *s, complex_dble *vd) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || !c.dfl.have_basis) { if (c.dfl.ready) fail("dfl_s2vd: no deflation subspace"); return; }
+  void *f = qcd::spinor_stage(c, 32, 0);
+  double2 *v = qcd::lbuf(c, 0);
+  if (!f || !v || qcd::ref32_in(c, s, f)) return;
+  qcd::dfl_restrict(c, 32, f, v, c.stream);
+  cudaMemcpyAsync(vd, v, (size_t)c.dfl.nv * sizeof(double2), cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+void dfl_vd2s(complex_dble *vd, spinor *s) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || !c.dfl.have_basis) { if (c.dfl.ready) fail("dfl_vd2s: no deflation subspace"); return; }
+  void *f = qcd::spinor_stage(c, 32, 0);
+  double2 *v = qcd::lbuf(c, 0);
+  if (!f || !v) return;
+  cudaMemcpyAsync(v, vd, (size_t)c.dfl.nv * sizeof(double2), cudaMemcpyDefault, c.stream);
+  qcd::dfl_prolong(c, v, f, c.stream);
+  qcd::ref32_out(c, f, s);
+}
+
+void set_Aw(double mu) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return;
+  qcd::dfl_set_Aw(c, mu, c.stream);
+}
+
+int set_Awhat(double mu) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1;
+  return qcd::dfl_set_Awhat(c, mu, c.stream);
+}
+
+static void little_apply(int which, complex_dble *v, complex_dble *w) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return;
+  qcd::DflState &d = c.dfl;
+  if (!d.aw_valid || (which == 1 && !d.awhat_valid)) { fail("Aw: the little operator is not set (set_Aw / set_Awhat)"); return; }
+  double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1), *t = qcd::lbuf(c, 2);
+  if (!a || !b || !t) return;
+  size_t nb = (size_t)d.nv * sizeof(double2);
+  cudaMemcpyAsync(a, v, nb, cudaMemcpyDefault, c.stream);
+  cudaMemcpyAsync(b, w, nb, cudaMemcpyDefault, c.stream);
+  if (which == 0) qcd::dfl_Aw(c, a, b, c.stream);
+  else qcd::dfl_Awhat(c, a, b, t, c.stream);
+  cudaMemcpyAsync(w, b, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+void Aw_dble(complex_dble *v, complex_dble *w) { little_apply(0, v, w); }
+void Awhat_dble(complex_dble *v, complex_dble *w) { little_apply(1, v, w); }
+
+double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1.0;
+  qcd::DflState &d = c.dfl;
+  double2 *a = qcd::lbuf(c, 2), *b = qcd::lbuf(c, 3);
+  if (!a || !b) return -1.0;
+  size_t nb = (size_t)d.nv * sizeof(double2);
+  cudaMemcpyAsync(a, eta, nb, cudaMemcpyDefault, c.stream);
+  double rho = qcd::dfl_ltl_gcr(c, mu, a, b, ifail, status, c.stream);
+  status[1] = 0;
+  cudaMemcpyAsync(psi, b, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+  return rho;
+}
+
+int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1;
+  return qcd::dfl_modes_dev(c, seed, ifail, status);
+}
+
+// dfl_modes.c:423 with the library's generator seeded by 1
+void dfl_modes(int *ifail, int *status) {
+  if (b200_dev_dfl_modes(1ull, ifail, status) < 0 && ifail[0] == 0) ifail[0] = -2;
+}
+
+double b200_dev_dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                            int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1.0;
+  return qcd::dfl_sap_gcr_dev(c, nkv, nmx, istop, res, mu, eta, psi, ifail, status);
+}
+
+// dfl_sap_gcr.c:353 on reference-layout FP64 fields (host or device)
+double dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi,
+                   int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1.0;
+  size_t nb = qcd::spinor_bytes(c, 64);
+  void *fe = nullptr, *fp = nullptr;
+  if (cudaMalloc(&fe, nb) != cudaSuccess || cudaMalloc(&fp, nb) != cudaSuccess) { fail("out of device memory"); return -1.0; }
+  if (qcd::stage_bytes_ok(c, nb)) return -1.0;
+  cudaMemcpyAsync(c.stage, eta, nb, cudaMemcpyDefault, c.stream);
+  qcd::spinor_from_ref(c, 64, c.stage, fe, c.stream);
+  double rho = qcd::dfl_sap_gcr_dev(c, nkv, nmx, istop, res, mu, fe, fp, ifail, status);
+  qcd::spinor_to_ref(c, 64, fp, c.stage, c.stream);
+  cudaMemcpyAsync(psi, c.stage, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+  cudaFree(fe);
+  cudaFree(fp);
+  return rho;
+}
+
+// dfl_sap_gcr.c:383: retry once with a regenerated subspace if the first
+// solve fails with ifail -1 or -2
+double dfl_sap_gcr2(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi,
+                    int *ifail, int *status) {
+  ifail[1] = 0;
+  for (int l = 0; l < 6; l++) status[l] = 0;
+  double rho = dfl_sap_gcr(nkv, nmx, istop, res, mu, eta, psi, ifail, status);
+  if (ifail[0] == -1 || ifail[0] == -2) {
+    int st2[2] = {0, 0};
+    b200_dev_dfl_modes(2ull, ifail + 1, st2);
+    status[4] = st2[0];
+    status[5] = st2[1];
+    if (ifail[1] == 0) rho = dfl_sap_gcr(nkv, nmx, istop, res, mu, eta, psi, ifail + 1, status + 3);
+  }
+  return rho;
+}
+
+}  // extern "C"

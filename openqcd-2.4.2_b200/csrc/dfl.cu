@@ -1,0 +1,875 @@
+// Local deflation on the device: block basis, restriction/prolongation, the
+// little Dirac operator, its even-odd preconditioned form and solver, the
+// subspace generation, and the deflated SAP+GCR solver.
+//
+// Reference: modules/dfl/dfl_subspace.c (dfl_s2vd :83, dfl_vd2s :126,
+// dfl_subspace :171), modules/little/Aw_ops.c (set_Aw :186, set_Awhat :223),
+// Aw_dble.c (Aw_dble :122, Awhat_dble :361), modules/dfl/ltl_gcr.c (:155),
+// modules/dfl/dfl_modes.c (:423), modules/dfl/dfl_sap_gcr.c (:212-381).
+//
+// The DFL blocks are the tiles of the device layout (the same block size as
+// the SAP blocks), so the sites of one DFL block are two contiguous chunks.
+// Little vectors hold Ns complex numbers per block in the reference's block
+// order: the nb/2 blocks of colour 0 first, each colour in lexicographic
+// order of the block coordinates (modules/block/blk_grid.c:20-32).  Little
+// matrices are stored column-major (entry (k,l) at [l*Ns + k]) so that the
+// threads of a block, one per row k, read consecutive words.
+#include "lib.h"
+#include <cfloat>
+#include <cmath>
+#include <functional>
+
+namespace qcd {
+
+// ------------------------------------------------------------- block maps
+static int lex_of_vd(const Geom &g, const std::vector<int> &bco, int n) {
+  const int nbh = g.nbl / 2;
+  const int colour = n >= nbh, h = n - colour * nbh;
+  const int q = 2 * h;
+  int s = 0;
+  for (int mu = 0; mu < 4; mu++) s += (bco[q] >> (8 * mu)) & 255;
+  return q + ((s & 1) != colour);
+}
+
+static int dfl_alloc(Ctx &c) {
+  DflState &d = c.dfl;
+  const int Ns = d.Ns, nb = c.g.nbl;
+  d.nb = nb;
+  d.nv = Ns * nb;
+  // block tables
+  std::vector<int> bco(nb), v2l(nb), l2v(nb), nbr(8 * nb);
+  cudaMemcpy(bco.data(), c.d_bcoord, nb * sizeof(int), cudaMemcpyDeviceToHost);
+  for (int n = 0; n < nb; n++) {
+    v2l[n] = lex_of_vd(c.g, bco, n);
+    l2v[v2l[n]] = n;
+  }
+  for (int n = 0; n < nb; n++) {
+    int b = v2l[n], x[4];
+    for (int mu = 0; mu < 4; mu++) x[mu] = (bco[b] >> (8 * mu)) & 255;
+    for (int ifc = 0; ifc < 8; ifc++) {
+      int mu = ifc >> 1, dir = (ifc & 1) ? 1 : -1;
+      int y[4] = {x[0], x[1], x[2], x[3]};
+      y[mu] = (y[mu] + dir + c.g.nb[mu]) % c.g.nb[mu];
+      int lb = ((y[0] * c.g.nb[1] + y[1]) * c.g.nb[2] + y[2]) * c.g.nb[3] + y[3];
+      nbr[8 * n + ifc] = l2v[lb];
+    }
+  }
+  auto up = [](int *&p, const std::vector<int> &v) {
+    cudaFree(p);
+    cudaMalloc(&p, v.size() * sizeof(int));
+    cudaMemcpy(p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice);
+  };
+  up(d.vd2lex, v2l);
+  up(d.nbr, nbr);
+  // basis and matrices
+  while ((int)d.basis.size() < Ns) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory (deflation basis)");
+    cudaMemset(p, 0, spinor_bytes(c, 32));
+    d.basis.push_back(p);
+  }
+  cudaFree(d.d_basis);
+  cudaMalloc(&d.d_basis, Ns * sizeof(void *));
+  cudaMemcpy(d.d_basis, d.basis.data(), Ns * sizeof(void *), cudaMemcpyHostToDevice);
+  size_t m = (size_t)nb * Ns * Ns * sizeof(double2);
+  double2 **mats[] = {&d.Ablk, &d.Ainv, &d.Ahop, &d.Mhop};
+  size_t sz[] = {m, m, 8 * m, 8 * m};
+  for (int i = 0; i < 4; i++) {
+    cudaFree(*mats[i]);
+    if (cudaMalloc(mats[i], sz[i]) != cudaSuccess) return fail("out of device memory (little operator)");
+  }
+  d.aw_valid = d.awhat_valid = false;
+  d.have_basis = false;
+  d.ready = true;
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("deflation: CUDA error in set-up");
+}
+
+// ------------------------------------------------ restriction / prolongation
+// vd[n*Ns + l] = (basis_l, s) on block n; FP32 products accumulated in double
+// and rounded to float, as spinor_prod returns them (dfl_subspace.c:83-123).
+template <typename R>
+__global__ void k_dfl_restrict(Geom g, const int *__restrict__ vd2lex, const float4 *const *__restrict__ basis,
+                               int Ns, const void *__restrict__ s, double2 *vd, int round_float) {
+  const int n = blockIdx.x, blk = __ldg(vd2lex + n);
+  __shared__ double red[2][32];
+  const int nsite = 2 * g.vbh;
+  for (int l = 0; l < Ns; l++) {
+    double re = 0.0, im = 0.0;
+    const float4 *bl = basis[l];
+    for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+      const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+      spinor<float> b = Store<float>::load_spinor(bl, chunk, si, g.vbh);
+      spinor<R> x = Store<R>::load_spinor(s, chunk, si, g.vbh);
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const double br = b.c[a].c[k].re, bi = b.c[a].c[k].im, xr = x.c[a].c[k].re, xi = x.c[a].c[k].im;
+          re += br * xr + bi * xi;
+          im += br * xi - bi * xr;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_down_sync(0xffffffffu, re, o);
+      im += __shfl_down_sync(0xffffffffu, im, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = re; red[1][threadIdx.x >> 5] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += red[0][w]; b += red[1][w]; }
+      if (round_float) { a = (double)(float)a; b = (double)(float)b; }
+      vd[(size_t)n * Ns + l] = make_double2(a, b);
+    }
+    __syncthreads();
+  }
+}
+
+// s = sum_l vd[n,l] basis_l on every block n, with float coefficients and
+// float accumulation (dfl_vd2s, dfl_subspace.c:126-167).
+__global__ void k_dfl_prolong(Geom g, const int *__restrict__ vd2lex, const float4 *const *__restrict__ basis,
+                              int Ns, const double2 *__restrict__ vd, float4 *s) {
+  const int n = blockIdx.x, blk = __ldg(vd2lex + n);
+  const int nsite = 2 * g.vbh;
+  for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+    const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+    spinor<float> acc;
+    szero(acc);
+    for (int l = 0; l < Ns; l++) {
+      const double2 z = vd[(size_t)n * Ns + l];
+      const float zr = (float)z.x, zi = (float)z.y;
+      spinor<float> b = Store<float>::load_spinor(basis[l], chunk, si, g.vbh);
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          acc.c[a].c[k].re += zr * b.c[a].c[k].re - zi * b.c[a].c[k].im;
+          acc.c[a].c[k].im += zr * b.c[a].c[k].im + zi * b.c[a].c[k].re;
+        }
+    }
+    Store<float>::store_spinor(s, chunk, si, g.vbh, acc);
+  }
+}
+
+// ------------------------------------------------------ block Gram-Schmidt
+// basis_l(block) = orthonormalised mode_l(block) against basis_0..l-1 of the
+// same block, in double precision (dfl_subspace.c:171-240).  One CTA per
+// block; the current vector lives in shared memory.
+__global__ void k_dfl_gs(Geom g, const int *__restrict__ vd2lex, float4 *const *basis,
+                         const float4 *const *__restrict__ modes, int Ns, int *fail) {
+  extern __shared__ double v[];   // [24][2*vbh]
+  const int n = blockIdx.x, blk = __ldg(vd2lex + n);
+  const int nsite = 2 * g.vbh;
+  __shared__ double red[2][32];
+  __shared__ double zsh[2];
+  for (int l = 0; l < Ns; l++) {
+    for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+      const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+      spinor<float> m = Store<float>::load_spinor(modes[l], chunk, si, g.vbh);
+#pragma unroll
+      for (int k = 0; k < 12; k++) {
+        v[(2 * k) * nsite + t] = m.c[k / 3].c[k % 3].re;
+        v[(2 * k + 1) * nsite + t] = m.c[k / 3].c[k % 3].im;
+      }
+    }
+    __syncthreads();
+    for (int j = 0; j <= l; j++) {
+      // j < l: z = (basis_j, v), v -= z basis_j ; j == l: normalise
+      double re = 0.0, im = 0.0;
+      for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+        const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+        if (j < l) {
+          spinor<float> b = Store<float>::load_spinor(basis[j], chunk, si, g.vbh);
+#pragma unroll
+          for (int k = 0; k < 12; k++) {
+            const double br = b.c[k / 3].c[k % 3].re, bi = b.c[k / 3].c[k % 3].im;
+            const double xr = v[(2 * k) * nsite + t], xi = v[(2 * k + 1) * nsite + t];
+            re += br * xr + bi * xi;
+            im += br * xi - bi * xr;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 24; k++) re += v[k * nsite + t] * v[k * nsite + t];
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_down_sync(0xffffffffu, re, o);
+        im += __shfl_down_sync(0xffffffffu, im, o);
+      }
+      if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = re; red[1][threadIdx.x >> 5] = im; }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += red[0][w]; b += red[1][w]; }
+        zsh[0] = a;
+        zsh[1] = b;
+      }
+      __syncthreads();
+      if (j < l) {
+        const double zr = zsh[0], zi = zsh[1];
+        for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+          const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+          spinor<float> b = Store<float>::load_spinor(basis[j], chunk, si, g.vbh);
+#pragma unroll
+          for (int k = 0; k < 12; k++) {
+            const double br = b.c[k / 3].c[k % 3].re, bi = b.c[k / 3].c[k % 3].im;
+            v[(2 * k) * nsite + t] -= zr * br - zi * bi;
+            v[(2 * k + 1) * nsite + t] -= zr * bi + zi * br;
+          }
+        }
+      } else {
+        const double nrm = sqrt(zsh[0]);
+        if (nrm == 0.0 && threadIdx.x == 0) atomicOr(fail, 1);
+        const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+        for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+          const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+          spinor<float> o;
+#pragma unroll
+          for (int k = 0; k < 12; k++)
+            o.c[k / 3].c[k % 3] = mk<float>((float)(v[(2 * k) * nsite + t] * inv), (float)(v[(2 * k + 1) * nsite + t] * inv));
+          Store<float>::store_spinor(basis[l], chunk, si, g.vbh, o);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ------------------------------------------------ little operator set-up
+// t = D_blk w (in-block hops only, Dirichlet exterior) + SW term with twisted
+// mass, or t = the hop of w across face ifc only; FP64 output from an FP32
+// input field.
+__global__ void k_dfl_dapply(Geom g, const float4 *__restrict__ w, double2 *t, const double2 *__restrict__ ud,
+                             const double2 *__restrict__ swd, double mu_e, double mu_o, int ifc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.vol) return;
+  const int chunk = i / g.vbh, si = i - chunk * g.vbh;
+  const int p = chunk >= g.nbl, blk = chunk - p * g.nbl;
+  Site x;
+  site_decode(g, p, blk, si, x);
+  spinor<double> acc, h;
+  szero(acc);
+  szero(h);
+  if (ifc < 0) {
+    spinor<float> in = Store<float>::load_spinor(w, chunk, si, g.vbh);
+    spinor<double> ind;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) ind.c[a].c[k] = mk<double>(in.c[a].c[k].re, in.c[a].c[k].im);
+    acc = apply_sw_site<double>(swd, chunk, si, g.vbh, p ? mu_o : mu_e, ind);
+  }
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+#pragma unroll
+    for (int dd = 0; dd < 2; dd++) {
+      const int dir = dd ? 1 : -1;
+      const bool cross = crosses_block(g, x, mu, dir);
+      const bool take = (ifc < 0) ? !cross : (cross && ifc == 2 * mu + dd);
+      if (!take) continue;
+      int c2, s2;
+      site_nbr(g, x, mu, dir, c2, s2);
+      spinor<float> nf = Store<float>::load_spinor(w, c2, s2, g.vbh);
+      spinor<double> nd;
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) nd.c[a].c[k] = mk<double>(nf.c[a].c[k].re, nf.c[a].c[k].im);
+      if (dir > 0) hop_fwd<double>(mu, Store<double>::load_link(ud, chunk, mu, si, g.vbh), nd, h);
+      else hop_bwd<double>(mu, Store<double>::load_link(ud, c2, mu, s2, g.vbh), nd, h);
+    }
+  }
+  sscale<double>(h, -0.5);
+  sadd(acc, h);
+  Store<double>::store_spinor(t, chunk, si, g.vbh, acc);
+}
+
+// M[n][col l] (entries k) = (basis_k, t) on block n, FP64 field t
+__global__ void k_dfl_project(Geom g, const int *__restrict__ vd2lex, const float4 *const *__restrict__ basis,
+                              int Ns, const double2 *__restrict__ t, double2 *M, size_t mstride, int l) {
+  const int n = blockIdx.x, blk = __ldg(vd2lex + n);
+  __shared__ double red[2][32];
+  const int nsite = 2 * g.vbh;
+  for (int k = 0; k < Ns; k++) {
+    double re = 0.0, im = 0.0;
+    for (int tt = threadIdx.x; tt < nsite; tt += blockDim.x) {
+      const int p = tt >= g.vbh, si = tt - p * g.vbh, chunk = p * g.nbl + blk;
+      spinor<float> b = Store<float>::load_spinor(basis[k], chunk, si, g.vbh);
+      spinor<double> x = Store<double>::load_spinor(t, chunk, si, g.vbh);
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const double br = b.c[a].c[c].re, bi = b.c[a].c[c].im, xr = x.c[a].c[c].re, xi = x.c[a].c[c].im;
+          re += br * xr + bi * xi;
+          im += br * xi - bi * xr;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_down_sync(0xffffffffu, re, o);
+      im += __shfl_down_sync(0xffffffffu, im, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = re; red[1][threadIdx.x >> 5] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double a = 0.0, b = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += red[0][w]; b += red[1][w]; }
+      M[n * mstride + (size_t)l * Ns + k] = make_double2(a, b);
+    }
+    __syncthreads();
+  }
+}
+
+// Batched inverse of Ns x Ns complex matrices (column-major) by Gauss-Jordan
+// elimination with partial pivoting, one CTA per matrix; flags matrices whose
+// Frobenius condition number exceeds 1e6 (modules/little/Aw_ops.c:35-40).
+__global__ void k_cinv(int Ns, const double2 *__restrict__ A, double2 *B, int *fail) {
+  extern __shared__ double2 sm[];   // a[Ns*Ns], b[Ns*Ns] row-major
+  double2 *a = sm, *b = sm + Ns * Ns;
+  __shared__ int piv;
+  __shared__ double fn[2];
+  __shared__ double2 fcol[64];
+  const size_t off = (size_t)blockIdx.x * Ns * Ns;
+  for (int e = threadIdx.x; e < Ns * Ns; e += blockDim.x) {
+    const int r = e / Ns, cc = e % Ns;
+    a[e] = A[off + (size_t)cc * Ns + r];
+    b[e] = make_double2(r == cc ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int e = 0; e < Ns * Ns; e++) s += a[e].x * a[e].x + a[e].y * a[e].y;
+    fn[0] = s;
+  }
+  for (int c = 0; c < Ns; c++) {
+    if (threadIdx.x == 0) {
+      int p = c;
+      double best = -1.0;
+      for (int r = c; r < Ns; r++) {
+        double v = a[r * Ns + c].x * a[r * Ns + c].x + a[r * Ns + c].y * a[r * Ns + c].y;
+        if (v > best) { best = v; p = r; }
+      }
+      piv = p;
+      if (best == 0.0) atomicOr(fail, 1);
+    }
+    __syncthreads();
+    const int p = piv;
+    if (p != c)
+      for (int j = threadIdx.x; j < Ns; j += blockDim.x) {
+        double2 t = a[c * Ns + j]; a[c * Ns + j] = a[p * Ns + j]; a[p * Ns + j] = t;
+        t = b[c * Ns + j]; b[c * Ns + j] = b[p * Ns + j]; b[p * Ns + j] = t;
+      }
+    __syncthreads();
+    double2 pv = a[c * Ns + c];
+    double d = pv.x * pv.x + pv.y * pv.y;
+    if (d == 0.0) d = 1.0;
+    const double qr = pv.x / d, qi = -pv.y / d;
+    __syncthreads();
+    for (int j = threadIdx.x; j < Ns; j += blockDim.x) {
+      double2 x = a[c * Ns + j];
+      a[c * Ns + j] = make_double2(x.x * qr - x.y * qi, x.x * qi + x.y * qr);
+      x = b[c * Ns + j];
+      b[c * Ns + j] = make_double2(x.x * qr - x.y * qi, x.x * qi + x.y * qr);
+    }
+    // the multipliers (column c) are read by every element of their row,
+    // so they are saved before the elimination overwrites them
+    for (int r = threadIdx.x; r < Ns; r += blockDim.x) fcol[r] = a[r * Ns + c];
+    __syncthreads();
+    for (int e = threadIdx.x; e < Ns * Ns; e += blockDim.x) {
+      const int r = e / Ns, j = e % Ns;
+      if (r == c) continue;
+      const double2 f = fcol[r];
+      const double2 ac = a[c * Ns + j], bc = b[c * Ns + j];
+      a[e] = make_double2(a[e].x - (f.x * ac.x - f.y * ac.y), a[e].y - (f.x * ac.y + f.y * ac.x));
+      b[e] = make_double2(b[e].x - (f.x * bc.x - f.y * bc.y), b[e].y - (f.x * bc.y + f.y * bc.x));
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < Ns * Ns; e += blockDim.x) {
+    const int r = e / Ns, cc = e % Ns;
+    B[off + (size_t)cc * Ns + r] = b[e];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int e = 0; e < Ns * Ns; e++) s += b[e].x * b[e].x + b[e].y * b[e].y;
+    if (fn[0] * s > 1.0e12) atomicOr(fail, 1);
+  }
+}
+
+// M[n][ifc] = Ainv[n] * Ahop[n][ifc]  (column-major products)
+__global__ void k_cmatmul8(int Ns, const double2 *__restrict__ Ainv, const double2 *__restrict__ Ahop, double2 *M) {
+  const int n = blockIdx.x >> 3, ifc = blockIdx.x & 7;
+  const double2 *a = Ainv + (size_t)n * Ns * Ns;
+  const double2 *h = Ahop + ((size_t)8 * n + ifc) * Ns * Ns;
+  double2 *m = M + ((size_t)8 * n + ifc) * Ns * Ns;
+  for (int e = threadIdx.x; e < Ns * Ns; e += blockDim.x) {
+    const int k = e % Ns, l = e / Ns;
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < Ns; j++) {
+      const double2 x = a[(size_t)j * Ns + k], y = h[(size_t)l * Ns + j];
+      re += x.x * y.x - x.y * y.y;
+      im += x.x * y.y + x.y * y.x;
+    }
+    m[(size_t)l * Ns + k] = make_double2(re, im);
+  }
+}
+
+// ----------------------------------------------------- little operator apply
+// mode 0: w[n] = Ablk[n] v[n] + sum_ifc Ahop[n][ifc] v[nbr]        all blocks
+// mode 1: w[n] = sum_ifc H[n][ifc] v[nbr]   for blocks in [b0, b0+cnt)
+// mode 2: w[n] = v[n] - sum_ifc H[n][ifc] u[nbr]
+// mode 3: w[n] = Ablk[n] v[n] (Ablk holding an inverse)
+__global__ void k_little(int mode, int Ns, int b0, const double2 *__restrict__ Ablk, const double2 *__restrict__ H,
+                         const int *__restrict__ nbr, const double2 *__restrict__ v, const double2 *__restrict__ u,
+                         double2 *w) {
+  const int n = b0 + blockIdx.x, k = threadIdx.x;
+  if (k >= Ns) return;
+  double re = 0.0, im = 0.0;
+  if (mode == 0 || mode == 3) {
+    const double2 *a = Ablk + (size_t)n * Ns * Ns;
+    const double2 *x = v + (size_t)n * Ns;
+    for (int l = 0; l < Ns; l++) {
+      const double2 aa = a[(size_t)l * Ns + k], xx = x[l];
+      re += aa.x * xx.x - aa.y * xx.y;
+      im += aa.x * xx.y + aa.y * xx.x;
+    }
+  }
+  if (mode != 3) {
+    const double2 *src = mode == 2 ? u : v;
+    for (int ifc = 0; ifc < 8; ifc++) {
+      const double2 *a = H + ((size_t)8 * n + ifc) * Ns * Ns;
+      const double2 *x = src + (size_t)__ldg(nbr + 8 * n + ifc) * Ns;
+      double tr = 0.0, ti = 0.0;
+      for (int l = 0; l < Ns; l++) {
+        const double2 aa = a[(size_t)l * Ns + k], xx = x[l];
+        tr += aa.x * xx.x - aa.y * xx.y;
+        ti += aa.x * xx.y + aa.y * xx.x;
+      }
+      re += tr;
+      im += ti;
+    }
+  }
+  if (mode == 2) {
+    const double2 vv = v[(size_t)n * Ns + k];
+    w[(size_t)n * Ns + k] = make_double2(vv.x - re, vv.y - im);
+  } else {
+    w[(size_t)n * Ns + k] = make_double2(re, im);
+  }
+}
+
+// ----------------------------------------------------------- host routines
+static int little_threads(int Ns) { return ((Ns + 31) / 32) * 32; }
+
+void dfl_release(Ctx &c) {
+  DflState &d = c.dfl;
+  for (void *p : d.basis) cudaFree(p);
+  for (void *p : d.modes) cudaFree(p);
+  for (double2 *p : d.lv) cudaFree(p);
+  for (double2 *p : d.lvd) cudaFree(p);
+  void *bufs[] = {d.vd2lex, d.nbr, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop};
+  for (void *p : bufs) cudaFree(p);
+  DflState fresh;
+  // the solver and generation parameters outlive a change of geometry
+  fresh.gen_set = d.gen_set;
+  fresh.nkv = d.nkv; fresh.nmx = d.nmx; fresh.nmx_gcr = d.nmx_gcr;
+  fresh.res = d.res; fresh.res_gcr = d.res_gcr;
+  fresh.gen_kappa = d.gen_kappa; fresh.gen_mu = d.gen_mu;
+  fresh.gen_ninv = d.gen_ninv; fresh.gen_nmr = d.gen_nmr; fresh.gen_ncy = d.gen_ncy;
+  d = fresh;
+}
+
+int dfl_set_parms(Ctx &c, const int bs[4], int Ns) {
+  for (int mu = 0; mu < 4; mu++)
+    if (bs[mu] != c.g.bs[mu]) return fail("set_dfl_parms: the DFL block size must equal the geometry block size");
+  // check_block_size (modules/flags/dfl_parms.c:175-205) without the
+  // per-thread rule, and the once-only rule of set_dfl_parms (:228)
+  for (int mu = 0; mu < 4; mu++) {
+    if (bs[mu] < 4 || bs[mu] > c.g.L[mu]) return fail("set_dfl_parms: block sizes are out of range");
+    if (bs[mu] & 1) return fail("set_dfl_parms: block sizes must be even");
+    if (c.g.nb[mu] & 1) return fail("set_dfl_parms: there must be an even number of blocks in each direction");
+  }
+  if (Ns < 2 || (Ns & 1) || Ns > 64) return fail("set_dfl_parms: Ns must be even and in [2, 64]");
+  if (c.dfl.ready && Ns != c.dfl.Ns) return fail("set_dfl_parms: bs[4] and Ns may be set only once");
+  if (c.dfl.ready) return 0;
+  c.dfl.Ns = Ns;
+  return dfl_alloc(c);
+}
+
+void dfl_restrict(Ctx &c, int prec, const void *s, double2 *vd, cudaStream_t st) {
+  DflState &d = c.dfl;
+  if (prec == 32)
+    k_dfl_restrict<float><<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, s, vd, 1);
+  else
+    k_dfl_restrict<double><<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, s, vd, 0);
+}
+
+void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st) {
+  DflState &d = c.dfl;
+  k_dfl_prolong<<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, vd, (float4 *)s);
+}
+
+// basis from Ns global mode fields (FP32, device layout)
+int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st) {
+  DflState &d = c.dfl;
+  float4 **dm = nullptr;
+  int *dfail = nullptr;
+  cudaMallocAsync(&dm, d.Ns * sizeof(void *), st);
+  cudaMallocAsync(&dfail, sizeof(int), st);
+  cudaMemcpyAsync(dm, modes.data(), d.Ns * sizeof(void *), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(dfail, 0, sizeof(int), st);
+  size_t shm = (size_t)24 * 2 * c.g.vbh * sizeof(double);
+  if (shm > 200 * 1024) return fail("dfl_subspace: block too large for shared memory");
+  cudaFuncSetAttribute(k_dfl_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  k_dfl_gs<<<d.nb, 256, shm, st>>>(c.g, d.vd2lex, (float4 *const *)d.d_basis, (const float4 *const *)dm, d.Ns, dfail);
+  int hf = 0;
+  cudaMemcpyAsync(&hf, dfail, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dm, st);
+  cudaFreeAsync(dfail, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail("dfl_subspace: CUDA error");
+  if (hf) return fail("dfl_subspace: degenerate block modes");
+  d.have_basis = true;
+  d.aw_valid = d.awhat_valid = false;
+  return 0;
+}
+
+// Little operator for twisted mass mu (set_Aw); returns 0
+int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st) {
+  DflState &d = c.dfl;
+  if (!d.have_basis) return fail("set_Aw: the deflation subspace is not set");
+  if (d.aw_valid && d.aw_mu == mu && d.aw_eo == c.eoflg) return 0;
+  void *t = nullptr;
+  if (cudaMallocAsync(&t, spinor_bytes(c, 64), st) != cudaSuccess) return fail("out of device memory");
+  const double muo = c.eoflg ? 0.0 : mu;
+  const int T = 128;
+  const unsigned nbk = (unsigned)((c.g.vol + T - 1) / T);
+  const size_t m2 = (size_t)d.Ns * d.Ns;
+  for (int l = 0; l < d.Ns; l++) {
+    k_dfl_dapply<<<nbk, T, 0, st>>>(c.g, (const float4 *)d.basis[l], (double2 *)t, c.ud, c.swd, mu, muo, -1);
+    k_dfl_project<<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, (const double2 *)t,
+                                        d.Ablk, m2, l);
+    for (int ifc = 0; ifc < 8; ifc++) {
+      k_dfl_dapply<<<nbk, T, 0, st>>>(c.g, (const float4 *)d.basis[l], (double2 *)t, c.ud, c.swd, mu, muo, ifc);
+      k_dfl_project<<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
+                                          (const double2 *)t, d.Ahop + ifc * m2, 8 * m2, l);
+    }
+  }
+  cudaFreeAsync(t, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail("set_Aw: CUDA error");
+  d.aw_valid = true;
+  d.aw_mu = mu;
+  d.aw_eo = c.eoflg;
+  d.awhat_valid = false;
+  return 0;
+}
+
+// Even-odd preconditioned little operator (set_Awhat): inverses of the
+// diagonal blocks and H = Ablk^-1 Ahop.  Returns 1 if an inversion was unsafe.
+int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st) {
+  DflState &d = c.dfl;
+  if (dfl_set_Aw(c, mu, st)) return -1;
+  if (d.awhat_valid) return d.awhat_fail;
+  int *dfail = nullptr;
+  cudaMallocAsync(&dfail, sizeof(int), st);
+  cudaMemsetAsync(dfail, 0, sizeof(int), st);
+  size_t shm = (size_t)2 * d.Ns * d.Ns * sizeof(double2);
+  cudaFuncSetAttribute(k_cinv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  k_cinv<<<d.nb, 256, shm, st>>>(d.Ns, d.Ablk, d.Ainv, dfail);
+  k_cmatmul8<<<8 * d.nb, 256, 0, st>>>(d.Ns, d.Ainv, d.Ahop, d.Mhop);
+  int hf = 0;
+  cudaMemcpyAsync(&hf, dfail, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(dfail, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail("set_Awhat: CUDA error");
+  d.awhat_valid = true;
+  d.awhat_fail = hf ? 1 : 0;
+  return d.awhat_fail;
+}
+
+// w = Aw v (Aw_dble) on all blocks
+void dfl_Aw(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  k_little<<<d.nb, little_threads(d.Ns), 0, st>>>(0, d.Ns, 0, d.Ablk, d.Ahop, d.nbr, v, nullptr, w);
+}
+
+// w_e = v_e - H_eo H_oe v_e (Awhat_dble): t holds the odd intermediate
+void dfl_Awhat(Ctx &c, const double2 *v, double2 *w, double2 *t, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int nbh = d.nb / 2, T = little_threads(d.Ns);
+  k_little<<<nbh, T, 0, st>>>(1, d.Ns, nbh, nullptr, d.Mhop, d.nbr, v, nullptr, t);
+  k_little<<<nbh, T, 0, st>>>(2, d.Ns, 0, nullptr, d.Mhop, d.nbr, v, t, w);
+}
+
+// ------------------------------------------------------------ little solver
+// Little-vector BLAS on nv complex numbers (FP64)
+static double lv_dot_re(Ctx &c, const double2 *x, const double2 *y, size_t n, double *im) {
+  double *scr, *od, r[4];
+  flat_scratch(c, &scr, &od);
+  flat_cdot(c, x, y, n, r, scr, od);
+  if (im) *im = r[2] + r[3];
+  return r[0] + r[1];
+}
+
+// ltl_gcr (modules/dfl/ltl_gcr.c:155): even-odd reduction of the little
+// system, GCR on Awhat for the even blocks to relative residue res (at most
+// nmx Krylov vectors, restart after nkv), back-substitution for the odd
+// blocks.  The reference additionally preconditions with a single-precision
+// GCR and deflates the little-little modes; this solver runs plain
+// double-precision GCR with the same stopping rule.  Returns the norm of the
+// residue of the even-odd preconditioned system; ifail 0, -1 (no
+// convergence) or -2 (unsafe inversion).
+double dfl_ltl_gcr(Ctx &c, double mu, const double2 *eta, double2 *psi, int *ifail, int *status,
+                   cudaStream_t st) {
+  DflState &d = c.dfl;
+  ifail[0] = 0;
+  status[0] = 0;
+  const size_t nv = (size_t)d.nv, nvh = nv / 2;
+  const int nbh = d.nb / 2, T = little_threads(d.Ns);
+  if (dfl_set_Awhat(c, mu, st)) {
+    ifail[0] = -2;
+    cudaMemsetAsync(psi, 0, nv * sizeof(double2), st);
+    return sqrt(lv_dot_re(c, eta, eta, nv, nullptr));
+  }
+  const int nkv = d.nkv;
+  while ((int)d.lv.size() < 2 * nkv + 6) {
+    double2 *p = nullptr;
+    if (cudaMalloc(&p, nv * sizeof(double2)) != cudaSuccess) { fail("out of device memory (little vectors)"); return -1; }
+    d.lv.push_back(p);
+  }
+  double2 *x = d.lv[0], *r = d.lv[1], *t = d.lv[2], *eh = d.lv[3], *w = d.lv[4], *y = d.lv[5];
+  double2 **p = &d.lv[6], **q = &d.lv[6 + nkv];
+  // eh_e = Aee^-1 (eta_e - Aeo Aoo^-1 eta_o)   [even half of eh]
+  cudaMemcpyAsync(w, eta, nv * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+  k_little<<<nbh, T, 0, st>>>(3, d.Ns, nbh, d.Ainv, nullptr, d.nbr, eta, nullptr, w);     // w_o = Aoo^-1 eta_o
+  k_little<<<nbh, T, 0, st>>>(2, d.Ns, 0, nullptr, d.Ahop, d.nbr, eta, w, t);             // t_e = eta_e - Aeo w_o
+  k_little<<<nbh, T, 0, st>>>(3, d.Ns, 0, d.Ainv, nullptr, d.nbr, t, nullptr, eh);        // eh_e = Aee^-1 t_e
+  // GCR on Awhat x = eh (even half)
+  cudaMemsetAsync(x, 0, nvh * sizeof(double2), st);
+  cudaMemcpyAsync(r, eh, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+  const double rn0 = sqrt(lv_dot_re(c, r, r, nvh, nullptr));
+  double rn = rn0;
+  const double tol = d.res * rn0;
+  int it = 0;
+  while (rn > tol && it < d.nmx) {
+    int k;
+    for (k = 0; k < nkv && it < d.nmx && rn > tol; k++, it++) {
+      cudaMemcpyAsync(p[k], r, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+      dfl_Awhat(c, p[k], q[k], y, st);
+      for (int l = 0; l < k; l++) {
+        double im;
+        double re = lv_dot_re(c, q[l], q[k], nvh, &im);
+        flat_caxpy(c, q[k], q[l], nvh, -re, -im);
+        flat_caxpy(c, p[k], p[l], nvh, -re, -im);
+      }
+      double nq = sqrt(lv_dot_re(c, q[k], q[k], nvh, nullptr));
+      if (nq == 0.0) break;
+      flat_cscale(c, q[k], nvh, 1.0 / nq);
+      flat_cscale(c, p[k], nvh, 1.0 / nq);
+      double im;
+      double re = lv_dot_re(c, q[k], r, nvh, &im);
+      flat_caxpy(c, x, p[k], nvh, re, im);
+      flat_caxpy(c, r, q[k], nvh, -re, -im);
+      rn = sqrt(lv_dot_re(c, r, r, nvh, nullptr));
+    }
+    // restart from the true residual
+    dfl_Awhat(c, x, w, y, st);
+    cudaMemcpyAsync(r, eh, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+    flat_caxpy(c, r, w, nvh, -1.0, 0.0);
+    rn = sqrt(lv_dot_re(c, r, r, nvh, nullptr));
+  }
+  status[0] = it;
+  if (rn > tol) ifail[0] = -1;
+  // psi_e = x_e ; psi_o = Aoo^-1 (eta_o - Aoe x_e)
+  cudaMemcpyAsync(psi, x, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+  k_little<<<nbh, T, 0, st>>>(2, d.Ns, nbh, nullptr, d.Ahop, d.nbr, eta, x, t);          // t_o = eta_o - Aoe x_e
+  k_little<<<nbh, T, 0, st>>>(3, d.Ns, nbh, d.Ainv, nullptr, d.nbr, t, nullptr, psi);     // psi_o
+  return rn;
+}
+
+// ------------------------------------------------------ deflated SAP+GCR
+static int reserve32(Ctx &c, std::vector<void *> &v, size_t n) {
+  while (v.size() < n) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory (workspace)");
+    v.push_back(p);
+  }
+  return 0;
+}
+
+// Mop of dfl_sap_gcr (modules/dfl/dfl_sap_gcr.c:212-241): little solve of the
+// restricted residue, prolongation, SAP on the remainder.
+static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, void *ws0, void *phib, int *lstat) {
+  DflState &d = c.dfl;
+  cudaStream_t st = c.stream;
+  double2 *vd = d.lvd[0];
+  int ifail, status[2];
+  dfl_restrict(c, 32, rho, vd, st);
+  dfl_ltl_gcr(c, mu, vd, vd, &ifail, status, st);
+  dfl_prolong(c, vd, ws0, st);
+  dirac_op<float>(c, 0, (float)mu, ws0, chi, c.tmp32, st);
+  la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - D ws0
+  la_zero(c, 32, phi, PAR_ALL, st);
+  sap_cycles(c, (float)mu, c.isolv, c.nmr, c.ncy, phi, chi, phib, st);
+  la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - chi
+  la_axpy(c, 32, phi, 1.0, 0.0, ws0, PAR_ALL, st);
+  lstat[0] += status[0];
+}
+
+static int ensure_lvd(Ctx &c) {
+  DflState &d = c.dfl;
+  while (d.lvd.size() < 2) {
+    double2 *p = nullptr;
+    if (cudaMalloc(&p, (size_t)d.nv * sizeof(double2)) != cudaSuccess) return fail("out of device memory");
+    d.lvd.push_back(p);
+  }
+  return 0;
+}
+
+// dfl_sap_gcr on device fields (FP64 eta, psi; psi may equal eta)
+double dfl_sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                       int *ifail, int *status) {
+  DflState &d = c.dfl;
+  ifail[0] = 0;
+  status[0] = status[1] = status[2] = 0;
+  if (!c.sap_set) { fail("dfl_sap_gcr: SAP parameters are not set"); return -1.0; }
+  if (!d.ready || !d.have_basis) { fail("dfl_sap_gcr: the deflation subspace is not set"); return -1.0; }
+  if (sap_prepare(c, c.stream) || ensure_lvd(c)) return -1.0;
+  cudaStream_t st = c.stream;
+  double rho;
+  {
+    double r[2];
+    if (istop) { la_unorm(c, 64, eta, PAR_ALL, r); rho = r[0]; }
+    else { la_norm2(c, 64, eta, PAR_ALL, r); rho = sqrt(r[0]); }
+  }
+  if (c.isolv == 1 && (c.sw_inv_fail & 2)) {
+    ifail[0] = -3;
+  } else if (dfl_set_Awhat(c, mu, st)) {
+    ifail[0] = -2;
+  } else if (rho != 0.0) {
+    if (reserve32(c, c.ws32, 2 * nkv + 3)) return -1.0;
+    while (c.ws64.size() < 3) {
+      void *p = nullptr;
+      if (cudaMalloc(&p, spinor_bytes(c, 64)) != cudaSuccess) { fail("out of device memory"); return -1.0; }
+      c.ws64.push_back(p);
+    }
+    void *rsd = c.ws64[1];
+    void *phib = c.ws32[2 * nkv + 1], *ws0 = c.ws32[2 * nkv + 2];
+    const double rho0 = rho;
+    la_copy(c, 64, eta, 64, rsd, PAR_ALL, st);
+    la_scale(c, 64, rsd, 1.0 / rho0, PAR_ALL, st);
+    int lstat = 0;
+    std::function<void(const void *, void *)> Dop = [&](const void *s, void *r) {
+      dirac_op<double>(c, 0, mu, s, r, c.tmp64, st);
+    };
+    std::function<void(int, const void *, void *, void *)> Mop = [&](int, const void *rh, void *ph, void *ch) {
+      dfl_mop(c, mu, rh, ph, ch, ws0, phib, &lstat);
+    };
+    std::vector<void *> phi(c.ws32.begin(), c.ws32.begin() + nkv),
+        chi(c.ws32.begin() + nkv + 1, c.ws32.begin() + 2 * nkv + 1);
+    rho = fgcr_core(dev_krylov_ops(c), nkv, nmx, istop, res, rsd, psi, status, Dop, Mop, phi, chi, c.ws32[nkv],
+                    c.ws64[0]);
+    la_scale(c, 64, psi, rho0, PAR_ALL, st);
+    rho *= rho0;
+    if (status[0] < 0) {
+      ifail[0] = -1;
+      status[0] = nmx;
+    }
+    if (status[0] > 0) status[1] = (lstat + status[0] / 2) / status[0];
+  } else {
+    la_zero(c, 64, psi, PAR_ALL, st);
+  }
+  if (ifail[0] <= -2 && psi != eta) la_zero(c, 64, psi, PAR_ALL, st);
+  cudaStreamSynchronize(st);
+  return rho;
+}
+
+// ---------------------------------------------------- subspace generation
+// dfl_modes (modules/dfl/dfl_modes.c:423-502): Ns random fields smoothed by
+// 1, 2 and 3 SAP cycles, block-orthonormalised, then ninv-3 steps of
+// deflated inverse iteration (little solve of the restricted mode, SAP on
+// the remainder), global renormalisation and block orthonormalisation.
+// The iteration uses the generation mass m0 = 1/(2 kappa) - 4, twisted mass
+// mu_gen and the twisted-mass eo flag set, as the reference does.
+int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
+  DflState &d = c.dfl;
+  ifail[0] = 0;
+  status[0] = status[1] = 0;
+  if (!d.ready) return fail("dfl_modes: deflation parameters are not set");
+  if (!d.gen_set) return fail("dfl_modes: subspace generation parameters are not set");
+  if (d.gen_kappa == 0.0) return fail("dfl_modes: kappa = 0 (infinite generation mass) is not supported");
+  if (!c.sap_set) return fail("dfl_modes: SAP parameters are not set");
+  cudaStream_t st = c.stream;
+  if (sap_prepare(c, st) || ensure_lvd(c) || reserve32(c, d.modes, d.Ns) || reserve32(c, c.ws32, 3)) return -1;
+  // generation mass and eo flag
+  const double m0_save = c.m0;
+  const int eo_save = c.eoflg;
+  const double m0g = 1.0 / (2.0 * d.gen_kappa) - 4.0;
+  if (m0g != c.m0) {
+    if (sw_shift_mass(c, m0g - c.m0, st)) return -1;
+    c.m0 = m0g;
+  }
+  c.eoflg = 1;
+  if (c.sw_inv_fail & 2) ifail[0] = -3;
+  void *ws0 = c.ws32[0], *ws1 = c.ws32[1], *phib = c.ws32[2];
+  const float mug = (float)d.gen_mu;
+  for (int l = 0; l < d.Ns; l++) gen_uniform_spinor32(c, d.modes[l], seed * 1000003ull + l, st);
+  if (ifail[0] == 0) {
+    int n;
+    for (n = 0; n < 3; n++) {
+      for (int l = 0; l < d.Ns; l++) {
+        la_copy(c, 32, d.modes[l], 32, ws0, PAR_ALL, st);
+        la_zero(c, 32, d.modes[l], PAR_ALL, st);
+        sap_cycles(c, mug, 1, d.gen_nmr, n + 1, d.modes[l], ws0, phib, st);
+      }
+    }
+    if (dfl_subspace_dev(c, d.modes, st)) return -1;
+    for (; n < d.gen_ninv && ifail[0] == 0; n++) {
+      if (dfl_set_Awhat(c, d.gen_mu, st)) {
+        ifail[0] = -2;
+        break;
+      }
+      for (int l = 0; l < d.Ns; l++) {
+        int lf, ls[2];
+        double2 *vd = d.lvd[0];
+        dfl_restrict(c, 32, d.modes[l], vd, st);
+        dfl_ltl_gcr(c, d.gen_mu, vd, vd, &lf, ls, st);
+        dfl_prolong(c, vd, ws1, st);
+        dirac_op<float>(c, 0, mug, ws1, ws0, c.tmp32, st);
+        la_diff(c, 32, d.modes[l], ws0, PAR_ALL, st);     // ws0 = mode - D ws1
+        la_zero(c, 32, d.modes[l], PAR_ALL, st);
+        sap_cycles(c, mug, 1, d.gen_nmr, d.gen_ncy, d.modes[l], ws0, phib, st);
+        la_axpy(c, 32, d.modes[l], 1.0, 0.0, ws1, PAR_ALL, st);
+        status[0] += ls[0];
+      }
+      // dfl_renormalize_modes (dfl_subspace.c:243-259)
+      for (int l = 0; l < d.Ns; l++) {
+        for (int j = 0; j < l; j++) {
+          double r[4];
+          la_dot(c, 32, d.modes[j], d.modes[l], PAR_ALL, r);
+          la_axpy(c, 32, d.modes[l], -(float)(r[0] + r[1]), -(float)(r[2] + r[3]), d.modes[j], PAR_ALL, st);
+        }
+        double r[2];
+        la_norm2(c, 32, d.modes[l], PAR_ALL, r);
+        float nrm = (float)sqrt((double)(float)(r[0] + r[1]));
+        if (nrm != 0.0f) la_scale(c, 32, d.modes[l], 1.0f / nrm, PAR_ALL, st);
+      }
+      if (dfl_subspace_dev(c, d.modes, st)) return -1;
+    }
+    const int nst = d.Ns * (n - 3);
+    if (nst > 0) status[0] = (status[0] + nst / 2) / nst;
+  } else {
+    if (dfl_subspace_dev(c, d.modes, st)) return -1;
+  }
+  // restore the mass and the eo flag
+  c.eoflg = eo_save;
+  if (c.m0 != m0_save) {
+    if (sw_shift_mass(c, m0_save - c.m0, st)) return -1;
+    c.m0 = m0_save;
+  }
+  d.aw_valid = d.awhat_valid = false;
+  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : fail("dfl_modes: CUDA error");
+}
+
+}  // namespace qcd

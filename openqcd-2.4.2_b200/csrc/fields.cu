@@ -205,4 +205,32 @@ int gen_spinor(const Ctx &c, int prec, void *dev, double sigma, uint64_t seed, c
   return cudaGetLastError() == cudaSuccess ? 0 : fail("gen_spinor: launch failed");
 }
 
+// Uniform random FP32 spinor field, every real component in [-0.5, 0.5)
+// (the distribution of dfl_modes.c random_fields, :248-274).
+__global__ void k_uniform_spinor(Geom g, float4 *dst, uint32_t k0, uint32_t k1) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= g.vol) return;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  int p = chunk >= g.nbl, blk = chunk - p * g.nbl;
+  Site xs;
+  site_decode(g, p, blk, s, xs);
+  uint32_t lex = 0;
+  for (int m = 0; m < 4; m++) lex = lex * g.L[m] + (xs.n[m] * g.bs[m] + xs.y[m]);
+  spinor<float> v;
+  for (int k = 0; k < 6; k++) {
+    P4 o = philox({lex, (uint32_t)k, 0x554e4946u, 0u}, k0, k1);
+    const float sc = 1.0f / 4294967296.0f;
+    int q = 2 * k;
+    v.c[q / 3].c[q % 3] = mk<float>(o.x * sc - 0.5f, o.y * sc - 0.5f);
+    v.c[(q + 1) / 3].c[(q + 1) % 3] = mk<float>(o.z * sc - 0.5f, o.w * sc - 0.5f);
+  }
+  Store<float>::store_spinor(dst, chunk, s, g.vbh, v);
+}
+
+int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st) {
+  int t = 128;
+  k_uniform_spinor<<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, (float4 *)dev, (uint32_t)seed, (uint32_t)(seed >> 32));
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("uniform spinor: launch failed");
+}
+
 }  // namespace qcd

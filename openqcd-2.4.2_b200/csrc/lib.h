@@ -11,6 +11,25 @@
 
 namespace qcd {
 
+// Deflation state (the reference's DFL block grid, little operator and
+// parameter sets dfl_parms, dfl_pro_parms, dfl_gen_parms).
+struct DflState {
+  bool ready = false, have_basis = false, gen_set = false;
+  int Ns = 0, nb = 0, nv = 0;
+  int nkv = 16, nmx = 256, nmx_gcr = 24;
+  double res = 1e-2, res_gcr = 1e-2;
+  double gen_kappa = 0.125, gen_mu = 0.0;
+  int gen_ninv = 4, gen_nmr = 4, gen_ncy = 4;
+  int *vd2lex = nullptr, *nbr = nullptr;
+  std::vector<void *> basis, modes;
+  void **d_basis = nullptr;
+  double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
+  bool aw_valid = false, awhat_valid = false;
+  int awhat_fail = 0, aw_eo = 0;
+  double aw_mu = 0.0;
+  std::vector<double2 *> lv, lvd;
+};
+
 // Everything the reference keeps in module-global state for this path:
 // geometry (lattice/geometry.c), the gauge field (uflds/uflds.c udfld/ufld),
 // the SW field (sw_term/swflds.c swdfld/swfld) and the parameter data base
@@ -57,6 +76,7 @@ struct Ctx {
   void *fstage[3] = {nullptr, nullptr, nullptr};   // staging of host operands
   size_t fstage_bytes[3] = {0, 0, 0};
   std::vector<void *> ws32, ws64;   // solver workspaces (reserve_ws / reserve_wsd)
+  DflState dfl;
 };
 
 Ctx &ctx();
@@ -142,8 +162,32 @@ double fgcr_core(const KrylovOps &o, int nkv, int nmx, int istop, double res, co
                  const std::function<void(int, const void *, void *, void *)> &Mop,
                  const std::vector<void *> &phi, const std::vector<void *> &chi, void *rho, void *wrk);
 
+KrylovOps dev_krylov_ops(Ctx &c);
+int flat_cdot(Ctx &c, const double2 *x, const double2 *y, size_t n, double *res_dd, double *scratch, double *out_dev);
+void flat_caxpy(Ctx &c, double2 *y, const double2 *x, size_t n, double ar, double ai);
+void flat_cscale(Ctx &c, double2 *y, size_t n, double a);
+int sw_shift_mass(Ctx &c, double dm, cudaStream_t st);
+int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st);
+
+// dfl.cu
+int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
+void dfl_release(Ctx &c);
+void dfl_restrict(Ctx &c, int prec, const void *s, double2 *vd, cudaStream_t st);
+void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st);
+int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st);
+int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st);
+int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st);
+void dfl_Aw(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
+void dfl_Awhat(Ctx &c, const double2 *v, double2 *w, double2 *t, cudaStream_t st);
+double dfl_ltl_gcr(Ctx &c, double mu, const double2 *eta, double2 *psi, int *ifail, int *status, cudaStream_t st);
+double dfl_sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
+                       int *ifail, int *status);
+int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status);
+
 // sap.cu
 int sap_prepare(Ctx &c, cudaStream_t st);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
+int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
+               cudaStream_t st);
 
 }  // namespace qcd

@@ -438,6 +438,14 @@ int sap_prepare(Ctx &c, cudaStream_t st) {
   return 0;
 }
 
+// ncy SAP cycles sap(mu, isolv, nmr, psi, rho) on FP32 device fields
+int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
+               cudaStream_t st) {
+  for (int n = 0; n < ncy; n++)
+    if (sap_cycle(c, mu, isolv, nmr, psi, rho, phi_blk, st)) return -1;
+  return 0;
+}
+
 // One SAP cycle sap(mu, isolv, nmr, psi, rho) on FP32 device fields.
 // phi_blk is a scratch FP32 field.
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st) {

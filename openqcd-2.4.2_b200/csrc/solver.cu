@@ -90,7 +90,7 @@ double fgcr_core(const KrylovOps &o, int nkv, int nmx, int istop, double res, co
 }
 
 // Vector operations on fields in the device layout (la_* of linalg.cu).
-static KrylovOps dev_ops(Ctx &c) {
+KrylovOps dev_krylov_ops(Ctx &c) {
   KrylovOps o;
   cudaStream_t st = c.stream;
   o.res32 = [&c](const void *x, int istop) {
@@ -128,7 +128,7 @@ double fgcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, const void *eta
   if (reserve(c, c.ws32, 2 * nkv + 1, 32) || reserve(c, c.ws64, 2, 64)) return -1.0;
   std::vector<void *> phi(c.ws32.begin(), c.ws32.begin() + nkv),
       chi(c.ws32.begin() + nkv + 1, c.ws32.begin() + 2 * nkv + 1);
-  return fgcr_core(dev_ops(c), nkv, nmx, istop, res, eta, psi, status, Dop, Mop, phi, chi, c.ws32[nkv], c.ws64[0]);
+  return fgcr_core(dev_krylov_ops(c), nkv, nmx, istop, res, eta, psi, status, Dop, Mop, phi, chi, c.ws32[nkv], c.ws64[0]);
 }
 
 // Device twin of sap_gcr(): eta, psi FP64 device fields (psi may equal eta).

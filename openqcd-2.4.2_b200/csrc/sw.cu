@@ -319,6 +319,31 @@ int sw_compute(Ctx &c, cudaStream_t st) {
   return sw_refresh_derived(c, st);
 }
 
+// Add dm to the diagonal of every Pauli matrix (a change of the bare mass
+// m0 in the SW term, whose diagonal is 4 + m0 + clover part), then refresh
+// the inverses and FP32 copies.
+__global__ void k_sw_shift(Geom g, double2 *swd, double dm) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= g.vol) return;
+  int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  for (int half = 0; half < 2; half++) {
+    double2 *p = swd + ((size_t)chunk * 36 + 18 * half) * g.vbh + s;
+    for (int k = 0; k < 3; k++) {   // u[0..5] are the real parts of planes 0..2
+      double2 v = p[(size_t)k * g.vbh];
+      v.x += dm;
+      v.y += dm;
+      p[(size_t)k * g.vbh] = v;
+    }
+  }
+}
+
+int sw_shift_mass(Ctx &c, double dm, cudaStream_t st) {
+  if (!c.have_sw) return fail("no SW field on the device");
+  int t = 128;
+  k_sw_shift<<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.swd, dm);
+  return sw_refresh_derived(c, st);
+}
+
 // ------------------------------------------------------------ FP32 links
 __global__ void k_links_f32(size_t n, const double2 *__restrict__ a, float2 *b) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;

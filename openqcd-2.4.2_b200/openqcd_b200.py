@@ -97,6 +97,29 @@ _SIGS = {
     "normalize": (C.c_float, [C.c_int, C.c_int, C.c_void_p]),
     "fgcr": (C.c_double, [C.c_int, DOP_T, MOP_T, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
                           C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_clear_error": (None, []),
+    "b200_set_dfl_parms": (C.c_int, [C.c_void_p, C.c_int]),
+    "b200_set_dfl_pro_parms": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]),
+    "b200_set_dfl_gen_parms": (C.c_int, [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
+    "b200_dfl_nv": (C.c_int, []),
+    "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
+    "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
+    "dfl_modes": (None, [C.c_void_p, C.c_void_p]),
+    "b200_dev_dfl_modes": (C.c_int, [C.c_ulonglong, C.c_void_p, C.c_void_p]),
+    "dfl_subspace": (None, [C.c_void_p]),
+    "dfl_s2vd": (None, [C.c_void_p, C.c_void_p]),
+    "dfl_vd2s": (None, [C.c_void_p, C.c_void_p]),
+    "set_Aw": (None, [C.c_double]),
+    "set_Awhat": (C.c_int, [C.c_double]),
+    "Aw_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Awhat_dble": (None, [C.c_void_p, C.c_void_p]),
+    "ltl_gcr": (C.c_double, [C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "dfl_sap_gcr": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
+    "dfl_sap_gcr2": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]),
+    "b200_dev_dfl_sap_gcr": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_dev_alloc_spinor": (C.c_void_p, [C.c_int]),
     "b200_dev_free": (None, [C.c_void_p]),
     "b200_dev_random_spinor": (C.c_int, [C.c_int, C.c_void_p, C.c_double, C.c_ulonglong]),
@@ -215,6 +238,15 @@ def random_ud(eps, seed):
 def _err_after():
     e = lib().b200_last_error()
     return e.decode() if e else ""
+
+
+def _void(f, *args):
+    """Call a void entry point and raise if it recorded an error."""
+    lib().b200_clear_error()
+    f(*args)
+    e = _err_after()
+    if e:
+        raise B200Error(e)
 
 
 def dirac_ref(op, prec, mu, s, r=None):
@@ -370,3 +402,105 @@ def time_Dw_dble_host(mu, s, r, n):
     ms = C.c_float(0.0)
     check(lib().b200_time_Dw_dble_host(mu, _ptr(s), _ptr(r), n, C.byref(ms)))
     return ms.value
+
+
+# ------------------------------------------------------------------ deflation
+def set_dfl_parms(bs, Ns):
+    b = np.ascontiguousarray(bs, dtype=np.int32)
+    check(lib().b200_set_dfl_parms(_ptr(b), Ns))
+    return lib().b200_dfl_nv()
+
+
+def set_dfl_pro_parms(nkv, nmx, res, nmx_gcr, res_gcr):
+    return check(lib().b200_set_dfl_pro_parms(nkv, nmx, res, nmx_gcr, res_gcr))
+
+
+def set_dfl_gen_parms(kappa, mu, ninv, nmr, ncy):
+    return check(lib().b200_set_dfl_gen_parms(kappa, mu, ninv, nmr, ncy))
+
+
+def dfl_set_basis(l, field):
+    return check(lib().b200_dfl_set_basis(l, _ptr(np.ascontiguousarray(field, dtype=np.float32))))
+
+
+def dfl_get_basis(l, vol):
+    out = np.zeros(vol * 24, dtype=np.float32)
+    check(lib().b200_dfl_get_basis(l, _ptr(out)))
+    return out
+
+
+def dfl_modes(seed=1):
+    ifail = C.c_int(0)
+    status = (C.c_int * 2)()
+    check(lib().b200_dev_dfl_modes(seed, C.byref(ifail), status))
+    return ifail.value, list(status)
+
+
+def dfl_subspace(modes):
+    arrs = [np.ascontiguousarray(m, dtype=np.float32) for m in modes]
+    ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    _void(lib().dfl_subspace, ptrs)
+
+
+def dfl_s2vd(s, nv):
+    s = np.ascontiguousarray(s, dtype=np.float32)
+    vd = np.zeros(2 * nv)
+    _void(lib().dfl_s2vd, _ptr(s), _ptr(vd))
+    return vd
+
+
+def dfl_vd2s(vd, vol):
+    vd = np.ascontiguousarray(vd, dtype=np.float64)
+    s = np.zeros(vol * 24, dtype=np.float32)
+    _void(lib().dfl_vd2s, _ptr(vd), _ptr(s))
+    return s
+
+
+def little(which, mu, v, w=None):
+    """which 0: set_Aw(mu), Aw_dble(v, w); 1: set_Awhat(mu), Awhat_dble."""
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float64, copy=True)
+    f = 0
+    if which == 0:
+        _void(lib().set_Aw, mu)
+        _void(lib().Aw_dble, _ptr(v), _ptr(w))
+    else:
+        f = check(lib().set_Awhat(mu))
+        _void(lib().Awhat_dble, _ptr(v), _ptr(w))
+    return w, f
+
+
+def ltl_gcr(mu, eta):
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    psi = np.zeros_like(eta)
+    ifail = C.c_int(0)
+    status = (C.c_int * 2)()
+    lib().b200_clear_error()
+    rho = lib().ltl_gcr(mu, _ptr(eta), _ptr(psi), C.byref(ifail), status)
+    if rho < 0:
+        raise B200Error(_err_after())
+    return psi, rho, ifail.value, list(status)
+
+
+def dfl_sap_gcr(nkv, nmx, istop, res, mu, eta):
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    psi = np.zeros_like(eta)
+    ifail = C.c_int(0)
+    status = (C.c_int * 3)()
+    lib().b200_clear_error()
+    rho = lib().dfl_sap_gcr(nkv, nmx, istop, res, mu, _ptr(eta), _ptr(psi), C.byref(ifail), status)
+    if rho < 0:
+        raise B200Error(_err_after())
+    return psi, rho, ifail.value, list(status)
+
+
+def dfl_sap_gcr2(nkv, nmx, istop, res, mu, eta):
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    psi = np.zeros_like(eta)
+    ifail = (C.c_int * 2)()
+    status = (C.c_int * 6)()
+    lib().b200_clear_error()
+    rho = lib().dfl_sap_gcr2(nkv, nmx, istop, res, mu, _ptr(eta), _ptr(psi), ifail, status)
+    if rho < 0:
+        raise B200Error(_err_after())
+    return psi, rho, list(ifail), list(status)

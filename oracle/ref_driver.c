@@ -417,3 +417,174 @@ float ref_norm_square(const float *s)
    release_ws();
    return n;
 }
+
+/* ------------------------------------------------------------ deflation */
+/* Deflation parameters and workspaces (modules/flags/dfl_parms.c:209-380). */
+#include "dfl.h"
+#include "little.h"
+#include "vflds.h"
+
+static int dfl_nv = 0;
+
+int ref_dfl_init(int b0, int b1, int b2, int b3, int Ns, int nkv, int nmx, double res, int nmx_gcr,
+                 double res_gcr, double kappa, double mu, int ninv, int nmr, int ncy)
+{
+   ENTER();
+   int bs[4], nb, isw;
+   bs[0] = b0; bs[1] = b1; bs[2] = b2; bs[3] = b3;
+   set_dfl_parms(bs, Ns);
+   set_dfl_pro_parms(nkv, nmx, res, nmx_gcr, res_gcr);
+   set_dfl_gen_parms(kappa, mu, ninv, nmr, ncy);
+   if (dfl_nv != 0)
+      return dfl_nv;
+   alloc_wv(2 * nmx_gcr + 5);
+   alloc_wvd(2 * nkv + 8);
+   need_ws(Ns + 2 * 40 + 4, 8);
+   blk_list(SAP_BLOCKS, &nb, &isw);
+   if (nb == 0) alloc_bgr(SAP_BLOCKS);
+   blk_list(DFL_BLOCKS, &nb, &isw);
+   if (nb == 0) alloc_bgr(DFL_BLOCKS);
+   blk_list(DFL_BLOCKS, &nb, &isw);
+   dfl_nv = Ns * nb;
+   return dfl_nv;
+}
+
+/* dfl_modes() (modules/dfl/dfl_modes.c:423): random fields, SAP smoothing,
+ * deflated inverse iteration, dfl_subspace().  Returns ifail. */
+int ref_dfl_modes(int seed, int *status)
+{
+   ENTER();
+   int ifail = 0;
+   start_ranlux(0, seed);
+   dfl_modes(&ifail, status);
+   return ifail;
+}
+
+/* Basis vector l of every DFL block, as one global field (ipt order). */
+void ref_dfl_get_basis(int l, float *out)
+{
+   ENTER();
+   int nb, isw, n;
+   spinor **ws = reserve_ws(1);
+   blk_list(DFL_BLOCKS, &nb, &isw);
+   for (n = 0; n < nb; n++)
+      assign_sblk2s(DFL_BLOCKS, n, ALL_PTS, l + 1, ws[0]);
+   memcpy(out, ws[0], VOLUME * sizeof(spinor));
+   release_ws();
+}
+
+static complex_dble *vd_copy(const double *v)
+{
+   complex_dble *p = aligned_alloc(64, ((size_t)dfl_nv * sizeof(complex_dble) + 63) / 64 * 64);
+   if (v) memcpy(p, v, (size_t)dfl_nv * sizeof(complex_dble));
+   else memset(p, 0, (size_t)dfl_nv * sizeof(complex_dble));
+   return p;
+}
+
+void ref_dfl_s2vd(const float *s, double *vd)
+{
+   ENTER();
+   spinor **ws = reserve_ws(1);
+   complex_dble *v = vd_copy(NULL);
+   memcpy(ws[0], s, VOLUME * sizeof(spinor));
+   dfl_s2vd(ws[0], v);
+   memcpy(vd, v, (size_t)dfl_nv * sizeof(complex_dble));
+   free(v);
+   release_ws();
+}
+
+void ref_dfl_vd2s(const double *vd, float *s)
+{
+   ENTER();
+   spinor **ws = reserve_ws(1);
+   complex_dble *v = vd_copy(vd);
+   dfl_vd2s(v, ws[0]);
+   memcpy(s, ws[0], VOLUME * sizeof(spinor));
+   free(v);
+   release_ws();
+}
+
+/* Little Dirac operator (modules/little/Aw_ops.c:186, :223; Aw_dble.c:122,
+ * :361): which = 0 Aw_dble after set_Aw(mu), 1 Awhat_dble after
+ * set_Awhat(mu) (even blocks only; w keeps its odd part). */
+int ref_little(int which, double mu, const double *v, double *w)
+{
+   ENTER();
+   int ifail = 0;
+   complex_dble *a = vd_copy(v), *b = vd_copy(w);
+   if (which == 0)
+   {
+      set_Aw(mu);
+      Aw_dble(a, b);
+   }
+   else
+   {
+      ifail = set_Awhat(mu);
+      Awhat_dble(a, b);
+   }
+   memcpy(w, b, (size_t)dfl_nv * sizeof(complex_dble));
+   free(a);
+   free(b);
+   return ifail;
+}
+
+double ref_ltl_gcr(double mu, const double *eta, double *psi, int *ifail, int *status)
+{
+   ENTER();
+   double rho;
+   complex_dble *a = vd_copy(eta), *b = vd_copy(NULL);
+   rho = ltl_gcr(mu, a, b, ifail, status);
+   memcpy(psi, b, (size_t)dfl_nv * sizeof(complex_dble));
+   free(a);
+   free(b);
+   return rho;
+}
+
+/* dfl_sap_gcr (modules/dfl/dfl_sap_gcr.c:353); status[3]. */
+double ref_dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const double *eta, double *psi,
+                       int *ifail, int *status)
+{
+   ENTER();
+   double rho;
+   spinor_dble **wsd;
+   need_ws(2 * nkv + 4, 8);
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], eta, VOLUME * sizeof(spinor_dble));
+   rho = dfl_sap_gcr(nkv, nmx, istop, res, mu, wsd[0], wsd[1], ifail, status);
+   memcpy(psi, wsd[1], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+   return rho;
+}
+
+/* Time one dfl_sap_gcr solve (wall clock, MPI_Wtime). */
+double ref_time_dfl_sap_gcr(int nkv, int nmx, double res, double mu, const double *eta, int *status)
+{
+   ENTER();
+   int ifail[1];
+   double t0, t1;
+   spinor_dble **wsd;
+   need_ws(2 * nkv + 4, 8);
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], eta, VOLUME * sizeof(spinor_dble));
+   t0 = MPI_Wtime();
+   dfl_sap_gcr(nkv, nmx, 0, res, mu, wsd[0], wsd[1], ifail, status);
+   t1 = MPI_Wtime();
+   release_wsd();
+   return t1 - t0;
+}
+
+double ref_time_sap_gcr(int nkv, int nmx, double res, double mu, const double *eta, int *status)
+{
+   ENTER();
+   int ifail[1];
+   double t0, t1;
+   spinor_dble **wsd;
+   need_ws(2 * nkv + 4, 8);
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], eta, VOLUME * sizeof(spinor_dble));
+   t0 = MPI_Wtime();
+   sap_gcr(nkv, nmx, 0, res, mu, wsd[0], wsd[1], ifail, status);
+   t1 = MPI_Wtime();
+   release_wsd();
+   return t1 - t0;
+}

@@ -215,3 +215,86 @@ class RefLib:
         self.lib.ref_norm_square.argtypes = [C.c_void_p]
         self.lib.ref_norm_square.restype = C.c_float
         return self.lib.ref_norm_square(self._p(s))
+
+    # ------------------------------------------------------------ deflation
+    def dfl_init(self, bs, Ns, nkv=16, nmx=256, res=1e-2, nmx_gcr=24, res_gcr=1e-2, kappa=0.125, mu=0.0,
+                 ninv=5, nmr=4, ncy=4):
+        l = self.lib
+        l.ref_dfl_init.argtypes = [C.c_int] * 7 + [C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+                                                    C.c_int, C.c_int, C.c_int]
+        self.nv = l.ref_dfl_init(bs[0], bs[1], bs[2], bs[3], Ns, nkv, nmx, res, nmx_gcr, res_gcr, kappa, mu,
+                                 ninv, nmr, ncy)
+        self.Ns = Ns
+        return self.nv
+
+    def dfl_modes(self, seed):
+        status = (C.c_int * 2)()
+        self.lib.ref_dfl_modes.argtypes = [C.c_int, C.c_void_p]
+        f = self.lib.ref_dfl_modes(seed, status)
+        return f, list(status)
+
+    def dfl_get_basis(self, l):
+        out = np.zeros(self.vol * 24, dtype=np.float32)
+        self.lib.ref_dfl_get_basis.argtypes = [C.c_int, C.c_void_p]
+        self.lib.ref_dfl_get_basis(l, self._p(out))
+        return out
+
+    def dfl_s2vd(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float32)
+        vd = np.zeros(2 * self.nv)
+        self.lib.ref_dfl_s2vd.argtypes = [C.c_void_p, C.c_void_p]
+        self.lib.ref_dfl_s2vd(self._p(s), self._p(vd))
+        return vd
+
+    def dfl_vd2s(self, vd):
+        vd = np.ascontiguousarray(vd, dtype=np.float64)
+        s = np.zeros(self.vol * 24, dtype=np.float32)
+        self.lib.ref_dfl_vd2s.argtypes = [C.c_void_p, C.c_void_p]
+        self.lib.ref_dfl_vd2s(self._p(vd), self._p(s))
+        return s
+
+    def little(self, which, mu, v, w=None):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float64, copy=True)
+        self.lib.ref_little.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        f = self.lib.ref_little(which, mu, self._p(v), self._p(w))
+        return w, f
+
+    def ltl_gcr(self, mu, eta):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        psi = np.zeros_like(eta)
+        ifail = C.c_int(0)
+        status = (C.c_int * 2)()
+        self.lib.ref_ltl_gcr.argtypes = [C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.ref_ltl_gcr.restype = C.c_double
+        rho = self.lib.ref_ltl_gcr(mu, self._p(eta), self._p(psi), C.byref(ifail), status)
+        return psi, rho, ifail.value, list(status)
+
+    def dfl_sap_gcr(self, nkv, nmx, istop, res, mu, eta):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        psi = np.zeros_like(eta)
+        ifail = C.c_int(0)
+        status = (C.c_int * 3)()
+        self.lib.ref_dfl_sap_gcr.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]
+        self.lib.ref_dfl_sap_gcr.restype = C.c_double
+        rho = self.lib.ref_dfl_sap_gcr(nkv, nmx, istop, res, mu, self._p(eta), self._p(psi), C.byref(ifail),
+                                       status)
+        return psi, rho, ifail.value, list(status)
+
+    def time_dfl_sap_gcr(self, nkv, nmx, res, mu, eta):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        status = (C.c_int * 3)()
+        self.lib.ref_time_dfl_sap_gcr.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                                  C.c_void_p]
+        self.lib.ref_time_dfl_sap_gcr.restype = C.c_double
+        t = self.lib.ref_time_dfl_sap_gcr(nkv, nmx, res, mu, self._p(eta), status)
+        return t, list(status)
+
+    def time_sap_gcr(self, nkv, nmx, res, mu, eta):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        status = (C.c_int * 3)()
+        self.lib.ref_time_sap_gcr.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+        self.lib.ref_time_sap_gcr.restype = C.c_double
+        t = self.lib.ref_time_sap_gcr(nkv, nmx, res, mu, self._p(eta), status)
+        return t, list(status)
