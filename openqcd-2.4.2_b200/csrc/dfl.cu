@@ -155,10 +155,10 @@ __global__ void k_dfl_prolong(Geom g, const int *__restrict__ vd2lex, const floa
 // ------------------------------------------------------ block Gram-Schmidt
 // basis_l(block) = orthonormalised mode_l(block) against basis_0..l-1 of the
 // same block, in double precision (dfl_subspace.c:171-240).  One CTA per
-// block; the current vector lives in shared memory.
+// block; the vector being orthonormalised is held in the FP64 work field,
+// each site read and written only by the thread that owns it.
 __global__ void k_dfl_gs(Geom g, const int *__restrict__ vd2lex, float4 *const *basis,
-                         const float4 *const *__restrict__ modes, int Ns, int *fail) {
-  extern __shared__ double v[];   // [24][2*vbh]
+                         const float4 *const *__restrict__ modes, int Ns, double2 *work, int *fail) {
   const int n = blockIdx.x, blk = __ldg(vd2lex + n);
   const int nsite = 2 * g.vbh;
   __shared__ double red[2][32];
@@ -167,30 +167,30 @@ __global__ void k_dfl_gs(Geom g, const int *__restrict__ vd2lex, float4 *const *
     for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
       const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
       spinor<float> m = Store<float>::load_spinor(modes[l], chunk, si, g.vbh);
+      spinor<double> md;
 #pragma unroll
-      for (int k = 0; k < 12; k++) {
-        v[(2 * k) * nsite + t] = m.c[k / 3].c[k % 3].re;
-        v[(2 * k + 1) * nsite + t] = m.c[k / 3].c[k % 3].im;
-      }
+      for (int k = 0; k < 12; k++) md.c[k / 3].c[k % 3] = mk<double>(m.c[k / 3].c[k % 3].re, m.c[k / 3].c[k % 3].im);
+      Store<double>::store_spinor(work, chunk, si, g.vbh, md);
     }
-    __syncthreads();
     for (int j = 0; j <= l; j++) {
       // j < l: z = (basis_j, v), v -= z basis_j ; j == l: normalise
       double re = 0.0, im = 0.0;
       for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
         const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+        spinor<double> x = Store<double>::load_spinor_rw(work, chunk, si, g.vbh);
         if (j < l) {
           spinor<float> b = Store<float>::load_spinor(basis[j], chunk, si, g.vbh);
 #pragma unroll
           for (int k = 0; k < 12; k++) {
             const double br = b.c[k / 3].c[k % 3].re, bi = b.c[k / 3].c[k % 3].im;
-            const double xr = v[(2 * k) * nsite + t], xi = v[(2 * k + 1) * nsite + t];
+            const double xr = x.c[k / 3].c[k % 3].re, xi = x.c[k / 3].c[k % 3].im;
             re += br * xr + bi * xi;
             im += br * xi - bi * xr;
           }
         } else {
 #pragma unroll
-          for (int k = 0; k < 24; k++) re += v[k * nsite + t] * v[k * nsite + t];
+          for (int k = 0; k < 12; k++)
+            re += x.c[k / 3].c[k % 3].re * x.c[k / 3].c[k % 3].re + x.c[k / 3].c[k % 3].im * x.c[k / 3].c[k % 3].im;
         }
       }
 #pragma unroll
@@ -207,28 +207,27 @@ __global__ void k_dfl_gs(Geom g, const int *__restrict__ vd2lex, float4 *const *
         zsh[1] = b;
       }
       __syncthreads();
-      if (j < l) {
-        const double zr = zsh[0], zi = zsh[1];
-        for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
-          const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+      const double zr = zsh[0], zi = zsh[1];
+      const double nrm = sqrt(zr);
+      if (j == l && nrm == 0.0 && threadIdx.x == 0) atomicOr(fail, 1);
+      const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+      for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
+        const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+        spinor<double> x = Store<double>::load_spinor_rw(work, chunk, si, g.vbh);
+        if (j < l) {
           spinor<float> b = Store<float>::load_spinor(basis[j], chunk, si, g.vbh);
 #pragma unroll
           for (int k = 0; k < 12; k++) {
             const double br = b.c[k / 3].c[k % 3].re, bi = b.c[k / 3].c[k % 3].im;
-            v[(2 * k) * nsite + t] -= zr * br - zi * bi;
-            v[(2 * k + 1) * nsite + t] -= zr * bi + zi * br;
+            x.c[k / 3].c[k % 3].re -= zr * br - zi * bi;
+            x.c[k / 3].c[k % 3].im -= zr * bi + zi * br;
           }
-        }
-      } else {
-        const double nrm = sqrt(zsh[0]);
-        if (nrm == 0.0 && threadIdx.x == 0) atomicOr(fail, 1);
-        const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-        for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
-          const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
+          Store<double>::store_spinor(work, chunk, si, g.vbh, x);
+        } else {
           spinor<float> o;
 #pragma unroll
           for (int k = 0; k < 12; k++)
-            o.c[k / 3].c[k % 3] = mk<float>((float)(v[(2 * k) * nsite + t] * inv), (float)(v[(2 * k + 1) * nsite + t] * inv));
+            o.c[k / 3].c[k % 3] = mk<float>((float)(x.c[k / 3].c[k % 3].re * inv), (float)(x.c[k / 3].c[k % 3].im * inv));
           Store<float>::store_spinor(basis[l], chunk, si, g.vbh, o);
         }
       }
@@ -521,10 +520,9 @@ int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st) 
   cudaMallocAsync(&dfail, sizeof(int), st);
   cudaMemcpyAsync(dm, modes.data(), d.Ns * sizeof(void *), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(dfail, 0, sizeof(int), st);
-  size_t shm = (size_t)24 * 2 * c.g.vbh * sizeof(double);
-  if (shm > 200 * 1024) return fail("dfl_subspace: block too large for shared memory");
-  cudaFuncSetAttribute(k_dfl_gs, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  k_dfl_gs<<<d.nb, 256, shm, st>>>(c.g, d.vd2lex, (float4 *const *)d.d_basis, (const float4 *const *)dm, d.Ns, dfail);
+  if (!c.tmp64 && cudaMalloc(&c.tmp64, spinor_bytes(c, 64)) != cudaSuccess) return fail("out of device memory");
+  k_dfl_gs<<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (float4 *const *)d.d_basis, (const float4 *const *)dm, d.Ns,
+                                 (double2 *)c.tmp64, dfail);
   int hf = 0;
   cudaMemcpyAsync(&hf, dfail, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(dm, st);

@@ -19,7 +19,10 @@
 // neighbouring sites read (the current even residual, the odd intermediate,
 // the even solution) live in shared memory as 24 planes of vbh floats, the
 // Dhat image of the residual stays in registers, links and SW matrices come
-// through the L1 cache.
+// through the L1 cache.  Fields that only their own site reads (the odd
+// start vector of the eo solve, the solution of the plain solve) are kept in
+// the phi output field, so that blocks of up to 768 sites per parity (6^4
+// blocks among them) fit into shared memory.
 #include "lib.h"
 
 namespace qcd {
@@ -115,6 +118,7 @@ __device__ __forceinline__ void block_allreduce(double v[NC], double *red) {
 // site; with separate set-up, MR and reconstruction code the kernel
 // overflowed the instruction cache.
 //   step 0         : V = W = A_o^-1 rho_o ;  S1 = rho_e - D_eo W ; S0 = 0
+//                    (V is kept in phi_o until the last step)
 //   step 1..nmr    : W = A_o^-1 D_oe S1 ;  s2 = (A_e + i mu g5) S1 - D_eo W ;
 //                    z = (s2,S1)/|s2|^2 ; S0 += z S1 ; S1 -= z s2
 //   step nmr+1     : phi_o = V - A_o^-1 D_oe S0 ; phi_e = S0 ; psi += phi ;
@@ -124,7 +128,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
   extern __shared__ float smem[];
   const Geom &g = a.g;
   const int ld = g.vbh;
-  float *S1 = smem, *W = smem + 24 * ld, *S0 = smem + 48 * ld, *V = smem + 72 * ld;
+  float *S1 = smem, *W = smem + 24 * ld, *S0 = smem + 48 * ld;
   __shared__ double red[3 * 32];
   __shared__ float zsh[2];
   __shared__ int stop;
@@ -146,12 +150,12 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
         else h = block_hop(a, 1, blk, s, last ? S0 : S1, ld);
         spinor<float> t = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h);
         if (step == 0) {
-          sm_store(V, ld, s, t);
+          Store<float>::store_spinor(a.phi, co, s, g.vbh, t);
           sm_store(W, ld, s, t);
         } else if (!last) {
           sm_store(W, ld, s, t);
         } else {
-          spinor<float> ph = sm_load(V, ld, s);
+          spinor<float> ph = Store<float>::load_spinor_rw(a.phi, co, s, g.vbh);
           ssub(ph, t);
           spinor<float> ps = Store<float>::load_spinor_rw(a.psi, co, s, g.vbh);
           sadd(ps, ph);
@@ -272,9 +276,8 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
   extern __shared__ float smem[];
   const Geom &g = a.g;
   const int ld = g.vbh;
-  // planes: S1 even, S1 odd, S0 even, S0 odd
+  // planes: S1 even, S1 odd; the solution S0 accumulates in phi
   float *S1[2] = {smem, smem + 24 * ld};
-  float *S0[2] = {smem + 48 * ld, smem + 72 * ld};
   __shared__ double red[3 * 32];
   __shared__ float zsh[2];
   __shared__ int stop;
@@ -290,7 +293,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         sm_store(S1[p], ld, s, Store<float>::load_spinor_rw(a.rho, p * g.nbl + blk, s, g.vbh));
         spinor<float> z;
         szero(z);
-        sm_store(S0[p], ld, s, z);
+        Store<float>::store_spinor(a.phi, p * g.nbl + blk, s, g.vbh, z);
       }
     }
   if (threadIdx.x == 0) stop = 0;
@@ -336,7 +339,8 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
       for (int k = 0; k < NS; k++) {
         int s = threadIdx.x + k * T;
         if (s < g.vbh) {
-          spinor<float> s1 = sm_load(S1[p], ld, s), s0 = sm_load(S0[p], ld, s);
+          const int ch = p * g.nbl + blk;
+          spinor<float> s1 = sm_load(S1[p], ld, s), s0 = Store<float>::load_spinor_rw(a.phi, ch, s, g.vbh);
 #pragma unroll
           for (int c = 0; c < 4; c++)
 #pragma unroll
@@ -347,7 +351,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
               s1.c[c].c[j].re -= zr * x2.re - zi * x2.im;
               s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
             }
-          sm_store(S0[p], ld, s, s0);
+          Store<float>::store_spinor(a.phi, ch, s, g.vbh, s0);
           sm_store(S1[p], ld, s, s1);
         }
       }
@@ -359,11 +363,10 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
       int s = threadIdx.x + k * T;
       if (s < g.vbh) {
         int ch = p * g.nbl + blk;
-        spinor<float> s0 = sm_load(S0[p], ld, s);
+        spinor<float> s0 = Store<float>::load_spinor_rw(a.phi, ch, s, g.vbh);
         spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ch, s, g.vbh);
         sadd(ps, s0);
         Store<float>::store_spinor(a.psi, ch, s, g.vbh, ps);
-        Store<float>::store_spinor(a.phi, ch, s, g.vbh, s0);
         Store<float>::store_spinor(a.rho, ch, s, g.vbh, sm_load(S1[p], ld, s));
       }
     }
@@ -411,6 +414,9 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
   Store<float>::store_spinor(a.rho, chunk, s, g.vbh, rr);
 }
 
+// dynamic shared memory a block kernel may use (of 227 KB per CTA)
+static const int SAP_SMEM_MAX = 224 * 1024;
+
 static int pick_threads(int vbh, int &ns) {
   for (ns = 1; ns <= 3; ns++) {
     int t = ((vbh + ns - 1) / ns + 31) / 32 * 32;
@@ -425,16 +431,13 @@ int sap_prepare(Ctx &c, cudaStream_t st) {
   int ns;
   int t = pick_threads(c.g.vbh, ns);
   if (!t) return fail("sap: block volume too large (at most 1536 sites)");
-  size_t eo = (size_t)96 * c.g.vbh * sizeof(float), pl = (size_t)96 * c.g.vbh * sizeof(float);
-  if (eo > 200 * 1024 || pl > 200 * 1024) {
-    if (pl > 200 * 1024 && c.isolv == 0) return fail("sap: block too large for the plain MR solver");
-  }
-  cudaFuncSetAttribute(k_sap_blocks_eo<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sap_blocks_eo<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sap_blocks_eo<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sap_blocks_plain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sap_blocks_plain<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_sap_blocks_plain<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  const int lim = SAP_SMEM_MAX;
+  cudaFuncSetAttribute(k_sap_blocks_eo<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sap_blocks_eo<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sap_blocks_eo<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sap_blocks_plain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sap_blocks_plain<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_sap_blocks_plain<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   return 0;
 }
 
@@ -462,8 +465,8 @@ int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *
   a.u = c.u32;
   a.sw = c.sw32;
   a.swinv = c.sw32_inv;
-  size_t shm = (size_t)96 * c.g.vbh * sizeof(float);
-  if (shm > 200 * 1024) return fail("sap: block too large for shared memory");
+  size_t shm = (size_t)(isolv ? 72 : 48) * c.g.vbh * sizeof(float);
+  if (!t || shm > SAP_SMEM_MAX) return fail("sap: block too large for shared memory");
   int nbh = c.g.nbl / 2;
   size_t nb_sites = (size_t)nbh * c.g.vb;
   for (int ic = 0; ic < 2; ic++) {

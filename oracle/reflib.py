@@ -17,6 +17,7 @@ GEOMETRIES = {
     (8, 8, 8, 16): (4, 4, 4, 8),         # 16 threads
     (16, 8, 8, 8): (4, 4, 4, 8),         # 16 threads
     (16, 16, 16, 16): (8, 8, 8, 8),      # 16 threads
+    (12, 12, 12, 12): (6, 6, 12, 12),    # 4 threads (6^4 blocks)
     (64, 32, 32, 32): (32, 16, 16, 32),  # 8 threads
 }
 
