@@ -174,6 +174,15 @@ double fgcr(int vol, void (*Dop)(spinor_dble *s, spinor_dble *r), void (*Mop)(in
             spinor **ws, spinor_dble **wsd, int nkv, int nmx, int istop, double res, spinor_dble *eta,
             spinor_dble *psi, int *status);
 
+/* Storage precision of the links and SW matrices read by the even-odd SAP
+ * block solver (no reference counterpart): 32 (default) as the reference;
+ * 16 reads FP16 copies of them, with FP32 work vectors and arithmetic. */
+int b200_set_sap_prec(int bits);
+/* Launch variant of the SAP block kernel picked by the autotuner for the
+ * current block size (prec 32 or 16): index, threads per block, time of one
+ * cycle's block sweeps in ms. */
+int b200_sap_tuning(int prec, int *variant, int *threads, float *ms);
+
 /* ------------------------------------------- deflation (dfl.h, little.h) */
 /* Parameters of set_dfl_parms (modules/flags/dfl_parms.c:209; the DFL block
  * size must equal the geometry block size), set_dfl_pro_parms (:286) and

@@ -151,13 +151,16 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   if (!c.stream && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail("no CUDA device available");
   // a new geometry invalidates every resident field
-  void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage};
+  void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage,
+                  c.u16, c.sw16, c.sw16_inv};
   for (void *p : bufs) cudaFree(p);
   for (void *p : c.ws32) cudaFree(p);
   for (void *p : c.ws64) cudaFree(p);
   c.ws32.clear(); c.ws64.clear();
   c.ud = nullptr; c.u32 = nullptr; c.swd = c.swd_inv = nullptr; c.sw32 = c.sw32_inv = nullptr;
   c.tmp64 = c.tmp32 = c.stage = nullptr; c.stage_bytes = 0;
+  c.u16 = c.sw16 = c.sw16_inv = nullptr; c.h16_valid = false;
+  c.sap_tuned_vbh[0] = c.sap_tuned_vbh[1] = 0;
   c.have_ud = c.have_sw = false;
   qcd::dfl_release(c);
   c.ready = false;
@@ -183,6 +186,23 @@ int b200_set_sap_parms(const int bs[4], int isolv, int nmr, int ncy) {
   if (isolv < 0 || isolv > 1 || nmr < 1 || ncy < 1) return fail("set_sap_parms: parameters are out of range");
   c.isolv = isolv; c.nmr = nmr; c.ncy = ncy;
   c.sap_set = true;
+  return 0;
+}
+
+int b200_set_sap_prec(int bits) {
+  if (bits != 16 && bits != 32) return fail("set_sap_prec: the storage precision must be 16 or 32");
+  ctx().sap_prec = bits;
+  return 0;
+}
+
+int b200_sap_tuning(int prec, int *variant, int *threads, float *ms) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  const int slot = prec == 16 ? 1 : 0;
+  if (c.sap_tuned_vbh[slot] != c.g.vbh) return fail("sap_tuning: the SAP kernel is not tuned for this geometry yet");
+  *variant = c.sap_variant[slot];
+  *threads = qcd::sap_variant_threads(c, slot);
+  *ms = c.sap_tuned_ms[slot];
   return 0;
 }
 

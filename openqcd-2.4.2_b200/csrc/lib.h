@@ -59,6 +59,15 @@ struct Ctx {
   double2 *swd_inv = nullptr;   // FP64 inverse (mu = 0) on all sites
   float4 *sw32 = nullptr;       // FP32 copies (assign_swd2sw)
   float4 *sw32_inv = nullptr;
+  // FP16 copies for the SAP block solver in half-precision storage
+  // (links as __half2 planes, Pauli matrices as 4-half uint2 planes)
+  int sap_prec = 32;
+  void *u16 = nullptr, *sw16 = nullptr, *sw16_inv = nullptr;
+  bool h16_valid = false;
+  // SAP block-kernel launch variant chosen by the autotuner, per storage
+  // precision (0: FP32, 1: FP16), for the block size it was tuned on
+  int sap_variant[2] = {0, 0}, sap_tuned_vbh[2] = {0, 0};
+  float sap_tuned_ms[2] = {0.0f, 0.0f};
   bool have_ud = false, have_sw = false, sw_inv_ok = false;
   int sw_inv_fail = 0;
 
@@ -186,6 +195,7 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status);
 
 // sap.cu
 int sap_prepare(Ctx &c, cudaStream_t st);
+int sap_variant_threads(const Ctx &c, int slot);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
                cudaStream_t st);

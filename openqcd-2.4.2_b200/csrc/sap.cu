@@ -24,6 +24,7 @@
 // the phi output field, so that blocks of up to 768 sites per parity (6^4
 // blocks among them) fit into shared memory.
 #include "lib.h"
+#include <cuda_fp16.h>
 
 namespace qcd {
 
@@ -34,8 +35,8 @@ struct SapArgs {
   int nmr;
   int eoflg;
   float4 *psi, *rho, *phi;
-  const float2 *u;
-  const float4 *sw, *swinv;
+  const void *u;
+  const void *sw, *swinv;
 };
 
 // block of the given colour with in-colour index h (block lex index of the
@@ -47,25 +48,85 @@ __device__ __forceinline__ int block_of_colour(const Geom &g, int h, int colour)
   return q + (((n[0] + n[1] + n[2] + n[3]) & 1) != colour);
 }
 
-// shared-memory spinor planes: plane k (0..23 reals) at sm[k*ld + s]
-__device__ __forceinline__ spinor<float> sm_load(const float *sm, int ld, int s) {
-  spinor<float> r;
+// Storage policies of the block solver.  Both keep the block work vectors
+// in shared memory as 24 float planes (plane k at sm[k*ld + s]); SapF32
+// reads the FP32 links and Pauli matrices, SapF16 FP16 copies of them (links
+// as __half2 planes, Pauli matrices as uint2 planes of four halves), with
+// all arithmetic in FP32.  (FP16 work vectors were tried: their rounding,
+// relative to each cycle's input residual, is of the size of the residual
+// reduction of five cycles and cost half as many GCR iterations again.)
+struct SapF32 {
+  using T = float;
+  static constexpr int NP = 24;
+  __device__ __forceinline__ static spinor<float> sm_load(const float *sm, int ld, int s) {
+    spinor<float> r;
 #pragma unroll
-  for (int k = 0; k < 12; k++) r.c[k / 3].c[k % 3] = mk<float>(sm[(2 * k) * ld + s], sm[(2 * k + 1) * ld + s]);
-  return r;
-}
-__device__ __forceinline__ void sm_store(float *sm, int ld, int s, const spinor<float> &v) {
-#pragma unroll
-  for (int k = 0; k < 12; k++) {
-    sm[(2 * k) * ld + s] = v.c[k / 3].c[k % 3].re;
-    sm[(2 * k + 1) * ld + s] = v.c[k / 3].c[k % 3].im;
+    for (int k = 0; k < 12; k++) r.c[k / 3].c[k % 3] = mk<float>(sm[(2 * k) * ld + s], sm[(2 * k + 1) * ld + s]);
+    return r;
   }
-}
+  __device__ __forceinline__ static void sm_store(float *sm, int ld, int s, const spinor<float> &v) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      sm[(2 * k) * ld + s] = v.c[k / 3].c[k % 3].re;
+      sm[(2 * k + 1) * ld + s] = v.c[k / 3].c[k % 3].im;
+    }
+  }
+  __device__ __forceinline__ static su3<float> link(const void *u, int chunk, int mu, int s, int vbh) {
+    return Store<float>::load_link(u, chunk, mu, s, vbh);
+  }
+  __device__ __forceinline__ static spinor<float> sw(const void *m, int chunk, int s, int vbh, float mu,
+                                                     const spinor<float> &in) {
+    return apply_sw_site<float>(m, chunk, s, vbh, mu, in);
+  }
+};
+
+struct SapF16 {
+  using T = float;
+  static constexpr int NP = 24;
+  __device__ __forceinline__ static spinor<float> sm_load(const float *sm, int ld, int s) {
+    return SapF32::sm_load(sm, ld, s);
+  }
+  __device__ __forceinline__ static void sm_store(float *sm, int ld, int s, const spinor<float> &v) {
+    SapF32::sm_store(sm, ld, s, v);
+  }
+  __device__ __forceinline__ static su3<float> link(const void *u, int chunk, int mu, int s, int vbh) {
+    const __half2 *p = (const __half2 *)u + ((size_t)chunk * 4 + mu) * 9 * vbh + s;
+    su3<float> r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const float2 f = __half22float2(__ldg(p + (size_t)k * vbh));
+      r.e[k] = mk<float>(f.x, f.y);
+    }
+    return r;
+  }
+  __device__ __forceinline__ static spinor<float> sw(const void *m, int chunk, int s, int vbh, float mu,
+                                                     const spinor<float> &in) {
+    spinor<float> out;
+    float u[36];
+    cpx<float> w[6], r[6];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      const uint2 *p = (const uint2 *)m + ((size_t)chunk * 18 + 9 * half) * vbh + s;
+#pragma unroll
+      for (int j = 0; j < 9; j++) {
+        uint2 v = __ldg(p + (size_t)j * vbh);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&v.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&v.y));
+        u[4 * j] = a.x; u[4 * j + 1] = a.y; u[4 * j + 2] = b.x; u[4 * j + 3] = b.y;
+      }
+      weyl_get(in, half, w);
+      mul_pauli<float>(half == 0 ? mu : -mu, u, w, r);
+      weyl_put(out, half, r);
+    }
+    return out;
+  }
+};
 
 // -1/2 * H restricted to the block (Dirichlet exterior): hop terms of the
 // field in shared memory (parity 1-p) around site (p, s) of block blk.
-__device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int blk, int s, const float *src,
-                                                   int ld) {
+template <class P>
+__device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int blk, int s,
+                                                   const typename P::T *src, int ld) {
   const Geom &g = a.g;
   int y[4];
   unpack4(__ldg(g.lcoord + p * g.vbh + s), y);
@@ -77,14 +138,14 @@ __device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int 
   for (int mu = 0; mu < 4; mu++) {
     if (y[mu] + 1 < g.bs[mu]) {
       int s2 = (l + g.lstr[mu]) >> 1;
-      spinor<float> sp = sm_load(src, ld, s2);
-      su3<float> uu = Store<float>::load_link(a.u, chunk, mu, s, g.vbh);
+      spinor<float> sp = P::sm_load(src, ld, s2);
+      su3<float> uu = P::link(a.u, chunk, mu, s, g.vbh);
       hop_fwd<float>(mu, uu, sp, h);
     }
     if (y[mu] > 0) {
       int s2 = (l - g.lstr[mu]) >> 1;
-      spinor<float> sm = sm_load(src, ld, s2);
-      su3<float> uu = Store<float>::load_link(a.u, ochunk, mu, s2, g.vbh);
+      spinor<float> sm = P::sm_load(src, ld, s2);
+      su3<float> uu = P::link(a.u, ochunk, mu, s2, g.vbh);
       hop_bwd<float>(mu, uu, sm, h);
     }
   }
@@ -123,37 +184,41 @@ __device__ __forceinline__ void block_allreduce(double v[NC], double *red) {
 //                    z = (s2,S1)/|s2|^2 ; S0 += z S1 ; S1 -= z s2
 //   step nmr+1     : phi_o = V - A_o^-1 D_oe S0 ; phi_e = S0 ; psi += phi ;
 //                    rho_e = S1 ; rho_o = -i mu g5 phi_o (0 with the eo flag)
-template <int NS>
-__global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
-  extern __shared__ float smem[];
+template <int NS, class P, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
+  using T = typename P::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *smem = reinterpret_cast<T *>(smem_raw);
   const Geom &g = a.g;
   const int ld = g.vbh;
-  float *S1 = smem, *W = smem + 24 * ld, *S0 = smem + 48 * ld;
+  T *S1 = smem, *W = smem + P::NP * ld, *S0 = smem + 2 * P::NP * ld;
   __shared__ double red[3 * 32];
   __shared__ float zsh[2];
   __shared__ int stop;
   const int blk = block_of_colour(g, blockIdx.x, a.colour);
   const int ce = blk, co = g.nbl + blk;
-  const int T = blockDim.x;
+  const int T_ = blockDim.x;
   const int nmr = a.nmr;
   if (threadIdx.x == 0) stop = 0;
-
   for (int step = 0; step <= nmr + 1; step++) {
     const bool last = step == nmr + 1;
     // ---- odd sites
 #pragma unroll
     for (int k = 0; k < NS; k++) {
-      int s = threadIdx.x + k * T;
+      int s = threadIdx.x + k * T_;
       if (s < g.vbh) {
         spinor<float> h;
-        if (step == 0) h = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
-        else h = block_hop(a, 1, blk, s, last ? S0 : S1, ld);
-        spinor<float> t = apply_sw_site<float>(a.swinv, co, s, g.vbh, 0.0f, h);
+        if (step == 0) {
+          h = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
+        } else {
+          h = block_hop<P>(a, 1, blk, s, last ? S0 : S1, ld);
+        }
+        spinor<float> t = P::sw(a.swinv, co, s, g.vbh, 0.0f, h);
         if (step == 0) {
           Store<float>::store_spinor(a.phi, co, s, g.vbh, t);
-          sm_store(W, ld, s, t);
+          P::sm_store(W, ld, s, t);
         } else if (!last) {
-          sm_store(W, ld, s, t);
+          P::sm_store(W, ld, s, t);
         } else {
           spinor<float> ph = Store<float>::load_spinor_rw(a.phi, co, s, g.vbh);
           ssub(ph, t);
@@ -181,14 +246,15 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
     if (last) {
 #pragma unroll
       for (int k = 0; k < NS; k++) {
-        int s = threadIdx.x + k * T;
+        int s = threadIdx.x + k * T_;
         if (s < g.vbh) {
-          spinor<float> s0 = sm_load(S0, ld, s);
+          spinor<float> s0 = P::sm_load(S0, ld, s);
+          spinor<float> r1 = P::sm_load(S1, ld, s);
           spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ce, s, g.vbh);
           sadd(ps, s0);
           Store<float>::store_spinor(a.psi, ce, s, g.vbh, ps);
           Store<float>::store_spinor(a.phi, ce, s, g.vbh, s0);
-          Store<float>::store_spinor(a.rho, ce, s, g.vbh, sm_load(S1, ld, s));
+          Store<float>::store_spinor(a.rho, ce, s, g.vbh, r1);
         }
       }
       break;
@@ -197,19 +263,19 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
     double v[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < NS; k++) {
-      int s = threadIdx.x + k * T;
+      int s = threadIdx.x + k * T_;
       if (s < g.vbh) {
-        spinor<float> hw = block_hop(a, 0, blk, s, W, ld);
+        spinor<float> hw = block_hop<P>(a, 0, blk, s, W, ld);
         if (step == 0) {
           spinor<float> r = Store<float>::load_spinor_rw(a.rho, ce, s, g.vbh);
           ssub(r, hw);
-          sm_store(S1, ld, s, r);
+          P::sm_store(S1, ld, s, r);
           spinor<float> z;
           szero(z);
-          sm_store(S0, ld, s, z);
+          P::sm_store(S0, ld, s, z);
         } else {
-          spinor<float> s1 = sm_load(S1, ld, s);
-          s2[k] = apply_sw_site<float>(a.sw, ce, s, g.vbh, a.mu, s1);
+          spinor<float> s1 = P::sm_load(S1, ld, s);
+          s2[k] = P::sw(a.sw, ce, s, g.vbh, a.mu, s1);
           ssub(s2[k], hw);
 #pragma unroll
           for (int c = 0; c < 4; c++)
@@ -247,9 +313,9 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
     const float zr = zsh[0], zi = zsh[1];
 #pragma unroll
     for (int k = 0; k < NS; k++) {
-      int s = threadIdx.x + k * T;
+      int s = threadIdx.x + k * T_;
       if (s < g.vbh) {
-        spinor<float> s1 = sm_load(S1, ld, s), s0 = sm_load(S0, ld, s);
+        spinor<float> s1 = P::sm_load(S1, ld, s), s0 = P::sm_load(S0, ld, s);
 #pragma unroll
         for (int c = 0; c < 4; c++)
 #pragma unroll
@@ -260,8 +326,8 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
             s1.c[c].c[j].re -= zr * x2.re - zi * x2.im;
             s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
           }
-        sm_store(S0, ld, s, s0);
-        sm_store(S1, ld, s, s1);
+        P::sm_store(S0, ld, s, s0);
+        P::sm_store(S1, ld, s, s1);
       }
     }
     __syncthreads();
@@ -273,7 +339,9 @@ __global__ void __launch_bounds__(256) k_sap_blocks_eo(SapArgs a) {
 // registers.  Sites are handled as (parity, s) pairs.
 template <int NS>
 __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
-  extern __shared__ float smem[];
+  using P = SapF32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float *smem = reinterpret_cast<float *>(smem_raw);
   const Geom &g = a.g;
   const int ld = g.vbh;
   // planes: S1 even, S1 odd; the solution S0 accumulates in phi
@@ -290,7 +358,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T;
       if (s < g.vbh) {
-        sm_store(S1[p], ld, s, Store<float>::load_spinor_rw(a.rho, p * g.nbl + blk, s, g.vbh));
+        P::sm_store(S1[p], ld, s, Store<float>::load_spinor_rw(a.rho, p * g.nbl + blk, s, g.vbh));
         spinor<float> z;
         szero(z);
         Store<float>::store_spinor(a.phi, p * g.nbl + blk, s, g.vbh, z);
@@ -307,9 +375,9 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
       for (int k = 0; k < NS; k++) {
         int s = threadIdx.x + k * T;
         if (s < g.vbh) {
-          spinor<float> s1 = sm_load(S1[p], ld, s);
+          spinor<float> s1 = P::sm_load(S1[p], ld, s);
           s2[p][k] = apply_sw_site<float>(a.sw, p * g.nbl + blk, s, g.vbh, p ? muo : a.mu, s1);
-          sadd(s2[p][k], block_hop(a, p, blk, s, S1[1 - p], ld));
+          sadd(s2[p][k], block_hop<P>(a, p, blk, s, S1[1 - p], ld));
 #pragma unroll
           for (int c = 0; c < 4; c++)
 #pragma unroll
@@ -340,7 +408,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         int s = threadIdx.x + k * T;
         if (s < g.vbh) {
           const int ch = p * g.nbl + blk;
-          spinor<float> s1 = sm_load(S1[p], ld, s), s0 = Store<float>::load_spinor_rw(a.phi, ch, s, g.vbh);
+          spinor<float> s1 = P::sm_load(S1[p], ld, s), s0 = Store<float>::load_spinor_rw(a.phi, ch, s, g.vbh);
 #pragma unroll
           for (int c = 0; c < 4; c++)
 #pragma unroll
@@ -352,7 +420,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
               s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
             }
           Store<float>::store_spinor(a.phi, ch, s, g.vbh, s0);
-          sm_store(S1[p], ld, s, s1);
+          P::sm_store(S1[p], ld, s, s1);
         }
       }
     __syncthreads();
@@ -367,7 +435,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ch, s, g.vbh);
         sadd(ps, s0);
         Store<float>::store_spinor(a.psi, ch, s, g.vbh, ps);
-        Store<float>::store_spinor(a.rho, ch, s, g.vbh, sm_load(S1[p], ld, s));
+        Store<float>::store_spinor(a.rho, ch, s, g.vbh, P::sm_load(S1[p], ld, s));
       }
     }
 }
@@ -375,6 +443,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
 // rho(y) -= D_{y,x} phi(x) for every site y of a block of colour 1-c and every
 // neighbour x of y in a (colour c) block: the block-boundary hop of the
 // reference's Dw_bnd/sap_com, as a gather.
+template <class P>
 __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
   const Geom &g = a.g;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -394,7 +463,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
       int c2, s2;
       site_nbr(g, x, mu, +1, c2, s2);
       spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = Store<float>::load_link(a.u, chunk, mu, s, g.vbh);
+      su3<float> uu = P::link(a.u, chunk, mu, s, g.vbh);
       hop_fwd<float>(mu, uu, sp, hsum);
       any = true;
     }
@@ -402,7 +471,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
       int c2, s2;
       site_nbr(g, x, mu, -1, c2, s2);
       spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = Store<float>::load_link(a.u, c2, mu, s2, g.vbh);
+      su3<float> uu = P::link(a.u, c2, mu, s2, g.vbh);
       hop_bwd<float>(mu, uu, sm, hsum);
       any = true;
     }
@@ -417,6 +486,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
 // dynamic shared memory a block kernel may use (of 227 KB per CTA)
 static const int SAP_SMEM_MAX = 224 * 1024;
 
+// Threads of the plain block kernel: up to three sites per thread.
 static int pick_threads(int vbh, int &ns) {
   for (ns = 1; ns <= 3; ns++) {
     int t = ((vbh + ns - 1) / ns + 31) / 32 * 32;
@@ -426,19 +496,166 @@ static int pick_threads(int vbh, int &ns) {
   return 0;
 }
 
-int sap_prepare(Ctx &c, cudaStream_t st) {
-  (void)st;
-  int ns;
-  int t = pick_threads(c.g.vbh, ns);
-  if (!t) return fail("sap: block volume too large (at most 1536 sites)");
-  const int lim = SAP_SMEM_MAX;
-  cudaFuncSetAttribute(k_sap_blocks_eo<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_sap_blocks_eo<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_sap_blocks_eo<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_sap_blocks_plain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_sap_blocks_plain<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_sap_blocks_plain<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+// FP16 copies of the FP32 links and Pauli matrices, same plane indexing
+__global__ void k_to_half2(size_t n, const float2 *__restrict__ a, __half2 *b) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = __float22half2_rn(__ldg(a + i));
+}
+__global__ void k_to_half4(size_t n, const float4 *__restrict__ a, uint2 *b) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) {
+    const float4 v = __ldg(a + i);
+    __half2 x = __floats2half2_rn(v.x, v.y), y = __floats2half2_rn(v.z, v.w);
+    b[i] = make_uint2(*reinterpret_cast<unsigned *>(&x), *reinterpret_cast<unsigned *>(&y));
+  }
+}
+
+static int sap_half_fields(Ctx &c, cudaStream_t st) {
+  if (c.h16_valid) return 0;
+  const size_t nl = (size_t)c.g.vol * 36, np = (size_t)c.g.vol * 18;
+  if (!c.u16 && cudaMalloc(&c.u16, nl * sizeof(__half2)) != cudaSuccess) return fail("out of device memory (FP16 links)");
+  if (!c.sw16 && cudaMalloc(&c.sw16, np * sizeof(uint2)) != cudaSuccess) return fail("out of device memory (FP16 SW)");
+  if (!c.sw16_inv && cudaMalloc(&c.sw16_inv, np * sizeof(uint2)) != cudaSuccess)
+    return fail("out of device memory (FP16 SW)");
+  k_to_half2<<<(unsigned)((nl + 255) / 256), 256, 0, st>>>(nl, c.u32, (__half2 *)c.u16);
+  k_to_half4<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(np, c.sw32, (uint2 *)c.sw16);
+  k_to_half4<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(np, c.sw32_inv, (uint2 *)c.sw16_inv);
+  if (cudaGetLastError() != cudaSuccess) return fail("sap: FP16 conversion failed");
+  c.h16_valid = true;
   return 0;
+}
+
+// Launch variants of the even-odd block kernel: sites per thread, the
+// launch bound and the register budget it implies.  The autotuner below
+// times every variant that fits the block on the resident fields and keeps
+// the fastest per block size and storage precision.
+struct EoVariant {
+  int ns, maxt;
+  void (*f32)(SapArgs);
+  void (*f16)(SapArgs);
+};
+static const EoVariant kEo[] = {
+    {1, 256, k_sap_blocks_eo<1, SapF32, 256, 2>, k_sap_blocks_eo<1, SapF16, 256, 2>},
+    {1, 672, k_sap_blocks_eo<1, SapF32, 672, 1>, k_sap_blocks_eo<1, SapF16, 672, 1>},
+    {2, 384, k_sap_blocks_eo<2, SapF32, 384, 1>, k_sap_blocks_eo<2, SapF16, 384, 1>},
+    {3, 256, k_sap_blocks_eo<3, SapF32, 256, 1>, k_sap_blocks_eo<3, SapF16, 256, 1>},
+};
+static const int kNEo = sizeof(kEo) / sizeof(kEo[0]);
+
+static int eo_threads(const EoVariant &v, int vbh) {
+  int t = ((vbh + v.ns - 1) / v.ns + 31) / 32 * 32;
+  return t > v.maxt ? 0 : t;
+}
+
+static size_t eo_smem(int vbh, bool half) {
+  (void)half;
+  return (size_t)vbh * 72 * sizeof(float);
+}
+
+static void launch_blocks(Ctx &c, const SapArgs &a, int isolv, bool half, cudaStream_t st) {
+  const int nbh = c.g.nbl / 2;
+  if (isolv) {
+    const EoVariant &v = kEo[c.sap_variant[half ? 1 : 0]];
+    const int t = eo_threads(v, c.g.vbh);
+    (half ? v.f16 : v.f32)<<<nbh, t, eo_smem(c.g.vbh, half), st>>>(a);
+  } else {
+    int ns;
+    int t = pick_threads(c.g.vbh, ns);
+    const size_t shm = (size_t)48 * c.g.vbh * sizeof(float);
+    if (ns == 1) k_sap_blocks_plain<1><<<nbh, t, shm, st>>>(a);
+    else if (ns == 2) k_sap_blocks_plain<2><<<nbh, t, shm, st>>>(a);
+    else k_sap_blocks_plain<3><<<nbh, t, shm, st>>>(a);
+  }
+}
+
+static SapArgs sap_args(Ctx &c, float mu, int nmr, bool half, void *psi, void *rho, void *phi) {
+  SapArgs a;
+  a.g = c.g;
+  a.colour = 0;
+  a.mu = mu;
+  a.nmr = nmr;
+  a.eoflg = c.eoflg;
+  a.psi = (float4 *)psi;
+  a.rho = (float4 *)rho;
+  a.phi = (float4 *)phi;
+  a.u = half ? (const void *)c.u16 : (const void *)c.u32;
+  a.sw = half ? (const void *)c.sw16 : (const void *)c.sw32;
+  a.swinv = half ? (const void *)c.sw16_inv : (const void *)c.sw32_inv;
+  return a;
+}
+
+// Time every fitting variant of the even-odd block kernel (both colours, 4
+// MR steps, on a random residual) and keep the fastest.
+static int sap_autotune(Ctx &c, bool half, cudaStream_t st) {
+  const int slot = half ? 1 : 0;
+  if (c.sap_tuned_vbh[slot] == c.g.vbh) return 0;
+  for (int i = 0; i < kNEo; i++) {
+    cudaFuncSetAttribute(kEo[i].f32, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+    cudaFuncSetAttribute(kEo[i].f16, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+  }
+  if (eo_smem(c.g.vbh, half) > (size_t)SAP_SMEM_MAX) return fail("sap: block too large for shared memory");
+  const size_t nb = spinor_bytes(c, 32);
+  void *psi = nullptr, *rho = nullptr, *phi = nullptr;
+  if (cudaMallocAsync(&psi, nb, st) != cudaSuccess || cudaMallocAsync(&rho, nb, st) != cudaSuccess ||
+      cudaMallocAsync(&phi, nb, st) != cudaSuccess)
+    return fail("sap: out of device memory (autotuning)");
+  cudaMemsetAsync(psi, 0, nb, st);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = -1;
+  float best_ms = 0.0f;
+  for (int i = 0; i < kNEo; i++) {
+    if (!eo_threads(kEo[i], c.g.vbh)) continue;
+    c.sap_variant[slot] = i;
+    SapArgs a = sap_args(c, 0.0f, 4, half, psi, rho, phi);
+    float tot = 0.0f;
+    for (int rep = 0; rep < 4; rep++) {
+      gen_uniform_spinor32(c, rho, 977ull + rep, st);
+      cudaEventRecord(e0, st);
+      for (int ic = 0; ic < 2; ic++) {
+        a.colour = ic;
+        launch_blocks(c, a, 1, half, st);
+      }
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) tot += ms;   // the first run warms up
+    }
+    if (cudaGetLastError() != cudaSuccess) continue;   // a variant that cannot launch is skipped
+    if (best < 0 || tot < best_ms) {
+      best = i;
+      best_ms = tot;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(psi, st);
+  cudaFreeAsync(rho, st);
+  cudaFreeAsync(phi, st);
+  if (best < 0) return fail("sap: no block-kernel variant fits this block size");
+  c.sap_variant[slot] = best;
+  c.sap_tuned_vbh[slot] = c.g.vbh;
+  c.sap_tuned_ms[slot] = best_ms / 3.0f;
+  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : fail("sap: CUDA error while autotuning");
+}
+
+int sap_variant_threads(const Ctx &c, int slot) { return eo_threads(kEo[c.sap_variant[slot]], c.g.vbh); }
+
+int sap_prepare(Ctx &c, cudaStream_t st) {
+  int ns;
+  if (!pick_threads(c.g.vbh, ns)) return fail("sap: block volume too large (at most 1536 sites)");
+  static bool attrs = false;
+  if (!attrs) {
+    cudaFuncSetAttribute(k_sap_blocks_plain<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+    cudaFuncSetAttribute(k_sap_blocks_plain<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+    cudaFuncSetAttribute(k_sap_blocks_plain<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+    attrs = true;
+  }
+  const bool half = c.sap_prec == 16;
+  if (half && sap_half_fields(c, st)) return -1;
+  return sap_autotune(c, half, st);
 }
 
 // ncy SAP cycles sap(mu, isolv, nmr, psi, rho) on FP32 device fields
@@ -450,37 +667,24 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
 }
 
 // One SAP cycle sap(mu, isolv, nmr, psi, rho) on FP32 device fields.
-// phi_blk is a scratch FP32 field.
+// phi_blk is a scratch FP32 field.  With the FP16 storage option the
+// even-odd block solver runs on FP16 copies of the links and SW matrices and
+// FP16 work vectors (the plain solver, isolv = 0, always runs in FP32).
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st) {
+  const bool half = isolv && c.sap_prec == 16;
+  if (isolv && c.sap_tuned_vbh[half ? 1 : 0] != c.g.vbh && sap_prepare(c, st)) return -1;
+  if (half && !c.h16_valid && sap_half_fields(c, st)) return -1;
   int ns;
-  int t = pick_threads(c.g.vbh, ns);
-  SapArgs a;
-  a.g = c.g;
-  a.mu = mu;
-  a.nmr = nmr;
-  a.eoflg = c.eoflg;
-  a.psi = (float4 *)psi;
-  a.rho = (float4 *)rho;
-  a.phi = (float4 *)phi_blk;
-  a.u = c.u32;
-  a.sw = c.sw32;
-  a.swinv = c.sw32_inv;
-  size_t shm = (size_t)(isolv ? 72 : 48) * c.g.vbh * sizeof(float);
-  if (!t || shm > SAP_SMEM_MAX) return fail("sap: block too large for shared memory");
-  int nbh = c.g.nbl / 2;
-  size_t nb_sites = (size_t)nbh * c.g.vb;
+  if (!pick_threads(c.g.vbh, ns) || (!isolv && (size_t)48 * c.g.vbh * sizeof(float) > (size_t)SAP_SMEM_MAX))
+    return fail("sap: block too large");
+  SapArgs a = sap_args(c, mu, nmr, half, psi, rho, phi_blk);
+  const size_t nb_sites = (size_t)(c.g.nbl / 2) * c.g.vb;
+  const unsigned nbnd = (unsigned)((nb_sites + 127) / 128);
   for (int ic = 0; ic < 2; ic++) {
     a.colour = ic;
-    if (isolv) {
-      if (ns == 1) k_sap_blocks_eo<1><<<nbh, t, shm, st>>>(a);
-      else if (ns == 2) k_sap_blocks_eo<2><<<nbh, t, shm, st>>>(a);
-      else k_sap_blocks_eo<3><<<nbh, t, shm, st>>>(a);
-    } else {
-      if (ns == 1) k_sap_blocks_plain<1><<<nbh, t, shm, st>>>(a);
-      else if (ns == 2) k_sap_blocks_plain<2><<<nbh, t, shm, st>>>(a);
-      else k_sap_blocks_plain<3><<<nbh, t, shm, st>>>(a);
-    }
-    k_sap_bnd<<<(unsigned)((nb_sites + 127) / 128), 128, 0, st>>>(a);
+    launch_blocks(c, a, isolv, half, st);
+    if (half) k_sap_bnd<SapF16><<<nbnd, 128, 0, st>>>(a);
+    else k_sap_bnd<SapF32><<<nbnd, 128, 0, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
 }

@@ -132,6 +132,7 @@ int sw_refresh_derived(Ctx &c, cudaStream_t st) {
   cudaFreeAsync(dfail, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return fail("sw_refresh_derived: CUDA error");
   c.sw_inv_fail = hf;   // bit 0: even sites unsafe, bit 1: odd sites unsafe
+  c.h16_valid = false;
   c.sw_inv_ok = (hf == 0);
   c.have_sw = true;
   return 0;
@@ -354,6 +355,7 @@ int links_refresh_f32(Ctx &c, cudaStream_t st) {
   size_t n = (size_t)c.g.vol * 36;
   if (!c.u32 && cudaMalloc(&c.u32, n * sizeof(float2)) != cudaSuccess) return fail("out of device memory (links)");
   k_links_f32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, c.ud, c.u32);
+  c.h16_valid = false;
   return cudaGetLastError() == cudaSuccess ? 0 : fail("links_refresh_f32: launch failed");
 }
 

@@ -98,6 +98,8 @@ _SIGS = {
     "fgcr": (C.c_double, [C.c_int, DOP_T, MOP_T, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
                           C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_clear_error": (None, []),
+    "b200_set_sap_prec": (C.c_int, [C.c_int]),
+    "b200_sap_tuning": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_set_dfl_parms": (C.c_int, [C.c_void_p, C.c_int]),
     "b200_set_dfl_pro_parms": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]),
     "b200_set_dfl_gen_parms": (C.c_int, [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
@@ -205,6 +207,16 @@ def set_parms(csw, m0, eoflg=0, bc=3):
 def set_sap_parms(bs, isolv, nmr, ncy):
     b = np.ascontiguousarray(bs, dtype=np.int32)
     return check(lib().b200_set_sap_parms(_ptr(b), isolv, nmr, ncy))
+
+
+def set_sap_prec(bits):
+    return check(lib().b200_set_sap_prec(bits))
+
+
+def sap_tuning(prec):
+    v, t, ms = C.c_int(0), C.c_int(0), C.c_float(0.0)
+    check(lib().b200_sap_tuning(prec, C.byref(v), C.byref(t), C.byref(ms)))
+    return v.value, t.value, ms.value
 
 
 def upload_ud(ud):
@@ -323,6 +335,16 @@ def dev_sap_gcr(nkv, nmx, istop, res, mu, eta, psi):
     if rho < 0:
         raise B200Error(_err_after())
     return rho, ifail.value, status.value
+
+
+def dev_dfl_sap_gcr(nkv, nmx, istop, res, mu, eta, psi):
+    ifail = C.c_int(0)
+    status = (C.c_int * 3)()
+    lib().b200_clear_error()
+    rho = lib().b200_dev_dfl_sap_gcr(nkv, nmx, istop, res, mu, eta.ptr, psi.ptr, C.byref(ifail), status)
+    if rho < 0:
+        raise B200Error(_err_after())
+    return rho, ifail.value, list(status)
 
 
 def sap_gcr(nkv, nmx, istop, res, mu, eta):
