@@ -192,6 +192,12 @@ int b200_set_dfl_pro_parms(int nkv, int nmx, double res, int nmx_gcr, double res
 int b200_set_dfl_gen_parms(double kappa, double mu, int ninv, int nmr, int ncy);
 /* Ns * (number of DFL blocks): the length of a little vector. */
 int b200_dfl_nv(void);
+/* Phase timers of the deflation code (no reference counterpart): with on=1
+ * the stream is synchronised at phase boundaries and seconds are summed into
+ * six slots (SAP smoothing of the modes, block Gram-Schmidt, little operator
+ * set-up, little solves, SAP in the preconditioner and inverse iteration,
+ * the rest); out (6 doubles, may be NULL) receives the sums so far. */
+int b200_dfl_profile(int on, double *out);
 /* Basis vector l of every block as one global FP32 field, reference layout. */
 int b200_dfl_set_basis(int l, const spinor *field);
 int b200_dfl_get_basis(int l, spinor *field);

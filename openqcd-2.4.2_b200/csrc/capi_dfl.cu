@@ -103,6 +103,17 @@ int b200_set_dfl_gen_parms(double kappa, double mu, int ninv, int nmr, int ncy) 
   return 0;
 }
 
+int b200_dfl_profile(int on, double *out) {
+  qcd::DflState &d = ctx().dfl;
+  if (out)
+    for (int k = 0; k < 6; k++) out[k] = d.prof[k];
+  if (on && !d.profile)
+    for (int k = 0; k < 6; k++) d.prof[k] = 0.0;
+  d.profile = on != 0;
+  d.prof_t0 = 0.0;
+  return 0;
+}
+
 int b200_dfl_nv(void) { return ctx().dfl.ready ? ctx().dfl.nv : 0; }
 
 // Load basis vector l of every block from a global field in the reference

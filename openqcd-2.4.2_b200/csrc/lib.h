@@ -28,6 +28,12 @@ struct DflState {
   int awhat_fail = 0, aw_eo = 0;
   double aw_mu = 0.0;
   std::vector<double2 *> lv, lvd;
+  // phase timers (seconds): 0 SAP smoothing of the modes, 1 block
+  // Gram-Schmidt, 2 little operator set-up, 3 little solves, 4 SAP in the
+  // deflated preconditioner and inverse iteration, 5 everything else
+  bool profile = false;
+  double prof[6] = {0, 0, 0, 0, 0, 0};
+  double prof_t0 = 0.0;
 };
 
 // Everything the reference keeps in module-global state for this path:

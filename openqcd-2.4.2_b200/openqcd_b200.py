@@ -104,6 +104,7 @@ _SIGS = {
     "b200_set_dfl_pro_parms": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]),
     "b200_set_dfl_gen_parms": (C.c_int, [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
     "b200_dfl_nv": (C.c_int, []),
+    "b200_dfl_profile": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "dfl_modes": (None, [C.c_void_p, C.c_void_p]),
@@ -439,6 +440,16 @@ def set_dfl_pro_parms(nkv, nmx, res, nmx_gcr, res_gcr):
 
 def set_dfl_gen_parms(kappa, mu, ninv, nmr, ncy):
     return check(lib().b200_set_dfl_gen_parms(kappa, mu, ninv, nmr, ncy))
+
+
+DFL_PHASES = ["sap_smoothing", "gram_schmidt", "little_setup", "little_solve", "sap", "other"]
+
+
+def dfl_profile(on):
+    """Switch the deflation phase timers on or off; returns the sums so far."""
+    out = np.zeros(6)
+    check(lib().b200_dfl_profile(1 if on else 0, _ptr(out)))
+    return dict(zip(DFL_PHASES, out.tolist()))
 
 
 def dfl_set_basis(l, field):
