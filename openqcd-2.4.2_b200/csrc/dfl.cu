@@ -15,6 +15,7 @@
 // matrices are stored column-major (entry (k,l) at [l*Ns + k]) so that the
 // threads of a block, one per row k, read consecutive words.
 #include "lib.h"
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <chrono>
@@ -77,6 +78,28 @@ static int dfl_alloc(Ctx &c) {
   };
   up(d.vd2lex, v2l);
   up(d.nbr, nbr);
+  // sites (p << 16 | s) of a block on each of its 8 faces, block-local
+  {
+    const int *bs = c.g.bs;
+    int fmax = 0;
+    for (int mu = 0; mu < 4; mu++) fmax = std::max(fmax, c.g.vb / bs[mu]);
+    std::vector<int> fs(8 * fmax, 0), nf(8, 0);
+    for (int y0 = 0; y0 < bs[0]; y0++)
+      for (int y1 = 0; y1 < bs[1]; y1++)
+        for (int y2 = 0; y2 < bs[2]; y2++)
+          for (int y3 = 0; y3 < bs[3]; y3++) {
+            const int y[4] = {y0, y1, y2, y3};
+            const int l = ((y0 * bs[1] + y1) * bs[2] + y2) * bs[3] + y3;
+            const int p = (y0 + y1 + y2 + y3) & 1;
+            for (int ifc = 0; ifc < 8; ifc++) {
+              const int mu = ifc >> 1;
+              if (y[mu] == ((ifc & 1) ? bs[mu] - 1 : 0)) fs[ifc * fmax + nf[ifc]++] = (p << 16) | (l >> 1);
+            }
+          }
+    up(d.faces, fs);
+    up(d.nfc, nf);
+    d.fmax = fmax;
+  }
   // basis and matrices
   while ((int)d.basis.size() < Ns) {
     void *p = nullptr;
@@ -301,6 +324,149 @@ __global__ void k_dfl_dapply(Geom g, const float4 *__restrict__ w, double2 *t, c
   Store<double>::store_spinor(t, chunk, si, g.vbh, acc);
 }
 
+// Little operator by block-local products (Aw_blk.c:242 set_Awblk and
+// Aw_hop.c:279 set_Awhop restated as small dense products).  CTA (n, 0)
+// computes Ablk[n](k,l) = (b_k, D_blk b_l) over the sites of block n, with
+// D_blk the SW term plus the hops inside the block; CTA (n, 1+ifc) computes
+// Ahop[n][ifc](k,l) = (b_k, H_ifc b_l) over the sites of block n on face
+// ifc, H_ifc the hop from the neighbouring block across that face.  The
+// sites are taken TS at a time: D b_l on the tile for all l goes to shared
+// memory in FP64 (Y), the basis on the tile in FP32 (B), and every thread
+// accumulates a 2x2 tile of (k,l) pairs in FP64.  Rows are stored in pairs
+// (l even, l odd interleaved) and padded to an odd length so that the
+// 16-byte loads of B by consecutive k are free of bank conflicts.
+template <int TS, int MAXT>
+__global__ void __launch_bounds__(256) k_aw_tiles(Geom g, const int *__restrict__ vd2lex,
+                                                  const float4 *const *__restrict__ basis, int Ns,
+                                                  const double2 *__restrict__ ud, const double2 *__restrict__ swd,
+                                                  double mu_e, double mu_o, const int *__restrict__ faces,
+                                                  const int *__restrict__ nfc, int fmax, double2 *Ablk,
+                                                  double2 *Ahop) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  constexpr int LD = TS * 12 + 1;
+  const int NT = Ns / 2;
+  double2 *Y = (double2 *)smraw;                         // [NT][LD][2]
+  float4 *B = (float4 *)(Y + (size_t)NT * LD * 2);       // [NT][LD]
+  const int n = blockIdx.x, blk = __ldg(vd2lex + n);
+  const int ifc = (int)blockIdx.y - 1;
+  const int nsites = ifc < 0 ? 2 * g.vbh : __ldg(nfc + ifc);
+  const int ntile = NT * NT;
+  double acc[MAXT][4][2];
+#pragma unroll
+  for (int j = 0; j < MAXT; j++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[j][q][0] = acc[j][q][1] = 0.0;
+
+  for (int t0 = 0; t0 < nsites; t0 += TS) {
+    // D b_l and b_l on the tile sites
+    for (int it = threadIdx.x; it < TS * Ns; it += blockDim.x) {
+      const int i = it % TS, l = it / TS, t = t0 + i;
+      spinor<double> y;
+      spinor<float> b;
+      szero(y);
+      szero(b);
+      if (t < nsites) {
+        int p, s;
+        if (ifc < 0) {
+          p = t >= g.vbh;
+          s = t - p * g.vbh;
+        } else {
+          const int f = __ldg(faces + ifc * fmax + t);
+          p = f >> 16;
+          s = f & 0xffff;
+        }
+        const int chunk = p * g.nbl + blk;
+        Site x;
+        site_decode(g, p, blk, s, x);
+        const float4 *bl = basis[l];
+        b = Store<float>::load_spinor(bl, chunk, s, g.vbh);
+        spinor<double> h;
+        szero(h);
+        if (ifc < 0) {
+          spinor<double> bd;
+#pragma unroll
+          for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) bd.c[a].c[k] = mk<double>(b.c[a].c[k].re, b.c[a].c[k].im);
+          y = apply_sw_site<double>(swd, chunk, s, g.vbh, p ? mu_o : mu_e, bd);
+#pragma unroll
+          for (int mu = 0; mu < 4; mu++)
+#pragma unroll
+            for (int dd = 0; dd < 2; dd++) {
+              const int dir = dd ? 1 : -1;
+              if (crosses_block(g, x, mu, dir)) continue;
+              int c2, s2;
+              site_nbr(g, x, mu, dir, c2, s2);
+              const spinor<float> nf = Store<float>::load_spinor(bl, c2, s2, g.vbh);
+              spinor<double> nd;
+#pragma unroll
+              for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int k = 0; k < 3; k++) nd.c[a].c[k] = mk<double>(nf.c[a].c[k].re, nf.c[a].c[k].im);
+              if (dir > 0) hop_fwd<double>(mu, Store<double>::load_link(ud, chunk, mu, s, g.vbh), nd, h);
+              else hop_bwd<double>(mu, Store<double>::load_link(ud, c2, mu, s2, g.vbh), nd, h);
+            }
+        } else {
+          const int mu = ifc >> 1, dir = (ifc & 1) ? 1 : -1;
+          int c2, s2;
+          site_nbr(g, x, mu, dir, c2, s2);
+          const spinor<float> nf = Store<float>::load_spinor(bl, c2, s2, g.vbh);
+          spinor<double> nd;
+#pragma unroll
+          for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) nd.c[a].c[k] = mk<double>(nf.c[a].c[k].re, nf.c[a].c[k].im);
+          if (dir > 0) hop_fwd<double>(mu, Store<double>::load_link(ud, chunk, mu, s, g.vbh), nd, h);
+          else hop_bwd<double>(mu, Store<double>::load_link(ud, c2, mu, s2, g.vbh), nd, h);
+        }
+        sscale<double>(h, -0.5);
+        sadd(y, h);
+      }
+      double2 *yd = Y + ((size_t)(l >> 1) * LD + i * 12) * 2 + (l & 1);
+      float2 *bd = (float2 *)(B + (size_t)(l >> 1) * LD + i * 12) + (l & 1);
+#pragma unroll
+      for (int k = 0; k < 12; k++) {
+        yd[2 * k] = make_double2(y.c[k / 3].c[k % 3].re, y.c[k / 3].c[k % 3].im);
+        bd[2 * k] = make_float2(b.c[k / 3].c[k % 3].re, b.c[k / 3].c[k % 3].im);
+      }
+    }
+    __syncthreads();
+    // (k,l) pairs: thread tile (kt, lt) holds k = 2kt, 2kt+1 and l = 2lt, 2lt+1
+#pragma unroll
+    for (int j = 0; j < MAXT; j++) {
+      const int q = threadIdx.x + j * blockDim.x;
+      if (q < ntile) {
+        const int kt = q % NT, lt = q / NT;
+        const float4 *bp = B + (size_t)kt * LD;
+        const double2 *yp = Y + (size_t)lt * LD * 2;
+        for (int e = 0; e < TS * 12; e++) {
+          const float4 bb = bp[e];
+          const double2 y0 = yp[2 * e], y1 = yp[2 * e + 1];
+          const double b0r = bb.x, b0i = bb.y, b1r = bb.z, b1i = bb.w;
+          acc[j][0][0] += b0r * y0.x + b0i * y0.y;  acc[j][0][1] += b0r * y0.y - b0i * y0.x;
+          acc[j][1][0] += b0r * y1.x + b0i * y1.y;  acc[j][1][1] += b0r * y1.y - b0i * y1.x;
+          acc[j][2][0] += b1r * y0.x + b1i * y0.y;  acc[j][2][1] += b1r * y0.y - b1i * y0.x;
+          acc[j][3][0] += b1r * y1.x + b1i * y1.y;  acc[j][3][1] += b1r * y1.y - b1i * y1.x;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const size_t npair = (size_t)Ns * Ns;
+  double2 *dst = ifc < 0 ? Ablk + n * npair : Ahop + ((size_t)8 * n + ifc) * npair;
+#pragma unroll
+  for (int j = 0; j < MAXT; j++) {
+    const int q = threadIdx.x + j * blockDim.x;
+    if (q < ntile) {
+      const int kt = q % NT, lt = q / NT, k = 2 * kt, l = 2 * lt;
+      dst[(size_t)l * Ns + k] = make_double2(acc[j][0][0], acc[j][0][1]);
+      dst[(size_t)(l + 1) * Ns + k] = make_double2(acc[j][1][0], acc[j][1][1]);
+      dst[(size_t)l * Ns + k + 1] = make_double2(acc[j][2][0], acc[j][2][1]);
+      dst[(size_t)(l + 1) * Ns + k + 1] = make_double2(acc[j][3][0], acc[j][3][1]);
+    }
+  }
+}
+
 // M[n][col l] (entries k) = (basis_k, t) on block n, FP64 field t
 __global__ void k_dfl_project(Geom g, const int *__restrict__ vd2lex, const float4 *const *__restrict__ basis,
                               int Ns, const double2 *__restrict__ t, double2 *M, size_t mstride, int l) {
@@ -485,7 +651,7 @@ void dfl_release(Ctx &c) {
   for (void *p : d.modes) cudaFree(p);
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
-  void *bufs[] = {d.vd2lex, d.nbr, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop};
+  void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop};
   for (void *p : bufs) cudaFree(p);
   DflState fresh;
   // the solver and generation parameters outlive a change of geometry
@@ -555,23 +721,21 @@ int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st) {
   DflState &d = c.dfl;
   if (!d.have_basis) return fail("set_Aw: the deflation subspace is not set");
   if (d.aw_valid && d.aw_mu == mu && d.aw_eo == c.eoflg) return 0;
-  void *t = nullptr;
-  if (cudaMallocAsync(&t, spinor_bytes(c, 64), st) != cudaSuccess) return fail("out of device memory");
   const double muo = c.eoflg ? 0.0 : mu;
-  const int T = 128;
-  const unsigned nbk = (unsigned)((c.g.vol + T - 1) / T);
-  const size_t m2 = (size_t)d.Ns * d.Ns;
-  for (int l = 0; l < d.Ns; l++) {
-    k_dfl_dapply<<<nbk, T, 0, st>>>(c.g, (const float4 *)d.basis[l], (double2 *)t, c.ud, c.swd, mu, muo, -1);
-    k_dfl_project<<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, (const double2 *)t,
-                                        d.Ablk, m2, l);
-    for (int ifc = 0; ifc < 8; ifc++) {
-      k_dfl_dapply<<<nbk, T, 0, st>>>(c.g, (const float4 *)d.basis[l], (double2 *)t, c.ud, c.swd, mu, muo, ifc);
-      k_dfl_project<<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
-                                          (const double2 *)t, d.Ahop + ifc * m2, 8 * m2, l);
-    }
+  constexpr int TS = 8, LD = TS * 12 + 1;
+  const int NT = d.Ns / 2, ntile = NT * NT;
+  const size_t shm = (size_t)NT * LD * (2 * sizeof(double2) + sizeof(float4));
+  const dim3 grid(d.nb, 9);
+  const float4 *const *bas = (const float4 *const *)d.d_basis;
+  if (ntile <= 256) {
+    cudaFuncSetAttribute(k_aw_tiles<TS, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k_aw_tiles<TS, 1><<<grid, 256, shm, st>>>(c.g, d.vd2lex, bas, d.Ns, c.ud, c.swd, mu, muo, d.faces, d.nfc,
+                                              d.fmax, d.Ablk, d.Ahop);
+  } else {
+    cudaFuncSetAttribute(k_aw_tiles<TS, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    k_aw_tiles<TS, 4><<<grid, 256, shm, st>>>(c.g, d.vd2lex, bas, d.Ns, c.ud, c.swd, mu, muo, d.faces, d.nfc,
+                                              d.fmax, d.Ablk, d.Ahop);
   }
-  cudaFreeAsync(t, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return fail("set_Aw: CUDA error");
   d.aw_valid = true;
   d.aw_mu = mu;

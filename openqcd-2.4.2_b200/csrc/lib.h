@@ -21,6 +21,7 @@ struct DflState {
   double gen_kappa = 0.125, gen_mu = 0.0;
   int gen_ninv = 4, gen_nmr = 4, gen_ncy = 4;
   int *vd2lex = nullptr, *nbr = nullptr;
+  int *faces = nullptr, *nfc = nullptr, fmax = 0;   // block-face site lists
   std::vector<void *> basis, modes;
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
