@@ -114,6 +114,41 @@ int b200_dfl_profile(int on, double *out) {
   return 0;
 }
 
+// Device timing of the deflation kernels (no reference counterpart): what =
+// 0 restriction of an FP32 field, 1 prolongation, 2 Awhat_dble, 3 Aw_dble,
+// 4 ltl_gcr on a random little vector (status[0] of the last solve in *its).
+int b200_dfl_time(int what, int n, float *ms, int *its) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1;
+  qcd::DflState &d = c.dfl;
+  if (!d.have_basis) return fail("dfl_time: no deflation subspace");
+  if ((what == 2 || what == 3 || what == 4) && qcd::dfl_set_Awhat(c, d.aw_valid ? d.aw_mu : 0.0, c.stream) < 0) return -1;
+  void *f = qcd::spinor_stage(c, 32, 0);
+  double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1), *t = qcd::lbuf(c, 2);
+  if (!f || !a || !b || !t) return -1;
+  qcd::gen_uniform_spinor32(c, f, 11, c.stream);
+  qcd::dfl_restrict(c, 32, f, a, c.stream);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, c.stream);
+  int st[2] = {0, 0}, fl = 0;
+  for (int i = 0; i < n; i++) {
+    if (what == 0) qcd::dfl_restrict(c, 32, f, b, c.stream);
+    else if (what == 1) qcd::dfl_prolong(c, a, f, c.stream);
+    else if (what == 2) qcd::dfl_Awhat(c, a, b, t, c.stream);
+    else if (what == 3) qcd::dfl_Aw(c, a, b, c.stream);
+    else qcd::dfl_ltl_gcr(c, d.aw_mu, a, b, &fl, st, c.stream);
+  }
+  cudaEventRecord(e1, c.stream);
+  cudaEventSynchronize(e1);
+  cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (its) *its = st[0];
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("dfl_time: CUDA error");
+}
+
 int b200_dfl_nv(void) { return ctx().dfl.ready ? ctx().dfl.nv : 0; }
 
 // Load basis vector l of every block from a global field in the reference

@@ -110,6 +110,9 @@ static int dfl_alloc(Ctx &c) {
   cudaFree(d.d_basis);
   cudaMalloc(&d.d_basis, Ns * sizeof(void *));
   cudaMemcpy(d.d_basis, d.basis.data(), Ns * sizeof(void *), cudaMemcpyHostToDevice);
+  cudaFree(d.rpart);
+  if (cudaMalloc(&d.rpart, (size_t)nb * 2 * Ns * sizeof(double2)) != cudaSuccess)
+    return fail("out of device memory (deflation)");
   size_t m = (size_t)nb * Ns * Ns * sizeof(double2);
   double2 **mats[] = {&d.Ablk, &d.Ainv, &d.Ahop, &d.Mhop};
   size_t sz[] = {m, m, 8 * m, 8 * m};
@@ -126,43 +129,74 @@ static int dfl_alloc(Ctx &c) {
 // ------------------------------------------------ restriction / prolongation
 // vd[n*Ns + l] = (basis_l, s) on block n; FP32 products accumulated in double
 // and rounded to float, as spinor_prod returns them (dfl_subspace.c:83-123).
+// Restriction by parity chunks: CTA (n, p) owns the vbh sites of parity p
+// of block n, one site per thread (the site's field values stay in
+// registers while the Ns basis vectors stream past); the 12 products of a
+// site are summed in the field's precision, everything after in double
+// (FP64 arithmetic per product halved the kernel's speed); per-warp partial sums
+// go to shared memory without a barrier per l, and the two parities are
+// added by k_dfl_restrict_fin in a fixed order.
+constexpr int RESTRICT_T = 704;
+
 template <typename R>
-__global__ void k_dfl_restrict(Geom g, const int *__restrict__ vd2lex, const float4 *const *__restrict__ basis,
-                               int Ns, const void *__restrict__ s, double2 *vd, int round_float) {
-  const int n = blockIdx.x, blk = __ldg(vd2lex + n);
-  __shared__ double red[2][32];
-  const int nsite = 2 * g.vbh;
+__global__ void __launch_bounds__(RESTRICT_T) k_dfl_restrict2(Geom g, const int *__restrict__ vd2lex,
+                                                              const float4 *const *__restrict__ basis, int Ns,
+                                                              const void *__restrict__ s, double2 *part) {
+  __shared__ double2 red[64][RESTRICT_T / 32 + 1];
+  const int n = blockIdx.x, p = blockIdx.y, blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const bool one = g.vbh <= (int)blockDim.x;
+  spinor<R> x;
+  szero(x);
+  if (one && (int)threadIdx.x < g.vbh) x = Store<R>::load_spinor(s, chunk, threadIdx.x, g.vbh);
   for (int l = 0; l < Ns; l++) {
     double re = 0.0, im = 0.0;
     const float4 *bl = basis[l];
-    for (int t = threadIdx.x; t < nsite; t += blockDim.x) {
-      const int p = t >= g.vbh, si = t - p * g.vbh, chunk = p * g.nbl + blk;
-      spinor<float> b = Store<float>::load_spinor(bl, chunk, si, g.vbh);
-      spinor<R> x = Store<R>::load_spinor(s, chunk, si, g.vbh);
+    for (int si = threadIdx.x; si < g.vbh; si += blockDim.x) {
+      const spinor<R> xx = one ? x : Store<R>::load_spinor(s, chunk, si, g.vbh);
+      const spinor<float> b = Store<float>::load_spinor(bl, chunk, si, g.vbh);
+      // the 12 products of a site in R, the sums over sites in double
+      R sr = 0, sim = 0;
 #pragma unroll
       for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-          const double br = b.c[a].c[k].re, bi = b.c[a].c[k].im, xr = x.c[a].c[k].re, xi = x.c[a].c[k].im;
-          re += br * xr + bi * xi;
-          im += br * xi - bi * xr;
+          const R br = b.c[a].c[k].re, bi = b.c[a].c[k].im, xr = xx.c[a].c[k].re, xi = xx.c[a].c[k].im;
+          sr += br * xr + bi * xi;
+          sim += br * xi - bi * xr;
         }
+      re += (double)sr;
+      im += (double)sim;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       re += __shfl_down_sync(0xffffffffu, re, o);
       im += __shfl_down_sync(0xffffffffu, im, o);
     }
-    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = re; red[1][threadIdx.x >> 5] = im; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double a = 0.0, b = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += red[0][w]; b += red[1][w]; }
-      if (round_float) { a = (double)(float)a; b = (double)(float)b; }
-      vd[(size_t)n * Ns + l] = make_double2(a, b);
-    }
-    __syncthreads();
+    if (lane == 0) red[l][wp] = make_double2(re, im);
   }
+  __syncthreads();
+  for (int l = threadIdx.x; l < Ns; l += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < nw; w++) {
+      re += red[l][w].x;
+      im += red[l][w].y;
+    }
+    part[((size_t)n * 2 + p) * Ns + l] = make_double2(re, im);
+  }
+}
+
+__global__ void k_dfl_restrict_fin(const double2 *__restrict__ part, int Ns, int nb, double2 *vd, int round_float) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb * Ns) return;
+  const int n = i / Ns, l = i - n * Ns;
+  const double2 a = part[((size_t)n * 2) * Ns + l], b = part[((size_t)n * 2 + 1) * Ns + l];
+  double re = a.x + b.x, im = a.y + b.y;
+  if (round_float) {
+    re = (double)(float)re;
+    im = (double)(float)im;
+  }
+  vd[i] = make_double2(re, im);
 }
 
 // s = sum_l vd[n,l] basis_l on every block n, with float coefficients and
@@ -604,46 +638,169 @@ __global__ void k_cmatmul8(int Ns, const double2 *__restrict__ Ainv, const doubl
 // mode 1: w[n] = sum_ifc H[n][ifc] v[nbr]   for blocks in [b0, b0+cnt)
 // mode 2: w[n] = v[n] - sum_ifc H[n][ifc] u[nbr]
 // mode 3: w[n] = Ablk[n] v[n] (Ablk holding an inverse)
-__global__ void k_little(int mode, int Ns, int b0, const double2 *__restrict__ Ablk, const double2 *__restrict__ H,
-                         const int *__restrict__ nbr, const double2 *__restrict__ v, const double2 *__restrict__ u,
-                         double2 *w) {
-  const int n = b0 + blockIdx.x, k = threadIdx.x;
-  if (k >= Ns) return;
-  double re = 0.0, im = 0.0;
-  if (mode == 0 || mode == 3) {
-    const double2 *a = Ablk + (size_t)n * Ns * Ns;
-    const double2 *x = v + (size_t)n * Ns;
-    for (int l = 0; l < Ns; l++) {
-      const double2 aa = a[(size_t)l * Ns + k], xx = x[l];
-      re += aa.x * xx.x - aa.y * xx.y;
-      im += aa.x * xx.y + aa.y * xx.x;
-    }
-  }
-  if (mode != 3) {
-    const double2 *src = mode == 2 ? u : v;
-    for (int ifc = 0; ifc < 8; ifc++) {
-      const double2 *a = H + ((size_t)8 * n + ifc) * Ns * Ns;
-      const double2 *x = src + (size_t)__ldg(nbr + 8 * n + ifc) * Ns;
-      double tr = 0.0, ti = 0.0;
-      for (int l = 0; l < Ns; l++) {
-        const double2 aa = a[(size_t)l * Ns + k], xx = x[l];
-        tr += aa.x * xx.x - aa.y * xx.y;
-        ti += aa.x * xx.y + aa.y * xx.x;
-      }
-      re += tr;
-      im += ti;
-    }
-  }
-  if (mode == 2) {
-    const double2 vv = v[(size_t)n * Ns + k];
-    w[(size_t)n * Ns + k] = make_double2(vv.x - re, vv.y - im);
+// One warp per matrix: warps 0..7 take the
+// eight face matrices, warp 8 (mode 0) or warp 0 (mode 3) the diagonal one;
+// lanes hold rows k and k+32, the column loop is unrolled four times so that
+// every lane keeps four independent 16-byte loads in flight; the warps'
+// partial rows are summed in shared memory.
+__global__ void __launch_bounds__(288) k_little_w(int mode, int Ns, int b0, const double2 *__restrict__ Ablk,
+                                                  const double2 *__restrict__ H, const int *__restrict__ nbr,
+                                                  const double2 *__restrict__ v, const double2 *__restrict__ u,
+                                                  double2 *w) {
+  __shared__ double2 part[9][64];
+  const int n = b0 + blockIdx.x, wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  const double2 *a, *x;
+  if (mode == 3 || wp == 8) {
+    a = Ablk + (size_t)n * Ns * Ns;
+    x = v + (size_t)n * Ns;
   } else {
-    w[(size_t)n * Ns + k] = make_double2(re, im);
+    a = H + ((size_t)8 * n + wp) * Ns * Ns;
+    x = (mode == 2 ? u : v) + (size_t)__ldg(nbr + 8 * n + wp) * Ns;
+  }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int k = lane + 32 * h;
+    if (k < Ns) {
+      double r0 = 0.0, i0 = 0.0, r1 = 0.0, i1 = 0.0;
+      int l = 0;
+      for (; l + 4 <= Ns; l += 4) {
+        const double2 a0 = __ldg(a + (size_t)l * Ns + k), a1 = __ldg(a + (size_t)(l + 1) * Ns + k);
+        const double2 a2 = __ldg(a + (size_t)(l + 2) * Ns + k), a3 = __ldg(a + (size_t)(l + 3) * Ns + k);
+        const double2 x0 = __ldg(x + l), x1 = __ldg(x + l + 1), x2 = __ldg(x + l + 2), x3 = __ldg(x + l + 3);
+        r0 += a0.x * x0.x - a0.y * x0.y; i0 += a0.x * x0.y + a0.y * x0.x;
+        r1 += a1.x * x1.x - a1.y * x1.y; i1 += a1.x * x1.y + a1.y * x1.x;
+        r0 += a2.x * x2.x - a2.y * x2.y; i0 += a2.x * x2.y + a2.y * x2.x;
+        r1 += a3.x * x3.x - a3.y * x3.y; i1 += a3.x * x3.y + a3.y * x3.x;
+      }
+      for (; l < Ns; l++) {
+        const double2 a0 = __ldg(a + (size_t)l * Ns + k), x0 = __ldg(x + l);
+        r0 += a0.x * x0.x - a0.y * x0.y; i0 += a0.x * x0.y + a0.y * x0.x;
+      }
+      part[wp][k] = make_double2(r0 + r1, i0 + i1);
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < Ns; k += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < nw; j++) {
+      re += part[j][k].x;
+      im += part[j][k].y;
+    }
+    if (mode == 2) {
+      const double2 vv = v[(size_t)n * Ns + k];
+      w[(size_t)n * Ns + k] = make_double2(vv.x - re, vv.y - im);
+    } else {
+      w[(size_t)n * Ns + k] = make_double2(re, im);
+    }
+  }
+}
+
+static void little_launch(int mode, int Ns, int b0, int nblk, const double2 *Ablk, const double2 *H, const int *nbr,
+                          const double2 *v, const double2 *u, double2 *w, cudaStream_t st) {
+  const int nw = mode == 3 ? 1 : (mode == 0 ? 9 : 8);
+  k_little_w<<<nblk, 32 * nw, 0, st>>>(mode, Ns, b0, Ablk, H, nbr, v, u, w);
+}
+
+// ------------------------------------------------ little-vector GCR kernels
+// Dots (Q_j, y) = sum_i conj(Q_j[i]) y[i] for j < k (k <= LMAXK) in one pass
+// over y, per-CTA partial sums, then a fixed-order final sum: deterministic.
+constexpr int LMAXK = 32, LGRID = 296;
+
+__global__ void __launch_bounds__(256) k_mdot(const double2 *const *__restrict__ Q, int k,
+                                              const double2 *__restrict__ y, int n, double2 *part) {
+  __shared__ double2 red[8][LMAXK];
+  double ar[LMAXK], ai[LMAXK];
+#pragma unroll
+  for (int j = 0; j < LMAXK; j++) ar[j] = ai[j] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 yy = y[i];
+#pragma unroll
+    for (int j = 0; j < LMAXK; j++)
+      if (j < k) {
+        const double2 q = Q[j][i];
+        ar[j] += q.x * yy.x + q.y * yy.y;
+        ai[j] += q.x * yy.y - q.y * yy.x;
+      }
+  }
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < LMAXK; j++)
+    if (j < k) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ar[j] += __shfl_down_sync(0xffffffffu, ar[j], o);
+        ai[j] += __shfl_down_sync(0xffffffffu, ai[j], o);
+      }
+      if (lane == 0) red[wp][j] = make_double2(ar[j], ai[j]);
+    }
+  __syncthreads();
+  if (threadIdx.x < k) {
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < 8; w++) {
+      re += red[w][threadIdx.x].x;
+      im += red[w][threadIdx.x].y;
+    }
+    part[blockIdx.x * LMAXK + threadIdx.x] = make_double2(re, im);
+  }
+}
+
+__global__ void k_mdot_fin(const double2 *__restrict__ part, int k, double2 *dots) {
+  const int j = threadIdx.x;
+  if (j >= k) return;
+  double re = 0.0, im = 0.0;
+  for (int b = 0; b < LGRID; b++) {
+    re += part[b * LMAXK + j].x;
+    im += part[b * LMAXK + j].y;
+  }
+  dots[j] = make_double2(re, im);
+}
+
+// qk -= sum_j dots[j] Q_j ; pk -= sum_j dots[j] P_j
+__global__ void k_gs_sub(const double2 *const *__restrict__ Q, const double2 *const *__restrict__ P, int k,
+                         const double2 *__restrict__ dots, double2 *qk, double2 *pk, int n) {
+  __shared__ double2 c[LMAXK];
+  if (threadIdx.x < k) c[threadIdx.x] = dots[threadIdx.x];
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 q = qk[i], p = pk[i];
+    for (int j = 0; j < k; j++) {
+      const double2 a = Q[j][i], b = P[j][i], z = c[j];
+      q.x -= z.x * a.x - z.y * a.y; q.y -= z.x * a.y + z.y * a.x;
+      p.x -= z.x * b.x - z.y * b.y; p.y -= z.x * b.y + z.y * b.x;
+    }
+    qk[i] = q;
+    pk[i] = p;
+  }
+}
+
+// qk, pk /= |qk| (nrm2 = |qk|^2, left unchanged when zero)
+__global__ void k_norm_scale(double2 *qk, double2 *pk, const double2 *__restrict__ nrm2, int n) {
+  const double s2 = nrm2[0].x;
+  if (!(s2 > 0.0)) return;
+  const double f = 1.0 / sqrt(s2);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double2 q = qk[i], p = pk[i];
+    qk[i] = make_double2(q.x * f, q.y * f);
+    pk[i] = make_double2(p.x * f, p.y * f);
+  }
+}
+
+// x += c pk ; r -= c qk with c = (qk, r)
+__global__ void k_xr_update(double2 *x, double2 *r, const double2 *__restrict__ pk, const double2 *__restrict__ qk,
+                            const double2 *__restrict__ cc, int n) {
+  const double2 z = cc[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 p = pk[i], q = qk[i];
+    double2 xx = x[i], rr = r[i];
+    xx.x += z.x * p.x - z.y * p.y; xx.y += z.x * p.y + z.y * p.x;
+    rr.x -= z.x * q.x - z.y * q.y; rr.y -= z.x * q.y + z.y * q.x;
+    x[i] = xx;
+    r[i] = rr;
   }
 }
 
 // ----------------------------------------------------------- host routines
-static int little_threads(int Ns) { return ((Ns + 31) / 32) * 32; }
 
 void dfl_release(Ctx &c) {
   DflState &d = c.dfl;
@@ -651,7 +808,9 @@ void dfl_release(Ctx &c) {
   for (void *p : d.modes) cudaFree(p);
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
-  void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop};
+  void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop,
+                  d.lvtab, d.ldots, d.lpart, d.rpart};
+  if (d.h_ldots) cudaFreeHost(d.h_ldots);
   for (void *p : bufs) cudaFree(p);
   DflState fresh;
   // the solver and generation parameters outlive a change of geometry
@@ -682,10 +841,13 @@ int dfl_set_parms(Ctx &c, const int bs[4], int Ns) {
 
 void dfl_restrict(Ctx &c, int prec, const void *s, double2 *vd, cudaStream_t st) {
   DflState &d = c.dfl;
-  if (prec == 32)
-    k_dfl_restrict<float><<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, s, vd, 1);
-  else
-    k_dfl_restrict<double><<<d.nb, 256, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns, s, vd, 0);
+  const dim3 grid(d.nb, 2);
+  const int t = std::min(RESTRICT_T, (c.g.vbh + 31) / 32 * 32);
+  const float4 *const *bas = (const float4 *const *)d.d_basis;
+  if (prec == 32) k_dfl_restrict2<float><<<grid, t, 0, st>>>(c.g, d.vd2lex, bas, d.Ns, s, d.rpart);
+  else k_dfl_restrict2<double><<<grid, t, 0, st>>>(c.g, d.vd2lex, bas, d.Ns, s, d.rpart);
+  const int nn = d.nb * d.Ns;
+  k_dfl_restrict_fin<<<(nn + 255) / 256, 256, 0, st>>>(d.rpart, d.Ns, d.nb, vd, prec == 32);
 }
 
 void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st) {
@@ -769,15 +931,15 @@ int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st) {
 // w = Aw v (Aw_dble) on all blocks
 void dfl_Aw(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
   DflState &d = c.dfl;
-  k_little<<<d.nb, little_threads(d.Ns), 0, st>>>(0, d.Ns, 0, d.Ablk, d.Ahop, d.nbr, v, nullptr, w);
+  little_launch(0, d.Ns, 0, d.nb, d.Ablk, d.Ahop, d.nbr, v, nullptr, w, st);
 }
 
 // w_e = v_e - H_eo H_oe v_e (Awhat_dble): t holds the odd intermediate
 void dfl_Awhat(Ctx &c, const double2 *v, double2 *w, double2 *t, cudaStream_t st) {
   DflState &d = c.dfl;
-  const int nbh = d.nb / 2, T = little_threads(d.Ns);
-  k_little<<<nbh, T, 0, st>>>(1, d.Ns, nbh, nullptr, d.Mhop, d.nbr, v, nullptr, t);
-  k_little<<<nbh, T, 0, st>>>(2, d.Ns, 0, nullptr, d.Mhop, d.nbr, v, t, w);
+  const int nbh = d.nb / 2;
+  little_launch(1, d.Ns, nbh, nbh, nullptr, d.Mhop, d.nbr, v, nullptr, t, st);
+  little_launch(2, d.Ns, 0, nbh, nullptr, d.Mhop, d.nbr, v, t, w, st);
 }
 
 // ------------------------------------------------------------ little solver
@@ -790,79 +952,134 @@ static double lv_dot_re(Ctx &c, const double2 *x, const double2 *y, size_t n, do
   return r[0] + r[1];
 }
 
+// Little-vector workspace of ltl_gcr: 2 nkv + 6 vectors of nv complex
+// doubles, a device table of the Krylov vectors' addresses (p_0..p_nkv-1,
+// q_0..q_nkv-1, r) for the multi-vector kernels, the dot buffers.
+static int ltl_ensure(Ctx &c) {
+  DflState &d = c.dfl;
+  const size_t nv = (size_t)d.nv;
+  const int nkv = d.nkv;
+  if (nkv > LMAXK) return fail("ltl_gcr: nkv must not exceed 32");
+  bool grown = false;
+  while ((int)d.lv.size() < 2 * nkv + 6) {
+    double2 *p = nullptr;
+    if (cudaMalloc(&p, nv * sizeof(double2)) != cudaSuccess) return fail("out of device memory (little vectors)");
+    d.lv.push_back(p);
+    grown = true;
+  }
+  if (!d.lvtab) {
+    if (cudaMalloc(&d.lvtab, (2 * LMAXK + 8) * sizeof(double2 *)) != cudaSuccess ||
+        cudaMalloc(&d.ldots, 64 * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&d.lpart, (size_t)LGRID * LMAXK * sizeof(double2)) != cudaSuccess ||
+        cudaMallocHost(&d.h_ldots, 4 * sizeof(double2)) != cudaSuccess)
+      return fail("out of device memory (little solver)");
+    grown = true;
+  }
+  if (grown || d.lvtab_nkv != nkv) {
+    std::vector<double2 *> tab(2 * nkv + 1);
+    for (int k = 0; k < nkv; k++) {
+      tab[k] = d.lv[6 + k];
+      tab[nkv + k] = d.lv[6 + nkv + k];
+    }
+    tab[2 * nkv] = d.lv[1];
+    cudaMemcpy(d.lvtab, tab.data(), tab.size() * sizeof(double2 *), cudaMemcpyHostToDevice);
+    d.lvtab_nkv = nkv;
+  }
+  return 0;
+}
+
+static void ldot(Ctx &c, double2 *const *Q, int k, const double2 *y, int n, double2 *out, cudaStream_t st) {
+  DflState &d = c.dfl;
+  k_mdot<<<LGRID, 256, 0, st>>>((const double2 *const *)Q, k, y, n, d.lpart);
+  k_mdot_fin<<<1, 32, 0, st>>>(d.lpart, k, out);
+}
+
 // ltl_gcr (modules/dfl/ltl_gcr.c:155): even-odd reduction of the little
 // system, GCR on Awhat for the even blocks to relative residue res (at most
 // nmx Krylov vectors, restart after nkv), back-substitution for the odd
 // blocks.  The reference additionally preconditions with a single-precision
 // GCR and deflates the little-little modes; this solver runs plain
-// double-precision GCR with the same stopping rule.  Returns the norm of the
-// residue of the even-odd preconditioned system; ifail 0, -1 (no
-// convergence) or -2 (unsafe inversion).
+// double-precision GCR with the same stopping rule.  The Krylov step runs on
+// the device: the Gram-Schmidt coefficients (classical Gram-Schmidt, applied
+// twice), the normalisation and the update coefficient never leave the GPU,
+// and the host reads two numbers per step (|q_k|^2 and |r|^2) for the
+// stopping test.  Returns the norm of the residue of the even-odd
+// preconditioned system; ifail 0, -1 (no convergence) or -2 (unsafe
+// inversion).
 double dfl_ltl_gcr(Ctx &c, double mu, const double2 *eta, double2 *psi, int *ifail, int *status,
                    cudaStream_t st) {
   DflState &d = c.dfl;
   ifail[0] = 0;
   status[0] = 0;
   const size_t nv = (size_t)d.nv, nvh = nv / 2;
-  const int nbh = d.nb / 2, T = little_threads(d.Ns);
+  const int nbh = d.nb / 2, n = (int)nvh;
   if (dfl_set_Awhat(c, mu, st)) {
     ifail[0] = -2;
     cudaMemsetAsync(psi, 0, nv * sizeof(double2), st);
     return sqrt(lv_dot_re(c, eta, eta, nv, nullptr));
   }
+  if (ltl_ensure(c)) return -1.0;
   const int nkv = d.nkv;
-  while ((int)d.lv.size() < 2 * nkv + 6) {
-    double2 *p = nullptr;
-    if (cudaMalloc(&p, nv * sizeof(double2)) != cudaSuccess) { fail("out of device memory (little vectors)"); return -1; }
-    d.lv.push_back(p);
-  }
   double2 *x = d.lv[0], *r = d.lv[1], *t = d.lv[2], *eh = d.lv[3], *w = d.lv[4], *y = d.lv[5];
   double2 **p = &d.lv[6], **q = &d.lv[6 + nkv];
+  double2 *const *Ptab = d.lvtab, *const *Qtab = d.lvtab + nkv, *const *Rtab = d.lvtab + 2 * nkv;
+  double2 *dots = d.ldots;
+  const unsigned gv = (unsigned)std::min<size_t>((nvh + 255) / 256, 4 * 148);
+  auto read3 = [&](double *nq2, double *rr) {
+    cudaMemcpyAsync(d.h_ldots, dots + 32, 3 * sizeof(double2), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    *nq2 = d.h_ldots[0].x;
+    *rr = d.h_ldots[2].x;
+  };
   // eh_e = Aee^-1 (eta_e - Aeo Aoo^-1 eta_o)   [even half of eh]
   cudaMemcpyAsync(w, eta, nv * sizeof(double2), cudaMemcpyDeviceToDevice, st);
-  k_little<<<nbh, T, 0, st>>>(3, d.Ns, nbh, d.Ainv, nullptr, d.nbr, eta, nullptr, w);     // w_o = Aoo^-1 eta_o
-  k_little<<<nbh, T, 0, st>>>(2, d.Ns, 0, nullptr, d.Ahop, d.nbr, eta, w, t);             // t_e = eta_e - Aeo w_o
-  k_little<<<nbh, T, 0, st>>>(3, d.Ns, 0, d.Ainv, nullptr, d.nbr, t, nullptr, eh);        // eh_e = Aee^-1 t_e
+  little_launch(3, d.Ns, nbh, nbh, d.Ainv, nullptr, d.nbr, eta, nullptr, w, st);    // w_o = Aoo^-1 eta_o
+  little_launch(2, d.Ns, 0, nbh, nullptr, d.Ahop, d.nbr, eta, w, t, st);            // t_e = eta_e - Aeo w_o
+  little_launch(3, d.Ns, 0, nbh, d.Ainv, nullptr, d.nbr, t, nullptr, eh, st);       // eh_e = Aee^-1 t_e
   // GCR on Awhat x = eh (even half)
   cudaMemsetAsync(x, 0, nvh * sizeof(double2), st);
   cudaMemcpyAsync(r, eh, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
-  const double rn0 = sqrt(lv_dot_re(c, r, r, nvh, nullptr));
+  double nq2 = 0.0, rr = 0.0;
+  ldot(c, Rtab, 1, r, n, dots + 34, st);
+  read3(&nq2, &rr);
+  const double rn0 = sqrt(rr);
   double rn = rn0;
   const double tol = d.res * rn0;
   int it = 0;
   while (rn > tol && it < d.nmx) {
-    int k;
-    for (k = 0; k < nkv && it < d.nmx && rn > tol; k++, it++) {
+    for (int k = 0; k < nkv && it < d.nmx && rn > tol; k++) {
       cudaMemcpyAsync(p[k], r, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
       dfl_Awhat(c, p[k], q[k], y, st);
-      for (int l = 0; l < k; l++) {
-        double im;
-        double re = lv_dot_re(c, q[l], q[k], nvh, &im);
-        flat_caxpy(c, q[k], q[l], nvh, -re, -im);
-        flat_caxpy(c, p[k], p[l], nvh, -re, -im);
-      }
-      double nq = sqrt(lv_dot_re(c, q[k], q[k], nvh, nullptr));
-      if (nq == 0.0) break;
-      flat_cscale(c, q[k], nvh, 1.0 / nq);
-      flat_cscale(c, p[k], nvh, 1.0 / nq);
-      double im;
-      double re = lv_dot_re(c, q[k], r, nvh, &im);
-      flat_caxpy(c, x, p[k], nvh, re, im);
-      flat_caxpy(c, r, q[k], nvh, -re, -im);
-      rn = sqrt(lv_dot_re(c, r, r, nvh, nullptr));
+      if (k > 0)
+        for (int pass = 0; pass < 2; pass++) {
+          ldot(c, Qtab, k, q[k], n, dots, st);
+          k_gs_sub<<<gv, 256, 0, st>>>(Qtab, Ptab, k, dots, q[k], p[k], n);
+        }
+      ldot(c, Qtab + k, 1, q[k], n, dots + 32, st);
+      k_norm_scale<<<gv, 256, 0, st>>>(q[k], p[k], dots + 32, n);
+      ldot(c, Qtab + k, 1, r, n, dots + 33, st);
+      k_xr_update<<<gv, 256, 0, st>>>(x, r, p[k], q[k], dots + 33, n);
+      ldot(c, Rtab, 1, r, n, dots + 34, st);
+      read3(&nq2, &rr);
+      if (nq2 == 0.0) break;
+      it++;
+      rn = sqrt(rr);
     }
     // restart from the true residual
     dfl_Awhat(c, x, w, y, st);
     cudaMemcpyAsync(r, eh, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
     flat_caxpy(c, r, w, nvh, -1.0, 0.0);
-    rn = sqrt(lv_dot_re(c, r, r, nvh, nullptr));
+    ldot(c, Rtab, 1, r, n, dots + 34, st);
+    read3(&nq2, &rr);
+    rn = sqrt(rr);
+    if (nq2 == 0.0 && rn > tol) break;   // the Krylov space collapsed
   }
   status[0] = it;
   if (rn > tol) ifail[0] = -1;
   // psi_e = x_e ; psi_o = Aoo^-1 (eta_o - Aoe x_e)
   cudaMemcpyAsync(psi, x, nvh * sizeof(double2), cudaMemcpyDeviceToDevice, st);
-  k_little<<<nbh, T, 0, st>>>(2, d.Ns, nbh, nullptr, d.Ahop, d.nbr, eta, x, t);          // t_o = eta_o - Aoe x_e
-  k_little<<<nbh, T, 0, st>>>(3, d.Ns, nbh, d.Ainv, nullptr, d.nbr, t, nullptr, psi);     // psi_o
+  little_launch(2, d.Ns, nbh, nbh, nullptr, d.Ahop, d.nbr, eta, x, t, st);          // t_o = eta_o - Aoe x_e
+  little_launch(3, d.Ns, nbh, nbh, d.Ainv, nullptr, d.nbr, t, nullptr, psi, st);     // psi_o
   return rn;
 }
 

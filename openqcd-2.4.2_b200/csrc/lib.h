@@ -22,6 +22,7 @@ struct DflState {
   int gen_ninv = 4, gen_nmr = 4, gen_ncy = 4;
   int *vd2lex = nullptr, *nbr = nullptr;
   int *faces = nullptr, *nfc = nullptr, fmax = 0;   // block-face site lists
+  double2 *rpart = nullptr;                          // restriction partial sums [nb][2][Ns]
   std::vector<void *> basis, modes;
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
@@ -29,6 +30,9 @@ struct DflState {
   int awhat_fail = 0, aw_eo = 0;
   double aw_mu = 0.0;
   std::vector<double2 *> lv, lvd;
+  double2 **lvtab = nullptr;    // device table of the little solver's Krylov vectors
+  double2 *ldots = nullptr, *lpart = nullptr, *h_ldots = nullptr;
+  int lvtab_nkv = 0;
   // phase timers (seconds): 0 SAP smoothing of the modes, 1 block
   // Gram-Schmidt, 2 little operator set-up, 3 little solves, 4 SAP in the
   // deflated preconditioner and inverse iteration, 5 everything else

@@ -105,6 +105,7 @@ _SIGS = {
     "b200_set_dfl_gen_parms": (C.c_int, [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
     "b200_dfl_nv": (C.c_int, []),
     "b200_dfl_profile": (C.c_int, [C.c_int, C.c_void_p]),
+    "b200_dfl_time": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "dfl_modes": (None, [C.c_void_p, C.c_void_p]),
@@ -450,6 +451,14 @@ def dfl_profile(on):
     out = np.zeros(6)
     check(lib().b200_dfl_profile(1 if on else 0, _ptr(out)))
     return dict(zip(DFL_PHASES, out.tolist()))
+
+
+def dfl_time(what, n):
+    """Device ms per call of a deflation kernel (0 restrict, 1 prolong,
+    2 Awhat_dble, 3 Aw_dble, 4 ltl_gcr) and the last solve's GCR steps."""
+    ms, its = C.c_float(0.0), C.c_int(0)
+    check(lib().b200_dfl_time(what, n, C.byref(ms), C.byref(its)))
+    return ms.value / n, its.value
 
 
 def dfl_set_basis(l, field):
