@@ -220,6 +220,18 @@ int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status);
                                            spinor_dble *psi, int *ifail, int *status);
 /* dfl_sap_gcr.c:383 */ double dfl_sap_gcr2(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta,
                                             spinor_dble *psi, int *ifail, int *status);
+/* Several right-hand sides solved together (no reference counterpart):
+ * nrhs systems Dw(mu[r]) psi[r] = eta[r] on device fields in the library's
+ * layout, each by the algorithm of sap_gcr (dfl = 0) or dfl_sap_gcr
+ * (dfl = 1, same mu for all systems) with its own Krylov space and stopping
+ * test; a system leaves the batch when it has converged.  With deflation
+ * the restriction, little solve and prolongation of all systems run as
+ * multi-right-hand-side kernels.  rho[r], ifail[r] and status[r] as in the
+ * single-system solvers (status[nrhs + r]: average little-solver steps). */
+int b200_dev_gcr_batch(int nrhs, int dfl, int nkv, int nmx, int istop, double res, const double *mu,
+                       void *const *eta, void *const *psi, double *rho, int *ifail, int *status);
+/* Free the solvers' cached work fields. */
+int b200_release_workspace(void);
 double b200_dev_dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
                             int *ifail, int *status);
 

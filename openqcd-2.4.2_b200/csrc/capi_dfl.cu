@@ -149,6 +149,27 @@ int b200_dfl_time(int what, int n, float *ms, int *its) {
   return cudaGetLastError() == cudaSuccess ? 0 : fail("dfl_time: CUDA error");
 }
 
+// Several systems at once (solver_batch.cu); device fields in the library's
+// layout.  status needs 2*nrhs entries when dfl != 0.
+int b200_dev_gcr_batch(int nrhs, int dfl, int nkv, int nmx, int istop, double res, const double *mu,
+                       void *const *eta, void *const *psi, double *rho, int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (!c.ready) return fail("geometry not set (call b200_geometry first)");
+  if (qcd::fields_ready(c)) return -1;
+  return qcd::gcr_batch(c, nrhs, dfl, nkv, nmx, istop, res, mu, (const void *const *)eta, psi, rho, ifail, status);
+}
+
+// Free the solvers' work fields (they are kept between calls otherwise).
+int b200_release_workspace(void) {
+  Ctx &c = ctx();
+  qcd::gcr_batch_release();
+  for (void *p : c.ws32) cudaFree(p);
+  for (void *p : c.ws64) cudaFree(p);
+  c.ws32.clear();
+  c.ws64.clear();
+  return cudaDeviceSynchronize() == cudaSuccess ? 0 : fail("CUDA error");
+}
+
 int b200_dfl_nv(void) { return ctx().dfl.ready ? ctx().dfl.nv : 0; }
 
 // Load basis vector l of every block from a global field in the reference

@@ -809,7 +809,7 @@ void dfl_release(Ctx &c) {
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
   void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop,
-                  d.lvtab, d.ldots, d.lpart, d.rpart};
+                  d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart};
   if (d.h_ldots) cudaFreeHost(d.h_ldots);
   for (void *p : bufs) cudaFree(p);
   DflState fresh;
@@ -1116,6 +1116,16 @@ static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, vo
   lstat[0] += status[0];
 }
 
+int ensure_lvd_n(Ctx &c, int n) {
+  DflState &d = c.dfl;
+  while ((int)d.lvd.size() < n) {
+    double2 *p = nullptr;
+    if (cudaMalloc(&p, (size_t)d.nv * sizeof(double2)) != cudaSuccess) return fail("out of device memory");
+    d.lvd.push_back(p);
+  }
+  return 0;
+}
+
 static int ensure_lvd(Ctx &c) {
   DflState &d = c.dfl;
   while (d.lvd.size() < 2) {
@@ -1277,6 +1287,9 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
     c.m0 = m0_save;
   }
   d.aw_valid = d.awhat_valid = false;
+  // the modes are regenerated from random fields by every call
+  for (void *p : d.modes) cudaFree(p);
+  d.modes.clear();
   return cudaStreamSynchronize(st) == cudaSuccess ? 0 : fail("dfl_modes: CUDA error");
 }
 

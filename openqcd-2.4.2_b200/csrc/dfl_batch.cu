@@ -1,0 +1,267 @@
+// Deflation for several right-hand sides at once: restriction,
+// prolongation, the little Dirac operator and the little solver applied to
+// NR fields / little vectors in one pass over the block basis and the
+// little-operator matrices, which dominate the memory traffic of these
+// steps (Ns FP32 basis fields, 8 nb Ns^2 FP64 matrix entries).  Each system
+// keeps its own arithmetic: the results equal those of the single-system
+// routines of dfl.cu up to the summation order.
+#include "lib.h"
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace qcd {
+
+constexpr int BT = 4;            // right-hand sides per pass over the basis / matrices
+
+// the fields or vectors of one pass, passed to the kernels by value
+template <int N> struct Ptrs {
+  void *p[N];
+};
+constexpr int BSPLIT_T = 352;    // threads of a restriction/prolongation CTA
+
+// sites of one parity chunk are split over nsplit CTAs of at most BSPLIT_T
+// threads, one site per thread
+static int chunk_split(int vbh) { return (vbh + BSPLIT_T - 1) / BSPLIT_T; }
+
+// ------------------------------------------------------------- restriction
+// part[(n, y, r, l)] = (basis_l, x_r) over the sites of CTA y of block n
+template <int NRT>
+__global__ void __launch_bounds__(BSPLIT_T) k_restrict_b(Geom g, const int *__restrict__ vd2lex,
+                                                         const float4 *const *__restrict__ basis, int Ns,
+                                                         Ptrs<NRT> x, int nsplit, double2 *part) {
+  extern __shared__ double2 red[];   // [Ns][NRT][nw]
+  const int n = blockIdx.x, y = blockIdx.y, p = y / nsplit, h = y - p * nsplit;
+  const int blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
+  const int per = (g.vbh + nsplit - 1) / nsplit, si = h * per + threadIdx.x;
+  const bool ok = (int)threadIdx.x < per && si < g.vbh;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  spinor<float> xs[NRT];
+#pragma unroll
+  for (int r = 0; r < NRT; r++) {
+    szero(xs[r]);
+    if (ok) xs[r] = Store<float>::load_spinor(x.p[r], chunk, si, g.vbh);
+  }
+  for (int l = 0; l < Ns; l++) {
+    spinor<float> b;
+    szero(b);
+    if (ok) b = Store<float>::load_spinor(basis[l], chunk, si, g.vbh);
+#pragma unroll
+    for (int r = 0; r < NRT; r++) {
+      float sr = 0.0f, sim = 0.0f;
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const cpx<float> bb = b.c[a].c[k], xx = xs[r].c[a].c[k];
+          sr += bb.re * xx.re + bb.im * xx.im;
+          sim += bb.re * xx.im - bb.im * xx.re;
+        }
+      double re = sr, im = sim;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_down_sync(0xffffffffu, re, o);
+        im += __shfl_down_sync(0xffffffffu, im, o);
+      }
+      if (lane == 0) red[((size_t)l * NRT + r) * nw + wp] = make_double2(re, im);
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < Ns * NRT; q += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < nw; w++) {
+      re += red[(size_t)q * nw + w].x;
+      im += red[(size_t)q * nw + w].y;
+    }
+    const int l = q / NRT, r = q - l * NRT;
+    part[(((size_t)n * gridDim.y + y) * NRT + r) * Ns + l] = make_double2(re, im);
+  }
+}
+
+// vd_r[n*Ns + l] = sum_y part[(n, y, r, l)], rounded to float
+template <int NRT>
+__global__ void k_restrict_b_fin(const double2 *__restrict__ part, int Ns, int nb, int ny, Ptrs<NRT> vd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (i >= nb * Ns) return;
+  const int n = i / Ns, l = i - n * Ns;
+  double re = 0.0, im = 0.0;
+  for (int y = 0; y < ny; y++) {
+    const double2 a = part[(((size_t)n * ny + y) * NRT + r) * Ns + l];
+    re += a.x;
+    im += a.y;
+  }
+  ((double2 *)vd.p[r])[i] = make_double2((double)(float)re, (double)(float)im);
+}
+
+// ------------------------------------------------------------ prolongation
+// s_r = sum_l vd_r[n, l] basis_l on every block n, float coefficients
+template <int NRT>
+__global__ void __launch_bounds__(BSPLIT_T) k_prolong_b(Geom g, const int *__restrict__ vd2lex,
+                                                        const float4 *const *__restrict__ basis, int Ns,
+                                                        Ptrs<NRT> vd, int nsplit, Ptrs<NRT> s) {
+  __shared__ float2 z[NRT][64];
+  const int n = blockIdx.x, y = blockIdx.y, p = y / nsplit, h = y - p * nsplit;
+  const int blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
+  for (int q = threadIdx.x; q < NRT * Ns; q += blockDim.x) {
+    const int r = q / Ns, l = q - r * Ns;
+    const double2 v = ((const double2 *)vd.p[r])[(size_t)n * Ns + l];
+    z[r][l] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncthreads();
+  const int per = (g.vbh + nsplit - 1) / nsplit, si = h * per + threadIdx.x;
+  if ((int)threadIdx.x >= per || si >= g.vbh) return;
+  spinor<float> acc[NRT];
+#pragma unroll
+  for (int r = 0; r < NRT; r++) szero(acc[r]);
+  for (int l = 0; l < Ns; l++) {
+    const spinor<float> b = Store<float>::load_spinor(basis[l], chunk, si, g.vbh);
+#pragma unroll
+    for (int r = 0; r < NRT; r++) {
+      const float zr = z[r][l].x, zi = z[r][l].y;
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          acc[r].c[a].c[k].re += zr * b.c[a].c[k].re - zi * b.c[a].c[k].im;
+          acc[r].c[a].c[k].im += zr * b.c[a].c[k].im + zi * b.c[a].c[k].re;
+        }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < NRT; r++) Store<float>::store_spinor(s.p[r], chunk, si, g.vbh, acc[r]);
+}
+
+// -------------------------------------------------- little operator, NR vectors
+// The modes of k_little_w (dfl.cu) applied to NRT vectors v_r, u_r -> w_r:
+// every matrix entry is loaded once for all of them.
+template <int NRT>
+__global__ void __launch_bounds__(288) k_little_b(int mode, int Ns, int b0, const double2 *__restrict__ Ablk,
+                                                  const double2 *__restrict__ H, const int *__restrict__ nbr,
+                                                  Ptrs<NRT> v, Ptrs<NRT> u, Ptrs<NRT> w) {
+  __shared__ double2 part[9][64][NRT];
+  const int n = b0 + blockIdx.x, wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nw = blockDim.x >> 5;
+  const bool diag = mode == 3 || wp == 8;
+  const double2 *a = diag ? Ablk + (size_t)n * Ns * Ns : H + ((size_t)8 * n + wp) * Ns * Ns;
+  const size_t xoff = diag ? (size_t)n * Ns : (size_t)__ldg(nbr + 8 * n + wp) * Ns;
+  const Ptrs<NRT> &src = (!diag && mode == 2) ? u : v;
+#pragma unroll
+  for (int hh = 0; hh < 2; hh++) {
+    const int k = lane + 32 * hh;
+    if (k < Ns) {
+      double re[NRT], im[NRT];
+#pragma unroll
+      for (int r = 0; r < NRT; r++) re[r] = im[r] = 0.0;
+      for (int l = 0; l < Ns; l++) {
+        const double2 aa = __ldg(a + (size_t)l * Ns + k);
+#pragma unroll
+        for (int r = 0; r < NRT; r++) {
+          const double2 xx = __ldg((const double2 *)src.p[r] + xoff + l);
+          re[r] += aa.x * xx.x - aa.y * xx.y;
+          im[r] += aa.x * xx.y + aa.y * xx.x;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < NRT; r++) part[wp][k][r] = make_double2(re[r], im[r]);
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < Ns * NRT; q += blockDim.x) {
+    const int k = q / NRT, r = q - k * NRT;
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < nw; j++) {
+      re += part[j][k][r].x;
+      im += part[j][k][r].y;
+    }
+    if (mode == 2) {
+      const double2 vv = ((const double2 *)v.p[r])[(size_t)n * Ns + k];
+      ((double2 *)w.p[r])[(size_t)n * Ns + k] = make_double2(vv.x - re, vv.y - im);
+    } else {
+      ((double2 *)w.p[r])[(size_t)n * Ns + k] = make_double2(re, im);
+    }
+  }
+}
+
+// ------------------------------------------------------------ host wrappers
+template <int N> static Ptrs<N> ptrs(const void *const *a) {
+  Ptrs<N> q;
+  for (int i = 0; i < N; i++) q.p[i] = a ? const_cast<void *>(a[i]) : nullptr;
+  return q;
+}
+
+int dfl_batch_alloc(Ctx &c) {
+  DflState &d = c.dfl;
+  if (d.bpart) return 0;
+  const int ns = chunk_split(c.g.vbh);
+  if (cudaMalloc(&d.bpart, (size_t)d.nb * 2 * ns * BT * d.Ns * sizeof(double2)) != cudaSuccess)
+    return fail("out of device memory (batched deflation)");
+  return 0;
+}
+
+template <int NRT>
+static void restrict_pass(Ctx &c, const void *const *x, double2 *const *vd, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
+  const size_t shm = (size_t)d.Ns * NRT * (t / 32) * sizeof(double2);
+  k_restrict_b<NRT><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
+                                                         ptrs<NRT>(x), ns, d.bpart);
+  const int nn = d.nb * d.Ns;
+  k_restrict_b_fin<NRT><<<dim3((nn + 255) / 256, NRT), 256, 0, st>>>(d.bpart, d.Ns, d.nb, 2 * ns,
+                                                                      ptrs<NRT>((const void *const *)vd));
+}
+
+// vd[r] = restriction of the FP32 fields x[r], r < nr
+void dfl_restrict_b(Ctx &c, int nr, const void *const *x, double2 *const *vd, cudaStream_t st) {
+  int r = 0;
+  for (; r + BT <= nr; r += BT) restrict_pass<BT>(c, x + r, vd + r, st);
+  for (; r + 2 <= nr; r += 2) restrict_pass<2>(c, x + r, vd + r, st);
+  for (; r < nr; r++) restrict_pass<1>(c, x + r, vd + r, st);
+}
+
+template <int NRT>
+static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
+  k_prolong_b<NRT><<<dim3(d.nb, 2 * ns), t, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
+                                                      ptrs<NRT>((const void *const *)vd), ns,
+                                                      ptrs<NRT>((const void *const *)s));
+}
+
+// s[r] = prolongation of the little vectors vd[r], r < nr
+void dfl_prolong_b(Ctx &c, int nr, const double2 *const *vd, void *const *s, cudaStream_t st) {
+  int r = 0;
+  for (; r + BT <= nr; r += BT) prolong_pass<BT>(c, vd + r, s + r, st);
+  for (; r + 2 <= nr; r += 2) prolong_pass<2>(c, vd + r, s + r, st);
+  for (; r < nr; r++) prolong_pass<1>(c, vd + r, s + r, st);
+}
+
+template <int NRT>
+static void little_pass(Ctx &c, int mode, int b0, int nblk, const double2 *A, const double2 *H,
+                        const double2 *const *v, const double2 *const *u, double2 *const *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int nw = mode == 3 ? 1 : (mode == 0 ? 9 : 8);
+  k_little_b<NRT><<<nblk, 32 * nw, 0, st>>>(mode, d.Ns, b0, A, H, d.nbr, ptrs<NRT>((const void *const *)v),
+                                            ptrs<NRT>((const void *const *)u), ptrs<NRT>((const void *const *)w));
+}
+
+void little_b(Ctx &c, int nr, int mode, int b0, int nblk, const double2 *A, const double2 *H,
+              const double2 *const *v, const double2 *const *u, double2 *const *w, cudaStream_t st) {
+  int r = 0;
+  for (; r + BT <= nr; r += BT) little_pass<BT>(c, mode, b0, nblk, A, H, v + r, u ? u + r : nullptr, w + r, st);
+  for (; r < nr; r++) little_pass<1>(c, mode, b0, nblk, A, H, v + r, u ? u + r : nullptr, w + r, st);
+}
+
+// w_r = Awhat v_r (even halves), t_r odd intermediates
+void dfl_Awhat_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, double2 *const *t, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int nbh = d.nb / 2;
+  little_b(c, nr, 1, nbh, nbh, nullptr, d.Mhop, v, nullptr, t, st);
+  little_b(c, nr, 2, 0, nbh, nullptr, d.Mhop, v, (const double2 *const *)t, w, st);
+}
+
+void dfl_Aw_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  little_b(c, nr, 0, 0, d.nb, d.Ablk, d.Ahop, v, nullptr, w, st);
+}
+
+}  // namespace qcd

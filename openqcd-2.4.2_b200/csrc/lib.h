@@ -23,6 +23,7 @@ struct DflState {
   int *vd2lex = nullptr, *nbr = nullptr;
   int *faces = nullptr, *nfc = nullptr, fmax = 0;   // block-face site lists
   double2 *rpart = nullptr;                          // restriction partial sums [nb][2][Ns]
+  double2 *bpart = nullptr;                          // the same for batched restriction
   std::vector<void *> basis, modes;
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
@@ -192,6 +193,22 @@ int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st
 // dfl.cu
 int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
+// dfl_batch.cu: the deflation steps for nr right-hand sides at once
+int dfl_batch_alloc(Ctx &c);
+int ensure_lvd_n(Ctx &c, int n);
+// solver_batch.cu
+int ltl_gcr_b(Ctx &c, double mu, int nr, const double2 *const *eta, double2 *const *psi, int *ifail, int *status,
+              cudaStream_t st);
+int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, const double *mu,
+              const void *const *eta, void *const *psi, double *rho, int *ifail, int *status);
+void gcr_batch_release();
+void ltl_batch_release();
+void dfl_restrict_b(Ctx &c, int nr, const void *const *x, double2 *const *vd, cudaStream_t st);
+void dfl_prolong_b(Ctx &c, int nr, const double2 *const *vd, void *const *s, cudaStream_t st);
+void little_b(Ctx &c, int nr, int mode, int b0, int nblk, const double2 *A, const double2 *H,
+              const double2 *const *v, const double2 *const *u, double2 *const *w, cudaStream_t st);
+void dfl_Awhat_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, double2 *const *t, cudaStream_t st);
+void dfl_Aw_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, cudaStream_t st);
 void dfl_restrict(Ctx &c, int prec, const void *s, double2 *vd, cudaStream_t st);
 void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st);
 int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st);

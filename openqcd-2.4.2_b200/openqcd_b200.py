@@ -105,6 +105,9 @@ _SIGS = {
     "b200_set_dfl_gen_parms": (C.c_int, [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
     "b200_dfl_nv": (C.c_int, []),
     "b200_dfl_profile": (C.c_int, [C.c_int, C.c_void_p]),
+    "b200_dev_gcr_batch": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_release_workspace": (C.c_int, []),
     "b200_dfl_time": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
@@ -347,6 +350,24 @@ def dev_dfl_sap_gcr(nkv, nmx, istop, res, mu, eta, psi):
     if rho < 0:
         raise B200Error(_err_after())
     return rho, ifail.value, list(status)
+
+
+def dev_gcr_batch(nkv, nmx, istop, res, mus, etas, psis, dfl=False):
+    """Solve len(etas) systems together (device fields); returns per-system
+    (rho, ifail, status[, little steps])."""
+    n = len(etas)
+    mu = (C.c_double * n)(*mus)
+    ep = (C.c_void_p * n)(*[e.ptr for e in etas])
+    pp = (C.c_void_p * n)(*[p.ptr for p in psis])
+    rho = (C.c_double * n)()
+    ifail = (C.c_int * n)()
+    status = (C.c_int * (2 * n))()
+    check(lib().b200_dev_gcr_batch(n, 1 if dfl else 0, nkv, nmx, istop, res, mu, ep, pp, rho, ifail, status))
+    return list(rho), list(ifail), list(status[:n]), list(status[n:])
+
+
+def release_workspace():
+    return check(lib().b200_release_workspace())
 
 
 def sap_gcr(nkv, nmx, istop, res, mu, eta):

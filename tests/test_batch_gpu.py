@@ -1,0 +1,113 @@
+"""Several right-hand sides solved together (b200_dev_gcr_batch, no reference
+counterpart).  Every system runs the reference's algorithm (fgcr with SAP,
+modules/sap/sap_gcr.c:140, or with deflated SAP, modules/dfl/dfl_sap_gcr.c:353)
+on its own Krylov space, so each must reach the FP64 true residual 1e-10,
+checked with the reference's Dw_dble, in the same number of steps as the
+single-system solver (plain: the same arithmetic, so the same solution to
+1e-12; deflated: the batched restriction and little solver sum in another
+order, so within one step and 1e-8).  Systems of different twisted masses
+and a zero source share a batch; systems leave it as they converge."""
+import numpy as np
+import pytest
+
+import openqcd_b200 as qb
+from helpers import Setup, rel_norm_err
+
+pytestmark = pytest.mark.gpu
+
+L = (8, 8, 8, 8)
+BS = (4, 4, 4, 4)
+NS = 8
+M0 = -0.2
+
+
+@pytest.fixture(scope="module")
+def setup():
+    s = Setup(L, BS, eps=0.4, csw=1.5, m0=M0)
+    qb.set_sap_parms(BS, 1, 4, 5)
+    return s
+
+
+def dev(prec, arr=None):
+    f = qb.DevField(prec)
+    if arr is not None:
+        f.from_ref(arr)
+    return f
+
+
+def true_res(setup, mu, psi, eta):
+    r = eta - setup.ref.dirac_dble(0, mu, psi)
+    return np.linalg.norm(r) / np.linalg.norm(eta)
+
+
+def test_plain_batch_matches_single(setup):
+    mus = [0.0, 0.02, 0.08]
+    etas = [setup.source(41 + i) for i in range(3)]
+    singles = []
+    for mu, eta in zip(mus, etas):
+        e, p = dev(64, eta), dev(64)
+        rho, ifail, st = qb.dev_sap_gcr(16, 256, 0, 1e-10, mu, e, p)
+        singles.append((p.to_ref(setup.vol), st))
+    E = [dev(64, e) for e in etas]
+    P = [dev(64) for _ in etas]
+    rho, ifail, st, _ = qb.dev_gcr_batch(16, 256, 0, 1e-10, mus, E, P)
+    assert ifail == [0, 0, 0]
+    for i in range(3):
+        psi = P[i].to_ref(setup.vol)
+        assert st[i] == singles[i][1]
+        assert rel_norm_err(psi, singles[i][0]) <= 1e-12
+        assert true_res(setup, mus[i], psi, etas[i]) <= 1.5e-10
+
+
+def test_plain_batch_zero_source(setup):
+    eta = setup.source(45)
+    E = [dev(64, np.zeros_like(eta)), dev(64, eta)]
+    P = [dev(64, eta), dev(64)]
+    rho, ifail, st, _ = qb.dev_gcr_batch(16, 256, 0, 1e-10, [0.0, 0.0], E, P)
+    assert rho[0] == 0.0 and ifail == [0, 0]
+    assert not P[0].to_ref(setup.vol).any()
+    assert true_res(setup, 0.0, P[1].to_ref(setup.vol), eta) <= 1.5e-10
+
+
+@pytest.fixture(scope="module")
+def dfl(setup):
+    setup.ref.set_sap_parms(BS, 1, 4, 5)
+    setup.nv = setup.ref.dfl_init(BS, NS, nkv=16, nmx=256, res=1e-2, nmx_gcr=24, res_gcr=1e-2,
+                                  kappa=1.0 / (2.0 * (4.0 + M0)), mu=0.0, ninv=5, nmr=4, ncy=4)
+    f, _ = setup.ref.dfl_modes(7)
+    assert f == 0
+    assert qb.set_dfl_parms(BS, NS) == setup.nv
+    qb.set_dfl_pro_parms(16, 256, 1e-2, 24, 1e-2)
+    for l in range(NS):
+        qb.dfl_set_basis(l, setup.ref.dfl_get_basis(l))
+    return setup
+
+
+@pytest.mark.parametrize("nr", [1, 5])
+def test_dfl_batch_matches_single(dfl, nr):
+    mu = 0.01
+    etas = [dfl.source(51 + i) for i in range(nr)]
+    singles = []
+    for eta in etas:
+        e, p = dev(64, eta), dev(64)
+        rho, ifail, st = qb.dev_dfl_sap_gcr(16, 256, 0, 1e-10, mu, e, p)
+        assert ifail == 0
+        singles.append((p.to_ref(dfl.vol), st[0]))
+    E = [dev(64, e) for e in etas]
+    P = [dev(64) for _ in etas]
+    rho, ifail, st, lst = qb.dev_gcr_batch(16, 256, 0, 1e-10, [mu] * nr, E, P, dfl=True)
+    assert ifail == [0] * nr
+    for i in range(nr):
+        psi = P[i].to_ref(dfl.vol)
+        assert abs(st[i] - singles[i][1]) <= 1, (st, [x[1] for x in singles])
+        assert lst[i] > 0
+        assert rel_norm_err(psi, singles[i][0]) <= 1e-8
+        assert true_res(dfl, mu, psi, etas[i]) <= 1.5e-10
+
+
+def test_dfl_batch_needs_one_mass(dfl):
+    E = [dev(64, dfl.source(60)), dev(64, dfl.source(61))]
+    P = [dev(64), dev(64)]
+    with pytest.raises(qb.B200Error):
+        qb.dev_gcr_batch(16, 256, 0, 1e-10, [0.0, 0.01], E, P, dfl=True)
+    qb.release_workspace()
