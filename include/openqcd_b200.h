@@ -201,7 +201,8 @@ int b200_dfl_profile(int on, double *out);
 /* Device time (CUDA events) of n calls of one deflation kernel (no
  * reference counterpart): what = 0 restriction of an FP32 field, 1
  * prolongation, 2 Awhat_dble, 3 Aw_dble, 4 ltl_gcr on a random little
- * vector (its: GCR steps of the last solve). */
+ * vector (its: GCR steps of the last solve), 5-7 the batched restriction,
+ * prolongation and little solver on four right-hand sides. */
 int b200_dfl_time(int what, int n, float *ms, int *its);
 /* Basis vector l of every block as one global FP32 field, reference layout. */
 int b200_dfl_set_basis(int l, const spinor *field);

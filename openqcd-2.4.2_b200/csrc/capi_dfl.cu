@@ -116,7 +116,9 @@ int b200_dfl_profile(int on, double *out) {
 
 // Device timing of the deflation kernels (no reference counterpart): what =
 // 0 restriction of an FP32 field, 1 prolongation, 2 Awhat_dble, 3 Aw_dble,
-// 4 ltl_gcr on a random little vector (status[0] of the last solve in *its).
+// 4 ltl_gcr on a random little vector (status[0] of the last solve in *its),
+// 5, 6, 7 the batched restriction, prolongation and little solver on four
+// right-hand sides.
 int b200_dfl_time(int what, int n, float *ms, int *its) {
   Ctx &c = ctx();
   if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1;
@@ -128,6 +130,20 @@ int b200_dfl_time(int what, int n, float *ms, int *its) {
   if (!f || !a || !b || !t) return -1;
   qcd::gen_uniform_spinor32(c, f, 11, c.stream);
   qcd::dfl_restrict(c, 32, f, a, c.stream);
+  // four fields and little vectors for the batched kernels (what >= 5)
+  const void *fs[4];
+  double2 *vs[4];
+  if (what >= 5) {
+    if (qcd::dfl_batch_alloc(c) || qcd::ensure_lvd_n(c, 8)) return -1;
+    for (int i = 0; i < 4; i++) {
+      void *fi = qcd::spinor_stage(c, 32, 1 + i);
+      if (!fi) return -1;
+      qcd::gen_uniform_spinor32(c, fi, 20 + i, c.stream);
+      fs[i] = fi;
+      vs[i] = d.lvd[4 + i];
+      cudaMemcpyAsync(vs[i], a, (size_t)d.nv * sizeof(double2), cudaMemcpyDeviceToDevice, c.stream);
+    }
+  }
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -138,7 +154,17 @@ int b200_dfl_time(int what, int n, float *ms, int *its) {
     else if (what == 1) qcd::dfl_prolong(c, a, f, c.stream);
     else if (what == 2) qcd::dfl_Awhat(c, a, b, t, c.stream);
     else if (what == 3) qcd::dfl_Aw(c, a, b, c.stream);
-    else qcd::dfl_ltl_gcr(c, d.aw_mu, a, b, &fl, st, c.stream);
+    else if (what == 4) qcd::dfl_ltl_gcr(c, d.aw_mu, a, b, &fl, st, c.stream);
+    else if (what == 5) qcd::dfl_restrict_b(c, 4, fs, vs, c.stream);
+    else if (what == 6) qcd::dfl_prolong_b(c, 4, (const double2 *const *)vs, (void *const *)fs, c.stream);
+    else if (what == 7 || what == 9) {
+      int f4[4], s4[4];
+      const int nr = what == 7 ? 4 : 1;
+      qcd::ltl_gcr_b(c, d.aw_mu, nr, (const double2 *const *)vs, vs + 4 - nr, f4, s4, c.stream);
+      st[0] = s4[0];
+    } else {
+      qcd::dfl_Awhat_b(c, 4, (const double2 *const *)vs, vs + 0, vs + 0, c.stream);
+    }
   }
   cudaEventRecord(e1, c.stream);
   cudaEventSynchronize(e1);
@@ -146,7 +172,8 @@ int b200_dfl_time(int what, int n, float *ms, int *its) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (its) *its = st[0];
-  return cudaGetLastError() == cudaSuccess ? 0 : fail("dfl_time: CUDA error");
+  if (cudaGetLastError() != cudaSuccess) return fail("dfl_time: CUDA error");
+  return qcd::dfl_batch_check(c);
 }
 
 // Several systems at once (solver_batch.cu); device fields in the library's

@@ -29,7 +29,7 @@ static double now_s() {
 }
 // with profiling on: wait for the stream and charge the time since the
 // previous mark to phase k
-static void mark(Ctx &c, int k) {
+void dfl_mark(Ctx &c, int k) {
   DflState &d = c.dfl;
   if (!d.profile) return;
   cudaStreamSynchronize(c.stream);
@@ -809,7 +809,7 @@ void dfl_release(Ctx &c) {
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
   void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop,
-                  d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart};
+                  d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart, d.kerr};
   if (d.h_ldots) cudaFreeHost(d.h_ldots);
   for (void *p : bufs) cudaFree(p);
   DflState fresh;
@@ -1100,17 +1100,17 @@ static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, vo
   cudaStream_t st = c.stream;
   double2 *vd = d.lvd[0];
   int ifail, status[2];
-  mark(c, 5);
+  dfl_mark(c, 5);
   dfl_restrict(c, 32, rho, vd, st);
   dfl_ltl_gcr(c, mu, vd, vd, &ifail, status, st);
   dfl_prolong(c, vd, ws0, st);
-  mark(c, 3);
+  dfl_mark(c, 3);
   dirac_op<float>(c, 0, (float)mu, ws0, chi, c.tmp32, st);
   la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - D ws0
   la_zero(c, 32, phi, PAR_ALL, st);
-  mark(c, 5);
+  dfl_mark(c, 5);
   sap_cycles(c, (float)mu, c.isolv, c.nmr, c.ncy, phi, chi, phib, st);
-  mark(c, 4);
+  dfl_mark(c, 4);
   la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - chi
   la_axpy(c, 32, phi, 1.0, 0.0, ws0, PAR_ALL, st);
   lstat[0] += status[0];
@@ -1154,9 +1154,9 @@ double dfl_sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double m
   }
   if (c.isolv == 1 && (c.sw_inv_fail & 2)) {
     ifail[0] = -3;
-  } else if ((mark(c, 5), dfl_set_Awhat(c, mu, st))) {
+  } else if ((dfl_mark(c, 5), dfl_set_Awhat(c, mu, st))) {
     ifail[0] = -2;
-  } else if ((mark(c, 2), rho != 0.0)) {
+  } else if ((dfl_mark(c, 2), rho != 0.0)) {
     if (reserve32(c, c.ws32, 2 * nkv + 3)) return -1.0;
     while (c.ws64.size() < 3) {
       void *p = nullptr;
@@ -1224,7 +1224,7 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   void *ws0 = c.ws32[0], *ws1 = c.ws32[1], *phib = c.ws32[2];
   const float mug = (float)d.gen_mu;
   for (int l = 0; l < d.Ns; l++) gen_uniform_spinor32(c, d.modes[l], seed * 1000003ull + l, st);
-  mark(c, -1);
+  dfl_mark(c, -1);
   if (ifail[0] == 0) {
     int n;
     for (n = 0; n < 3; n++) {
@@ -1234,28 +1234,28 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
         sap_cycles(c, mug, 1, d.gen_nmr, n + 1, d.modes[l], ws0, phib, st);
       }
     }
-    mark(c, 0);
+    dfl_mark(c, 0);
     if (dfl_subspace_dev(c, d.modes, st)) return -1;
-    mark(c, 1);
+    dfl_mark(c, 1);
     for (; n < d.gen_ninv && ifail[0] == 0; n++) {
       if (dfl_set_Awhat(c, d.gen_mu, st)) {
         ifail[0] = -2;
         break;
       }
-      mark(c, 2);
+      dfl_mark(c, 2);
       for (int l = 0; l < d.Ns; l++) {
         int lf, ls[2];
         double2 *vd = d.lvd[0];
         dfl_restrict(c, 32, d.modes[l], vd, st);
         dfl_ltl_gcr(c, d.gen_mu, vd, vd, &lf, ls, st);
         dfl_prolong(c, vd, ws1, st);
-        mark(c, 3);
+        dfl_mark(c, 3);
         dirac_op<float>(c, 0, mug, ws1, ws0, c.tmp32, st);
         la_diff(c, 32, d.modes[l], ws0, PAR_ALL, st);     // ws0 = mode - D ws1
         la_zero(c, 32, d.modes[l], PAR_ALL, st);
-        mark(c, 5);
+        dfl_mark(c, 5);
         sap_cycles(c, mug, 1, d.gen_nmr, d.gen_ncy, d.modes[l], ws0, phib, st);
-        mark(c, 4);
+        dfl_mark(c, 4);
         la_axpy(c, 32, d.modes[l], 1.0, 0.0, ws1, PAR_ALL, st);
         status[0] += ls[0];
       }
@@ -1271,9 +1271,9 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
         float nrm = (float)sqrt((double)(float)(r[0] + r[1]));
         if (nrm != 0.0f) la_scale(c, 32, d.modes[l], 1.0f / nrm, PAR_ALL, st);
       }
-      mark(c, 5);
+      dfl_mark(c, 5);
       if (dfl_subspace_dev(c, d.modes, st)) return -1;
-      mark(c, 1);
+      dfl_mark(c, 1);
     }
     const int nst = d.Ns * (n - 3);
     if (nst > 0) status[0] = (status[0] + nst / 2) / nst;

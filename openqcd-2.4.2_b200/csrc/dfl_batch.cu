@@ -6,6 +6,7 @@
 // keeps its own arithmetic: the results equal those of the single-system
 // routines of dfl.cu up to the summation order.
 #include "lib.h"
+#include "tma.cuh"
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -182,6 +183,161 @@ __global__ void __launch_bounds__(288) k_little_b(int mode, int Ns, int b0, cons
   }
 }
 
+// ----------------------------------------------- TMA-staged variants
+// The same restriction and prolongation with the basis planes of the
+// CTA's sites streamed into shared memory by bulk asynchronous copies
+// (cp.async.bulk, one per plane and basis vector, issued by one thread),
+// double-buffered so that the copy of basis vector l+1 overlaps the
+// arithmetic on vector l.  A plane segment is cnt consecutive float4 at
+// ((chunk*6 + j)*vbh + s0): 16-byte aligned, cnt*16 bytes.
+template <int NRT, bool RESTRICT>
+__global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__restrict__ vd2lex,
+                                                         const float4 *const *__restrict__ basis, int Ns,
+                                                         Ptrs<NRT> fld, Ptrs<NRT> vd, int nsplit, double2 *part,
+                                                         int *err) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ float2 z[RESTRICT ? 1 : NRT][64];
+  const int n = blockIdx.x, y = blockIdx.y, p = y / nsplit, h = y - p * nsplit;
+  const int blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
+  const int per = (g.vbh + nsplit - 1) / nsplit, s0 = h * per, cnt = min(per, g.vbh - s0);
+  const int si = s0 + threadIdx.x;
+  const bool ok = (int)threadIdx.x < cnt;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  float4 *buf = (float4 *)smraw;                                  // [2][6][per]
+  double2 *red = (double2 *)(buf + (size_t)12 * per);             // [Ns][NRT][nw]
+  const unsigned bytes = (unsigned)cnt * 16u;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  if (!RESTRICT)
+    for (int q = threadIdx.x; q < NRT * Ns; q += blockDim.x) {
+      const int r = q / Ns, l = q - r * Ns;
+      const double2 v = ((const double2 *)vd.p[r])[(size_t)n * Ns + l];
+      z[r][l] = make_float2((float)v.x, (float)v.y);
+    }
+  __syncthreads();
+  auto issue = [&](int l, int stg) {
+    mbar_expect_tx(&bar[stg], 6u * bytes);
+    const float4 *src = basis[l] + (size_t)chunk * 6 * g.vbh + s0;
+#pragma unroll
+    for (int j = 0; j < 6; j++) bulk_g2s(buf + ((size_t)stg * 6 + j) * per, src + (size_t)j * g.vbh, bytes, &bar[stg]);
+  };
+  spinor<float> xs[NRT];
+#pragma unroll
+  for (int r = 0; r < NRT; r++) {
+    szero(xs[r]);
+    if (RESTRICT && ok) xs[r] = Store<float>::load_spinor(fld.p[r], chunk, si, g.vbh);
+  }
+  if (threadIdx.x == 0 && Ns > 0) issue(0, 0);
+  for (int l = 0; l < Ns; l++) {
+    const int stg = l & 1;
+    if (threadIdx.x == 0 && l + 1 < Ns) issue(l + 1, stg ^ 1);
+    mbar_wait(&bar[stg], (unsigned)(l >> 1) & 1u, err);
+    spinor<float> b;
+    szero(b);
+    if (ok)
+#pragma unroll
+      for (int j = 0; j < 6; j++) {
+        const float4 v = buf[((size_t)stg * 6 + j) * per + threadIdx.x];
+        const int k = 2 * j;
+        b.c[k / 3].c[k % 3] = mk<float>(v.x, v.y);
+        b.c[(k + 1) / 3].c[(k + 1) % 3] = mk<float>(v.z, v.w);
+      }
+    if constexpr (RESTRICT && NRT == 4) {
+      // the 8 sums of a warp (4 fields x re, im) by a reduce-scatter
+      // butterfly: 9 shuffles instead of 40; lane L ends with the sum of
+      // value (L>>4 & 1)*4 + (L>>3 & 1)*2 + (L>>2 & 1)
+      float v[8];
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        float sr = 0.0f, sim = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const cpx<float> bb = b.c[a].c[k], xx = xs[r].c[a].c[k];
+            sr += bb.re * xx.re + bb.im * xx.im;
+            sim += bb.re * xx.im - bb.im * xx.re;
+          }
+        v[2 * r] = sr;
+        v[2 * r + 1] = sim;
+      }
+      const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float snd = h16 ? v[i] : v[i + 4], keep = h16 ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, snd, 16);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const float snd = h8 ? v[i] : v[i + 2], keep = h8 ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, snd, 8);
+      }
+      {
+        const float snd = h4 ? v[0] : v[1], keep = h4 ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, snd, 4);
+      }
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+      if ((lane & 3) == 0) {
+        const int idx = (h16 ? 4 : 0) + (h8 ? 2 : 0) + (h4 ? 1 : 0), r = idx >> 1;
+        double2 *dst = &red[((size_t)l * NRT + r) * nw + wp];
+        if (idx & 1) dst->y = v[0];
+        else dst->x = v[0];
+      }
+    } else
+#pragma unroll
+    for (int r = 0; r < NRT; r++) {
+      if (RESTRICT) {
+        float sr = 0.0f, sim = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            const cpx<float> bb = b.c[a].c[k], xx = xs[r].c[a].c[k];
+            sr += bb.re * xx.re + bb.im * xx.im;
+            sim += bb.re * xx.im - bb.im * xx.re;
+          }
+        // a warp's 32 site products are summed in FP32 (the result is
+        // rounded to FP32), the warps' sums in double
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          sr += __shfl_down_sync(0xffffffffu, sr, o);
+          sim += __shfl_down_sync(0xffffffffu, sim, o);
+        }
+        if (lane == 0) red[((size_t)l * NRT + r) * nw + wp] = make_double2(sr, sim);
+      } else {
+        const float zr = z[r][l].x, zi = z[r][l].y;
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            xs[r].c[a].c[k].re += zr * b.c[a].c[k].re - zi * b.c[a].c[k].im;
+            xs[r].c[a].c[k].im += zr * b.c[a].c[k].im + zi * b.c[a].c[k].re;
+          }
+      }
+    }
+    __syncthreads();   // buffer stg is refilled by the copy issued in iteration l + 1
+  }
+  if (RESTRICT) {
+    for (int q = threadIdx.x; q < Ns * NRT; q += blockDim.x) {
+      double re = 0.0, im = 0.0;
+      for (int w = 0; w < nw; w++) {
+        re += red[(size_t)q * nw + w].x;
+        im += red[(size_t)q * nw + w].y;
+      }
+      const int l = q / NRT, r = q - l * NRT;
+      part[(((size_t)n * gridDim.y + y) * NRT + r) * Ns + l] = make_double2(re, im);
+    }
+  } else if (ok) {
+#pragma unroll
+    for (int r = 0; r < NRT; r++) Store<float>::store_spinor(fld.p[r], chunk, si, g.vbh, xs[r]);
+  }
+}
+
 // ------------------------------------------------------------ host wrappers
 template <int N> static Ptrs<N> ptrs(const void *const *a) {
   Ptrs<N> q;
@@ -193,8 +349,23 @@ int dfl_batch_alloc(Ctx &c) {
   DflState &d = c.dfl;
   if (d.bpart) return 0;
   const int ns = chunk_split(c.g.vbh);
-  if (cudaMalloc(&d.bpart, (size_t)d.nb * 2 * ns * BT * d.Ns * sizeof(double2)) != cudaSuccess)
+  if (cudaMalloc(&d.bpart, (size_t)d.nb * 2 * ns * BT * d.Ns * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc(&d.kerr, sizeof(int)) != cudaSuccess)
     return fail("out of device memory (batched deflation)");
+  cudaMemset(d.kerr, 0, sizeof(int));
+  return 0;
+}
+
+// 0, or -1 with an error message if a kernel's bounded wait gave up
+int dfl_batch_check(Ctx &c) {
+  DflState &d = c.dfl;
+  if (!d.kerr) return 0;
+  int h = 0;
+  cudaMemcpy(&h, d.kerr, sizeof(int), cudaMemcpyDeviceToHost);
+  if (h) {
+    cudaMemset(d.kerr, 0, sizeof(int));
+    return fail("deflation: a bulk copy did not complete in time");
+  }
   return 0;
 }
 
@@ -202,9 +373,11 @@ template <int NRT>
 static void restrict_pass(Ctx &c, const void *const *x, double2 *const *vd, cudaStream_t st) {
   DflState &d = c.dfl;
   const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
-  const size_t shm = (size_t)d.Ns * NRT * (t / 32) * sizeof(double2);
-  k_restrict_b<NRT><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
-                                                         ptrs<NRT>(x), ns, d.bpart);
+  const size_t shm = (size_t)12 * per * sizeof(float4) + (size_t)d.Ns * NRT * (t / 32) * sizeof(double2);
+  cudaFuncSetAttribute(k_dfl_stream<NRT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  k_dfl_stream<NRT, true><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
+                                                               d.Ns, ptrs<NRT>(x), ptrs<NRT>(nullptr), ns, d.bpart,
+                                                               d.kerr);
   const int nn = d.nb * d.Ns;
   k_restrict_b_fin<NRT><<<dim3((nn + 255) / 256, NRT), 256, 0, st>>>(d.bpart, d.Ns, d.nb, 2 * ns,
                                                                       ptrs<NRT>((const void *const *)vd));
@@ -222,9 +395,12 @@ template <int NRT>
 static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st) {
   DflState &d = c.dfl;
   const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
-  k_prolong_b<NRT><<<dim3(d.nb, 2 * ns), t, 0, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
-                                                      ptrs<NRT>((const void *const *)vd), ns,
-                                                      ptrs<NRT>((const void *const *)s));
+  const size_t shm = (size_t)12 * per * sizeof(float4);
+  cudaFuncSetAttribute(k_dfl_stream<NRT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  k_dfl_stream<NRT, false><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
+                                                                d.Ns, ptrs<NRT>((const void *const *)s),
+                                                                ptrs<NRT>((const void *const *)vd), ns, nullptr,
+                                                                d.kerr);
 }
 
 // s[r] = prolongation of the little vectors vd[r], r < nr

@@ -24,6 +24,7 @@ struct DflState {
   int *faces = nullptr, *nfc = nullptr, fmax = 0;   // block-face site lists
   double2 *rpart = nullptr;                          // restriction partial sums [nb][2][Ns]
   double2 *bpart = nullptr;                          // the same for batched restriction
+  int *kerr = nullptr;                               // error flag of bounded waits in kernels
   std::vector<void *> basis, modes;
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
@@ -195,7 +196,9 @@ int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
 // dfl_batch.cu: the deflation steps for nr right-hand sides at once
 int dfl_batch_alloc(Ctx &c);
+void dfl_mark(Ctx &c, int k);
 int ensure_lvd_n(Ctx &c, int n);
+int dfl_batch_check(Ctx &c);
 // solver_batch.cu
 int ltl_gcr_b(Ctx &c, double mu, int nr, const double2 *const *eta, double2 *const *psi, int *ifail, int *status,
               cudaStream_t st);

@@ -452,6 +452,9 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
     if (A.empty()) break;
     const int na = (int)A.size();
     // --- Mop for all active systems: phi_k = M rho, chi_k = D phi_k
+    // (phase timers, when on: 3 deflation, 4 SAP, 2 rest of Mop,
+    // 1 orthogonalisation, 0 restarts)
+    dfl_mark(c, -1);
     if (dfl) {
       std::vector<const void *> rh(na);
       std::vector<double2 *> v(na);
@@ -465,15 +468,19 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       dfl_restrict_b(c, na, rh.data(), v.data(), st);
       if (ltl_gcr_b(c, mu[0], na, (const double2 *const *)v.data(), v.data(), lf.data(), ls.data(), st)) return -1;
       dfl_prolong_b(c, na, (const double2 *const *)v.data(), w0.data(), st);
+      dfl_mark(c, 3);
       for (int i = 0; i < na; i++) {
         SysState &y = S[A[i]];
         void *ph = y.phi[y.k], *ch = y.chi[y.k];
         dirac_op<float>(c, 0, (float)y.mu, y.ws0, ch, c.tmp32, st);
         la_diff(c, 32, y.rho, ch, PAR_ALL, st);        // ch = rho - D ws0
         la_zero(c, 32, ph, PAR_ALL, st);
+        dfl_mark(c, 2);
         sap_cycles(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ph, ch, phib, st);
+        dfl_mark(c, 4);
         la_diff(c, 32, y.rho, ch, PAR_ALL, st);        // ch = rho - ch
         la_axpy(c, 32, ph, 1.0, 0.0, y.ws0, PAR_ALL, st);
+        dfl_mark(c, 2);
         y.lstat += ls[i];
       }
     } else {
@@ -482,8 +489,11 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
         void *ph = y.phi[y.k], *ch = y.chi[y.k];
         la_zero(c, 32, ph, PAR_ALL, st);
         la_copy(c, 32, y.rho, 32, ch, PAR_ALL, st);
+        dfl_mark(c, 2);
         sap_cycles(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ph, ch, phib, st);
+        dfl_mark(c, 4);
         la_diff(c, 32, y.rho, ch, PAR_ALL, st);
+        dfl_mark(c, 2);
       }
     }
     // --- the rest of gcr_step, and restarts, per system (fgcr.c:157-299)
@@ -500,6 +510,7 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       o.axpy32(y.rho, -y.cc[k].re, -y.cc[k].im, y.chi[k]);
       y.rn = o.res32(y.rho, istop);
       y.status += 1;
+      dfl_mark(c, 1);
       if (y.rn <= y.tol || y.rn < PRECISION_LIMIT * y.rn_old || k == nkv - 1 || y.status >= nmx) {
         // update_psi (fgcr.c:181)
         for (int l = k; l >= 0; l--) {
@@ -521,6 +532,7 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
         y.rn = o.res32(y.rho, istop);
         y.k = 0;
         y.rn_old = y.rn;
+        dfl_mark(c, 0);
         if (y.rn <= y.tol) {
           y.active = false;
         } else if (y.status >= nmx) {
@@ -545,7 +557,8 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
     status[r] = ifail[r] == -1 ? nmx : y.status;
     if (dfl && y.status > 0) status[nr + r] = (y.lstat + y.status / 2) / y.status;
   }
-  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : fail("gcr_batch: CUDA error");
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail("gcr_batch: CUDA error");
+  return dfl ? dfl_batch_check(c) : 0;
 }
 
 }  // namespace qcd
