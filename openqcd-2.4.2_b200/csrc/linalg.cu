@@ -1,7 +1,8 @@
 // BLAS-1 on spinor fields in the device layout, with the reference's
 // precision rules: products of FP32 fields accumulate in double
-// (modules/linalg/salg.c:1050-1078), products of FP64 fields accumulate in
-// double-double (modules/linalg/salg_dble.c:2319-2357 with utils/qsum.c).
+// (modules/linalg/salg.c:1050-1078; here after summing the four products of
+// a float4 in FP32), products of FP64 fields accumulate in double-double
+// (modules/linalg/salg_dble.c:2319-2357 with utils/qsum.c).
 //
 // A parity half of a field is a contiguous range (even chunks come first), so
 // everything here works on flat arrays: FP64 fields as double2 (one complex
@@ -85,6 +86,10 @@ __global__ void k_finish(const double *__restrict__ part, int nb, double *out) {
   }
 }
 
+// FP32 fields: the products of one float4 (two complex components) are
+// summed in FP32 and that sum is added in double (per-product FP64
+// arithmetic made these reductions FP64-throughput bound on B200, at about
+// half their bandwidth-bound speed)
 template <typename R>
 __global__ void k_norm2(const void *__restrict__ x, Range r, double *part) {
   double v[1] = {0.0};
@@ -94,7 +99,7 @@ __global__ void k_norm2(const void *__restrict__ x, Range r, double *part) {
       v[0] += a.x * a.x + a.y * a.y;
     } else {
       float4 a = __ldg((const float4 *)x + r.beg + i);
-      v[0] += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w;
+      v[0] += (double)(a.x * a.x + a.y * a.y + a.z * a.z + a.w * a.w);
     }
   }
   block_store<1>(v, part);
@@ -110,8 +115,8 @@ __global__ void k_dot(const void *__restrict__ x, const void *__restrict__ y, Ra
       v[1] += a.x * b.y - a.y * b.x;
     } else {
       float4 a = __ldg((const float4 *)x + r.beg + i), b = __ldg((const float4 *)y + r.beg + i);
-      v[0] += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
-      v[1] += (double)a.x * b.y - (double)a.y * b.x + (double)a.z * b.w - (double)a.w * b.z;
+      v[0] += (double)(a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w);
+      v[1] += (double)(a.x * b.y - a.y * b.x + a.z * b.w - a.w * b.z);
     }
   }
   block_store<2>(v, part);

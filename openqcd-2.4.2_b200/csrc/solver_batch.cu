@@ -328,6 +328,228 @@ int ltl_gcr_b(Ctx &c, double mu, int nr, const double2 *const *eta, double2 *con
   return 0;
 }
 
+// ------------------------------------------ fused orthogonalisation (FP32)
+// One gcr_step of fgcr.c:157 for a system in three passes instead of about
+// 5k+9: (1) all k products (chi_l, chi_k) in one pass over chi_k; (2)
+// chi_k -= sum_l a_lk chi_l together with |chi_k|^2 and (chi_k, rho); (3)
+// chi_k /= |chi_k|, rho -= c chi_k together with |rho|^2.  Products are
+// accumulated in FP32 over runs of 16 float4, in double beyond, and summed
+// over a fixed grid.  This is
+// classical Gram-Schmidt where the reference applies the products one by
+// one (modified Gram-Schmidt); in exact arithmetic the two agree.
+constexpr int OG = 1184, OK_ = 32;
+struct F2Ptrs {
+  const float4 *p[OK_];
+};
+struct F2Coef {
+  float2 c[OK_];
+};
+
+// products summed in FP32 over runs of 16 grid-stride steps, the runs in
+// double (FP64 adds per element halved the speed of these kernels)
+template <int KM>
+__global__ void __launch_bounds__(256) k_fmdot(F2Ptrs q, int k, const float4 *__restrict__ y, size_t n,
+                                               double2 *part) {
+  __shared__ double2 red[8][KM];
+  double ar[KM], ai[KM];
+#pragma unroll
+  for (int j = 0; j < KM; j++) ar[j] = ai[j] = 0.0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  while (i < n) {
+    float fr[KM], fi[KM];
+#pragma unroll
+    for (int j = 0; j < KM; j++) fr[j] = fi[j] = 0.0f;
+    for (int t = 0; t < 16 && i < n; t++, i += stride) {
+      const float4 yy = __ldg(y + i);
+#pragma unroll
+      for (int j = 0; j < KM; j++)
+        if (j < k) {
+          const float4 a = __ldg(q.p[j] + i);
+          fr[j] += a.x * yy.x + a.y * yy.y + a.z * yy.z + a.w * yy.w;
+          fi[j] += a.x * yy.y - a.y * yy.x + a.z * yy.w - a.w * yy.z;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KM; j++) {
+      ar[j] += fr[j];
+      ai[j] += fi[j];
+    }
+  }
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < KM; j++)
+    if (j < k) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ar[j] += __shfl_down_sync(0xffffffffu, ar[j], o);
+        ai[j] += __shfl_down_sync(0xffffffffu, ai[j], o);
+      }
+      if (lane == 0) red[wp][j] = make_double2(ar[j], ai[j]);
+    }
+  __syncthreads();
+  if ((int)threadIdx.x < k) {
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < 8; w++) {
+      re += red[w][threadIdx.x].x;
+      im += red[w][threadIdx.x].y;
+    }
+    part[blockIdx.x * OK_ + threadIdx.x] = make_double2(re, im);
+  }
+}
+
+__global__ void k_fsum(const double2 *__restrict__ part, int k, double2 *out) {
+  const int j = threadIdx.x;
+  if (j >= k) return;
+  double re = 0.0, im = 0.0;
+  for (int b = 0; b < OG; b++) {
+    re += part[b * OK_ + j].x;
+    im += part[b * OK_ + j].y;
+  }
+  out[j] = make_double2(re, im);
+}
+
+// block sums of two products into part[b*OK_ + 0, 1]
+__device__ __forceinline__ void block_sum2(double a0, double a1, double a2, double2 *part) {
+  __shared__ double red[3][8];
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_down_sync(0xffffffffu, a0, o);
+    a1 += __shfl_down_sync(0xffffffffu, a1, o);
+    a2 += __shfl_down_sync(0xffffffffu, a2, o);
+  }
+  if (lane == 0) {
+    red[0][wp] = a0;
+    red[1][wp] = a1;
+    red[2][wp] = a2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int w = 0; w < 8; w++) {
+      s0 += red[0][w];
+      s1 += red[1][w];
+      s2 += red[2][w];
+    }
+    part[blockIdx.x * OK_] = make_double2(s0, 0.0);
+    part[blockIdx.x * OK_ + 1] = make_double2(s1, s2);
+  }
+}
+
+// chi_k -= sum_l c_l chi_l ; partial |chi_k|^2 and (chi_k, rho)
+template <int KM>
+__global__ void __launch_bounds__(256) k_fgs(F2Ptrs q, int k, F2Coef c, float4 *chik, const float4 *__restrict__ rho,
+                                             size_t n, double2 *part) {
+  double nn = 0.0, dr = 0.0, di = 0.0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  while (i < n) {
+    float fn = 0.0f, fr = 0.0f, fi = 0.0f;
+    for (int t = 0; t < 16 && i < n; t++, i += stride) {
+      float4 x = chik[i];
+#pragma unroll
+      for (int j = 0; j < KM; j++)
+        if (j < k) {
+          const float4 a = __ldg(q.p[j] + i);
+          const float2 z = c.c[j];
+          x.x -= z.x * a.x - z.y * a.y;
+          x.y -= z.x * a.y + z.y * a.x;
+          x.z -= z.x * a.z - z.y * a.w;
+          x.w -= z.x * a.w + z.y * a.z;
+        }
+      chik[i] = x;
+      const float4 r = __ldg(rho + i);
+      fn += x.x * x.x + x.y * x.y + x.z * x.z + x.w * x.w;
+      fr += x.x * r.x + x.y * r.y + x.z * r.z + x.w * r.w;
+      fi += x.x * r.y - x.y * r.x + x.z * r.w - x.w * r.z;
+    }
+    nn += fn;
+    dr += fr;
+    di += fi;
+  }
+  block_sum2(nn, dr, di, part);
+}
+
+// chi_k *= s ; rho -= c chi_k ; partial |rho|^2
+__global__ void __launch_bounds__(256) k_fupd(float4 *chik, float4 *rho, float s, float2 c, size_t n, double2 *part) {
+  double nn = 0.0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  while (i < n) {
+    float fn = 0.0f;
+    for (int t = 0; t < 16 && i < n; t++, i += stride) {
+      float4 x = chik[i], r = rho[i];
+      x.x *= s;
+      x.y *= s;
+      x.z *= s;
+      x.w *= s;
+      r.x -= c.x * x.x - c.y * x.y;
+      r.y -= c.x * x.y + c.y * x.x;
+      r.z -= c.x * x.z - c.y * x.w;
+      r.w -= c.x * x.w + c.y * x.z;
+      chik[i] = x;
+      rho[i] = r;
+      fn += r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w;
+    }
+    nn += fn;
+  }
+  block_sum2(nn, 0.0, 0.0, part);
+}
+
+struct OrthoBufs {
+  double2 *part = nullptr, *out = nullptr, *h = nullptr;
+};
+static OrthoBufs g_ob;
+
+static int ortho_alloc() {
+  if (g_ob.part) return 0;
+  if (cudaMalloc(&g_ob.part, (size_t)OG * OK_ * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc(&g_ob.out, OK_ * sizeof(double2)) != cudaSuccess ||
+      cudaMallocHost(&g_ob.h, OK_ * sizeof(double2)) != cudaSuccess)
+    return fail("out of memory (orthogonalisation buffers)");
+  return 0;
+}
+
+static void ortho_read(cudaStream_t st, int k) {
+  k_fsum<<<1, 32, 0, st>>>(g_ob.part, k, g_ob.out);
+  cudaMemcpyAsync(g_ob.h, g_ob.out, k * sizeof(double2), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+}
+
+// gcr_step for one system with the fused passes (istop = 0): returns rn
+static double gcr_step_fused(const Ctx &c, int nkv, int k, const std::vector<void *> &chi, void *rho,
+                             std::vector<cplxf> &a, std::vector<float> &b, std::vector<cplxf> &cc,
+                             cudaStream_t st) {
+  const size_t n = (size_t)c.g.vol * 6;   // float4 elements of an FP32 field
+  F2Ptrs q;
+  for (int j = 0; j < OK_; j++) q.p[j] = j < k ? (const float4 *)chi[j] : nullptr;
+  F2Coef co;
+  for (int j = 0; j < OK_; j++) co.c[j] = make_float2(0.0f, 0.0f);
+  if (k > 0) {
+    if (k <= 8) k_fmdot<8><<<OG, 256, 0, st>>>(q, k, (const float4 *)chi[k], n, g_ob.part);
+    else if (k <= 16) k_fmdot<16><<<OG, 256, 0, st>>>(q, k, (const float4 *)chi[k], n, g_ob.part);
+    else k_fmdot<32><<<OG, 256, 0, st>>>(q, k, (const float4 *)chi[k], n, g_ob.part);
+    ortho_read(st, k);
+    for (int l = 0; l < k; l++) {
+      const cplxf z = {(float)g_ob.h[l].x, (float)g_ob.h[l].y};
+      a[(size_t)nkv * l + k] = z;
+      co.c[l] = make_float2(z.re, z.im);
+    }
+  }
+  if (k <= 8) k_fgs<8><<<OG, 256, 0, st>>>(q, k, co, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
+  else if (k <= 16) k_fgs<16><<<OG, 256, 0, st>>>(q, k, co, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
+  else k_fgs<32><<<OG, 256, 0, st>>>(q, k, co, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
+  ortho_read(st, 2);
+  const float bn = (float)sqrt((double)(float)g_ob.h[0].x);
+  b[k] = bn;
+  const float s = bn != 0.0f ? 1.0f / bn : 0.0f;
+  cc[k] = {(float)g_ob.h[1].x * s, (float)g_ob.h[1].y * s};
+  k_fupd<<<OG, 256, 0, st>>>((float4 *)chi[k], (float4 *)rho, s, make_float2(cc[k].re, cc[k].im), n, g_ob.part);
+  ortho_read(st, 1);
+  return sqrt((double)(float)g_ob.h[0].x);
+}
+
 // ------------------------------------------------------------- outer solver
 struct SysState {
   double mu = 0.0, rho0 = 0.0, rn = 0.0, tol = 0.0, rn_old = 0.0;
@@ -379,7 +601,7 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       if (mu[r] != mu[0]) return fail("gcr_batch: deflation needs the same twisted mass for all systems");
     if (dfl_batch_alloc(c)) return -1;
   }
-  if (sap_prepare(c, st)) return -1;
+  if (sap_prepare(c, st) || ortho_alloc()) return -1;
   const int per32 = 2 * nkv + 1 + (dfl ? 1 : 0);
   if (bw_reserve(c, g_bw.f32, (size_t)nr * per32 + 1, 32) || bw_reserve(c, g_bw.f64, (size_t)nr + 1, 64)) return -1;
   if (!c.tmp32 && cudaMalloc(&c.tmp32, spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory");
@@ -500,15 +722,19 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
     for (int r : A) {
       SysState &y = S[r];
       const int k = y.k;
-      for (int l = 0; l < k; l++) {
-        cplxf z = o.dot32(y.chi[l], y.chi[k]);
-        y.a[(size_t)nkv * l + k] = z;
-        o.axpy32(y.chi[k], -z.re, -z.im, y.chi[l]);
+      if (istop == 0 && nkv <= OK_) {
+        y.rn = gcr_step_fused(c, nkv, k, y.chi, y.rho, y.a, y.b, y.cc, st);
+      } else {
+        for (int l = 0; l < k; l++) {
+          cplxf z = o.dot32(y.chi[l], y.chi[k]);
+          y.a[(size_t)nkv * l + k] = z;
+          o.axpy32(y.chi[k], -z.re, -z.im, y.chi[l]);
+        }
+        y.b[k] = o.normalize32(y.chi[k]);
+        y.cc[k] = o.dot32(y.chi[k], y.rho);
+        o.axpy32(y.rho, -y.cc[k].re, -y.cc[k].im, y.chi[k]);
+        y.rn = o.res32(y.rho, istop);
       }
-      y.b[k] = o.normalize32(y.chi[k]);
-      y.cc[k] = o.dot32(y.chi[k], y.rho);
-      o.axpy32(y.rho, -y.cc[k].re, -y.cc[k].im, y.chi[k]);
-      y.rn = o.res32(y.rho, istop);
       y.status += 1;
       dfl_mark(c, 1);
       if (y.rn <= y.tol || y.rn < PRECISION_LIMIT * y.rn_old || k == nkv - 1 || y.status >= nmx) {

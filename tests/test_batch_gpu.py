@@ -2,11 +2,12 @@
 counterpart).  Every system runs the reference's algorithm (fgcr with SAP,
 modules/sap/sap_gcr.c:140, or with deflated SAP, modules/dfl/dfl_sap_gcr.c:353)
 on its own Krylov space, so each must reach the FP64 true residual 1e-10,
-checked with the reference's Dw_dble, in the same number of steps as the
-single-system solver (plain: the same arithmetic, so the same solution to
-1e-12; deflated: the batched restriction and little solver sum in another
-order, so within one step and 1e-8).  Systems of different twisted masses
-and a zero source share a batch; systems leave it as they converge."""
+checked with the reference's Dw_dble, in the number of steps of the
+single-system solver give or take one, with a solution equal to the
+single-system one to 1e-8 (the batched solver orthogonalises by classical
+Gram-Schmidt in fused passes, and its restriction and little solver sum in
+another order).  Systems of different twisted masses and a zero source
+share a batch; systems leave it as they converge."""
 import numpy as np
 import pytest
 
@@ -54,8 +55,8 @@ def test_plain_batch_matches_single(setup):
     assert ifail == [0, 0, 0]
     for i in range(3):
         psi = P[i].to_ref(setup.vol)
-        assert st[i] == singles[i][1]
-        assert rel_norm_err(psi, singles[i][0]) <= 1e-12
+        assert abs(st[i] - singles[i][1]) <= 1, (st, [x[1] for x in singles])
+        assert rel_norm_err(psi, singles[i][0]) <= 1e-8
         assert true_res(setup, mus[i], psi, etas[i]) <= 1.5e-10
 
 
