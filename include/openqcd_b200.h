@@ -236,6 +236,35 @@ int b200_release_workspace(void);
 double b200_dev_dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, const void *eta, void *psi,
                             int *ifail, int *status);
 
+/* --------------------------------------------- learned preconditioner */
+/* A gauge-equivariant parallel-transport convolutional network (no
+ * reference counterpart): three linear layers of 4 -> 8 -> 8 -> 4 colour-
+ * triplet channels with complex weights per direction (self and the 8
+ * hops), colour moved by the links only.  Weights are packed per layer as
+ * [9][Cout][Cin] complex floats (re, im); b200_net_nweights() floats in
+ * all.  Fields are FP32 device fields in the library's layout. */
+int b200_net_nweights(void);
+/* weights close to scale * identity plus small random couplings */
+int b200_net_init(unsigned long long seed, float scale);
+int b200_net_set_weights(const float *w);
+int b200_net_get_weights(float *w);
+/* out = M in; half != 0 uses the FP16-rounded weights (FP32 arithmetic) */
+int b200_net_apply(const void *in, void *out, int half);
+/* loss |M r - e|^2/|e|^2 of one pair and its gradient with respect to the
+ * real and imaginary parts of the weights (packed like the weights) */
+int b200_net_grad(const void *r, const void *e, double *loss, float *grad);
+/* steps of Adam on minibatches of `batch` of the npairs (r, e) pairs,
+ * on the device; loss_hist[step] = minibatch loss (may be NULL) */
+int b200_net_train(int npairs, void *const *r, void *const *e, int steps, int batch, float lr,
+                   unsigned long long seed, float *loss_hist);
+/* training pairs from the plain solver: r Gaussian, e = Dw(mu)^-1 r */
+int b200_net_make_pairs(int npairs, void *const *r, void *const *e, double mu, double res,
+                        unsigned long long seed);
+/* preconditioner of sap_gcr: 0 SAP (default), 1 the network (SAP once a
+ * step reduces the residual by less than 10 %), 2 the network followed by
+ * SAP on its residual, 3 none */
+int b200_set_precond(int kind);
+
 /* ------------------------------------ device-resident fields (own layout) */
 /* prec = 64 (spinor_dble) or 32 (spinor).  Operator codes for
  * b200_dev_dirac: 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo, 5 Dwhat. */

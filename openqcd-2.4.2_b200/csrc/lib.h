@@ -43,6 +43,20 @@ struct DflState {
   double prof_t0 = 0.0;
 };
 
+// The learned preconditioner (net.cu): host master weights with Adam
+// moments, device copies (FP32, adjoint layers, FP16-rounded), gradient
+// accumulators and activation fields.
+struct NetState {
+  bool ready = false;
+  std::vector<float> w[3], m[3], v[3];
+  int t = 0;
+  float2 *dev_w[3] = {nullptr, nullptr, nullptr}, *dev_wadj[3] = {nullptr, nullptr, nullptr};
+  float2 *dev_w16[3] = {nullptr, nullptr, nullptr};
+  double2 *dev_grad[3] = {nullptr, nullptr, nullptr};
+  float2 *part = nullptr;
+  std::vector<void *> f;
+};
+
 // Everything the reference keeps in module-global state for this path:
 // geometry (lattice/geometry.c), the gauge field (uflds/uflds.c udfld/ufld),
 // the SW field (sw_term/swflds.c swdfld/swfld) and the parameter data base
@@ -99,6 +113,10 @@ struct Ctx {
   size_t fstage_bytes[3] = {0, 0, 0};
   std::vector<void *> ws32, ws64;   // solver workspaces (reserve_ws / reserve_wsd)
   DflState dfl;
+  NetState net;
+  // preconditioner of sap_gcr: 0 SAP, 1 network (SAP when the residual
+  // stalls), 2 network then SAP on the remainder, 3 none
+  int precond = 0;
 };
 
 Ctx &ctx();
@@ -194,6 +212,16 @@ int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st
 // dfl.cu
 int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
+// net.cu
+int net_set_weights(Ctx &c, const float *w);
+int net_get_weights(Ctx &c, float *w);
+int net_nweights();
+int net_init(Ctx &c, uint64_t seed, float scale);
+int net_apply(Ctx &c, const void *in, void *out, bool half, cudaStream_t st);
+int net_grad(Ctx &c, const void *r, const void *e, double *loss, float *grad);
+int net_train(Ctx &c, int npairs, const void *const *r, const void *const *e, int steps, int batch, float lr,
+              uint64_t seed, float *loss_hist);
+void net_release(Ctx &c);
 // dfl_batch.cu: the deflation steps for nr right-hand sides at once
 int dfl_batch_alloc(Ctx &c);
 void dfl_mark(Ctx &c, int k);

@@ -155,11 +155,50 @@ double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, c
       const float muf = (float)mu;
       const int isolv = c.isolv, nmr = c.nmr, ncy = c.ncy;
       DopFn Dop = [&](const void *s, void *r) { dirac_op<double>(c, 0, mu, s, r, c.tmp64, c.stream); };
-      MopFn Mop = [&](int, const void *rh, void *ph, void *ch) {
+      const int kind = c.precond;
+      if (kind == 1 || kind == 2) {
+        if (!c.net.ready) { fail("sap_gcr: the network preconditioner has no weights"); return -1.0; }
+        if (reserve(c, c.ws32, 2 * nkv + 3, 32)) return -1.0;
+      }
+      void *ws2 = (kind == 1 || kind == 2) ? c.ws32[2 * nkv + 2] : nullptr;
+      bool fallback = false;
+      double rn_prev = -1.0;
+      auto sap_mop = [&](const void *rh, void *ph, void *ch) {
         la_zero(c, 32, ph, PAR_ALL, c.stream);
         la_copy(c, 32, rh, 32, ch, PAR_ALL, c.stream);
         for (int n = 0; n < ncy; n++) sap_cycle(c, muf, isolv, nmr, ph, ch, phib, c.stream);
         la_diff(c, 32, rh, ch, PAR_ALL, c.stream);
+      };
+      MopFn Mop = [&](int, const void *rh, void *ph, void *ch) {
+        if (kind == 0) {
+          sap_mop(rh, ph, ch);
+        } else if (kind == 3) {
+          la_copy(c, 32, rh, 32, ph, PAR_ALL, c.stream);
+          dirac_op<float>(c, 0, muf, ph, ch, c.tmp32, c.stream);
+        } else if (kind == 1) {
+          // the network, until a step reduces the residual by less than
+          // 10 %; SAP from then on
+          double r2[2];
+          la_norm2(c, 32, rh, PAR_ALL, r2);
+          const double rn = sqrt(r2[0] + r2[1]);
+          if (rn_prev > 0.0 && rn > 0.9 * rn_prev) fallback = true;
+          rn_prev = rn;
+          if (fallback) {
+            sap_mop(rh, ph, ch);
+          } else {
+            net_apply(c, rh, ph, true, c.stream);
+            dirac_op<float>(c, 0, muf, ph, ch, c.tmp32, c.stream);
+          }
+        } else {
+          // the network, then SAP on what it leaves: ph = M rh + SAP(rh - D M rh)
+          net_apply(c, rh, ws2, true, c.stream);
+          dirac_op<float>(c, 0, muf, ws2, ch, c.tmp32, c.stream);
+          la_diff(c, 32, rh, ch, PAR_ALL, c.stream);            // ch = rh - D M rh
+          la_zero(c, 32, ph, PAR_ALL, c.stream);
+          for (int n = 0; n < ncy; n++) sap_cycle(c, muf, isolv, nmr, ph, ch, phib, c.stream);
+          la_diff(c, 32, rh, ch, PAR_ALL, c.stream);            // ch = rh - final residual = D ph_total
+          la_axpy(c, 32, ph, 1.0, 0.0, ws2, PAR_ALL, c.stream);
+        }
       };
       // psi may alias eta: fgcr only reads rsd from here on
       rho = fgcr_dev(c, nkv, nmx, istop, res, rsd, psi, status, Dop, Mop);

@@ -108,6 +108,16 @@ _SIGS = {
     "b200_dev_gcr_batch": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_release_workspace": (C.c_int, []),
+    "b200_net_nweights": (C.c_int, []),
+    "b200_net_init": (C.c_int, [C.c_ulonglong, C.c_float]),
+    "b200_net_set_weights": (C.c_int, [C.c_void_p]),
+    "b200_net_get_weights": (C.c_int, [C.c_void_p]),
+    "b200_net_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "b200_net_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_net_train": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_ulonglong,
+                                 C.c_void_p]),
+    "b200_net_make_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_ulonglong]),
+    "b200_set_precond": (C.c_int, [C.c_int]),
     "b200_dfl_time": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
@@ -567,3 +577,54 @@ def dfl_sap_gcr2(nkv, nmx, istop, res, mu, eta):
     if rho < 0:
         raise B200Error(_err_after())
     return psi, rho, list(ifail), list(status)
+
+
+# ------------------------------------------------------ learned preconditioner
+def net_nweights():
+    return lib().b200_net_nweights()
+
+
+def net_init(seed=1, scale=0.25):
+    return check(lib().b200_net_init(seed, scale))
+
+
+def net_set_weights(w):
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    return check(lib().b200_net_set_weights(_ptr(w)))
+
+
+def net_get_weights():
+    w = np.zeros(net_nweights(), dtype=np.float32)
+    check(lib().b200_net_get_weights(_ptr(w)))
+    return w
+
+
+def net_apply(inp, out, half=True):
+    return check(lib().b200_net_apply(inp.ptr, out.ptr, 1 if half else 0))
+
+
+def net_grad(r, e):
+    loss = C.c_double(0.0)
+    g = np.zeros(net_nweights(), dtype=np.float32)
+    check(lib().b200_net_grad(r.ptr, e.ptr, C.byref(loss), _ptr(g)))
+    return loss.value, g
+
+
+def net_train(rs, es, steps, batch, lr, seed=1):
+    n = len(rs)
+    rp = (C.c_void_p * n)(*[x.ptr for x in rs])
+    ep = (C.c_void_p * n)(*[x.ptr for x in es])
+    hist = np.zeros(max(steps, 1), dtype=np.float32)
+    check(lib().b200_net_train(n, rp, ep, steps, batch, lr, seed, _ptr(hist)))
+    return hist[:steps]
+
+
+def net_make_pairs(rs, es, mu, res, seed=1):
+    n = len(rs)
+    rp = (C.c_void_p * n)(*[x.ptr for x in rs])
+    ep = (C.c_void_p * n)(*[x.ptr for x in es])
+    return check(lib().b200_net_make_pairs(n, rp, ep, mu, res, seed))
+
+
+def set_precond(kind):
+    return check(lib().b200_set_precond(kind))
