@@ -270,6 +270,9 @@ int b200_set_precond(int kind);
  * b200_dev_dirac: 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo, 5 Dwhat. */
 void *b200_dev_alloc_spinor(int prec);
 void b200_dev_free(void *p);
+/* Point source: zero except component (spin, colour) = 1 at site x (x[0]
+ * time); the sources of the batched-solve workload. */
+int b200_dev_point_source(int prec, void *f, const int x[4], int spin, int colour);
 int b200_dev_random_spinor(int prec, void *f, double sigma, unsigned long long seed);
 int b200_dev_from_ref(int prec, const void *q, void *f);
 int b200_dev_to_ref(int prec, const void *f, void *q);

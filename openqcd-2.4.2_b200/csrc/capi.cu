@@ -163,6 +163,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   c.sap_tuned_vbh[0] = c.sap_tuned_vbh[1] = 0;
   c.have_ud = c.have_sw = false;
   qcd::dfl_release(c);
+  qcd::net_fields_release(c);
   c.ready = false;
   if (geometry_init(c, L, bs, ipt)) return -1;
   c.ready = true;
@@ -373,6 +374,36 @@ void *b200_dev_alloc_spinor(int prec) {
   return p;
 }
 void b200_dev_free(void *p) { cudaFree(p); }
+
+// Point source: f = 0 except component (spin, colour) = 1 at the site with
+// coordinates x[0..3] (x0 = time).
+int b200_dev_point_source(int prec, void *f, const int x[4], int spin, int colour) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  if (spin < 0 || spin > 3 || colour < 0 || colour > 2) return fail("point_source: spin or colour out of range");
+  int n[4], y[4];
+  for (int mu = 0; mu < 4; mu++) {
+    if (x[mu] < 0 || x[mu] >= c.g.L[mu]) return fail("point_source: site out of range");
+    n[mu] = x[mu] / c.g.bs[mu];
+    y[mu] = x[mu] % c.g.bs[mu];
+  }
+  const int blk = ((n[0] * c.g.nb[1] + n[1]) * c.g.nb[2] + n[2]) * c.g.nb[3] + n[3];
+  const int l = ((y[0] * c.g.bs[1] + y[1]) * c.g.bs[2] + y[2]) * c.g.bs[3] + y[3];
+  const int p = (x[0] + x[1] + x[2] + x[3]) & 1, sidx = l >> 1, chunk = p * c.g.nbl + blk;
+  const int k = 3 * spin + colour;
+  cudaMemsetAsync(f, 0, spinor_bytes(c, prec), c.stream);
+  if (prec == 64) {
+    const double2 one = make_double2(1.0, 0.0);
+    cudaMemcpyAsync((double2 *)f + ((size_t)chunk * 12 + k) * c.g.vbh + sidx, &one, sizeof(one),
+                    cudaMemcpyHostToDevice, c.stream);
+  } else {
+    const float one = 1.0f;
+    // FP32 plane j = k/2 holds components 2j and 2j+1 as (re, im, re, im)
+    cudaMemcpyAsync((float *)((float4 *)f + ((size_t)chunk * 6 + k / 2) * c.g.vbh + sidx) + 2 * (k & 1), &one,
+                    sizeof(one), cudaMemcpyHostToDevice, c.stream);
+  }
+  return b200_sync();
+}
 
 int b200_dev_random_spinor(int prec, void *f, double sigma, unsigned long long seed) {
   Ctx &c = ctx();

@@ -222,6 +222,7 @@ int net_grad(Ctx &c, const void *r, const void *e, double *loss, float *grad);
 int net_train(Ctx &c, int npairs, const void *const *r, const void *const *e, int steps, int batch, float lr,
               uint64_t seed, float *loss_hist);
 void net_release(Ctx &c);
+void net_fields_release(Ctx &c);
 // dfl_batch.cu: the deflation steps for nr right-hand sides at once
 int dfl_batch_alloc(Ctx &c);
 void dfl_mark(Ctx &c, int k);

@@ -445,6 +445,12 @@ int net_train(Ctx &c, int npairs, const void *const *r, const void *const *e, in
   return 0;
 }
 
+// activation fields are sized for the geometry; the weights are kept
+void net_fields_release(Ctx &c) {
+  for (void *p : c.net.f) cudaFree(p);
+  c.net.f.clear();
+}
+
 void net_release(Ctx &c) {
   NetState &n = c.net;
   for (int l = 0; l < NLAY; l++) {

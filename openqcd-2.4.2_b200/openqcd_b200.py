@@ -108,6 +108,7 @@ _SIGS = {
     "b200_dev_gcr_batch": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_release_workspace": (C.c_int, []),
+    "b200_dev_point_source": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
     "b200_net_nweights": (C.c_int, []),
     "b200_net_init": (C.c_int, [C.c_ulonglong, C.c_float]),
     "b200_net_set_weights": (C.c_int, [C.c_void_p]),
@@ -329,6 +330,11 @@ class DevField:
 
     def random(self, sigma, seed):
         check(lib().b200_dev_random_spinor(self.prec, self.ptr, sigma, seed))
+        return self
+
+    def point(self, x, spin, colour):
+        xs = np.ascontiguousarray(x, dtype=np.int32)
+        check(lib().b200_dev_point_source(self.prec, self.ptr, _ptr(xs), spin, colour))
         return self
 
     def norm2(self):

@@ -112,3 +112,17 @@ def test_dfl_batch_needs_one_mass(dfl):
     with pytest.raises(qb.B200Error):
         qb.dev_gcr_batch(16, 256, 0, 1e-10, [0.0, 0.01], E, P, dfl=True)
     qb.release_workspace()
+
+
+def test_point_source(setup):
+    f = dev(64)
+    x = (3, 1, 4, 2)
+    f.point(x, 2, 1)
+    q = f.to_ref(setup.vol).reshape(setup.vol, 24)
+    lex = ((x[0] * L[1] + x[1]) * L[2] + x[2]) * L[3] + x[3]
+    ix = setup.ipt[lex]
+    assert q[ix, 2 * (3 * 2 + 1)] == 1.0 and np.count_nonzero(q) == 1
+    g = qb.DevField(32)
+    g.point(x, 3, 2)
+    q = g.to_ref(setup.vol).reshape(setup.vol, 24)
+    assert q[ix, 2 * (3 * 3 + 2)] == 1.0 and np.count_nonzero(q) == 1
