@@ -222,12 +222,21 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solver", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-solver", action="store_true",
+                    help="run only the 48^3x96 solver comparison, with profiler collection around the chosen solve")
+    ap.add_argument("--solver-lattice", default=None, help="L0,L1,L2,L3 for --profile-solver (smaller cases)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     d = Dist()
     try:
         if args.impl == "reference":
             return run_reference(args, d)
+        if args.profile_solver:
+            import openqcd_b200 as qb
+            qb.set_device(d.local)
+            L = tuple(int(x) for x in args.solver_lattice.split(",")) if args.solver_lattice else None
+            print(json.dumps(solver_c3(qb, profile=True, lattice=L)))
+            return 0
         return run_b200(args, d)
     finally:
         d.close()
@@ -247,7 +256,7 @@ def true_residual(qb, mu, eta, psi):
     return float(n)
 
 
-def solver_c3(qb):
+def solver_c3(qb, profile=False, lattice=None):
     """The mixed-precision deflated solve on 48^3x96 (links exp(0.3 X),
     m0 = -0.05, csw = 1.7, bs = 6^4, Ns = 28, Gaussian sources, FP64
     residual 1e-10): the plain GPU sap_gcr (one right-hand side, FP32 SAP
@@ -255,7 +264,7 @@ def solver_c3(qb):
     four right-hand sides at once, nkv = 8, ncy = 2).  Seconds per
     right-hand side of the solves; the subspace generation is reported
     apart (it is done once per gauge field)."""
-    L, BSx, NS = SOLVER_L, SOLVER_BS, 28
+    L, BSx, NS = (lattice or SOLVER_L), SOLVER_BS, 28
     qb.geometry(L, BSx, qb.even_first_ipt(L))
     qb.set_parms(CSW, M0, 0)
     qb.random_ud(EPS, 20251204)
@@ -288,10 +297,14 @@ def solver_c3(qb):
     P = [qb.DevField(64) for _ in range(nr)]
     qb.dev_gcr_batch(8, 256, 0, 1e-10, [0.0] * nr, E, P, dfl=True)      # warm-up
     qb.lib().b200_sync()
+    if profile:
+        qb.check(qb.lib().b200_profiler(1))
     t0 = time.time()
     rhos, ifails, sts, lst = qb.dev_gcr_batch(8, 256, 0, 1e-10, [0.0] * nr, E, P, dfl=True)
     qb.lib().b200_sync()
     t_chosen = (time.time() - t0) / nr
+    if profile:
+        qb.check(qb.lib().b200_profiler(0))
     out["chosen"] = {"s_per_rhs": t_chosen, "iterations": sts, "little_steps": lst, "ifail": ifails,
                      "true_residual": max(true_residual(qb, 0.0, E[i], P[i]) for i in range(nr)),
                      "setup_s": t_setup, "setup_ifail": f,

@@ -178,6 +178,9 @@ double fgcr(int vol, void (*Dop)(spinor_dble *s, spinor_dble *r), void (*Mop)(in
  * block solver (no reference counterpart): 32 (default) as the reference;
  * 16 reads FP16 copies of them, with FP32 work vectors and arithmetic. */
 int b200_set_sap_prec(int bits);
+/* Start (on != 0) or stop profiler collection around a region of interest
+ * (for ncu --profile-from-start off). */
+int b200_profiler(int on);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32 or 16): index, threads per block, time of one
  * cycle's block sweeps in ms. */

@@ -1,6 +1,7 @@
 // The C ABI: library context, error handling, and every extern "C" entry
 // point declared in include/openqcd_b200.h.
 #include "lib.h"
+#include <cuda_profiler_api.h>
 #include "../../include/openqcd_b200.h"
 #include <cstdio>
 #include <cstdlib>
@@ -188,6 +189,13 @@ int b200_set_sap_parms(const int bs[4], int isolv, int nmr, int ncy) {
   c.isolv = isolv; c.nmr = nmr; c.ncy = ncy;
   c.sap_set = true;
   return 0;
+}
+
+// Start (on != 0) or stop the CUDA profiler's collection, for profiles of a
+// chosen region (ncu --profile-from-start off).
+int b200_profiler(int on) {
+  cudaDeviceSynchronize();
+  return (on ? cudaProfilerStart() : cudaProfilerStop()) == cudaSuccess ? 0 : fail("profiler start/stop failed");
 }
 
 int b200_set_sap_prec(int bits) {

@@ -99,6 +99,7 @@ _SIGS = {
                           C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_clear_error": (None, []),
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
+    "b200_profiler": (C.c_int, [C.c_int]),
     "b200_sap_tuning": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_set_dfl_parms": (C.c_int, [C.c_void_p, C.c_int]),
     "b200_set_dfl_pro_parms": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double]),
