@@ -184,11 +184,12 @@ __global__ void __launch_bounds__(288) k_little_b(int mode, int Ns, int b0, cons
 }
 
 // ----------------------------------------------- TMA-staged variants
+constexpr int NSTAGE = 3;        // depth of the shared-memory copy ring
 // The same restriction and prolongation with the basis planes of the
 // CTA's sites streamed into shared memory by bulk asynchronous copies
 // (cp.async.bulk, one per plane and basis vector, issued by one thread),
-// double-buffered so that the copy of basis vector l+1 overlaps the
-// arithmetic on vector l.  A plane segment is cnt consecutive float4 at
+// in a ring of NSTAGE buffers so that the copies of basis vectors l+1 ..
+// l+NSTAGE-1 overlap the arithmetic on vector l.  A plane segment is cnt consecutive float4 at
 // ((chunk*6 + j)*vbh + s0): 16-byte aligned, cnt*16 bytes.
 template <int NRT, bool RESTRICT>
 __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__restrict__ vd2lex,
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__re
                                                          Ptrs<NRT> fld, Ptrs<NRT> vd, int nsplit, double2 *part,
                                                          int *err) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar[NSTAGE];
   __shared__ float2 z[RESTRICT ? 1 : NRT][64];
   const int n = blockIdx.x, y = blockIdx.y, p = y / nsplit, h = y - p * nsplit;
   const int blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
@@ -204,12 +205,11 @@ __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__re
   const int si = s0 + threadIdx.x;
   const bool ok = (int)threadIdx.x < cnt;
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  float4 *buf = (float4 *)smraw;                                  // [2][6][per]
-  double2 *red = (double2 *)(buf + (size_t)12 * per);             // [Ns][NRT][nw]
+  float4 *buf = (float4 *)smraw;                                  // [NSTAGE][6][per]
+  double2 *red = (double2 *)(buf + (size_t)NSTAGE * 6 * per);     // [Ns][NRT][nw]
   const unsigned bytes = (unsigned)cnt * 16u;
   if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
+    for (int k = 0; k < NSTAGE; k++) mbar_init(&bar[k], 1);
     mbar_fence_init();
   }
   if (!RESTRICT)
@@ -231,11 +231,13 @@ __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__re
     szero(xs[r]);
     if (RESTRICT && ok) xs[r] = Store<float>::load_spinor(fld.p[r], chunk, si, g.vbh);
   }
-  if (threadIdx.x == 0 && Ns > 0) issue(0, 0);
+  if (threadIdx.x == 0)
+    for (int l = 0; l < NSTAGE - 1 && l < Ns; l++) issue(l, l);
   for (int l = 0; l < Ns; l++) {
-    const int stg = l & 1;
-    if (threadIdx.x == 0 && l + 1 < Ns) issue(l + 1, stg ^ 1);
-    mbar_wait(&bar[stg], (unsigned)(l >> 1) & 1u, err);
+    const int stg = l % NSTAGE;
+    // the buffer of vector l-1 was released by the barrier that ended step l-1
+    if (threadIdx.x == 0 && l + NSTAGE - 1 < Ns) issue(l + NSTAGE - 1, (l + NSTAGE - 1) % NSTAGE);
+    mbar_wait(&bar[stg], (unsigned)(l / NSTAGE) & 1u, err);
     spinor<float> b;
     szero(b);
     if (ok)
@@ -320,7 +322,7 @@ __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__re
           }
       }
     }
-    __syncthreads();   // buffer stg is refilled by the copy issued in iteration l + 1
+    __syncthreads();   // buffer stg is refilled by the copy issued in step l + 1
   }
   if (RESTRICT) {
     for (int q = threadIdx.x; q < Ns * NRT; q += blockDim.x) {
@@ -373,7 +375,7 @@ template <int NRT>
 static void restrict_pass(Ctx &c, const void *const *x, double2 *const *vd, cudaStream_t st) {
   DflState &d = c.dfl;
   const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
-  const size_t shm = (size_t)12 * per * sizeof(float4) + (size_t)d.Ns * NRT * (t / 32) * sizeof(double2);
+  const size_t shm = (size_t)NSTAGE * 6 * per * sizeof(float4) + (size_t)d.Ns * NRT * (t / 32) * sizeof(double2);
   cudaFuncSetAttribute(k_dfl_stream<NRT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   k_dfl_stream<NRT, true><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
                                                                d.Ns, ptrs<NRT>(x), ptrs<NRT>(nullptr), ns, d.bpart,
@@ -395,7 +397,7 @@ template <int NRT>
 static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st) {
   DflState &d = c.dfl;
   const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
-  const size_t shm = (size_t)12 * per * sizeof(float4);
+  const size_t shm = (size_t)NSTAGE * 6 * per * sizeof(float4);
   cudaFuncSetAttribute(k_dfl_stream<NRT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   k_dfl_stream<NRT, false><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
                                                                 d.Ns, ptrs<NRT>((const void *const *)s),

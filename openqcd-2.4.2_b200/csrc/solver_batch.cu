@@ -398,15 +398,25 @@ __global__ void __launch_bounds__(256) k_fmdot(F2Ptrs q, int k, const float4 *__
   }
 }
 
-__global__ void k_fsum(const double2 *__restrict__ part, int k, double2 *out) {
-  const int j = threadIdx.x;
-  if (j >= k) return;
+// out[j] = sum over the OG partials of product j: CTA j, fixed tree
+__global__ void __launch_bounds__(256) k_fsum(const double2 *__restrict__ part, double2 *out) {
+  __shared__ double2 red[256];
+  const int j = blockIdx.x;
   double re = 0.0, im = 0.0;
-  for (int b = 0; b < OG; b++) {
+  for (int b = threadIdx.x; b < OG; b += blockDim.x) {
     re += part[b * OK_ + j].x;
     im += part[b * OK_ + j].y;
   }
-  out[j] = make_double2(re, im);
+  red[threadIdx.x] = make_double2(re, im);
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+      red[threadIdx.x].x += red[threadIdx.x + h].x;
+      red[threadIdx.x].y += red[threadIdx.x + h].y;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = red[0];
 }
 
 // block sums of two products into part[b*OK_ + 0, 1]
@@ -512,7 +522,7 @@ static int ortho_alloc() {
 }
 
 static void ortho_read(cudaStream_t st, int k) {
-  k_fsum<<<1, 32, 0, st>>>(g_ob.part, k, g_ob.out);
+  k_fsum<<<k, 256, 0, st>>>(g_ob.part, g_ob.out);
   cudaMemcpyAsync(g_ob.h, g_ob.out, k * sizeof(double2), cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
 }
