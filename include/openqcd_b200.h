@@ -181,9 +181,14 @@ int b200_set_sap_prec(int bits);
 /* Start (on != 0) or stop profiler collection around a region of interest
  * (for ncu --profile-from-start off). */
 int b200_profiler(int on);
+/* on != 0 (default): when every link satisfies the SU(3) relation
+ * row3 = +-conj(row1 x row2), the even-odd SAP block solver reads FP32
+ * links as their first two rows and rebuilds the third (no reference
+ * counterpart; 2/3 of the link bytes, results equal to FP32 rounding). */
+int b200_set_sap_link12(int on);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
- * current block size (prec 32 or 16): index, threads per block, time of one
- * cycle's block sweeps in ms. */
+ * current block size (prec 32, 16, or 12 for the 12-real links): index,
+ * threads per block, time of one cycle's block sweeps in ms. */
 int b200_sap_tuning(int prec, int *variant, int *threads, float *ms);
 
 /* ------------------------------------------- deflation (dfl.h, little.h) */

@@ -153,7 +153,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
     return fail("no CUDA device available");
   // a new geometry invalidates every resident field
   void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage,
-                  c.u16, c.sw16, c.sw16_inv};
+                  c.u16, c.sw16, c.sw16_inv, c.u12};
   for (void *p : bufs) cudaFree(p);
   for (void *p : c.ws32) cudaFree(p);
   for (void *p : c.ws64) cudaFree(p);
@@ -161,7 +161,8 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   c.ud = nullptr; c.u32 = nullptr; c.swd = c.swd_inv = nullptr; c.sw32 = c.sw32_inv = nullptr;
   c.tmp64 = c.tmp32 = c.stage = nullptr; c.stage_bytes = 0;
   c.u16 = c.sw16 = c.sw16_inv = nullptr; c.h16_valid = false;
-  c.sap_tuned_vbh[0] = c.sap_tuned_vbh[1] = 0;
+  c.sap_tuned_vbh[0] = c.sap_tuned_vbh[1] = c.sap_tuned_vbh[2] = 0;
+  c.u12 = nullptr; c.u12_valid = c.u12_ok = false;
   c.have_ud = c.have_sw = false;
   qcd::dfl_release(c);
   qcd::net_fields_release(c);
@@ -204,10 +205,15 @@ int b200_set_sap_prec(int bits) {
   return 0;
 }
 
+int b200_set_sap_link12(int on) {
+  ctx().sap_link12 = on != 0;
+  return 0;
+}
+
 int b200_sap_tuning(int prec, int *variant, int *threads, float *ms) {
   Ctx &c = ctx();
   if (check_ready(c)) return -1;
-  const int slot = prec == 16 ? 1 : 0;
+  const int slot = prec == 16 ? 1 : (prec == 12 ? 2 : 0);
   if (c.sap_tuned_vbh[slot] != c.g.vbh) return fail("sap_tuning: the SAP kernel is not tuned for this geometry yet");
   *variant = c.sap_variant[slot];
   *threads = qcd::sap_variant_threads(c, slot);

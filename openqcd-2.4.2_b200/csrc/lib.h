@@ -93,8 +93,13 @@ struct Ctx {
   bool h16_valid = false;
   // SAP block-kernel launch variant chosen by the autotuner, per storage
   // precision (0: FP32, 1: FP16), for the block size it was tuned on
-  int sap_variant[2] = {0, 0}, sap_tuned_vbh[2] = {0, 0};
-  float sap_tuned_ms[2] = {0.0f, 0.0f};
+  int sap_variant[3] = {0, 0, 0}, sap_tuned_vbh[3] = {0, 0, 0};
+  float sap_tuned_ms[3] = {0.0f, 0.0f, 0.0f};
+  // 12-real FP32 links for the SAP block solver (first two rows; the third
+  // is rebuilt), used when every link passes the SU(3) check
+  int sap_link12 = 1;
+  void *u12 = nullptr;
+  bool u12_valid = false, u12_ok = false;
   bool have_ud = false, have_sw = false, sw_inv_ok = false;
   int sw_inv_fail = 0;
 
@@ -256,6 +261,7 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status);
 // sap.cu
 int sap_prepare(Ctx &c, cudaStream_t st);
 int sap_variant_threads(const Ctx &c, int slot);
+int sap_storage_mode(Ctx &c);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
                cudaStream_t st);

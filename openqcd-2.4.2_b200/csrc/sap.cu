@@ -35,7 +35,8 @@ struct SapArgs {
   int nmr;
   int eoflg;
   float4 *psi, *rho, *phi;
-  const void *u;
+  const void *u;        // links as the block solver's policy reads them
+  const void *ub;       // links for the block-boundary hops (FP32 or FP16, 18 reals)
   const void *sw, *swinv;
 };
 
@@ -119,6 +120,46 @@ struct SapF16 {
       weyl_put(out, half, r);
     }
     return out;
+  }
+};
+
+// FP32 with the links stored as their first two rows (12 reals, planes
+// ((chunk*4 + mu)*6 + k)*vbh + s) and the third row rebuilt as the complex
+// conjugate of the cross product of the first two, exact for SU(3).  The
+// hops inside a block never use the time-boundary links that carry the
+// antiperiodic sign (a block does not wrap), and the library checks all
+// other links for the SU(3) relation before it selects this policy.
+struct SapF32R {
+  using T = float;
+  static constexpr int NP = 24;
+  __device__ __forceinline__ static spinor<float> sm_load(const float *sm, int ld, int s) {
+    return SapF32::sm_load(sm, ld, s);
+  }
+  __device__ __forceinline__ static void sm_store(float *sm, int ld, int s, const spinor<float> &v) {
+    SapF32::sm_store(sm, ld, s, v);
+  }
+  __device__ __forceinline__ static su3<float> link(const void *u, int chunk, int mu, int s, int vbh) {
+    const float2 *p = (const float2 *)u + ((size_t)chunk * 4 + mu) * 6 * vbh + s;
+    su3<float> r;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const float2 v = __ldg(p + (size_t)k * vbh);
+      r.e[k] = mk<float>(v.x, v.y);
+    }
+    // row 3 = conj(row 1 x row 2)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const int a = (j + 1) % 3, b = (j + 2) % 3;
+      const cpx<float> x1 = r.e[a], y2 = r.e[3 + b], x2 = r.e[b], y1 = r.e[3 + a];
+      const float re = x1.re * y2.re - x1.im * y2.im - (x2.re * y1.re - x2.im * y1.im);
+      const float im = x1.re * y2.im + x1.im * y2.re - (x2.re * y1.im + x2.im * y1.re);
+      r.e[6 + j] = mk<float>(re, -im);
+    }
+    return r;
+  }
+  __device__ __forceinline__ static spinor<float> sw(const void *m, int chunk, int s, int vbh, float mu,
+                                                     const spinor<float> &in) {
+    return apply_sw_site<float>(m, chunk, s, vbh, mu, in);
   }
 };
 
@@ -463,7 +504,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
       int c2, s2;
       site_nbr(g, x, mu, +1, c2, s2);
       spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = P::link(a.u, chunk, mu, s, g.vbh);
+      su3<float> uu = P::link(a.ub, chunk, mu, s, g.vbh);
       hop_fwd<float>(mu, uu, sp, hsum);
       any = true;
     }
@@ -471,7 +512,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
       int c2, s2;
       site_nbr(g, x, mu, -1, c2, s2);
       spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = P::link(a.u, c2, mu, s2, g.vbh);
+      su3<float> uu = P::link(a.ub, c2, mu, s2, g.vbh);
       hop_bwd<float>(mu, uu, sm, hsum);
       any = true;
     }
@@ -525,20 +566,73 @@ static int sap_half_fields(Ctx &c, cudaStream_t st) {
   return 0;
 }
 
+// 12-real copies of the FP32 links (first two rows) and a check that every
+// link satisfies row3 = +-conj(row1 x row2) to FP32 accuracy (the sign is
+// the antiperiodic boundary phase); bad[0] counts links that do not.
+__global__ void k_links12(size_t nlink, const float2 *__restrict__ u32, float2 *u12, int vbh, int *bad) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= nlink) return;
+  const size_t cm = i / vbh, s = i - cm * vbh;   // cm = chunk*4 + mu
+  const float2 *p = u32 + cm * 9 * vbh + s;
+  float2 e[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) e[k] = p[(size_t)k * vbh];
+  float2 *q = u12 + cm * 6 * vbh + s;
+#pragma unroll
+  for (int k = 0; k < 6; k++) q[(size_t)k * vbh] = e[k];
+  float dp = 0.0f, dm = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const int a = (j + 1) % 3, b = (j + 2) % 3;
+    const float re = e[a].x * e[3 + b].x - e[a].y * e[3 + b].y - (e[b].x * e[3 + a].x - e[b].y * e[3 + a].y);
+    const float im = -(e[a].x * e[3 + b].y + e[a].y * e[3 + b].x - (e[b].x * e[3 + a].y + e[b].y * e[3 + a].x));
+    dp = fmaxf(dp, fabsf(re - e[6 + j].x) + fabsf(im - e[6 + j].y));
+    dm = fmaxf(dm, fabsf(re + e[6 + j].x) + fabsf(im + e[6 + j].y));
+  }
+  if (fminf(dp, dm) > 1e-5f) atomicAdd(bad, 1);
+}
+
+static int sap_link12_fields(Ctx &c, cudaStream_t st) {
+  if (c.u12_valid) return 0;
+  const size_t nlink = (size_t)c.g.vol * 4;
+  if (!c.u12 && cudaMalloc(&c.u12, nlink * 6 * sizeof(float2)) != cudaSuccess)
+    return fail("out of device memory (12-real links)");
+  int *bad = nullptr;
+  if (cudaMallocAsync(&bad, sizeof(int), st) != cudaSuccess) return fail("out of device memory");
+  cudaMemsetAsync(bad, 0, sizeof(int), st);
+  k_links12<<<(unsigned)((nlink + 255) / 256), 256, 0, st>>>(nlink, c.u32, (float2 *)c.u12, c.g.vbh, bad);
+  int h = 0;
+  cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(bad, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return fail("sap: 12-real link conversion failed");
+  c.u12_ok = h == 0;
+  c.u12_valid = true;
+  return 0;
+}
+
+// storage mode of the even-odd block solver: 0 FP32, 1 FP16, 2 FP32 with
+// 12-real links (the FP32 default when all links pass the SU(3) check)
+static int sap_mode(Ctx &c, int isolv, cudaStream_t st) {
+  if (!isolv) return 0;
+  if (c.sap_prec == 16) return 1;
+  if (!c.sap_link12) return 0;
+  if (sap_link12_fields(c, st)) return -1;
+  return c.u12_ok ? 2 : 0;
+}
+
 // Launch variants of the even-odd block kernel: sites per thread, the
 // launch bound and the register budget it implies.  The autotuner below
 // times every variant that fits the block on the resident fields and keeps
-// the fastest per block size and storage precision.
+// the fastest per block size and storage mode.
 struct EoVariant {
   int ns, maxt;
-  void (*f32)(SapArgs);
-  void (*f16)(SapArgs);
+  void (*k[3])(SapArgs);   // per storage mode
 };
 static const EoVariant kEo[] = {
-    {1, 256, k_sap_blocks_eo<1, SapF32, 256, 2>, k_sap_blocks_eo<1, SapF16, 256, 2>},
-    {1, 672, k_sap_blocks_eo<1, SapF32, 672, 1>, k_sap_blocks_eo<1, SapF16, 672, 1>},
-    {2, 384, k_sap_blocks_eo<2, SapF32, 384, 1>, k_sap_blocks_eo<2, SapF16, 384, 1>},
-    {3, 256, k_sap_blocks_eo<3, SapF32, 256, 1>, k_sap_blocks_eo<3, SapF16, 256, 1>},
+    {1, 256, {k_sap_blocks_eo<1, SapF32, 256, 2>, k_sap_blocks_eo<1, SapF16, 256, 2>, k_sap_blocks_eo<1, SapF32R, 256, 2>}},
+    {1, 672, {k_sap_blocks_eo<1, SapF32, 672, 1>, k_sap_blocks_eo<1, SapF16, 672, 1>, k_sap_blocks_eo<1, SapF32R, 672, 1>}},
+    {2, 384, {k_sap_blocks_eo<2, SapF32, 384, 1>, k_sap_blocks_eo<2, SapF16, 384, 1>, k_sap_blocks_eo<2, SapF32R, 384, 1>}},
+    {3, 256, {k_sap_blocks_eo<3, SapF32, 256, 1>, k_sap_blocks_eo<3, SapF16, 256, 1>, k_sap_blocks_eo<3, SapF32R, 256, 1>}},
 };
 static const int kNEo = sizeof(kEo) / sizeof(kEo[0]);
 
@@ -547,17 +641,14 @@ static int eo_threads(const EoVariant &v, int vbh) {
   return t > v.maxt ? 0 : t;
 }
 
-static size_t eo_smem(int vbh, bool half) {
-  (void)half;
-  return (size_t)vbh * 72 * sizeof(float);
-}
+static size_t eo_smem(int vbh) { return (size_t)vbh * 72 * sizeof(float); }
 
-static void launch_blocks(Ctx &c, const SapArgs &a, int isolv, bool half, cudaStream_t st) {
+static void launch_blocks(Ctx &c, const SapArgs &a, int isolv, int mode, cudaStream_t st) {
   const int nbh = c.g.nbl / 2;
   if (isolv) {
-    const EoVariant &v = kEo[c.sap_variant[half ? 1 : 0]];
+    const EoVariant &v = kEo[c.sap_variant[mode]];
     const int t = eo_threads(v, c.g.vbh);
-    (half ? v.f16 : v.f32)<<<nbh, t, eo_smem(c.g.vbh, half), st>>>(a);
+    v.k[mode]<<<nbh, t, eo_smem(c.g.vbh), st>>>(a);
   } else {
     int ns;
     int t = pick_threads(c.g.vbh, ns);
@@ -568,8 +659,9 @@ static void launch_blocks(Ctx &c, const SapArgs &a, int isolv, bool half, cudaSt
   }
 }
 
-static SapArgs sap_args(Ctx &c, float mu, int nmr, bool half, void *psi, void *rho, void *phi) {
+static SapArgs sap_args(Ctx &c, float mu, int nmr, int mode, void *psi, void *rho, void *phi) {
   SapArgs a;
+  const bool half = mode == 1;
   a.g = c.g;
   a.colour = 0;
   a.mu = mu;
@@ -578,7 +670,8 @@ static SapArgs sap_args(Ctx &c, float mu, int nmr, bool half, void *psi, void *r
   a.psi = (float4 *)psi;
   a.rho = (float4 *)rho;
   a.phi = (float4 *)phi;
-  a.u = half ? (const void *)c.u16 : (const void *)c.u32;
+  a.u = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
+  a.ub = half ? (const void *)c.u16 : (const void *)c.u32;
   a.sw = half ? (const void *)c.sw16 : (const void *)c.sw32;
   a.swinv = half ? (const void *)c.sw16_inv : (const void *)c.sw32_inv;
   return a;
@@ -586,14 +679,12 @@ static SapArgs sap_args(Ctx &c, float mu, int nmr, bool half, void *psi, void *r
 
 // Time every fitting variant of the even-odd block kernel (both colours, 4
 // MR steps, on a random residual) and keep the fastest.
-static int sap_autotune(Ctx &c, bool half, cudaStream_t st) {
-  const int slot = half ? 1 : 0;
-  if (c.sap_tuned_vbh[slot] == c.g.vbh) return 0;
-  for (int i = 0; i < kNEo; i++) {
-    cudaFuncSetAttribute(kEo[i].f32, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
-    cudaFuncSetAttribute(kEo[i].f16, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
-  }
-  if (eo_smem(c.g.vbh, half) > (size_t)SAP_SMEM_MAX) return fail("sap: block too large for shared memory");
+static int sap_autotune(Ctx &c, int mode, cudaStream_t st) {
+  if (c.sap_tuned_vbh[mode] == c.g.vbh) return 0;
+  for (int i = 0; i < kNEo; i++)
+    for (int m = 0; m < 3; m++)
+      cudaFuncSetAttribute(kEo[i].k[m], cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+  if (eo_smem(c.g.vbh) > (size_t)SAP_SMEM_MAX) return fail("sap: block too large for shared memory");
   const size_t nb = spinor_bytes(c, 32);
   void *psi = nullptr, *rho = nullptr, *phi = nullptr;
   if (cudaMallocAsync(&psi, nb, st) != cudaSuccess || cudaMallocAsync(&rho, nb, st) != cudaSuccess ||
@@ -607,15 +698,15 @@ static int sap_autotune(Ctx &c, bool half, cudaStream_t st) {
   float best_ms = 0.0f;
   for (int i = 0; i < kNEo; i++) {
     if (!eo_threads(kEo[i], c.g.vbh)) continue;
-    c.sap_variant[slot] = i;
-    SapArgs a = sap_args(c, 0.0f, 4, half, psi, rho, phi);
+    c.sap_variant[mode] = i;
+    SapArgs a = sap_args(c, 0.0f, 4, mode, psi, rho, phi);
     float tot = 0.0f;
     for (int rep = 0; rep < 4; rep++) {
       gen_uniform_spinor32(c, rho, 977ull + rep, st);
       cudaEventRecord(e0, st);
       for (int ic = 0; ic < 2; ic++) {
         a.colour = ic;
-        launch_blocks(c, a, 1, half, st);
+        launch_blocks(c, a, 1, mode, st);
       }
       cudaEventRecord(e1, st);
       cudaEventSynchronize(e1);
@@ -635,9 +726,9 @@ static int sap_autotune(Ctx &c, bool half, cudaStream_t st) {
   cudaFreeAsync(rho, st);
   cudaFreeAsync(phi, st);
   if (best < 0) return fail("sap: no block-kernel variant fits this block size");
-  c.sap_variant[slot] = best;
-  c.sap_tuned_vbh[slot] = c.g.vbh;
-  c.sap_tuned_ms[slot] = best_ms / 3.0f;
+  c.sap_variant[mode] = best;
+  c.sap_tuned_vbh[mode] = c.g.vbh;
+  c.sap_tuned_ms[mode] = best_ms / 3.0f;
   return cudaStreamSynchronize(st) == cudaSuccess ? 0 : fail("sap: CUDA error while autotuning");
 }
 
@@ -653,10 +744,14 @@ int sap_prepare(Ctx &c, cudaStream_t st) {
     cudaFuncSetAttribute(k_sap_blocks_plain<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
     attrs = true;
   }
-  const bool half = c.sap_prec == 16;
-  if (half && sap_half_fields(c, st)) return -1;
-  return sap_autotune(c, half, st);
+  if (c.sap_prec == 16 && sap_half_fields(c, st)) return -1;
+  const int mode = sap_mode(c, 1, st);
+  if (mode < 0) return -1;
+  return sap_autotune(c, mode, st);
 }
+
+// storage mode in use (for reports): 0 FP32, 1 FP16, 2 FP32 with 12-real links
+int sap_storage_mode(Ctx &c) { return sap_mode(c, 1, c.stream); }
 
 // ncy SAP cycles sap(mu, isolv, nmr, psi, rho) on FP32 device fields
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
@@ -667,23 +762,24 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
 }
 
 // One SAP cycle sap(mu, isolv, nmr, psi, rho) on FP32 device fields.
-// phi_blk is a scratch FP32 field.  With the FP16 storage option the
-// even-odd block solver runs on FP16 copies of the links and SW matrices and
-// FP16 work vectors (the plain solver, isolv = 0, always runs in FP32).
+// phi_blk is a scratch FP32 field.  The even-odd block solver (isolv = 1)
+// reads the links and SW matrices in the storage mode of sap_mode(); the
+// plain solver (isolv = 0) always in FP32.
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st) {
-  const bool half = isolv && c.sap_prec == 16;
-  if (isolv && c.sap_tuned_vbh[half ? 1 : 0] != c.g.vbh && sap_prepare(c, st)) return -1;
-  if (half && !c.h16_valid && sap_half_fields(c, st)) return -1;
+  const int mode = sap_mode(c, isolv, st);
+  if (mode < 0) return -1;
+  if (isolv && c.sap_tuned_vbh[mode] != c.g.vbh && sap_prepare(c, st)) return -1;
+  if (mode == 1 && !c.h16_valid && sap_half_fields(c, st)) return -1;
   int ns;
   if (!pick_threads(c.g.vbh, ns) || (!isolv && (size_t)48 * c.g.vbh * sizeof(float) > (size_t)SAP_SMEM_MAX))
     return fail("sap: block too large");
-  SapArgs a = sap_args(c, mu, nmr, half, psi, rho, phi_blk);
+  SapArgs a = sap_args(c, mu, nmr, mode, psi, rho, phi_blk);
   const size_t nb_sites = (size_t)(c.g.nbl / 2) * c.g.vb;
   const unsigned nbnd = (unsigned)((nb_sites + 127) / 128);
   for (int ic = 0; ic < 2; ic++) {
     a.colour = ic;
-    launch_blocks(c, a, isolv, half, st);
-    if (half) k_sap_bnd<SapF16><<<nbnd, 128, 0, st>>>(a);
+    launch_blocks(c, a, isolv, mode, st);
+    if (mode == 1) k_sap_bnd<SapF16><<<nbnd, 128, 0, st>>>(a);
     else k_sap_bnd<SapF32><<<nbnd, 128, 0, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");

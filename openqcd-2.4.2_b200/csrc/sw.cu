@@ -356,6 +356,7 @@ int links_refresh_f32(Ctx &c, cudaStream_t st) {
   if (!c.u32 && cudaMalloc(&c.u32, n * sizeof(float2)) != cudaSuccess) return fail("out of device memory (links)");
   k_links_f32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, c.ud, c.u32);
   c.h16_valid = false;
+  c.u12_valid = false;
   return cudaGetLastError() == cudaSuccess ? 0 : fail("links_refresh_f32: launch failed");
 }
 

@@ -99,6 +99,7 @@ _SIGS = {
                           C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_clear_error": (None, []),
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
+    "b200_set_sap_link12": (C.c_int, [C.c_int]),
     "b200_profiler": (C.c_int, [C.c_int]),
     "b200_sap_tuning": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_set_dfl_parms": (C.c_int, [C.c_void_p, C.c_int]),
@@ -228,6 +229,10 @@ def set_sap_parms(bs, isolv, nmr, ncy):
 
 def set_sap_prec(bits):
     return check(lib().b200_set_sap_prec(bits))
+
+
+def set_sap_link12(on):
+    return check(lib().b200_set_sap_link12(1 if on else 0))
 
 
 def sap_tuning(prec):
