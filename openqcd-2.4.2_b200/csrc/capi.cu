@@ -199,6 +199,14 @@ int b200_profiler(int on) {
   return (on ? cudaProfilerStart() : cudaProfilerStop()) == cudaSuccess ? 0 : fail("profiler start/stop failed");
 }
 
+int b200_dev_dirac_multi(int n, float mu, void *const *s, void *const *r, void *const *sub) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1;
+  if (n < 1) return fail("dirac_multi: no fields");
+  if (qcd::dirac_multi32(c, n, mu, s, r, sub, c.stream)) return fail("dirac_multi: launch failed");
+  return b200_sync();
+}
+
 int b200_set_sap_prec(int bits) {
   if (bits != 16 && bits != 32) return fail("set_sap_prec: the storage precision must be 16 or 32");
   ctx().sap_prec = bits;

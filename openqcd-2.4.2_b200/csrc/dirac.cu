@@ -155,6 +155,102 @@ int dwhat_dble_halfscratch(const Ctx &c, double mu, const void *s, void *r, void
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+// Dw on NRT FP32 fields at once: every link and SW matrix of a site is
+// loaded once for all right-hand sides.  r_j = D s_j, or r_j = sub_j - D s_j
+// when sub is given (the residual update of the deflated preconditioner
+// fused into the operator).
+template <int NRT> struct MPtrs {
+  void *p[NRT];
+};
+
+template <int NRT>
+__global__ void __launch_bounds__(128, 2) dirac_multi_kernel(Geom g, MPtrs<NRT> s, MPtrs<NRT> r, MPtrs<NRT> sub,
+                                                             int has_sub, const void *__restrict__ u,
+                                                             const void *__restrict__ sw, float mu_e, float mu_o,
+                                                             const int *__restrict__ sched) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.vol) return;
+  const int b = i / g.vb, rr = i - b * g.vb;
+  const int p = rr >= g.vbh, si = rr - p * g.vbh;
+  const int blk = sched ? __ldg(sched + b) : b;
+  Site x;
+  site_decode(g, p, blk, si, x);
+  const int chunk = p * g.nbl + blk;
+  spinor<float> acc[NRT];
+  {
+    float m[36];
+    cpx<float> w[6], o[6];
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      Store<float>::load_pauli(sw, chunk, half, si, g.vbh, m);
+      const float mu = (p == 0 ? mu_e : mu_o) * (half == 0 ? 1.0f : -1.0f);
+#pragma unroll
+      for (int j = 0; j < NRT; j++) {
+        const spinor<float> in = Store<float>::load_spinor(s.p[j], chunk, si, g.vbh);
+        weyl_get(in, half, w);
+        mul_pauli<float>(mu, m, w, o);
+        weyl_put(acc[j], half, o);
+      }
+    }
+  }
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++)
+#pragma unroll
+    for (int dd = 0; dd < 2; dd++) {
+      int c2, s2;
+      site_nbr(g, x, mu, dd ? -1 : 1, c2, s2);
+      const su3<float> uu = dd ? Store<float>::load_link(u, c2, mu, s2, g.vbh) : Store<float>::load_link(u, chunk, mu, si, g.vbh);
+#pragma unroll
+      for (int j = 0; j < NRT; j++) {
+        const spinor<float> nb = Store<float>::load_spinor(s.p[j], c2, s2, g.vbh);
+        spinor<float> t;
+        szero(t);
+        if (dd) hop_bwd<float>(mu, uu, nb, t);
+        else hop_fwd<float>(mu, uu, nb, t);
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) {
+            acc[j].c[a].c[k].re -= 0.5f * t.c[a].c[k].re;
+            acc[j].c[a].c[k].im -= 0.5f * t.c[a].c[k].im;
+          }
+      }
+    }
+#pragma unroll
+  for (int j = 0; j < NRT; j++) {
+    if (has_sub) {
+      spinor<float> v = Store<float>::load_spinor(sub.p[j], chunk, si, g.vbh);
+      ssub(v, acc[j]);
+      Store<float>::store_spinor(r.p[j], chunk, si, g.vbh, v);
+    } else {
+      Store<float>::store_spinor(r.p[j], chunk, si, g.vbh, acc[j]);
+    }
+  }
+}
+
+template <int NRT>
+static void multi_pass(const Ctx &c, float mu, void *const *sv, void *const *rv, void *const *subv, cudaStream_t st) {
+  MPtrs<NRT> a, b, d;
+  for (int j = 0; j < NRT; j++) {
+    a.p[j] = sv[j];
+    b.p[j] = rv[j];
+    d.p[j] = subv ? subv[j] : nullptr;
+  }
+  const float muo = c.eoflg ? 0.0f : mu;
+  dirac_multi_kernel<NRT><<<(c.g.vol + 127) / 128, 128, 0, st>>>(c.g, a, b, d, subv != nullptr, c.u32, c.sw32, mu,
+                                                                 muo, c.sched);
+}
+
+// r[j] = Dw(mu) s[j] (or sub[j] - Dw s[j]) for n FP32 fields, four at a time
+int dirac_multi32(const Ctx &c, int n, float mu, void *const *sv, void *const *rv, void *const *subv,
+                  cudaStream_t st) {
+  int j = 0;
+  for (; j + 4 <= n; j += 4) multi_pass<4>(c, mu, sv + j, rv + j, subv ? subv + j : nullptr, st);
+  for (; j + 2 <= n; j += 2) multi_pass<2>(c, mu, sv + j, rv + j, subv ? subv + j : nullptr, st);
+  for (; j < n; j++) multi_pass<1>(c, mu, sv + j, rv + j, subv ? subv + j : nullptr, st);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 template int dirac_op<double>(const Ctx &, int, double, const void *, void *, void *, cudaStream_t);
 template int dirac_op<float>(const Ctx &, int, float, const void *, void *, void *, cudaStream_t);
 

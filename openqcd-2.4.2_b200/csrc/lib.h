@@ -230,6 +230,8 @@ void net_release(Ctx &c);
 void net_fields_release(Ctx &c);
 // dfl_batch.cu: the deflation steps for nr right-hand sides at once
 int dfl_batch_alloc(Ctx &c);
+int dirac_multi32(const Ctx &c, int n, float mu, void *const *sv, void *const *rv, void *const *subv,
+                  cudaStream_t st);
 void dfl_mark(Ctx &c, int k);
 int ensure_lvd_n(Ctx &c, int n);
 int dfl_batch_check(Ctx &c);

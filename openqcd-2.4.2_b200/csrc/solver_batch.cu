@@ -701,11 +701,18 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       if (ltl_gcr_b(c, mu[0], na, (const double2 *const *)v.data(), v.data(), lf.data(), ls.data(), st)) return -1;
       dfl_prolong_b(c, na, (const double2 *const *)v.data(), w0.data(), st);
       dfl_mark(c, 3);
+      {
+        // ch = rho - D ws0 for all active systems, links and SW read once per four
+        std::vector<void *> chs(na), rhs(na);
+        for (int i = 0; i < na; i++) {
+          chs[i] = S[A[i]].chi[S[A[i]].k];
+          rhs[i] = S[A[i]].rho;
+        }
+        dirac_multi32(c, na, (float)mu[0], w0.data(), chs.data(), rhs.data(), st);
+      }
       for (int i = 0; i < na; i++) {
         SysState &y = S[A[i]];
         void *ph = y.phi[y.k], *ch = y.chi[y.k];
-        dirac_op<float>(c, 0, (float)y.mu, y.ws0, ch, c.tmp32, st);
-        la_diff(c, 32, y.rho, ch, PAR_ALL, st);        // ch = rho - D ws0
         la_zero(c, 32, ph, PAR_ALL, st);
         dfl_mark(c, 2);
         sap_cycles(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ph, ch, phib, st);

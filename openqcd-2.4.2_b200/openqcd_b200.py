@@ -100,6 +100,7 @@ _SIGS = {
     "b200_clear_error": (None, []),
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
     "b200_set_sap_link12": (C.c_int, [C.c_int]),
+    "b200_dev_dirac_multi": (C.c_int, [C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_profiler": (C.c_int, [C.c_int]),
     "b200_sap_tuning": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_set_dfl_parms": (C.c_int, [C.c_void_p, C.c_int]),
@@ -345,6 +346,14 @@ class DevField:
 
     def norm2(self):
         return lib().b200_dev_norm2(self.prec, self.ptr)
+
+
+def dev_dirac_multi(mu, ss, rs, subs=None):
+    n = len(ss)
+    sp = (C.c_void_p * n)(*[x.ptr for x in ss])
+    rp = (C.c_void_p * n)(*[x.ptr for x in rs])
+    up = (C.c_void_p * n)(*[x.ptr for x in subs]) if subs else None
+    return check(lib().b200_dev_dirac_multi(n, mu, sp, rp, up))
 
 
 def dev_dirac(op, mu, s, r):
