@@ -195,6 +195,20 @@ int b200_set_sap_link12(int on);
  * threads per block, time of one cycle's block sweeps in ms. */
 int b200_sap_tuning(int prec, int *variant, int *threads, float *ms);
 
+/* ------------------------------------------------------ archive.h, uflds.h */
+/* Files in openQCD's universal format (main/README.io), little-endian.  The
+ * gauge field is read from / written to the device copy (the antiperiodic
+ * phase is removed on export and applied on import); import requires the
+ * file's lattice sizes to equal the geometry (no extension; mask unused)
+ * and marks the SW term stale (call b200_sw_term()).  Spinor arrays are in
+ * the reference layout (host or device). */
+/* archive.c:804 */ void export_cnfg(char *out);
+/* archive.c:878 */ void import_cnfg(char *in, int mask);
+/* sarchive.c:424 */ void export_sfld(char *out, int eo, spinor_dble *sd);
+/* sarchive.c:522 */ void import_sfld(char *in, int eo, spinor_dble *sd);
+/* plaq_sum.c:161 plaq_sum_dble(1) of the device gauge field */
+double b200_plaq_sum(void);
+
 /* ------------------------------------------- deflation (dfl.h, little.h) */
 /* Parameters of set_dfl_parms (modules/flags/dfl_parms.c:209; the DFL block
  * size must equal the geometry block size), set_dfl_pro_parms (:286) and

@@ -207,6 +207,20 @@ int b200_dev_dirac_multi(int n, float mu, void *const *s, void *const *r, void *
   return b200_sync();
 }
 
+// ------------------------------------------------------------ archives
+// archive.c:804, :878 and sarchive.c:424, :522; files in the universal format
+void export_cnfg(char *out) { qcd::export_cnfg(ctx(), out); }
+void import_cnfg(char *in, int mask) { qcd::import_cnfg(ctx(), in, mask); }
+void export_sfld(char *out, int eo, spinor_dble *sd) { qcd::export_sfld(ctx(), out, eo, sd); }
+void import_sfld(char *in, int eo, spinor_dble *sd) { qcd::import_sfld(ctx(), in, eo, sd); }
+
+// plaq_sum_dble(1) (modules/uflds/plaq_sum.c:161) of the device gauge field
+double b200_plaq_sum(void) {
+  double s = 0.0;
+  if (qcd::plaq_sum(ctx(), &s)) return -1.0e300;
+  return s;
+}
+
 int b200_set_sap_prec(int bits) {
   if (bits != 16 && bits != 32) return fail("set_sap_prec: the storage precision must be 16 or 32");
   ctx().sap_prec = bits;

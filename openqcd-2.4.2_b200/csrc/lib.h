@@ -217,6 +217,12 @@ int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st
 // dfl.cu
 int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
+// archive.cu
+int plaq_sum(Ctx &c, double *sum);
+int export_cnfg(Ctx &c, const char *out);
+int import_cnfg(Ctx &c, const char *in, int mask);
+int export_sfld(Ctx &c, const char *out, int eo, const void *sd);
+int import_sfld(Ctx &c, const char *in, int eo, void *sd);
 // net.cu
 int net_set_weights(Ctx &c, const float *w);
 int net_get_weights(Ctx &c, float *w);

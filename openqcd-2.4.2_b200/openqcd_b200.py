@@ -100,6 +100,11 @@ _SIGS = {
     "b200_clear_error": (None, []),
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
     "b200_set_sap_link12": (C.c_int, [C.c_int]),
+    "export_cnfg": (None, [C.c_char_p]),
+    "import_cnfg": (None, [C.c_char_p, C.c_int]),
+    "export_sfld": (None, [C.c_char_p, C.c_int, C.c_void_p]),
+    "import_sfld": (None, [C.c_char_p, C.c_int, C.c_void_p]),
+    "b200_plaq_sum": (C.c_double, []),
     "b200_dev_dirac_multi": (C.c_int, [C.c_int, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_profiler": (C.c_int, [C.c_int]),
     "b200_sap_tuning": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -649,3 +654,30 @@ def net_make_pairs(rs, es, mu, res, seed=1):
 
 def set_precond(kind):
     return check(lib().b200_set_precond(kind))
+
+
+# ------------------------------------------------------------------- archives
+def export_cnfg(path):
+    _void(lib().export_cnfg, path.encode())
+
+
+def import_cnfg(path, mask=0):
+    _void(lib().import_cnfg, path.encode(), mask)
+
+
+def export_sfld(path, eo, sd):
+    sd = np.ascontiguousarray(sd, dtype=np.float64)
+    _void(lib().export_sfld, path.encode(), eo, _ptr(sd))
+
+
+def import_sfld(path, eo, sd):
+    sd = np.array(sd, dtype=np.float64, copy=True)
+    _void(lib().import_sfld, path.encode(), eo, _ptr(sd))
+    return sd
+
+
+def plaq_sum():
+    v = lib().b200_plaq_sum()
+    if v < -1e299:
+        raise B200Error(_err_after())
+    return v

@@ -299,3 +299,27 @@ class RefLib:
         self.lib.ref_time_sap_gcr.restype = C.c_double
         t = self.lib.ref_time_sap_gcr(nkv, nmx, res, mu, self._p(eta), status)
         return t, list(status)
+
+    # ------------------------------------------------------------- archives
+    def export_cnfg(self, path):
+        self.lib.ref_export_cnfg.argtypes = [C.c_char_p]
+        self.lib.ref_export_cnfg(path.encode())
+
+    def import_cnfg(self, path):
+        self.lib.ref_import_cnfg.argtypes = [C.c_char_p]
+        self.lib.ref_import_cnfg(path.encode())
+
+    def export_sfld(self, path, eo, sd):
+        sd = np.ascontiguousarray(sd, dtype=np.float64)
+        self.lib.ref_export_sfld.argtypes = [C.c_char_p, C.c_int, C.c_void_p]
+        self.lib.ref_export_sfld(path.encode(), eo, self._p(sd))
+
+    def import_sfld(self, path, eo):
+        out = np.zeros(self.vol * 24)
+        self.lib.ref_import_sfld.argtypes = [C.c_char_p, C.c_int, C.c_void_p]
+        self.lib.ref_import_sfld(path.encode(), eo, self._p(out))
+        return out
+
+    def plaq_sum(self):
+        self.lib.ref_plaq_sum.restype = C.c_double
+        return self.lib.ref_plaq_sum()
