@@ -195,6 +195,19 @@ int b200_set_sap_link12(int on);
  * threads per block, time of one cycle's block sweeps in ms. */
 int b200_sap_tuning(int prec, int *variant, int *threads, float *ms);
 
+/* ------------------------------------------------------------- forces.h */
+/* CG on the normal equations Dw(mu)^dag Dw(mu) psi = eta (cgne.c:452 with
+ * the drivers of forces/tmcg.c): tmcg on all sites, tmcgeo with the even-odd
+ * preconditioned Dwhat on the even sites (ifail -3: unsafe odd SW
+ * inversion).  Reference-layout FP64 fields (host or device). */
+/* tmcg.c:118 */ double tmcg(int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi,
+                             int *ifail, int *status);
+/* tmcg.c:206 */ double tmcgeo(int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi,
+                               int *ifail, int *status);
+/* the same on device fields in the library's layout (eo selects tmcgeo) */
+double b200_dev_tmcg(int eo, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
+                     int *status);
+
 /* ------------------------------------------------------ archive.h, uflds.h */
 /* Files in openQCD's universal format (main/README.io), little-endian.  The
  * gauge field is read from / written to the device copy (the antiperiodic

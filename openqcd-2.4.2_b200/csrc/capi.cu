@@ -207,6 +207,49 @@ int b200_dev_dirac_multi(int n, float mu, void *const *s, void *const *r, void *
   return b200_sync();
 }
 
+// ------------------------------------------------------- CG normal equations
+// tmcg.c:118 / :206 on reference-layout FP64 fields (host or device)
+static double tmcg_ref_layout(int eo, int nmx, int istop, double res, double mu, spinor_dble *eta,
+                              spinor_dble *psi, int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1.0;
+  const size_t nb = spinor_bytes(c, 64);
+  if (ensure_stage(c, nb)) return -1.0;
+  void *fe = nullptr, *fp = nullptr;
+  if (cudaMalloc(&fe, nb) != cudaSuccess || cudaMalloc(&fp, nb) != cudaSuccess) {
+    fail("out of device memory");
+    return -1.0;
+  }
+  cudaMemcpyAsync(c.stage, eta, nb, cudaMemcpyDefault, c.stream);
+  spinor_from_ref(c, 64, c.stage, fe, c.stream);
+  cudaMemcpyAsync(c.stage, psi, nb, cudaMemcpyDefault, c.stream);   // odd sites of psi kept with eo = 1
+  spinor_from_ref(c, 64, c.stage, fp, c.stream);
+  const double rho = qcd::tmcg_dev(c, eo, nmx, istop, res, mu, fe, fp, ifail, status);
+  spinor_to_ref(c, 64, fp, c.stage, c.stream);
+  cudaMemcpyAsync(psi, c.stage, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+  cudaFree(fe);
+  cudaFree(fp);
+  return rho;
+}
+
+double tmcg(int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi, int *ifail,
+            int *status) {
+  return tmcg_ref_layout(0, nmx, istop, res, mu, eta, psi, ifail, status);
+}
+
+double tmcgeo(int nmx, int istop, double res, double mu, spinor_dble *eta, spinor_dble *psi, int *ifail,
+              int *status) {
+  return tmcg_ref_layout(1, nmx, istop, res, mu, eta, psi, ifail, status);
+}
+
+double b200_dev_tmcg(int eo, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
+                     int *status) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1.0;
+  return qcd::tmcg_dev(c, eo, nmx, istop, res, mu, eta, psi, ifail, status);
+}
+
 // ------------------------------------------------------------ archives
 // archive.c:804, :878 and sarchive.c:424, :522; files in the universal format
 void export_cnfg(char *out) { qcd::export_cnfg(ctx(), out); }

@@ -217,6 +217,9 @@ int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st
 // dfl.cu
 int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
+// solver_cg.cu
+double tmcg_dev(Ctx &c, int eo, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
+                int *status);
 // archive.cu
 int plaq_sum(Ctx &c, double *sum);
 int export_cnfg(Ctx &c, const char *out);

@@ -100,6 +100,12 @@ _SIGS = {
     "b200_clear_error": (None, []),
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
     "b200_set_sap_link12": (C.c_int, [C.c_int]),
+    "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                          C.c_void_p]),
+    "tmcgeo": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                            C.c_void_p]),
+    "b200_dev_tmcg": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
     "export_cnfg": (None, [C.c_char_p]),
     "import_cnfg": (None, [C.c_char_p, C.c_int]),
     "export_sfld": (None, [C.c_char_p, C.c_int, C.c_void_p]),
@@ -681,3 +687,18 @@ def plaq_sum():
     if v < -1e299:
         raise B200Error(_err_after())
     return v
+
+
+# ------------------------------------------------------- CG, normal equations
+def tmcg(nmx, istop, res, mu, eta, eo=False, psi0=None):
+    """tmcg (eo False) or tmcgeo (eo True) on reference-layout arrays."""
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    psi = np.zeros_like(eta) if psi0 is None else np.array(psi0, dtype=np.float64, copy=True)
+    ifail = C.c_int(0)
+    status = C.c_int(0)
+    f = lib().tmcgeo if eo else lib().tmcg
+    lib().b200_clear_error()
+    rho = f(nmx, istop, res, mu, _ptr(eta), _ptr(psi), C.byref(ifail), C.byref(status))
+    if rho < 0:
+        raise B200Error(_err_after())
+    return psi, rho, ifail.value, status.value

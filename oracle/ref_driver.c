@@ -636,3 +636,26 @@ double ref_plaq_sum(void)
    ENTER();
    return plaq_sum_dble(1);
 }
+
+
+/* ------------------------------------------------------------------ tmcg */
+#include "forces.h"
+
+double ref_tmcg(int eo, int nmx, int istop, double res, double mu, const double *eta, double *psi, int *ifail,
+                int *status)
+{
+   ENTER();
+   double rho;
+   spinor_dble **wsd;
+   need_ws(40, 8);
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], eta, VOLUME * sizeof(spinor_dble));
+   memcpy(wsd[1], psi, VOLUME * sizeof(spinor_dble));
+   if (eo)
+      rho = tmcgeo(nmx, istop, res, mu, wsd[0], wsd[1], ifail, status);
+   else
+      rho = tmcg(nmx, istop, res, mu, wsd[0], wsd[1], ifail, status);
+   memcpy(psi, wsd[1], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+   return rho;
+}

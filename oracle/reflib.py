@@ -323,3 +323,15 @@ class RefLib:
     def plaq_sum(self):
         self.lib.ref_plaq_sum.restype = C.c_double
         return self.lib.ref_plaq_sum()
+
+    def tmcg(self, nmx, istop, res, mu, eta, eo=False, psi0=None):
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        psi = np.zeros_like(eta) if psi0 is None else np.array(psi0, dtype=np.float64, copy=True)
+        ifail = C.c_int(0)
+        status = C.c_int(0)
+        self.lib.ref_tmcg.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+        self.lib.ref_tmcg.restype = C.c_double
+        rho = self.lib.ref_tmcg(1 if eo else 0, nmx, istop, res, mu, self._p(eta), self._p(psi), C.byref(ifail),
+                                C.byref(status))
+        return psi, rho, ifail.value, status.value
