@@ -207,6 +207,18 @@ int b200_sap_tuning(int prec, int *variant, int *threads, float *ms);
 /* the same on device fields in the library's layout (eo selects tmcgeo) */
 double b200_dev_tmcg(int eo, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
                      int *status);
+/* Multi-shift CG (linsolv/mscg.c:387 with the driver forces/tmcgm.c:100):
+ * (Dwhat^dag Dwhat + mu[k]^2) psi[k] = eta on the even sites for nmu shifts
+ * at once, each to its own relative residual res[k]; status = total CG
+ * iterations including the final residual checks (ifail -1: not converged,
+ * status nmx; -3: unsafe odd SW inversion).  Reference-layout FP64 fields
+ * (host or device); the odd sites of psi[k] are kept. */
+/* tmcgm.c:100 */ void tmcgm(int nmx, int istop, double *res, int nmu, double *mu, spinor_dble *eta,
+                             spinor_dble **psi, int *ifail, int *status);
+/* the same on device fields in the library's layout; returns 0, or -1 on an
+ * error (message from b200_last_error) */
+int b200_dev_tmcgm(int nmx, int istop, const double *res, int nmu, const double *mu, const void *eta,
+                   void *const *psi, int *ifail, int *status);
 
 /* ------------------------------------------------------ archive.h, uflds.h */
 /* Files in openQCD's universal format (main/README.io), little-endian.  The

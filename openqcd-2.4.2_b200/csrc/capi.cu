@@ -250,6 +250,50 @@ double b200_dev_tmcg(int eo, int nmx, int istop, double res, double mu, const vo
   return qcd::tmcg_dev(c, eo, nmx, istop, res, mu, eta, psi, ifail, status);
 }
 
+// tmcgm.c:100 on reference-layout FP64 fields (host or device): the even
+// sites of eta and of the nmu solutions psi[k]
+void tmcgm(int nmx, int istop, double *res, int nmu, double *mu, spinor_dble *eta, spinor_dble **psi, int *ifail,
+           int *status) {
+  Ctx &c = ctx();
+  ifail[0] = 0;
+  status[0] = 0;
+  if (check_fields(c)) return;
+  if (nmu < 0) {
+    fail("mscg: parameters are out of range");
+    return;
+  }
+  const size_t nb = spinor_bytes(c, 64);
+  if (ensure_stage(c, nb)) return;
+  std::vector<void *> f(nmu + 1, nullptr);
+  for (auto &q : f)
+    if (cudaMalloc(&q, nb) != cudaSuccess) {
+      for (void *p : f) cudaFree(p);
+      fail("out of device memory");
+      return;
+    }
+  cudaMemcpyAsync(c.stage, eta, nb, cudaMemcpyDefault, c.stream);
+  spinor_from_ref(c, 64, c.stage, f[0], c.stream);
+  for (int k = 0; k < nmu; k++) {   // odd sites of psi[k] are kept
+    cudaMemcpyAsync(c.stage, psi[k], nb, cudaMemcpyDefault, c.stream);
+    spinor_from_ref(c, 64, c.stage, f[k + 1], c.stream);
+  }
+  const int rc = qcd::tmcgm_dev(c, nmx, istop, res, nmu, mu, f[0], f.data() + 1, ifail, status);
+  if (rc == 0)
+    for (int k = 0; k < nmu; k++) {
+      spinor_to_ref(c, 64, f[k + 1], c.stage, c.stream);
+      cudaMemcpyAsync(psi[k], c.stage, nb, cudaMemcpyDefault, c.stream);
+    }
+  cudaStreamSynchronize(c.stream);
+  for (void *p : f) cudaFree(p);
+}
+
+int b200_dev_tmcgm(int nmx, int istop, const double *res, int nmu, const double *mu, const void *eta,
+                   void *const *psi, int *ifail, int *status) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1;
+  return qcd::tmcgm_dev(c, nmx, istop, res, nmu, mu, eta, psi, ifail, status);
+}
+
 // ------------------------------------------------------------ archives
 // archive.c:804, :878 and sarchive.c:424, :522; files in the universal format
 void export_cnfg(char *out) { qcd::export_cnfg(ctx(), out); }

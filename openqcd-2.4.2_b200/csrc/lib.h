@@ -165,6 +165,9 @@ enum { PAR_ALL = 2, PAR_EVEN = 0, PAR_ODD = 1 };
 int la_norm2(Ctx &c, int prec, const void *x, int par, double *res_dd);                 // |x|^2 -> (hi,lo)
 int la_dot(Ctx &c, int prec, const void *x, const void *y, int par, double *res);       // (x,y) -> re,im (dd each)
 int la_unorm(Ctx &c, int prec, const void *x, int par, double *res);                    // max site norm
+int la_xr_norm2(Ctx &c, void *x, void *r, const void *p, const void *ap, double a, int par,
+                double *res_dd);                                 // FP64: x += a p, r -= a ap, |r|^2
+int la_mulg5_norm2(Ctx &c, void *x, int par, double *res_dd);    // FP64: x = g5 x, |x|^2
 void la_zero(const Ctx &c, int prec, void *x, int par, cudaStream_t st);
 void la_copy(const Ctx &c, int prec_in, const void *x, int prec_out, void *y, int par, cudaStream_t st);
 void la_scale(const Ctx &c, int prec, void *x, double a, int par, cudaStream_t st);
@@ -220,6 +223,8 @@ void dfl_release(Ctx &c);
 // solver_cg.cu
 double tmcg_dev(Ctx &c, int eo, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
                 int *status);
+int tmcgm_dev(Ctx &c, int nmx, int istop, const double *res, int nmu, const double *mu, const void *eta,
+              void *const *psi, int *ifail, int *status);
 // archive.cu
 int plaq_sum(Ctx &c, double *sum);
 int export_cnfg(Ctx &c, const char *out);

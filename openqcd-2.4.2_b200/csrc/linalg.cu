@@ -192,6 +192,63 @@ int la_dot(Ctx &c, int prec, const void *x, const void *y, int par, double *res)
   return finish(c, 2, res);
 }
 
+// x += a p ; r -= a ap ; then |r|^2 -- the FP64 CG update of the
+// multi-shift solver (modules/linsolv/mscg.c:242-275, cg_step2 with the norm
+// of cg_step3) in one pass
+__global__ void k_xr_norm2(Range rg, double2 *__restrict__ x, double2 *__restrict__ r,
+                           const double2 *__restrict__ p, const double2 *__restrict__ ap, double a,
+                           double *part) {
+  double v[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)RT + threadIdx.x; i < rg.n; i += (size_t)RB * RT) {
+    const size_t j = rg.beg + i;
+    const double2 pp = __ldg(p + j), aa = __ldg(ap + j);
+    double2 xx = x[j], rr = r[j];
+    xx.x += a * pp.x;
+    xx.y += a * pp.y;
+    rr.x -= a * aa.x;
+    rr.y -= a * aa.y;
+    x[j] = xx;
+    r[j] = rr;
+    v[0] += rr.x * rr.x + rr.y * rr.y;
+  }
+  block_store<1>(v, part);
+}
+
+int la_xr_norm2(Ctx &c, void *x, void *r, const void *p, const void *ap, double a, int par, double *res) {
+  if (ensure_red(c)) return -1;
+  Range rg = range(c, 64, par);
+  k_xr_norm2<<<RB, RT, 0, c.stream>>>(rg, (double2 *)x, (double2 *)r, (const double2 *)p, (const double2 *)ap, a,
+                                      c.red);
+  k_finish<1><<<1, 32, 0, c.stream>>>(c.red, RB, c.red_out);
+  return finish(c, 1, res);
+}
+
+// x -> gamma5 x on a parity range of an FP64 field (spin components 2, 3 of
+// every site change sign: double2 planes 6..11 of a chunk), then |x|^2
+__global__ void k_mulg5_norm2(Range rg, double2 *__restrict__ x, int vbh, double *part) {
+  double v[1] = {0.0};
+  const size_t per = (size_t)12 * vbh;
+  for (size_t i = blockIdx.x * (size_t)RT + threadIdx.x; i < rg.n; i += (size_t)RB * RT) {
+    const size_t j = rg.beg + i;
+    double2 xx = x[j];
+    if ((j % per) / vbh >= 6) {
+      xx.x = -xx.x;
+      xx.y = -xx.y;
+      x[j] = xx;
+    }
+    v[0] += xx.x * xx.x + xx.y * xx.y;
+  }
+  block_store<1>(v, part);
+}
+
+int la_mulg5_norm2(Ctx &c, void *x, int par, double *res) {
+  if (ensure_red(c)) return -1;
+  Range rg = range(c, 64, par);
+  k_mulg5_norm2<<<RB, RT, 0, c.stream>>>(rg, (double2 *)x, c.g.vbh, c.red);
+  k_finish<1><<<1, 32, 0, c.stream>>>(c.red, RB, c.red_out);
+  return finish(c, 1, res);
+}
+
 int la_unorm(Ctx &c, int prec, const void *x, int par, double *res) {
   if (ensure_red(c)) return -1;
   int c0 = par == PAR_ODD ? c.g.nbl : 0;

@@ -106,6 +106,10 @@ _SIGS = {
                             C.c_void_p]),
     "b200_dev_tmcg": (C.c_double, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
+    "tmcgm": (None, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                     C.c_void_p]),
+    "b200_dev_tmcgm": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
     "export_cnfg": (None, [C.c_char_p]),
     "import_cnfg": (None, [C.c_char_p, C.c_int]),
     "export_sfld": (None, [C.c_char_p, C.c_int, C.c_void_p]),
@@ -421,6 +425,27 @@ def sap_gcr(nkv, nmx, istop, res, mu, eta):
     if rho < 0:
         raise B200Error(_err_after())
     return psi, rho, ifail.value, status.value
+
+
+def tmcgm(nmx, istop, res, mu, eta, psi0=None):
+    """tmcgm on reference-layout arrays: res and mu are sequences of equal
+    length; returns (list of solutions, ifail, status).  Only the even sites
+    of the solutions are computed; their odd sites are those of psi0."""
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    res = np.ascontiguousarray(res, dtype=np.float64)
+    nmu = len(mu)
+    eta = np.ascontiguousarray(eta, dtype=np.float64)
+    psi = [np.zeros_like(eta) if psi0 is None else np.array(psi0[k], dtype=np.float64, copy=True)
+           for k in range(nmu)]
+    ptrs = (C.c_void_p * max(nmu, 1))(*[_ptr(p) for p in psi])
+    ifail = C.c_int(0)
+    status = C.c_int(0)
+    lib().b200_clear_error()
+    lib().tmcgm(nmx, istop, _ptr(res), nmu, _ptr(mu), _ptr(eta), ptrs, C.byref(ifail), C.byref(status))
+    err = _err_after()
+    if err:
+        raise B200Error(err)
+    return psi, ifail.value, status.value
 
 
 def sap_ref(mu, isolv, nmr, psi, rho):

@@ -659,3 +659,28 @@ double ref_tmcg(int eo, int nmx, int istop, double res, double mu, const double 
    release_wsd();
    return rho;
 }
+
+
+/* ----------------------------------------------------------------- tmcgm */
+/* tmcgm (modules/forces/tmcgm.c:100) on copies of eta and of the nmu
+ * solution fields psi[k] (psi: nmu consecutive fields) */
+void ref_tmcgm(int nmx, int istop, const double *res, int nmu, const double *mu, const double *eta, double *psi,
+               int *ifail, int *status)
+{
+   ENTER();
+   int k;
+   spinor_dble **wsd, *ps[64];
+   need_ws(40, 2 * nmu + 8);
+   wsd = reserve_wsd(1 + nmu);
+   memcpy(wsd[0], eta, VOLUME * sizeof(spinor_dble));
+   for (k = 0; k < nmu; k++)
+   {
+      ps[k] = wsd[1 + k];
+      memcpy(ps[k], psi + (size_t)k * VOLUME * 24, VOLUME * sizeof(spinor_dble));
+   }
+   ifail[0] = 0;
+   tmcgm(nmx, istop, (double *)res, nmu, (double *)mu, wsd[0], ps, ifail, status);
+   for (k = 0; k < nmu; k++)
+      memcpy(psi + (size_t)k * VOLUME * 24, ps[k], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+}

@@ -335,3 +335,20 @@ class RefLib:
         rho = self.lib.ref_tmcg(1 if eo else 0, nmx, istop, res, mu, self._p(eta), self._p(psi), C.byref(ifail),
                                 C.byref(status))
         return psi, rho, ifail.value, status.value
+
+    def tmcgm(self, nmx, istop, res, mu, eta, psi0=None):
+        """tmcgm for len(mu) <= 64 shifts; returns (solutions, ifail, status)"""
+        eta = np.ascontiguousarray(eta, dtype=np.float64)
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        res = np.ascontiguousarray(res, dtype=np.float64)
+        nmu = len(mu)
+        assert nmu <= 64
+        psi = np.zeros((nmu, eta.size)) if psi0 is None else np.array(psi0, dtype=np.float64, copy=True)
+        ifail = C.c_int(0)
+        status = C.c_int(0)
+        self.lib.ref_tmcgm.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p]
+        self.lib.ref_tmcgm.restype = None
+        self.lib.ref_tmcgm(nmx, istop, self._p(res), nmu, self._p(mu), self._p(eta), self._p(psi), C.byref(ifail),
+                           C.byref(status))
+        return [psi[k] for k in range(nmu)], ifail.value, status.value
