@@ -544,7 +544,8 @@ def run_b200(args, d):
             "config": {"workload": WORKLOAD, "lattice": list(L), "block": list(BS), "global_batch": 1,
                        "parallelism": "replicas%d" % d.world if d.world > 1 else "single",
                        "l2": "inputs larger than L2 (3.2 GB per application), no flush"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "roofline": {"bound": "hbm", "kernel": "dirac_staged_kernel<OP_SW|OP_HOP, all sites> (Dw_dble, SW staged)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_launch": bytes_step},
             "e2e": e2e,

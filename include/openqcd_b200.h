@@ -190,6 +190,12 @@ int b200_profiler(int on);
  * links as their first two rows and rebuilds the third (no reference
  * counterpart; 2/3 of the link bytes, results equal to FP32 rounding). */
 int b200_set_sap_link12(int on);
+/* mode != 0 (default): the FP64 operators with an SW term (all but
+ * Dwoe_dble and Dweo_dble) stage each tile's SW matrices in shared memory
+ * with bulk asynchronous copies; 0 reads them directly.  Same arithmetic,
+ * identical results.  Returns the previous mode (no reference
+ * counterpart). */
+int b200_set_dw_staged(int mode);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32, 16, or 12 for the 12-real links): index,
  * threads per block, time of one cycle's block sweeps in ms. */

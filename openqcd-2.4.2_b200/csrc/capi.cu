@@ -136,7 +136,15 @@ int b200_memcpy(void *dst, const void *src, size_t bytes) {
   return cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) == cudaSuccess ? 0 : fail("memcpy failed");
 }
 void b200_set_fatal(int on) { g_fatal = on != 0; }
-int b200_sync(void) { return cudaStreamSynchronize(ctx().stream) == cudaSuccess ? 0 : fail("CUDA error"); }
+int b200_sync(void) {
+  Ctx &c = ctx();
+  if (cudaStreamSynchronize(c.stream) != cudaSuccess) return fail("CUDA error");
+  if (c.h_kerr && *(volatile int *)c.h_kerr) {
+    *(volatile int *)c.h_kerr = 0;
+    return fail("a kernel gave up waiting for its bulk copies (results invalid)");
+  }
+  return 0;
+}
 int b200_volume(void) { return ctx().ready ? ctx().g.vol : 0; }
 
 int b200_set_device(int dev) {
@@ -151,6 +159,12 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   Ctx &c = ctx();
   if (!c.stream && cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
     return fail("no CUDA device available");
+  if (!c.h_kerr) {
+    if (cudaHostAlloc((void **)&c.h_kerr, sizeof(int), cudaHostAllocMapped) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&c.d_kerr, c.h_kerr, 0) != cudaSuccess)
+      return fail("no page-locked memory for the kernel error flag");
+    *(volatile int *)c.h_kerr = 0;
+  }
   // a new geometry invalidates every resident field
   void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage,
                   c.u16, c.sw16, c.sw16_inv, c.u12};
@@ -317,6 +331,13 @@ int b200_set_sap_prec(int bits) {
 int b200_set_sap_link12(int on) {
   ctx().sap_link12 = on != 0;
   return 0;
+}
+
+int b200_set_dw_staged(int mode) {
+  Ctx &c = ctx();
+  const int prev = c.dw_staged;
+  c.dw_staged = mode != 0;
+  return prev;
 }
 
 int b200_sap_tuning(int prec, int *variant, int *threads, float *ms) {

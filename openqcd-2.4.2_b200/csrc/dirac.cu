@@ -20,10 +20,77 @@
 // It is a pure gather: each thread reads the spinors of its 8 neighbours and
 // the 8 links that touch its site, and writes only its own site.
 #include "lib.h"
+#include "tma.cuh"
 
 namespace qcd {
 
 enum { OP_SW = 1, OP_HOP = 2, OP_HOPSUB = 4, OP_INV = 8, OP_ACC = 16 };
+
+// L2 residency: the SW matrices are read once per application and the
+// output is not read back by the launch, so both go through L2 with the
+// evict-first policy (ld.global.cs / st.global.cs, or a cache hint on the
+// bulk copies).  The neighbour spinors and links, read by several CTAs at
+// different times (block faces), then stay in L2 longer.
+#ifndef DW_NO_HINTS
+#define DW_HINTS 1
+#else
+#define DW_HINTS 0
+#endif
+
+__device__ __forceinline__ void load_pauli_cs(const double2 *base, int chunk, int half, int s, int vbh,
+                                              double u[36]) {
+  const double2 *p = base + ((size_t)chunk * 36 + 18 * half) * vbh + s;
+#pragma unroll
+  for (int k = 0; k < 18; k++) {
+    const double2 v = DW_HINTS ? __ldcs(p + (size_t)k * vbh) : __ldg(p + (size_t)k * vbh);
+    u[2 * k] = v.x;
+    u[2 * k + 1] = v.y;
+  }
+}
+__device__ __forceinline__ spinor<double> apply_sw_site_cs(const void *sw, int chunk, int s, int vbh, double mu,
+                                                           const spinor<double> &in) {
+  spinor<double> out;
+  double u[36];
+  cpx<double> w[6], r[6];
+#pragma unroll
+  for (int half = 0; half < 2; half++) {
+    load_pauli_cs((const double2 *)sw, chunk, half, s, vbh, u);
+    weyl_get(in, half, w);
+    mul_pauli<double>(half == 0 ? mu : -mu, u, w, r);
+    weyl_put(out, half, r);
+  }
+  return out;
+}
+
+// FP64: SW read and output written with the evict-first policy; FP32 as is
+template <typename R> struct DwIO {
+  __device__ __forceinline__ static spinor<R> sw(const void *m, int chunk, int s, int vbh, R mu, const spinor<R> &in) {
+    return apply_sw_site<R>(m, chunk, s, vbh, mu, in);
+  }
+  __device__ __forceinline__ static void store(void *r, int chunk, int s, int vbh, const spinor<R> &v) {
+    Store<R>::store_spinor(r, chunk, s, vbh, v);
+  }
+};
+__device__ __forceinline__ void store_spinor_cs(double2 *base, int chunk, int s, int vbh, const spinor<double> &r);
+template <> struct DwIO<double> {
+  __device__ __forceinline__ static spinor<double> sw(const void *m, int chunk, int s, int vbh, double mu,
+                                                      const spinor<double> &in) {
+    return apply_sw_site_cs(m, chunk, s, vbh, mu, in);
+  }
+  __device__ __forceinline__ static void store(void *r, int chunk, int s, int vbh, const spinor<double> &v) {
+    store_spinor_cs((double2 *)r, chunk, s, vbh, v);
+  }
+};
+
+__device__ __forceinline__ void store_spinor_cs(double2 *base, int chunk, int s, int vbh, const spinor<double> &r) {
+  double2 *p = base + (size_t)chunk * 12 * vbh + s;
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    const double2 v = make_double2(r.c[k / 3].c[k % 3].re, r.c[k / 3].c[k % 3].im);
+    if (DW_HINTS) __stcs(p + (size_t)k * vbh, v);
+    else p[(size_t)k * vbh] = v;
+  }
+}
 
 // RHALF / THALF = 1: the output r / the hop field t is a half-field holding
 // only the odd chunks (chunk index counted from the first odd chunk).
@@ -69,7 +136,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
   spinor<R> acc;
   if (OPS & OP_SW) {
     spinor<R> in = Store<R>::load_spinor(s, chunk, si, g.vbh);
-    acc = apply_sw_site<R>(sw, chunk, si, g.vbh, p == 0 ? mu_e : mu_o, in);
+    acc = DwIO<R>::sw(sw, chunk, si, g.vbh, p == 0 ? mu_e : mu_o, in);
   } else {
     szero(acc);
   }
@@ -94,7 +161,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
       }
     }
     sscale<R>(h, (R)-0.5);
-    if (OPS & OP_INV) h = apply_sw_site<R>(swinv, chunk, si, g.vbh, (R)0, h);
+    if (OPS & OP_INV) h = DwIO<R>::sw(swinv, chunk, si, g.vbh, (R)0, h);
     if (OPS & OP_HOP) sadd(acc, h);
     else ssub(acc, h);
   }
@@ -105,10 +172,155 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
     sadd(old, acc);
     Store<R>::store_spinor(r, rchunk, si, g.vbh, old);
   } else {
-    Store<R>::store_spinor(r, rchunk, si, g.vbh, acc);
+    DwIO<R>::store(r, rchunk, si, g.vbh, acc);
   }
 }
 
+
+// ------------------------------------------------------------------------
+// FP64 operator with the SW matrices staged in shared memory.  A CTA owns a
+// tile of DWT_TS consecutive sites of one chunk.  At its start one warp
+// issues bulk asynchronous copies (cp.async.bulk with the evict-first L2
+// policy, completed on an mbarrier; no multicast) of the tile's 36 SW
+// planes; they are needed only after the hop loop, so the copy overlaps it
+// and the SW bytes (43 % of the reads) leave the warps' load chains.
+// Spinors and links are read from global memory, where the compiler hoists
+// the loads of later directions.  Same arithmetic as dirac_kernel
+// (operators without OP_ACC).
+//
+// Tried and dropped (B200, 32^3x64, 4^4 blocks): staging the forward links
+// too, in two rotating stages (0.81 ms against 0.72 ms direct: the barrier
+// per direction stops the load hoisting); staging the block's other-parity
+// spinor chunk so that in-block hops read shared memory (0.79 ms: the copy's
+// latency at the CTA start is exposed and the L2 traffic hardly fell, L1
+// already caught those reads); three CTAs per SM (168 registers, 0.91 ms).
+constexpr int DWT_TS = 128;
+#ifndef DWT_MINB
+#define DWT_MINB 2
+#endif
+constexpr size_t DWT_SMEM = (size_t)36 * DWT_TS * sizeof(double2);     // 73,728 B
+
+__device__ __forceinline__ spinor<double> apply_sw_smem(const double2 *sm, int t, double mu,
+                                                        const spinor<double> &in) {
+  spinor<double> out;
+  double u[36];
+  cpx<double> w[6], r[6];
+#pragma unroll
+  for (int half = 0; half < 2; half++) {
+#pragma unroll
+    for (int k = 0; k < 18; k++) {
+      const double2 v = sm[(18 * half + k) * DWT_TS + t];
+      u[2 * k] = v.x;
+      u[2 * k + 1] = v.y;
+    }
+    weyl_get(in, half, w);
+    mul_pauli<double>(half == 0 ? mu : -mu, u, w, r);
+    weyl_put(out, half, r);
+  }
+  return out;
+}
+
+template <int OPS, int PAR>
+__global__ void __launch_bounds__(DWT_TS, DWT_MINB)
+    dirac_staged_kernel(Geom g, const double2 *__restrict__ s, const double2 *__restrict__ t, double2 *r,
+                        const double2 *__restrict__ u, const double2 *__restrict__ swm, double mu_e, double mu_o,
+                        const int *__restrict__ sched, int tpc, int *err) {
+  extern __shared__ __align__(128) unsigned char dwt_smem[];
+  double2 *sw_s = (double2 *)dwt_smem;          // [36][DWT_TS]
+  __shared__ uint64_t bar[1];
+  constexpr bool HAS_SW = (OPS & (OP_SW | OP_INV)) != 0;
+  const int tid = threadIdx.x;
+  int p, blk, tile;
+  if (PAR == 2) {
+    const int b = blockIdx.x / (2 * tpc);
+    const int rr = blockIdx.x - b * 2 * tpc;
+    p = rr / tpc;
+    tile = rr - p * tpc;
+    blk = sched ? __ldg(sched + b) : b;
+  } else {
+    p = PAR;
+    blk = blockIdx.x / tpc;
+    tile = blockIdx.x - blk * tpc;
+    if (sched) blk = __ldg(sched + blk);
+  }
+  const int si0 = tile * DWT_TS;
+  const int nsite = min(DWT_TS, g.vbh - si0);
+  const int chunk = p * g.nbl + blk;
+  const unsigned pbytes = (unsigned)nsite * 16u;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (HAS_SW && tid < 32) {
+    if (tid == 0) mbar_expect_tx(&bar[0], 36 * pbytes);
+    __syncwarp();
+    const uint64_t pol = l2_policy_evict_first();
+    for (int k = tid; k < 36; k += 32) {
+      const double2 *src = swm + ((size_t)chunk * 36 + k) * g.vbh + si0;
+      if (DW_HINTS) bulk_g2s_hint(sw_s + k * DWT_TS, src, pbytes, &bar[0], pol);
+      else bulk_g2s(sw_s + k * DWT_TS, src, pbytes, &bar[0]);
+    }
+  }
+  const bool active = tid < nsite;
+  const int si = si0 + tid;
+  bool ok = true;
+  if (active) {
+    Site x;
+    site_decode(g, p, blk, si, x);
+    spinor<double> h;
+    szero(h);
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      int c2, s2;
+      site_nbr(g, x, mu, +1, c2, s2);
+      const spinor<double> sp = Store<double>::load_spinor(t, c2, s2, g.vbh);
+      const su3<double> uu = Store<double>::load_link(u, chunk, mu, si, g.vbh);
+      hop_fwd<double>(mu, uu, sp, h);
+      site_nbr(g, x, mu, -1, c2, s2);
+      const spinor<double> sm = Store<double>::load_spinor(t, c2, s2, g.vbh);
+      const su3<double> ub = Store<double>::load_link(u, c2, mu, s2, g.vbh);
+      hop_bwd<double>(mu, ub, sm, h);
+    }
+    sscale<double>(h, -0.5);
+    const double mux = p == 0 ? mu_e : mu_o;
+    if (OPS & OP_INV) {
+      ok &= mbar_wait_st(&bar[0], 0u, err);
+      h = apply_sw_smem(sw_s, tid, 0.0, h);
+    }
+    spinor<double> acc;
+    if (OPS & OP_SW) {
+      const spinor<double> in = Store<double>::load_spinor(s, chunk, si, g.vbh);
+      ok &= mbar_wait_st(&bar[0], 0u, err);
+      acc = apply_sw_smem(sw_s, tid, mux, in);
+    } else {
+      szero(acc);
+    }
+    if (OPS & OP_HOP) sadd(acc, h);
+    else if (OPS & OP_HOPSUB) ssub(acc, h);
+    store_spinor_cs(r, chunk, si, g.vbh, acc);
+  }
+  // a thread whose wait gave up waits once more (bounded) for the copies
+  // still addressed to this CTA's shared memory before the CTA exits (thread
+  // 0 always has a site and waits on the barrier when it was armed)
+  if (!ok && HAS_SW) mbar_wait_st(&bar[0], 0u, err);
+}
+
+template <int OPS, int PAR>
+static void launch_staged(const Ctx &c, const void *s, const void *t, void *r, double mu_e, double mu_o,
+                          cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(dirac_staged_kernel<OPS, PAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DWT_SMEM);
+    attr = true;
+  }
+  const int tpc = (c.g.vbh + DWT_TS - 1) / DWT_TS;
+  const int nchunk = PAR == 2 ? 2 * c.g.nbl : c.g.nbl;
+  const void *swm = (OPS & OP_INV) ? (const void *)c.swd_inv : (const void *)c.swd;
+  dirac_staged_kernel<OPS, PAR><<<nchunk * tpc, DWT_TS, DWT_SMEM, st>>>(
+      c.g, (const double2 *)s, (const double2 *)t, (double2 *)r, (const double2 *)c.ud, (const double2 *)swm, mu_e,
+      mu_o, c.sched, tpc, c.d_kerr);
+}
 
 template <typename R, int OPS, int PAR>
 static void launch(const Ctx &c, const void *s, const void *t, void *r, R mu_e, R mu_o, bool inv,
@@ -117,10 +329,14 @@ static void launch(const Ctx &c, const void *s, const void *t, void *r, R mu_e, 
   const void *sw = sizeof(R) == 8 ? (const void *)c.swd : (const void *)c.sw32;
   const void *swinv = sizeof(R) == 8 ? (const void *)c.swd_inv : (const void *)c.sw32_inv;
   (void)inv;
+  if (sizeof(R) == 8 && !(OPS & OP_ACC) && (OPS & (OP_SW | OP_INV)) && c.dw_staged && c.d_kerr) {
+    launch_staged<OPS, PAR>(c, s, t, r, (double)mu_e, (double)mu_o, st);
+    return;
+  }
   int n = PAR == 2 ? c.g.vol : c.g.volh;
   int threads = 128;
   dirac_kernel<R, OPS, PAR><<<(n + threads - 1) / threads, threads, 0, st>>>(c.g, s, t, r, u, sw, swinv, mu_e, mu_o,
-                                                                           PAR == 2 ? c.sched : nullptr);
+                                                                           c.sched);
 }
 
 // op: 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo, 5 Dwhat.  tmp: a scratch field

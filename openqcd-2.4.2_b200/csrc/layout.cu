@@ -11,7 +11,9 @@
 // every device site to those positions; the conversion kernels are plain
 // gathers.
 #include "lib.h"
+#include <algorithm>
 #include <cstring>
+#include <utility>
 
 namespace qcd {
 
@@ -35,12 +37,26 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
   g.bstr[3] = 1; g.bstr[2] = g.nb[3]; g.bstr[1] = g.nb[3] * g.nb[2]; g.bstr[0] = g.nb[3] * g.nb[2] * g.nb[1];
 
   std::vector<int> bco(g.nbl), lco(g.vb), sch(g.nbl);
+  std::vector<std::pair<uint64_t, int>> key(g.nbl);
   for (int b = 0; b < g.nbl; b++) {
     int n[4], r = b;
     for (int mu = 3; mu >= 0; mu--) { n[mu] = r % g.nb[mu]; r /= g.nb[mu]; }
     bco[b] = pack4(n);
-    sch[b] = b;
+    // Morton key: the bits of the four block coordinates interleaved
+    uint64_t k = 0;
+    for (int bit = 0; bit < 8; bit++)
+      for (int mu = 0; mu < 4; mu++) k |= (uint64_t)((n[mu] >> bit) & 1) << (4 * bit + 3 - mu);
+    key[b] = {k, b};
   }
+  // Traversal order of the full-lattice operator kernels: blocks sorted by
+  // Morton key, so that the neighbours of a block in every direction are
+  // visited a short time before or after it and their face data are still
+  // in L2 (in lexicographic order the neighbours along x0 are
+  // nb1*nb2*nb3 blocks away, more than the L2 holds on large lattices).
+#ifndef BLOCK_ORDER_LEX
+  std::sort(key.begin(), key.end());
+#endif
+  for (int b = 0; b < g.nbl; b++) sch[b] = key[b].second;
   for (int l = 0; l < g.vb; l++) {
     int y[4], r = l;
     for (int mu = 3; mu >= 0; mu--) { y[mu] = r % bs[mu]; r /= bs[mu]; }

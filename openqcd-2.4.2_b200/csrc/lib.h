@@ -113,6 +113,12 @@ struct Ctx {
   double *h_red = nullptr;      // pinned host mirror of red_out
   int red_blocks = 0;
   cudaStream_t stream = nullptr;
+  // error flag of bounded waits in the operator kernels: page-locked host
+  // memory mapped into the device (h_kerr host view, d_kerr device view)
+  int *h_kerr = nullptr, *d_kerr = nullptr;
+  // FP64 operators with an SW term: SW matrices staged in shared memory by
+  // bulk copies (1) or read directly (0)
+  int dw_staged = 1;
   int nthread = 1;              // the caller's NTHREAD, for icom & 0x2 in the BLAS drop-ins
   void *fstage[3] = {nullptr, nullptr, nullptr};   // staging of host operands
   size_t fstage_bytes[3] = {0, 0, 0};

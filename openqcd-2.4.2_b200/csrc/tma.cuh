@@ -36,6 +36,23 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
       : "memory");
 }
 
+// L2 policy for data read once (evict first), for the cache-hint form below
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+
+// bulk_g2s with an L2 cache-eviction policy
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -52,6 +69,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *e
   for (int it = 0; it < (1 << 22); it++)
     if (mbar_try_wait(bar, parity)) return true;
   atomicOr(err, 1);
+  return false;
+}
+
+// the same with the error recorded by a plain store (for a flag in mapped
+// host memory, where device atomics are not guaranteed)
+__device__ __forceinline__ bool mbar_wait_st(uint64_t *bar, unsigned parity, int *err) {
+  for (int it = 0; it < (1 << 22); it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  *(volatile int *)err = 1;
   return false;
 }
 

@@ -100,6 +100,7 @@ _SIGS = {
     "b200_clear_error": (None, []),
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
     "b200_set_sap_link12": (C.c_int, [C.c_int]),
+    "b200_set_dw_staged": (C.c_int, [C.c_int]),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_void_p]),
     "tmcgeo": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -249,6 +250,12 @@ def set_sap_prec(bits):
 
 def set_sap_link12(on):
     return check(lib().b200_set_sap_link12(1 if on else 0))
+
+
+def set_dw_staged(mode):
+    """FP64 operators: 1 SW matrices staged in shared memory (default), 0
+    read directly; returns the previous mode"""
+    return lib().b200_set_dw_staged(int(mode))
 
 
 def sap_tuning(prec):
