@@ -261,7 +261,7 @@ def solver_c3(qb, profile=False, lattice=None):
     m0 = -0.05, csw = 1.7, bs = 6^4, Ns = 28, Gaussian sources, FP64
     residual 1e-10): the plain GPU sap_gcr (one right-hand side, FP32 SAP
     with nkv = 16, ncy = 5) against the chosen solver (deflated SAP+GCR on
-    four right-hand sides at once, nkv = 8, ncy = 2).  Seconds per
+    four right-hand sides at once, nkv = 8, nmr = 3, ncy = 2).  Seconds per
     right-hand side of the solves; the subspace generation is reported
     apart (it is done once per gauge field)."""
     L, BSx, NS = (lattice or SOLVER_L), SOLVER_BS, 28
@@ -292,7 +292,7 @@ def solver_c3(qb, profile=False, lattice=None):
     qb.lib().b200_sync()
     t_setup = time.time() - t0
     nr = 4
-    qb.set_sap_parms(BSx, 1, 4, 2)
+    qb.set_sap_parms(BSx, 1, 3, 2)
     E = [eta] + [qb.DevField(64).random(1.0, 100 + i) for i in range(nr - 1)]
     P = [qb.DevField(64) for _ in range(nr)]
     qb.dev_gcr_batch(8, 256, 0, 1e-10, [0.0] * nr, E, P, dfl=True)      # warm-up
@@ -309,7 +309,7 @@ def solver_c3(qb, profile=False, lattice=None):
                      "true_residual": max(true_residual(qb, 0.0, E[i], P[i]) for i in range(nr)),
                      "setup_s": t_setup, "setup_ifail": f,
                      "solver": "dfl_sap_gcr batched over 4 right-hand sides: Ns=28 deflation (subspace by "
-                               "dfl_modes, ninv=10), nkv=8, isolv=1, nmr=4, ncy=2, FP32 SAP/Krylov, FP64 "
+                               "dfl_modes, ninv=10), nkv=8, isolv=1, nmr=3, ncy=2, FP32 SAP/Krylov, FP64 "
                                "residual, multi-RHS restriction/prolongation/little solver"}
     out["speedup_per_rhs"] = t_plain / t_chosen
     for fld in E + P:
