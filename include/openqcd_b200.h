@@ -73,6 +73,9 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt);
  * set_sw_parms (:920, m0), set_tm_parms (:963, eoflg) and set_sap_parms
  * (modules/flags/sap_parms.c:112). */
 int b200_set_lat_parms(double csw);
+/* the SW type isw of set_lat_parms (lat_parms.c:216): 0 traditional, 1
+ * exponential form c exp{[csw/(4+m0)] (i/4) sigma F} (sw_term.c:46-49) */
+int b200_set_sw_type(int isw);
 int b200_set_bc_parms(int type);
 int b200_set_sw_parms(double m0);
 int b200_set_tm_parms(int eoflg);

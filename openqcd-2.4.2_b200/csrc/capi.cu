@@ -187,6 +187,12 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
 }
 
 int b200_set_lat_parms(double csw) { ctx().csw = csw; ctx().have_sw = false; return 0; }
+int b200_set_sw_type(int isw) {
+  if (isw < 0 || isw > 1) return fail("set_lat_parms: the SW type isw must be either 0 or 1");
+  ctx().isw = isw;
+  ctx().have_sw = false;
+  return 0;
+}
 int b200_set_bc_parms(int type) {
   if (type != 3) return fail("set_bc_parms: only boundary condition type 3 is supported");
   ctx().bc = type;

@@ -76,6 +76,7 @@ struct Ctx {
   // parameters
   double csw = 0.0, m0 = 0.0;
   int bc = 3, eoflg = 0;
+  int isw = 0;                  // SW term: 0 traditional, 1 exponential
   int isolv = 1, nmr = 4, ncy = 5;
   bool sap_set = false;
 
@@ -152,7 +153,7 @@ int pauli_from_ref(Ctx &c, const void *qsw, cudaStream_t st);                   
 int pauli_to_ref(const Ctx &c, int which, void *qsw, cudaStream_t st);
 
 // sw.cu
-int sw_refresh_derived(Ctx &c, cudaStream_t st);     // inverses + FP32 copies from swd
+int sw_refresh_derived(Ctx &c, cudaStream_t st, bool inv_given = false);   // inverses + FP32 copies from swd
 int sw_compute(Ctx &c, cudaStream_t st);             // SW term from the links (sw_term)
 int links_refresh_f32(Ctx &c, cudaStream_t st);      // u32 from ud
 int apply_sw_ref_layout(int prec, int vol, double mu, const void *m, const void *s, void *r, cudaStream_t st);

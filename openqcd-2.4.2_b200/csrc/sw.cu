@@ -2,6 +2,8 @@
 // inversion with the reference's safety criterion, FP32 copies, and the
 // site-local apply_sw/apply_swinv on arrays in the reference's storage order.
 #include "lib.h"
+#include <cfloat>
+#include <cmath>
 
 namespace qcd {
 
@@ -87,6 +89,9 @@ __device__ int inv_pauli(double mu, const double u[36], double out[36]) {
 }
 
 // swd -> swd_inv (all sites, mu = 0), sw32, sw32_inv
+// INV = false: swd_inv already holds the inverses (exponential SW term),
+// only the FP32 copies are made
+template <bool INV>
 __global__ void k_sw_derive(Geom g, const double2 *__restrict__ swd, double2 *swd_inv, float4 *sw32,
                             float4 *sw32_inv, int *fail) {
   int d = blockIdx.x * blockDim.x + threadIdx.x;
@@ -97,9 +102,17 @@ __global__ void k_sw_derive(Geom g, const double2 *__restrict__ swd, double2 *sw
     double u[36], v[36];
     const double2 *src = swd + ((size_t)chunk * 36 + 18 * half) * g.vbh + s;
     for (int k = 0; k < 18; k++) { double2 x = src[(size_t)k * g.vbh]; u[2 * k] = x.x; u[2 * k + 1] = x.y; }
-    bad |= inv_pauli(0.0, u, v);
     double2 *dst = swd_inv + ((size_t)chunk * 36 + 18 * half) * g.vbh + s;
-    for (int k = 0; k < 18; k++) dst[(size_t)k * g.vbh] = make_double2(v[2 * k], v[2 * k + 1]);
+    if (INV) {
+      bad |= inv_pauli(0.0, u, v);
+      for (int k = 0; k < 18; k++) dst[(size_t)k * g.vbh] = make_double2(v[2 * k], v[2 * k + 1]);
+    } else {
+      for (int k = 0; k < 18; k++) {
+        const double2 x = dst[(size_t)k * g.vbh];
+        v[2 * k] = x.x;
+        v[2 * k + 1] = x.y;
+      }
+    }
     float4 *d32 = sw32 + ((size_t)chunk * 18 + 9 * half) * g.vbh + s;
     float4 *i32 = sw32_inv + ((size_t)chunk * 18 + 9 * half) * g.vbh + s;
     for (int j = 0; j < 9; j++) {
@@ -120,13 +133,16 @@ static int alloc_sw(Ctx &c) {
   return 0;
 }
 
-int sw_refresh_derived(Ctx &c, cudaStream_t st) {
+int sw_refresh_derived(Ctx &c, cudaStream_t st, bool inv_given) {
   if (alloc_sw(c)) return -1;
   int *dfail;
   if (cudaMallocAsync(&dfail, sizeof(int), st) != cudaSuccess) return fail("allocation failed");
   cudaMemsetAsync(dfail, 0, sizeof(int), st);
   int t = 128;
-  k_sw_derive<<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.swd, c.swd_inv, c.sw32, c.sw32_inv, dfail);
+  if (inv_given)
+    k_sw_derive<false><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.swd, c.swd_inv, c.sw32, c.sw32_inv, dfail);
+  else
+    k_sw_derive<true><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.swd, c.swd_inv, c.sw32, c.sw32_inv, dfail);
   int hf = 0;
   cudaMemcpyAsync(&hf, dfail, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(dfail, st);
@@ -282,7 +298,141 @@ __device__ __forceinline__ void apply_pmap(const PMap *m, int n, const double X[
 // :247-345 set_swd, periodic case): with c2 = -csw/2,
 //   upper = c2*(F23-F01, F31-F02, F12-F03) mapped by pmap1/2/3, + (4+m0) on the diagonal
 //   lower = c2*(F23+F01, F31+F02, F12+F03) likewise.
-__global__ void k_sw_term(Geom g, const double2 *__restrict__ ud, double2 *swd, double c1, double c2) {
+// ------------------------------------------------ exponential SW term
+// isw = 1 (modules/sw_term/sw_term.c:46-49, swexp.c): the SW matrices are
+// c exp(A) with A = c2/c * (clover term) traceless Hermitian, and their
+// inverses (1/c) exp(-A).  exp(A) is its Taylor series to order n (the order
+// of sw_order(), sw_term.c:95) reduced to a polynomial of degree 5 in A by
+// the characteristic polynomial A^6 = -(p4 A^4 + p3 A^3 + p2 A^2 + p1 A + p0)
+// (Cayley-Hamilton; A traceless, so no A^5 term), the p_k from the power
+// sums s_k = tr A^k by Newton's identities; the series is folded in from its
+// highest term down (Horner).
+struct ExpCoef {
+  int n;
+  double c[100];   // 1/k!, k = 0..n
+};
+
+typedef double2 cmat6[6][6];
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ void cmat_mul(const cmat6 a, const cmat6 b, cmat6 out) {
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      double2 z = make_double2(0.0, 0.0);
+      for (int k = 0; k < 6; k++) {
+        const double2 t = cmul(a[i][k], b[k][j]);
+        z.x += t.x;
+        z.y += t.y;
+      }
+      out[i][j] = z;
+    }
+}
+
+// r * sum_k q_k A^k from A, A^2, A^3: (q0 + q1 A + q2 A^2) + (q3 + q4 A + q5 A^2) A^3,
+// packed as a Pauli matrix (the result is Hermitian)
+__device__ void exp_pack(const cmat6 A, const cmat6 A2, const cmat6 A3, const double q[6], double r, double out[36]) {
+  cmat6 M;
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 6; j++) {
+      const double d = i == j ? q[3] : 0.0;
+      M[i][j] = make_double2(d + q[4] * A[i][j].x + q[5] * A2[i][j].x, q[4] * A[i][j].y + q[5] * A2[i][j].y);
+    }
+  int k = 6;
+  for (int i = 0; i < 6; i++)
+    for (int j = i; j < 6; j++) {
+      double2 z = make_double2((i == j ? q[0] : 0.0) + q[1] * A[i][j].x + q[2] * A2[i][j].x,
+                               q[1] * A[i][j].y + q[2] * A2[i][j].y);
+      for (int l = 0; l < 6; l++) {
+        const double2 t = cmul(M[i][l], A3[l][j]);
+        z.x += t.x;
+        z.y += t.y;
+      }
+      if (i == j) {
+        out[i] = r * z.x;
+      } else {
+        out[k] = r * z.x;
+        out[k + 1] = r * z.y;
+        k += 2;
+      }
+    }
+}
+
+// Taylor coefficients (sign = -1: of exp(-A)) folded to degree 5
+__device__ void exp_fold(const ExpCoef &ec, double sign, const double p[5], double q[6]) {
+  const int n = ec.n;
+  auto cs = [&](int k) { return (sign < 0.0 && (k & 1)) ? -ec.c[k] : ec.c[k]; };
+  if (n > 5) {
+    for (int j = 0; j < 6; j++) q[j] = cs(n - 5 + j);
+    for (int k = n - 6; k >= 0; k--) {
+      const double q5 = q[5];
+      q[5] = q[4];
+      q[4] = q[3] - q5 * p[4];
+      q[3] = q[2] - q5 * p[3];
+      q[2] = q[1] - q5 * p[2];
+      q[1] = q[0] - q5 * p[1];
+      q[0] = cs(k) - q5 * p[0];
+    }
+  } else {
+    for (int j = 0; j < 6; j++) q[j] = j <= n ? cs(j) : 0.0;
+  }
+}
+
+// u: the Pauli matrix of A; B = r exp(A), Binv = (1/r) exp(-A)
+__device__ void sw_exp_site(const double u[36], const ExpCoef &ec, double r, double B[36], double Binv[36]) {
+  cmat6 A, A2, A3;
+  int k = 6;
+  for (int i = 0; i < 6; i++) {
+    A[i][i] = make_double2(u[i], 0.0);
+    for (int j = i + 1; j < 6; j++) {
+      A[i][j] = make_double2(u[k], u[k + 1]);
+      A[j][i] = make_double2(u[k], -u[k + 1]);
+      k += 2;
+    }
+  }
+  cmat_mul(A, A, A2);
+  cmat_mul(A2, A, A3);
+  double s2 = 0.0, s3 = 0.0, s4 = 0.0, s5 = 0.0, s6 = 0.0;
+  for (int i = 0; i < 6; i++) {
+    s2 += A2[i][i].x;
+    s3 += A3[i][i].x;
+    for (int j = 0; j < 6; j++) {
+      s4 += A2[i][j].x * A2[i][j].x + A2[i][j].y * A2[i][j].y;   // tr A^4 = sum |(A^2)_ij|^2
+      s6 += A3[i][j].x * A3[i][j].x + A3[i][j].y * A3[i][j].y;   // tr A^6
+      s5 += cmul(A2[i][j], A3[j][i]).x;                          // tr A^5
+    }
+  }
+  double p[5];
+  p[4] = -0.5 * s2;
+  p[3] = -s3 / 3.0;
+  p[2] = (s2 * s2 - 2.0 * s4) / 8.0;
+  p[1] = (5.0 * s2 * s3 - 6.0 * s5) / 30.0;
+  p[0] = (8.0 * s3 * s3 - 24.0 * s6 + s2 * (18.0 * s4 - 3.0 * s2 * s2)) / 144.0;
+  double q[6];
+  exp_fold(ec, 1.0, p, q);
+  exp_pack(A, A2, A3, q, r, B);
+  exp_fold(ec, -1.0, p, q);
+  exp_pack(A, A2, A3, q, 1.0 / r, Binv);
+}
+
+// sw_order (sw_term.c:95-121): the Taylor order that reaches machine
+// precision for matrices with |A| <= 3 csw/(4+m0); -1 if none below 100
+static int sw_exp_order(double csw, double m0) {
+  const double c = 3.0 * std::fabs(csw / (4.0 + m0));
+  double a = c * std::exp(c), b = DBL_EPSILON;
+  for (int n = 1; n < 100; n++) {
+    a *= c;
+    b *= (double)(n + 1);
+    if (a < b) return n;
+  }
+  return -1;
+}
+
+template <bool ISW>
+__global__ void k_sw_term(Geom g, const double2 *__restrict__ ud, double2 *swd, double2 *swd_inv, double c1,
+                          double c2, ExpCoef ec) {
   int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= g.vol) return;
   int chunk = d / g.vbh, s = d - chunk * g.vbh;
@@ -304,9 +454,19 @@ __global__ void k_sw_term(Geom g, const double2 *__restrict__ ud, double2 *swd, 
     apply_pmap(pmap2, 17, X, u);
     for (int k = 0; k < 9; k++) X[k] = c2 * (F[5][k] + sg * F[2][k]);
     apply_pmap(pmap3, 18, X, u);
-    for (int k = 0; k < 6; k++) u[k] += c1;
     double2 *dst = swd + ((size_t)chunk * 36 + 18 * half) * g.vbh + s;
-    for (int k = 0; k < 18; k++) dst[(size_t)k * g.vbh] = make_double2(u[2 * k], u[2 * k + 1]);
+    if (ISW) {
+      double B[36], Bi[36];
+      sw_exp_site(u, ec, c1, B, Bi);
+      double2 *dsti = swd_inv + ((size_t)chunk * 36 + 18 * half) * g.vbh + s;
+      for (int k = 0; k < 18; k++) {
+        dst[(size_t)k * g.vbh] = make_double2(B[2 * k], B[2 * k + 1]);
+        dsti[(size_t)k * g.vbh] = make_double2(Bi[2 * k], Bi[2 * k + 1]);
+      }
+    } else {
+      for (int k = 0; k < 6; k++) u[k] += c1;
+      for (int k = 0; k < 18; k++) dst[(size_t)k * g.vbh] = make_double2(u[2 * k], u[2 * k + 1]);
+    }
   }
 }
 
@@ -315,9 +475,21 @@ int sw_compute(Ctx &c, cudaStream_t st) {
   if (c.bc != 3) return fail("sw_term: only periodic boundary conditions (type 3) are supported");
   if (alloc_sw(c)) return -1;
   int t = 64;
-  k_sw_term<<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ud, c.swd, 4.0 + c.m0, -0.5 * c.csw);
+  const double c1 = 4.0 + c.m0;
+  ExpCoef ec{};
+  if (c.isw) {
+    ec.n = sw_exp_order(c.csw, c.m0);
+    if (ec.n < 0) return fail("sw_order: SW parameters are out of range");
+    ec.c[0] = 1.0;
+    for (int k = 1; k <= ec.n; k++) ec.c[k] = ec.c[k - 1] / (double)k;
+    k_sw_term<true><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw / c1, ec);
+  } else {
+    k_sw_term<false><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw, ec);
+  }
   if (cudaGetLastError() != cudaSuccess) return fail("sw_term: launch failed");
-  return sw_refresh_derived(c, st);
+  // the exponential form brings its exact inverse (1/c) exp(-A): no
+  // numerical inversion, no failure (sw_term.c:312-320)
+  return sw_refresh_derived(c, st, c.isw != 0);
 }
 
 // Add dm to the diagonal of every Pauli matrix (a change of the bare mass
@@ -340,6 +512,15 @@ __global__ void k_sw_shift(Geom g, double2 *swd, double dm) {
 
 int sw_shift_mass(Ctx &c, double dm, cudaStream_t st) {
   if (!c.have_sw) return fail("no SW field on the device");
+  if (c.isw) {
+    // exponential form: the mass enters the exponent, so recompute from the
+    // links (as the reference's sw_term does after set_sw_parms)
+    const double m0 = c.m0;
+    c.m0 = m0 + dm;
+    const int rc = sw_compute(c, st);
+    c.m0 = m0;
+    return rc;
+  }
   int t = 128;
   k_sw_shift<<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.swd, dm);
   return sw_refresh_derived(c, st);

@@ -44,6 +44,7 @@ _SIGS = {
     "b200_set_device": (C.c_int, [C.c_int]),
     "b200_geometry": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_set_lat_parms": (C.c_int, [C.c_double]),
+    "b200_set_sw_type": (C.c_int, [C.c_int]),
     "b200_set_bc_parms": (C.c_int, [C.c_int]),
     "b200_set_sw_parms": (C.c_int, [C.c_double]),
     "b200_set_tm_parms": (C.c_int, [C.c_int]),
@@ -231,9 +232,10 @@ def geometry(L, bs, ipt=None):
     return check(lib().b200_geometry(_ptr(Lc), _ptr(bc), None if ip is None else _ptr(ip)))
 
 
-def set_parms(csw, m0, eoflg=0, bc=3):
+def set_parms(csw, m0, eoflg=0, bc=3, isw=0):
     L = lib()
     check(L.b200_set_lat_parms(csw))
+    check(L.b200_set_sw_type(isw))
     check(L.b200_set_bc_parms(bc))
     check(L.b200_set_sw_parms(m0))
     check(L.b200_set_tm_parms(eoflg))

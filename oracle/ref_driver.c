@@ -65,7 +65,7 @@ static void need_ws(int n, int nd)
 
 /* Geometry, parameter data base and random-number generator.  Must be called
  * once per process before any other ref_ function. */
-void ref_init(int bc, int seed, double csw, double m0, int eoflg)
+void ref_init_isw(int bc, int seed, double csw, double m0, int eoflg, int isw)
 {
    ENTER();
    int provided;
@@ -76,7 +76,7 @@ void ref_init(int bc, int seed, double csw, double m0, int eoflg)
       MPI_Init_thread(NULL, NULL, MPI_THREAD_FUNNELED, &provided);
       omp_set_num_threads(NTHREAD);
       omp_set_dynamic(0);
-      set_lat_parms(6.0, 1.0, 0, NULL, 0, csw);
+      set_lat_parms(6.0, 1.0, 0, NULL, isw, csw);
       set_bc_parms(bc, 1.0, 1.0, 1.0, 1.0, phi, phip, theta);
       start_ranlux(0, seed);
       geometry();
@@ -86,6 +86,11 @@ void ref_init(int bc, int seed, double csw, double m0, int eoflg)
    set_sw_parms(m0);
    set_tm_parms(eoflg);
    need_ws(40, 8);
+}
+
+void ref_init(int bc, int seed, double csw, double m0, int eoflg)
+{
+   ref_init_isw(bc, seed, csw, m0, eoflg, 0);
 }
 
 void ref_set_sw_parms(double m0) { ENTER(); set_sw_parms(m0); set_flags(ERASED_SWD); }

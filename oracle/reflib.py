@@ -53,13 +53,23 @@ def ensure_built(L, T=None, ref="/root/reference", portable=False):
 
 
 class RefLib:
-    def __init__(self, L, T=None, portable=False):
+    def __init__(self, L, T=None, portable=False, private=False):
+        """private: load a private copy of the library (its own parameter
+        data base, e.g. for a second SW type in the same process; the
+        reference's set_lat_parms can be called only once per instance)."""
         T = T or GEOMETRIES[tuple(L)]
         self.L = tuple(L)
         self.portable = portable
         path = lib_path(L, T, portable)
         if not os.path.exists(path):
             raise RuntimeError("reference oracle not built: " + path)
+        if private:
+            import shutil
+            import tempfile
+            d = tempfile.mkdtemp(prefix="refcopy")
+            cp = os.path.join(d, os.path.basename(path))
+            shutil.copyfile(path, cp)
+            path = cp
         self.lib = C.CDLL(path)
         l = self.lib
         l.ref_init.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int]
@@ -85,8 +95,9 @@ class RefLib:
     def _p(a):
         return a.ctypes.data_as(C.c_void_p)
 
-    def init(self, bc=3, seed=1234, csw=1.5, m0=0.0, eoflg=0):
-        self.lib.ref_init(bc, seed, csw, m0, eoflg)
+    def init(self, bc=3, seed=1234, csw=1.5, m0=0.0, eoflg=0, isw=0):
+        self.lib.ref_init_isw.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
+        self.lib.ref_init_isw(bc, seed, csw, m0, eoflg, isw)
 
     def set_sw_parms(self, m0):
         self.lib.ref_set_sw_parms(m0)
