@@ -199,6 +199,15 @@ int b200_set_sap_link12(int on);
  * identical results.  Returns the previous mode (no reference
  * counterpart). */
 int b200_set_dw_staged(int mode);
+/* on != 0 (default): the SAP preconditioner's launch sequence (ncy cycles of
+ * block solves and boundary updates with the copies around them) is
+ * captured as a CUDA graph on its first use with a given set of fields and
+ * parameters and replayed afterwards; 0 launches the kernels one by one
+ * (and frees the cached graphs).  Returns the previous setting.
+ * b200_graphs_cached: the number of executable graphs held (no reference
+ * counterpart). */
+int b200_set_cuda_graphs(int on);
+int b200_graphs_cached(void);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32, 16, or 12 for the 12-real links): index,
  * threads per block, time of one cycle's block sweeps in ms. */

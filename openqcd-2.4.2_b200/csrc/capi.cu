@@ -167,7 +167,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   }
   // a new geometry invalidates every resident field
   void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage,
-                  c.u16, c.sw16, c.sw16_inv, c.u12};
+                  c.u16, c.sw16, c.sw16_inv, c.u12, c.sap_fld[0], c.sap_fld[1], c.sap_fld[2]};
   for (void *p : bufs) cudaFree(p);
   for (void *p : c.ws32) cudaFree(p);
   for (void *p : c.ws64) cudaFree(p);
@@ -177,9 +177,11 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   c.u16 = c.sw16 = c.sw16_inv = nullptr; c.h16_valid = false;
   c.sap_tuned_vbh[0] = c.sap_tuned_vbh[1] = c.sap_tuned_vbh[2] = 0;
   c.u12 = nullptr; c.u12_valid = c.u12_ok = false;
+  c.sap_fld[0] = c.sap_fld[1] = c.sap_fld[2] = nullptr;
   c.have_ud = c.have_sw = false;
   qcd::dfl_release(c);
   qcd::net_fields_release(c);
+  qcd::graphs_release();
   c.ready = false;
   if (geometry_init(c, L, bs, ipt)) return -1;
   c.ready = true;
@@ -338,6 +340,16 @@ int b200_set_sap_link12(int on) {
   ctx().sap_link12 = on != 0;
   return 0;
 }
+
+int b200_set_cuda_graphs(int on) {
+  Ctx &c = ctx();
+  const int prev = c.use_graphs;
+  c.use_graphs = on != 0;
+  if (!c.use_graphs) qcd::graphs_release();
+  return prev;
+}
+
+int b200_graphs_cached(void) { return (int)qcd::graphs_cached(); }
 
 int b200_set_dw_staged(int mode) {
   Ctx &c = ctx();
@@ -596,8 +608,7 @@ int b200_dev_sap(float mu, int isolv, int nmr, int ncy, void *psi, void *rho) {
   if (check_fields(c) || ensure_tmp(c)) return -1;
   if (isolv == 1 && (c.sw_inv_fail & 2)) return fail("sap: the SW term on the odd sites is not safely invertible");
   if (sap_prepare(c, c.stream)) return -1;
-  for (int n = 0; n < ncy; n++)
-    if (sap_cycle(c, mu, isolv, nmr, psi, rho, c.tmp32, c.stream)) return -1;
+  if (sap_cycles(c, mu, isolv, nmr, ncy, psi, rho, c.tmp32, c.stream)) return -1;
   return b200_sync();
 }
 

@@ -194,6 +194,12 @@ int b200_release_workspace(void) {
   for (void *p : c.ws64) cudaFree(p);
   c.ws32.clear();
   c.ws64.clear();
+  // the SAP graphs address the library-owned SAP fields: both go together
+  qcd::graphs_release();
+  for (int k = 0; k < 3; k++) {
+    cudaFree(c.sap_fld[k]);
+    c.sap_fld[k] = nullptr;
+  }
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : fail("CUDA error");
 }
 

@@ -120,6 +120,10 @@ struct Ctx {
   // FP64 operators with an SW term: SW matrices staged in shared memory by
   // bulk copies (1) or read directly (0)
   int dw_staged = 1;
+  // repeated launch sequences (the SAP preconditioner) run as CUDA graphs,
+  // on three library-owned FP32 fields (solution, residual, block scratch)
+  int use_graphs = 1;
+  void *sap_fld[3] = {nullptr, nullptr, nullptr};
   int nthread = 1;              // the caller's NTHREAD, for icom & 0x2 in the BLAS drop-ins
   void *fstage[3] = {nullptr, nullptr, nullptr};   // staging of host operands
   size_t fstage_bytes[3] = {0, 0, 0};
@@ -163,6 +167,12 @@ int apply_swinv_ref_layout(int vol, double mu, const void *m, const void *s, voi
 // fields.cu
 int gen_links(Ctx &c, double eps, uint64_t seed, cudaStream_t st);
 int gen_spinor(const Ctx &c, int prec, void *dev, double sigma, uint64_t seed, cudaStream_t st);
+
+// graph.cu: run launch() captured as a CUDA graph, replayed while key
+// (the bytes of everything the launches depend on) repeats
+int graph_run(Ctx &c, const void *key, size_t keylen, cudaStream_t st, const std::function<int()> &launch);
+void graphs_release();
+size_t graphs_cached();
 
 // linalg.cu : BLAS-1 on device-layout spinor fields.  "n" = number of sites
 // counted from the start of the field (vol for full fields, volh for even).
@@ -288,5 +298,8 @@ int sap_storage_mode(Ctx &c);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
                cudaStream_t st);
+// psi = ncy cycles on rho = rh, then rho = rh - rho (the sap_gcr preconditioner)
+int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
+            cudaStream_t st);
 
 }  // namespace qcd

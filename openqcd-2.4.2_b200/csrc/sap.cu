@@ -24,6 +24,7 @@
 // the phi output field, so that blocks of up to 768 sites per parity (6^4
 // blocks among them) fit into shared memory.
 #include "lib.h"
+#include <cstring>
 #include <cuda_fp16.h>
 
 namespace qcd {
@@ -661,6 +662,7 @@ static void launch_blocks(Ctx &c, const SapArgs &a, int isolv, int mode, cudaStr
 
 static SapArgs sap_args(Ctx &c, float mu, int nmr, int mode, void *psi, void *rho, void *phi) {
   SapArgs a;
+  std::memset(&a, 0, sizeof(a));   // the bytes are also a CUDA-graph key
   const bool half = mode == 1;
   a.g = c.g;
   a.colour = 0;
@@ -753,19 +755,10 @@ int sap_prepare(Ctx &c, cudaStream_t st) {
 // storage mode in use (for reports): 0 FP32, 1 FP16, 2 FP32 with 12-real links
 int sap_storage_mode(Ctx &c) { return sap_mode(c, 1, c.stream); }
 
-// ncy SAP cycles sap(mu, isolv, nmr, psi, rho) on FP32 device fields
-int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
-               cudaStream_t st) {
-  for (int n = 0; n < ncy; n++)
-    if (sap_cycle(c, mu, isolv, nmr, psi, rho, phi_blk, st)) return -1;
-  return 0;
-}
-
-// One SAP cycle sap(mu, isolv, nmr, psi, rho) on FP32 device fields.
-// phi_blk is a scratch FP32 field.  The even-odd block solver (isolv = 1)
-// reads the links and SW matrices in the storage mode of sap_mode(); the
-// plain solver (isolv = 0) always in FP32.
-int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st) {
+// Everything a SAP cycle needs before its launches (storage mode, derived
+// link/SW copies, autotuned variant), done outside any stream capture.
+// Returns the storage mode or -1.
+static int sap_ready(Ctx &c, int isolv, cudaStream_t st) {
   const int mode = sap_mode(c, isolv, st);
   if (mode < 0) return -1;
   if (isolv && c.sap_tuned_vbh[mode] != c.g.vbh && sap_prepare(c, st)) return -1;
@@ -773,7 +766,12 @@ int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *
   int ns;
   if (!pick_threads(c.g.vbh, ns) || (!isolv && (size_t)48 * c.g.vbh * sizeof(float) > (size_t)SAP_SMEM_MAX))
     return fail("sap: block too large");
-  SapArgs a = sap_args(c, mu, nmr, mode, psi, rho, phi_blk);
+  return mode;
+}
+
+// the launches of one cycle: block solves and boundary updates, colour 0
+// then colour 1 (sap.c:720)
+static void sap_cycle_launch(Ctx &c, SapArgs a, int isolv, int mode, cudaStream_t st) {
   const size_t nb_sites = (size_t)(c.g.nbl / 2) * c.g.vb;
   const unsigned nbnd = (unsigned)((nb_sites + 127) / 128);
   for (int ic = 0; ic < 2; ic++) {
@@ -782,6 +780,85 @@ int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *
     if (mode == 1) k_sap_bnd<SapF16><<<nbnd, 128, 0, st>>>(a);
     else k_sap_bnd<SapF32><<<nbnd, 128, 0, st>>>(a);
   }
+}
+
+namespace {
+struct SapKey {
+  int tag, isolv, mode, variant, ncy, pad;
+  SapArgs a;
+};
+}  // namespace
+
+// ph = sap psi, ch = rh - sap rho: the output step of the preconditioner
+__global__ void k_sap_out(size_t n, const float4 *__restrict__ spsi, const float4 *__restrict__ srho,
+                          const float4 *__restrict__ rh, float4 *ph, float4 *ch) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 a = rh[i], b = srho[i];
+  ph[i] = spsi[i];
+  ch[i] = make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+
+int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
+               cudaStream_t st) {
+  const int mode = sap_ready(c, isolv, st);
+  if (mode < 0) return -1;
+  const SapArgs a = sap_args(c, mu, nmr, mode, psi, rho, phi_blk);
+  for (int n = 0; n < ncy; n++) sap_cycle_launch(c, a, isolv, mode, st);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+}
+
+// The preconditioner of sap_gcr (sap_gcr.c:126-134): psi = ncy SAP cycles
+// from psi = 0 on rho = rh, then rho = rh - rho (= D psi).  With CUDA graphs
+// on, the cycles run on three library-owned fields (solution, residual,
+// block scratch) whose addresses never change, so the captured sequence
+// (zero the solution, ncy x [block solves, boundary updates] per colour) is
+// one graph per parameter set, replayed at every GCR step: rh is copied in
+// before the replay and the results copied out after it.
+int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
+            cudaStream_t st) {
+  if (!c.use_graphs) {
+    la_zero(c, 32, psi, PAR_ALL, st);
+    la_copy(c, 32, rh, 32, rho, PAR_ALL, st);
+    if (sap_cycles(c, mu, isolv, nmr, ncy, psi, rho, phi_blk, st)) return -1;
+    la_diff(c, 32, rh, rho, PAR_ALL, st);
+    return 0;
+  }
+  for (int k = 0; k < 3; k++)
+    if (!c.sap_fld[k] && cudaMalloc(&c.sap_fld[k], spinor_bytes(c, 32)) != cudaSuccess)
+      return fail("out of device memory (SAP graph fields)");
+  const int mode = sap_ready(c, isolv, st);
+  if (mode < 0) return -1;
+  void *spsi = c.sap_fld[0], *srho = c.sap_fld[1], *sphi = c.sap_fld[2];
+  SapKey key;
+  std::memset(&key, 0, sizeof(key));
+  key.tag = 0x5a9;
+  key.isolv = isolv;
+  key.mode = mode;
+  key.variant = c.sap_variant[mode];
+  key.ncy = ncy;
+  key.a = sap_args(c, mu, nmr, mode, spsi, srho, sphi);
+  la_copy(c, 32, rh, 32, srho, PAR_ALL, st);
+  const int rc = graph_run(c, &key, sizeof(key), st, [&]() {
+    la_zero(c, 32, spsi, PAR_ALL, st);
+    for (int n = 0; n < ncy; n++) sap_cycle_launch(c, key.a, isolv, mode, st);
+    return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+  });
+  if (rc) return -1;
+  const size_t n = (size_t)c.g.vol * 6;
+  k_sap_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, (const float4 *)spsi, (const float4 *)srho,
+                                                           (const float4 *)rh, (float4 *)psi, (float4 *)rho);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+}
+
+// One SAP cycle sap(mu, isolv, nmr, psi, rho) on FP32 device fields.
+// phi_blk is a scratch FP32 field.  The even-odd block solver (isolv = 1)
+// reads the links and SW matrices in the storage mode of sap_mode(); the
+// plain solver (isolv = 0) always in FP32.
+int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st) {
+  const int mode = sap_ready(c, isolv, st);
+  if (mode < 0) return -1;
+  sap_cycle_launch(c, sap_args(c, mu, nmr, mode, psi, rho, phi_blk), isolv, mode, st);
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
 }
 

@@ -164,10 +164,7 @@ double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, c
       bool fallback = false;
       double rn_prev = -1.0;
       auto sap_mop = [&](const void *rh, void *ph, void *ch) {
-        la_zero(c, 32, ph, PAR_ALL, c.stream);
-        la_copy(c, 32, rh, 32, ch, PAR_ALL, c.stream);
-        for (int n = 0; n < ncy; n++) sap_cycle(c, muf, isolv, nmr, ph, ch, phib, c.stream);
-        la_diff(c, 32, rh, ch, PAR_ALL, c.stream);
+        qcd::sap_mop(c, muf, isolv, nmr, ncy, rh, ph, ch, phib, c.stream);
       };
       MopFn Mop = [&](int, const void *rh, void *ph, void *ch) {
         if (kind == 0) {
@@ -195,7 +192,7 @@ double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, c
           dirac_op<float>(c, 0, muf, ws2, ch, c.tmp32, c.stream);
           la_diff(c, 32, rh, ch, PAR_ALL, c.stream);            // ch = rh - D M rh
           la_zero(c, 32, ph, PAR_ALL, c.stream);
-          for (int n = 0; n < ncy; n++) sap_cycle(c, muf, isolv, nmr, ph, ch, phib, c.stream);
+          sap_cycles(c, muf, isolv, nmr, ncy, ph, ch, phib, c.stream);
           la_diff(c, 32, rh, ch, PAR_ALL, c.stream);            // ch = rh - final residual = D ph_total
           la_axpy(c, 32, ph, 1.0, 0.0, ws2, PAR_ALL, c.stream);
         }

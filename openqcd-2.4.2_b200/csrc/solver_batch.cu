@@ -726,13 +726,9 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       for (int r : A) {
         SysState &y = S[r];
         void *ph = y.phi[y.k], *ch = y.chi[y.k];
-        la_zero(c, 32, ph, PAR_ALL, st);
-        la_copy(c, 32, y.rho, 32, ch, PAR_ALL, st);
         dfl_mark(c, 2);
-        sap_cycles(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ph, ch, phib, st);
+        sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, y.rho, ph, ch, phib, st);
         dfl_mark(c, 4);
-        la_diff(c, 32, y.rho, ch, PAR_ALL, st);
-        dfl_mark(c, 2);
       }
     }
     // --- the rest of gcr_step, and restarts, per system (fgcr.c:157-299)

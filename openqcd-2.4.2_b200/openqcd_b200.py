@@ -102,6 +102,8 @@ _SIGS = {
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
     "b200_set_sap_link12": (C.c_int, [C.c_int]),
     "b200_set_dw_staged": (C.c_int, [C.c_int]),
+    "b200_set_cuda_graphs": (C.c_int, [C.c_int]),
+    "b200_graphs_cached": (C.c_int, []),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_void_p]),
     "tmcgeo": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -252,6 +254,16 @@ def set_sap_prec(bits):
 
 def set_sap_link12(on):
     return check(lib().b200_set_sap_link12(1 if on else 0))
+
+
+def set_cuda_graphs(on):
+    """SAP preconditioner as CUDA graphs (default on); returns the previous
+    setting"""
+    return lib().b200_set_cuda_graphs(1 if on else 0)
+
+
+def graphs_cached():
+    return lib().b200_graphs_cached()
 
 
 def set_dw_staged(mode):
