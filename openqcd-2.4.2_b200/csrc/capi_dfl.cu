@@ -118,7 +118,9 @@ int b200_dfl_profile(int on, double *out) {
 // 0 restriction of an FP32 field, 1 prolongation, 2 Awhat_dble, 3 Aw_dble,
 // 4 ltl_gcr on a random little vector (status[0] of the last solve in *its),
 // 5, 6, 7 the batched restriction, prolongation and little solver on four
-// right-hand sides.
+// right-hand sides, 8 the batched Awhat, 9 the batched little solver on one
+// right-hand side, 10 the block orthonormalisation of the subspace (in
+// place), 11 the little-operator set-up (set_Awhat).
 int b200_dfl_time(int what, int n, float *ms, int *its) {
   Ctx &c = ctx();
   if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1;
@@ -162,6 +164,11 @@ int b200_dfl_time(int what, int n, float *ms, int *its) {
       const int nr = what == 7 ? 4 : 1;
       qcd::ltl_gcr_b(c, d.aw_mu, nr, (const double2 *const *)vs, vs + 4 - nr, f4, s4, c.stream);
       st[0] = s4[0];
+    } else if (what == 10) {
+      qcd::dfl_subspace_dev(c, d.basis, c.stream);   // re-orthonormalise the basis in place
+    } else if (what == 11) {
+      d.awhat_valid = d.aw_valid = false;
+      qcd::dfl_set_Awhat(c, d.aw_mu, c.stream);
     } else {
       qcd::dfl_Awhat_b(c, 4, (const double2 *const *)vs, vs + 0, vs + 0, c.stream);
     }

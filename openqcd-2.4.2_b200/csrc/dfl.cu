@@ -809,7 +809,7 @@ void dfl_release(Ctx &c) {
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
   void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop,
-                  d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart, d.kerr};
+                  d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart, d.kerr, d.gram, d.tri, d.gfail};
   if (d.h_ldots) cudaFreeHost(d.h_ldots);
   for (void *p : bufs) cudaFree(p);
   DflState fresh;
@@ -858,6 +858,20 @@ void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st) {
 // basis from Ns global mode fields (FP32, device layout)
 int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st) {
   DflState &d = c.dfl;
+  if (gram_supported(c)) {
+    // block-wise Cholesky QR (the Q of the block Gram-Schmidt of
+    // dfl_subspace.c:171-240, to rounding): modes -> basis
+    float4 **dm = nullptr;
+    if (cudaMalloc(&dm, d.Ns * sizeof(void *)) != cudaSuccess) return fail("out of device memory");
+    cudaMemcpy(dm, modes.data(), d.Ns * sizeof(void *), cudaMemcpyHostToDevice);
+    const int rc = dfl_cholqr(c, (const float4 *const *)dm, (float4 *const *)d.d_basis, false, st);
+    cudaFree(dm);
+    if (rc < 0) return -1;
+    if (rc) return fail("dfl_subspace: degenerate block modes");
+    d.have_basis = true;
+    d.aw_valid = d.awhat_valid = false;
+    return 0;
+  }
   float4 **dm = nullptr;
   int *dfail = nullptr;
   cudaMallocAsync(&dm, d.Ns * sizeof(void *), st);
@@ -1210,7 +1224,17 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   if (d.gen_kappa == 0.0) return fail("dfl_modes: kappa = 0 (infinite generation mass) is not supported");
   if (!c.sap_set) return fail("dfl_modes: SAP parameters are not set");
   cudaStream_t st = c.stream;
-  if (sap_prepare(c, st) || ensure_lvd(c) || reserve32(c, d.modes, d.Ns) || reserve32(c, c.ws32, 3)) return -1;
+  if (sap_prepare(c, st) || ensure_lvd(c) || reserve32(c, d.modes, d.Ns) || reserve32(c, c.ws32, 9) ||
+      dfl_batch_alloc(c) || ensure_lvd_n(c, 4))
+    return -1;
+  // device table of the mode fields (for the Cholesky QR kernels)
+  float4 **dmodes = nullptr;
+  if (cudaMalloc(&dmodes, d.Ns * sizeof(void *)) != cudaSuccess) return fail("out of device memory");
+  cudaMemcpy(dmodes, d.modes.data(), d.Ns * sizeof(void *), cudaMemcpyHostToDevice);
+  struct FreeTab {
+    float4 **p;
+    ~FreeTab() { cudaFree(p); }
+  } free_tab{dmodes};
   // generation mass and eo flag
   const double m0_save = c.m0;
   const int eo_save = c.eoflg;
@@ -1221,7 +1245,7 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   }
   c.eoflg = 1;
   if (c.sw_inv_fail & 2) ifail[0] = -3;
-  void *ws0 = c.ws32[0], *ws1 = c.ws32[1], *phib = c.ws32[2];
+  void *ws0 = c.ws32[0], *phib = c.ws32[8];
   const float mug = (float)d.gen_mu;
   for (int l = 0; l < d.Ns; l++) gen_uniform_spinor32(c, d.modes[l], seed * 1000003ull + l, st);
   dfl_mark(c, -1);
@@ -1243,33 +1267,55 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
         break;
       }
       dfl_mark(c, 2);
-      for (int l = 0; l < d.Ns; l++) {
-        int lf, ls[2];
-        double2 *vd = d.lvd[0];
-        dfl_restrict(c, 32, d.modes[l], vd, st);
-        dfl_ltl_gcr(c, d.gen_mu, vd, vd, &lf, ls, st);
-        dfl_prolong(c, vd, ws1, st);
-        dfl_mark(c, 3);
-        dirac_op<float>(c, 0, mug, ws1, ws0, c.tmp32, st);
-        la_diff(c, 32, d.modes[l], ws0, PAR_ALL, st);     // ws0 = mode - D ws1
-        la_zero(c, 32, d.modes[l], PAR_ALL, st);
-        dfl_mark(c, 5);
-        sap_cycles(c, mug, 1, d.gen_nmr, d.gen_ncy, d.modes[l], ws0, phib, st);
-        dfl_mark(c, 4);
-        la_axpy(c, 32, d.modes[l], 1.0, 0.0, ws1, PAR_ALL, st);
-        status[0] += ls[0];
-      }
-      // dfl_renormalize_modes (dfl_subspace.c:243-259)
-      for (int l = 0; l < d.Ns; l++) {
-        for (int j = 0; j < l; j++) {
-          double r[4];
-          la_dot(c, 32, d.modes[j], d.modes[l], PAR_ALL, r);
-          la_axpy(c, 32, d.modes[l], -(float)(r[0] + r[1]), -(float)(r[2] + r[3]), d.modes[j], PAR_ALL, st);
+      // one step of the deflated inverse iteration per mode
+      // (dfl_modes.c:354-380: restriction, little solve, prolongation,
+      // residual, SAP on it), the deflation part for four modes at a time
+      // with the multi-right-hand-side kernels
+      for (int l0 = 0; l0 < d.Ns; l0 += 4) {
+        const int na = std::min(4, d.Ns - l0);
+        const void *rh[4];
+        double2 *vd[4];
+        void *w1[4], *w0[4], *md[4];
+        int lf[4], ls[4];
+        for (int i = 0; i < na; i++) {
+          rh[i] = d.modes[l0 + i];
+          md[i] = d.modes[l0 + i];
+          vd[i] = d.lvd[i];
+          w0[i] = c.ws32[i];
+          w1[i] = c.ws32[4 + i];
         }
-        double r[2];
-        la_norm2(c, 32, d.modes[l], PAR_ALL, r);
-        float nrm = (float)sqrt((double)(float)(r[0] + r[1]));
-        if (nrm != 0.0f) la_scale(c, 32, d.modes[l], 1.0f / nrm, PAR_ALL, st);
+        dfl_restrict_b(c, na, rh, vd, st);
+        if (ltl_gcr_b(c, d.gen_mu, na, (const double2 *const *)vd, vd, lf, ls, st)) return -1;
+        dfl_prolong_b(c, na, (const double2 *const *)vd, w1, st);
+        dfl_mark(c, 3);
+        dirac_multi32(c, na, mug, w1, w0, md, st);          // w0 = mode - D w1
+        dfl_mark(c, 5);
+        for (int i = 0; i < na; i++) {
+          la_zero(c, 32, d.modes[l0 + i], PAR_ALL, st);
+          sap_cycles(c, mug, 1, d.gen_nmr, d.gen_ncy, d.modes[l0 + i], w0[i], phib, st);
+          la_axpy(c, 32, d.modes[l0 + i], 1.0, 0.0, w1[i], PAR_ALL, st);
+          status[0] += ls[i];
+        }
+        dfl_mark(c, 4);
+      }
+      // dfl_renormalize_modes (dfl_subspace.c:243-259): the global modes
+      // orthonormalised in order, here by Cholesky QR over the lattice
+      if (gram_supported(c)) {
+        const int rc = dfl_cholqr(c, (const float4 *const *)dmodes, (float4 *const *)dmodes, true, st);
+        if (rc < 0) return -1;
+        if (rc) return fail("dfl_modes: the modes became linearly dependent");
+      } else {
+        for (int l = 0; l < d.Ns; l++) {
+          for (int j = 0; j < l; j++) {
+            double r[4];
+            la_dot(c, 32, d.modes[j], d.modes[l], PAR_ALL, r);
+            la_axpy(c, 32, d.modes[l], -(float)(r[0] + r[1]), -(float)(r[2] + r[3]), d.modes[j], PAR_ALL, st);
+          }
+          double r[2];
+          la_norm2(c, 32, d.modes[l], PAR_ALL, r);
+          float nrm = (float)sqrt((double)(float)(r[0] + r[1]));
+          if (nrm != 0.0f) la_scale(c, 32, d.modes[l], 1.0f / nrm, PAR_ALL, st);
+        }
       }
       dfl_mark(c, 5);
       if (dfl_subspace_dev(c, d.modes, st)) return -1;

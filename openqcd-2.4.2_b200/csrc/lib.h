@@ -34,6 +34,10 @@ struct DflState {
   std::vector<double2 *> lv, lvd;
   double2 **lvtab = nullptr;    // device table of the little solver's Krylov vectors
   double2 *ldots = nullptr, *lpart = nullptr, *h_ldots = nullptr;
+  // Cholesky QR of the modes: Gram matrices (per block, then the lattice
+  // sum), inverse Cholesky factors, failure flag
+  double2 *gram = nullptr, *tri = nullptr;
+  int *gfail = nullptr;
   int lvtab_nkv = 0;
   // phase timers (seconds): 0 SAP smoothing of the modes, 1 block
   // Gram-Schmidt, 2 little operator set-up, 3 little solves, 4 SAP in the
@@ -237,6 +241,9 @@ int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st
 // dfl.cu
 int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
+// dfl_gram.cu
+bool gram_supported(const Ctx &c);
+int dfl_cholqr(Ctx &c, const float4 *const *dv, float4 *const *dw, bool global, cudaStream_t st);
 // solver_cg.cu
 double tmcg_dev(Ctx &c, int eo, int nmx, int istop, double res, double mu, const void *eta, void *psi, int *ifail,
                 int *status);

@@ -465,6 +465,19 @@ int ref_dfl_modes(int seed, int *status)
    return ifail;
 }
 
+/* dfl_subspace() (modules/dfl/dfl_subspace.c:171) on Ns FP32 fields given
+ * one after another in ipt order. */
+void ref_dfl_subspace(int Ns, const float *modes)
+{
+   ENTER();
+   int l;
+   spinor **ws = reserve_ws(Ns);
+   for (l = 0; l < Ns; l++)
+      memcpy(ws[l], modes + (size_t)l * VOLUME * 24, VOLUME * sizeof(spinor));
+   dfl_subspace(ws);
+   release_ws();
+}
+
 /* Basis vector l of every DFL block, as one global field (ipt order). */
 void ref_dfl_get_basis(int l, float *out)
 {

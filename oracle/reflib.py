@@ -245,6 +245,11 @@ class RefLib:
         f = self.lib.ref_dfl_modes(seed, status)
         return f, list(status)
 
+    def dfl_subspace(self, modes):
+        m = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float32) for x in modes]))
+        self.lib.ref_dfl_subspace.argtypes = [C.c_int, C.c_void_p]
+        self.lib.ref_dfl_subspace(len(modes), self._p(m))
+
     def dfl_get_basis(self, l):
         out = np.zeros(self.vol * 24, dtype=np.float32)
         self.lib.ref_dfl_get_basis.argtypes = [C.c_int, C.c_void_p]

@@ -190,3 +190,25 @@ def test_dfl_errors(setup):
         qb.set_dfl_parms((8, 4, 4, 4), NS)
     with pytest.raises(qb.B200Error):
         qb.set_dfl_parms(BS, 7)
+
+
+@pytest.mark.parametrize("spread", [1.0, 1e-2])
+def test_dfl_subspace_cholesky_qr(setup, spread):
+    """dfl_subspace on the same FP32 modes as the reference's block
+    Gram-Schmidt (dfl_subspace.c:171): the device's Cholesky QR gives the
+    same Q to FP32 rounding, for Gaussian modes and for modes that are
+    nearly parallel (a common field plus 1 % of noise, block condition
+    numbers ~1e2)."""
+    base = setup.source(90)
+    modes = [((1.0 - spread) * base + spread * setup.source(91 + l)).astype(np.float32) for l in range(NS)]
+    tol = 2e-6 if spread == 1.0 else 1e-4
+    try:
+        setup.ref.dfl_subspace(modes)
+        ref = [setup.ref.dfl_get_basis(l) for l in range(NS)]
+        qb.dfl_subspace(modes)
+        dev = [qb.dfl_get_basis(l, setup.vol) for l in range(NS)]
+        for l in range(NS):
+            assert rel_norm_err(dev[l], ref[l]) <= tol, (l, rel_norm_err(dev[l], ref[l]))
+    finally:
+        setup.ref.dfl_subspace(setup.basis)
+        load_reference_basis(setup)
