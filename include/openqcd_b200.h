@@ -285,7 +285,39 @@ int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status);
 /* Aw_ops.c:223 */ int set_Awhat(double mu);
 /* Aw_dble.c:122 */ void Aw_dble(complex_dble *v, complex_dble *w);
 /* Aw_dble.c:361 */ void Awhat_dble(complex_dble *v, complex_dble *w);
+/* The even-odd pieces of the little operator (even blocks first in a
+ * little vector; the untouched half of w is unchanged) and the FP32 little
+ * operators (FP32 arithmetic on the FP32-rounded matrices). */
+/* Aw_dble.c:202 */ void Aweeinv_dble(complex_dble *v, complex_dble *w);
+/* Aw_dble.c:234 */ void Awooinv_dble(complex_dble *v, complex_dble *w);
+/* Aw_dble.c:266 */ void Awoe_dble(complex_dble *v, complex_dble *w);
+/* Aw_dble.c:306 */ void Aweo_dble(complex_dble *v, complex_dble *w);
+/* Aw.c:122 */ void Aw(complex *v, complex *w);
+/* Aw.c:361 */ void Awhat(complex *v, complex *w);
+/* Global-mode ("little-little") deflation of the even-odd little system:
+ * the little modes are the modes of the last dfl_subspace()/dfl_modes()
+ * call in the block basis; set_ltl_modes returns 1 if the little-little
+ * operator is not safely invertible.  ltl_matrix points to its inverse
+ * (host memory, Ns x Ns row-major) until the next set_ltl_modes. */
+/* ltl_modes.c:286 */ int set_ltl_modes(void);
+/* ltl_modes.c:301 */ complex_dble *ltl_matrix(void);
+/* ltl_modes.c:307 */ void dfl_Lvd(complex_dble *vd);
+/* ltl_modes.c:339 */ void dfl_LRvd(complex_dble *vd, complex_dble *wd);
+/* ltl_modes.c:382 */ void dfl_RLvd(complex_dble *vd, complex_dble *wd);
+/* ltl_modes.c:417 */ void dfl_Lv(complex *v);
+/* ltl_gcr solves the little equation with the solver chosen by
+ * b200_set_ltl_solver: 0 (default) the device GCR on the even-odd little
+ * system (status[1] = 0), 1 the reference's algorithm, flexible FP64 GCR
+ * (fgcr4vd.c) preconditioned by FP32 GCR (gcr4v.c) with global-mode
+ * deflation (status[1] = the FP32 GCR's Krylov vectors).  The deflated
+ * solvers (dfl_sap_gcr, dfl_sap_gcr2) use the same choice.  Returns the
+ * previous choice (no reference counterpart). */
 /* ltl_gcr.c:155 */ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int *status);
+int b200_set_ltl_solver(int kind);
+/* Little mode l (nv complex floats) for a subspace uploaded as a basis with
+ * b200_dfl_set_basis; dfl_subspace() and dfl_modes() set them themselves
+ * (no reference counterpart). */
+int b200_dfl_set_lmode(int l, const complex *v);
 /* dfl_sap_gcr.c:353 */ double dfl_sap_gcr(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta,
                                            spinor_dble *psi, int *ifail, int *status);
 /* dfl_sap_gcr.c:383 */ double dfl_sap_gcr2(int nkv, int nmx, int istop, double res, double mu, spinor_dble *eta,

@@ -120,13 +120,16 @@ int b200_dfl_profile(int on, double *out) {
 // 5, 6, 7 the batched restriction, prolongation and little solver on four
 // right-hand sides, 8 the batched Awhat, 9 the batched little solver on one
 // right-hand side, 10 the block orthonormalisation of the subspace (in
-// place), 11 the little-operator set-up (set_Awhat).
+// place), 11 the little-operator set-up (set_Awhat), 12 ltl_gcr with the
+// reference's algorithm (fgcr4vd + gcr4v + global-mode deflation).
 int b200_dfl_time(int what, int n, float *ms, int *its) {
   Ctx &c = ctx();
   if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return -1;
   qcd::DflState &d = c.dfl;
   if (!d.have_basis) return fail("dfl_time: no deflation subspace");
-  if ((what == 2 || what == 3 || what == 4) && qcd::dfl_set_Awhat(c, d.aw_valid ? d.aw_mu : 0.0, c.stream) < 0) return -1;
+  if ((what == 2 || what == 3 || what == 4 || what == 12) &&
+      qcd::dfl_set_Awhat(c, d.aw_valid ? d.aw_mu : 0.0, c.stream) < 0)
+    return -1;
   void *f = qcd::spinor_stage(c, 32, 0);
   double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1), *t = qcd::lbuf(c, 2);
   if (!f || !a || !b || !t) return -1;
@@ -157,6 +160,7 @@ int b200_dfl_time(int what, int n, float *ms, int *its) {
     else if (what == 2) qcd::dfl_Awhat(c, a, b, t, c.stream);
     else if (what == 3) qcd::dfl_Aw(c, a, b, c.stream);
     else if (what == 4) qcd::dfl_ltl_gcr(c, d.aw_mu, a, b, &fl, st, c.stream);
+    else if (what == 12) qcd::ltl_gcr_ref(c, d.aw_mu, a, b, &fl, st, c.stream);
     else if (what == 5) qcd::dfl_restrict_b(c, 4, fs, vs, c.stream);
     else if (what == 6) qcd::dfl_prolong_b(c, 4, (const double2 *const *)vs, (void *const *)fs, c.stream);
     else if (what == 7 || what == 9) {
@@ -221,6 +225,7 @@ int b200_dfl_set_basis(int l, const spinor *field) {
   if (qcd::ref32_in(c, field, c.dfl.basis[l])) return -1;
   c.dfl.have_basis = true;
   c.dfl.aw_valid = c.dfl.awhat_valid = false;
+  qcd::ltl_forget_lmodes(c);   // they belong to the previous basis
   return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("CUDA error");
 }
 
@@ -241,7 +246,7 @@ void dfl_subspace(spinor **mds) {
     if (!f || qcd::ref32_in(c, mds[l], f)) return;
     modes.push_back(f);
   }
-  qcd::dfl_subspace_dev(c, modes, c.stream);
+  qcd::dfl_subspace_dev(c, modes, c.stream, true);
 }
 
 void dfl_s2vd(spinor *s, complex_dble *vd) {
@@ -305,11 +310,132 @@ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int 
   if (!a || !b) return -1.0;
   size_t nb = (size_t)d.nv * sizeof(double2);
   cudaMemcpyAsync(a, eta, nb, cudaMemcpyDefault, c.stream);
-  double rho = qcd::dfl_ltl_gcr(c, mu, a, b, ifail, status, c.stream);
-  status[1] = 0;
+  double rho;
+  if (d.ltl_kind == 1) {
+    rho = qcd::ltl_gcr_ref(c, mu, a, b, ifail, status, c.stream);
+  } else {
+    rho = qcd::dfl_ltl_gcr(c, mu, a, b, ifail, status, c.stream);
+    status[1] = 0;
+  }
   cudaMemcpyAsync(psi, b, nb, cudaMemcpyDefault, c.stream);
   cudaStreamSynchronize(c.stream);
   return rho;
+}
+
+int b200_set_ltl_solver(int kind) {
+  Ctx &c = ctx();
+  if (kind < 0 || kind > 1) return fail("set_ltl_solver: kind must be 0 or 1");
+  const int prev = c.dfl.ltl_kind;
+  c.dfl.ltl_kind = kind;
+  return prev;
+}
+
+// ---- the eo pieces and the FP32 little operator (Aw_dble.c, Aw.c)
+static void little_eo(int which, complex_dble *v, complex_dble *w) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return;
+  qcd::DflState &d = c.dfl;
+  if (!d.awhat_valid) { fail("Aw: the even-odd preconditioned little operator is not set (set_Awhat)"); return; }
+  double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1);
+  if (!a || !b) return;
+  const size_t nb = (size_t)d.nv * sizeof(double2);
+  cudaMemcpyAsync(a, v, nb, cudaMemcpyDefault, c.stream);
+  cudaMemcpyAsync(b, w, nb, cudaMemcpyDefault, c.stream);
+  if (which == 0) qcd::dfl_Aweeinv(c, a, b, c.stream);
+  else if (which == 1) qcd::dfl_Awooinv(c, a, b, c.stream);
+  else if (which == 2) qcd::dfl_Awoe(c, a, b, c.stream);
+  else qcd::dfl_Aweo(c, a, b, c.stream);
+  cudaMemcpyAsync(w, b, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+void Aweeinv_dble(complex_dble *v, complex_dble *w) { little_eo(0, v, w); }
+void Awooinv_dble(complex_dble *v, complex_dble *w) { little_eo(1, v, w); }
+void Awoe_dble(complex_dble *v, complex_dble *w) { little_eo(2, v, w); }
+void Aweo_dble(complex_dble *v, complex_dble *w) { little_eo(3, v, w); }
+
+static void little_f32(int which, complex *v, complex *w) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return;
+  qcd::DflState &d = c.dfl;
+  if (!d.aw_valid || (which == 1 && !d.awhat_valid)) { fail("Aw: the little operator is not set (set_Aw / set_Awhat)"); return; }
+  double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1);   // used as float2 buffers
+  if (!a || !b) return;
+  const size_t nb = (size_t)d.nv * sizeof(float2);
+  cudaMemcpyAsync(a, v, nb, cudaMemcpyDefault, c.stream);
+  cudaMemcpyAsync(b, w, nb, cudaMemcpyDefault, c.stream);
+  qcd::little32_apply(c, which, (const float2 *)a, (float2 *)b);
+  cudaMemcpyAsync(w, b, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+void Aw(complex *v, complex *w) { little_f32(0, v, w); }
+void Awhat(complex *v, complex *w) { little_f32(1, v, w); }
+
+// ---- global-mode deflation (ltl_modes.c)
+int set_ltl_modes(void) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return -1;
+  if (!c.dfl.awhat_valid) return fail("set_ltl_modes: the even-odd preconditioned little operator is not set");
+  return qcd::ltl_set_modes(c);
+}
+
+complex_dble *ltl_matrix(void) {
+  const double *m = qcd::ltl_matrix_host(ctx());
+  return (complex_dble *)m;
+}
+
+static int ltl_ready(Ctx &c) {
+  if (qcd::dfl_ready(c)) return -1;
+  if (!qcd::ltl_matrix_host(c)) return fail("little modes are not set (set_ltl_modes)");
+  return 0;
+}
+
+void dfl_Lvd(complex_dble *vd) {
+  Ctx &c = ctx();
+  if (ltl_ready(c)) return;
+  double2 *a = qcd::lbuf(c, 0);
+  const size_t nb = (size_t)c.dfl.nv * sizeof(double2);
+  cudaMemcpyAsync(a, vd, nb, cudaMemcpyDefault, c.stream);
+  qcd::dfl_Lvd_dev(c, a);
+  cudaMemcpyAsync(vd, a, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+static void ltl_pair(int which, complex_dble *vd, complex_dble *wd) {
+  Ctx &c = ctx();
+  if (ltl_ready(c)) return;
+  double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1);
+  const size_t nb = (size_t)c.dfl.nv * sizeof(double2);
+  cudaMemcpyAsync(a, vd, nb, cudaMemcpyDefault, c.stream);
+  cudaMemcpyAsync(b, wd, nb, cudaMemcpyDefault, c.stream);
+  if (which == 0) qcd::dfl_LRvd_dev(c, a, b);
+  else qcd::dfl_RLvd_dev(c, a, b);
+  cudaMemcpyAsync(vd, a, nb, cudaMemcpyDefault, c.stream);
+  cudaMemcpyAsync(wd, b, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+void dfl_LRvd(complex_dble *vd, complex_dble *wd) { ltl_pair(0, vd, wd); }
+void dfl_RLvd(complex_dble *vd, complex_dble *wd) { ltl_pair(1, vd, wd); }
+
+void dfl_Lv(complex *v) {
+  Ctx &c = ctx();
+  if (ltl_ready(c)) return;
+  double2 *a = qcd::lbuf(c, 0);
+  const size_t nb = (size_t)c.dfl.nv * sizeof(float2);
+  cudaMemcpyAsync(a, v, nb, cudaMemcpyDefault, c.stream);
+  qcd::dfl_Lv_dev(c, (float2 *)a);
+  cudaMemcpyAsync(v, a, nb, cudaMemcpyDefault, c.stream);
+  cudaStreamSynchronize(c.stream);
+}
+
+// little mode l (the mode's coefficients in the block basis, complex
+// floats, nv of them): load, for a subspace that was uploaded as a basis
+int b200_dfl_set_lmode(int l, const complex *v) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return -1;
+  return qcd::ltl_lmode_set(c, l, v);
 }
 
 int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status) {

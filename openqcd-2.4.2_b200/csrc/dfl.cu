@@ -812,6 +812,7 @@ void dfl_release(Ctx &c) {
                   d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart, d.kerr, d.gram, d.tri, d.gfail};
   if (d.h_ldots) cudaFreeHost(d.h_ldots);
   for (void *p : bufs) cudaFree(p);
+  ltl_ref_release(c);
   DflState fresh;
   // the solver and generation parameters outlive a change of geometry
   fresh.gen_set = d.gen_set;
@@ -819,6 +820,7 @@ void dfl_release(Ctx &c) {
   fresh.res = d.res; fresh.res_gcr = d.res_gcr;
   fresh.gen_kappa = d.gen_kappa; fresh.gen_mu = d.gen_mu;
   fresh.gen_ninv = d.gen_ninv; fresh.gen_nmr = d.gen_nmr; fresh.gen_ncy = d.gen_ncy;
+  fresh.ltl_kind = d.ltl_kind;
   d = fresh;
 }
 
@@ -856,8 +858,16 @@ void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st) {
 }
 
 // basis from Ns global mode fields (FP32, device layout)
-int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st) {
+int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st, bool lmodes) {
   DflState &d = c.dfl;
+  if (lmodes) {
+    const int rc = dfl_subspace_dev(c, modes, st, false);
+    if (rc) return rc;
+    // the modes in the new basis, for the little solver's global-mode
+    // deflation (dfl_subspace.c stores them as Gram-Schmidt coefficients)
+    return ltl_lmodes_from_fields(c, modes, st);
+  }
+  ltl_invalidate(c);
   if (gram_supported(c)) {
     // block-wise Cholesky QR (the Q of the block Gram-Schmidt of
     // dfl_subspace.c:171-240, to rounding): modes -> basis
@@ -938,6 +948,7 @@ int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st) {
   cudaFreeAsync(dfail, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return fail("set_Awhat: CUDA error");
   d.awhat_valid = true;
+  d.awhat_ver++;
   d.awhat_fail = hf ? 1 : 0;
   return d.awhat_fail;
 }
@@ -946,6 +957,26 @@ int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st) {
 void dfl_Aw(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
   DflState &d = c.dfl;
   little_launch(0, d.Ns, 0, d.nb, d.Ablk, d.Ahop, d.nbr, v, nullptr, w, st);
+}
+
+// Aw_dble.c:202-359, on all little vectors of nv entries (even blocks
+// first): w_e = Aee^-1 v_e, w_o = Aoo^-1 v_o, w_o = Aoe v_e, w_e -= Aeo v_o;
+// the other half of w is unchanged
+void dfl_Aweeinv(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  little_launch(3, d.Ns, 0, d.nb / 2, d.Ainv, nullptr, d.nbr, v, nullptr, w, st);
+}
+void dfl_Awooinv(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  little_launch(3, d.Ns, d.nb / 2, d.nb / 2, d.Ainv, nullptr, d.nbr, v, nullptr, w, st);
+}
+void dfl_Awoe(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  little_launch(1, d.Ns, d.nb / 2, d.nb / 2, nullptr, d.Ahop, d.nbr, v, nullptr, w, st);
+}
+void dfl_Aweo(Ctx &c, const double2 *v, double2 *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  little_launch(2, d.Ns, 0, d.nb / 2, nullptr, d.Ahop, d.nbr, w, v, w, st);
 }
 
 // w_e = v_e - H_eo H_oe v_e (Awhat_dble): t holds the odd intermediate
@@ -1113,10 +1144,11 @@ static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, vo
   DflState &d = c.dfl;
   cudaStream_t st = c.stream;
   double2 *vd = d.lvd[0];
-  int ifail, status[2];
+  int ifail, status[2] = {0, 0};
   dfl_mark(c, 5);
   dfl_restrict(c, 32, rho, vd, st);
-  dfl_ltl_gcr(c, mu, vd, vd, &ifail, status, st);
+  if (d.ltl_kind == 1) ltl_gcr_ref(c, mu, vd, vd, &ifail, status, st);
+  else dfl_ltl_gcr(c, mu, vd, vd, &ifail, status, st);
   dfl_prolong(c, vd, ws0, st);
   dfl_mark(c, 3);
   dirac_op<float>(c, 0, (float)mu, ws0, chi, c.tmp32, st);
@@ -1128,6 +1160,7 @@ static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, vo
   la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - chi
   la_axpy(c, 32, phi, 1.0, 0.0, ws0, PAR_ALL, st);
   lstat[0] += status[0];
+  lstat[1] += status[1];
 }
 
 int ensure_lvd_n(Ctx &c, int n) {
@@ -1182,12 +1215,12 @@ double dfl_sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double m
     const double rho0 = rho;
     la_copy(c, 64, eta, 64, rsd, PAR_ALL, st);
     la_scale(c, 64, rsd, 1.0 / rho0, PAR_ALL, st);
-    int lstat = 0;
+    int lstat[2] = {0, 0};
     std::function<void(const void *, void *)> Dop = [&](const void *s, void *r) {
       dirac_op<double>(c, 0, mu, s, r, c.tmp64, st);
     };
     std::function<void(int, const void *, void *, void *)> Mop = [&](int, const void *rh, void *ph, void *ch) {
-      dfl_mop(c, mu, rh, ph, ch, ws0, phib, &lstat);
+      dfl_mop(c, mu, rh, ph, ch, ws0, phib, lstat);
     };
     std::vector<void *> phi(c.ws32.begin(), c.ws32.begin() + nkv),
         chi(c.ws32.begin() + nkv + 1, c.ws32.begin() + 2 * nkv + 1);
@@ -1199,7 +1232,10 @@ double dfl_sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double m
       ifail[0] = -1;
       status[0] = nmx;
     }
-    if (status[0] > 0) status[1] = (lstat + status[0] / 2) / status[0];
+    if (status[0] > 0) {
+      status[1] = (lstat[0] + status[0] / 2) / status[0];
+      status[2] = (lstat[1] + status[0] / 2) / status[0];
+    }
   } else {
     la_zero(c, 64, psi, PAR_ALL, st);
   }
@@ -1323,6 +1359,8 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
     }
     const int nst = d.Ns * (n - 3);
     if (nst > 0) status[0] = (status[0] + nst / 2) / nst;
+    // the modes in the final basis (little modes of the little solver)
+    if (ltl_lmodes_from_fields(c, d.modes, st)) return -1;
   } else {
     if (dfl_subspace_dev(c, d.modes, st)) return -1;
   }

@@ -11,6 +11,8 @@
 
 namespace qcd {
 
+struct LtlRef;
+
 // Deflation state (the reference's DFL block grid, little operator and
 // parameter sets dfl_parms, dfl_pro_parms, dfl_gen_parms).
 struct DflState {
@@ -38,6 +40,10 @@ struct DflState {
   // sum), inverse Cholesky factors, failure flag
   double2 *gram = nullptr, *tri = nullptr;
   int *gfail = nullptr;
+  // little solver: 0 the device GCR, 1 the reference's algorithm (ltl_ref.cu)
+  int ltl_kind = 0;
+  int awhat_ver = 0;   // incremented whenever the preconditioned operator is rebuilt
+  struct LtlRef *ltlref = nullptr;
   int lvtab_nkv = 0;
   // phase timers (seconds): 0 SAP smoothing of the modes, 1 block
   // Gram-Schmidt, 2 little operator set-up, 3 little solves, 4 SAP in the
@@ -241,6 +247,21 @@ int gen_uniform_spinor32(const Ctx &c, void *dev, uint64_t seed, cudaStream_t st
 // dfl.cu
 int dfl_set_parms(Ctx &c, const int bs[4], int Ns);
 void dfl_release(Ctx &c);
+// ltl_ref.cu: the reference's little solver (fgcr4vd + gcr4v + global-mode
+// deflation) and the FP32 little operators
+void ltl_ref_release(Ctx &c);
+void ltl_invalidate(Ctx &c);
+void ltl_forget_lmodes(Ctx &c);
+int ltl_lmodes_from_fields(Ctx &c, const std::vector<void *> &modes, cudaStream_t st);
+int ltl_lmode_set(Ctx &c, int l, const void *v32);
+int ltl_set_modes(Ctx &c);
+double ltl_gcr_ref(Ctx &c, double mu, const double2 *eta, double2 *psi, int *ifail, int *status, cudaStream_t st);
+void dfl_Lvd_dev(Ctx &c, double2 *vd);
+void dfl_LRvd_dev(Ctx &c, double2 *vd, double2 *wd);
+void dfl_RLvd_dev(Ctx &c, double2 *vd, double2 *wd);
+void dfl_Lv_dev(Ctx &c, float2 *v);
+int little32_apply(Ctx &c, int which, const float2 *v, float2 *w);
+const double *ltl_matrix_host(Ctx &c);
 // dfl_gram.cu
 bool gram_supported(const Ctx &c);
 int dfl_cholqr(Ctx &c, const float4 *const *dv, float4 *const *dw, bool global, cudaStream_t st);
@@ -288,7 +309,11 @@ void dfl_Awhat_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, dou
 void dfl_Aw_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, cudaStream_t st);
 void dfl_restrict(Ctx &c, int prec, const void *s, double2 *vd, cudaStream_t st);
 void dfl_prolong(Ctx &c, const double2 *vd, void *s, cudaStream_t st);
-int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st);
+int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st, bool lmodes = false);
+void dfl_Aweeinv(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
+void dfl_Awooinv(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
+void dfl_Awoe(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
+void dfl_Aweo(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
 int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st);
 int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st);
 void dfl_Aw(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);

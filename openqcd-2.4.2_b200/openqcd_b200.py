@@ -102,6 +102,20 @@ _SIGS = {
     "b200_set_sap_prec": (C.c_int, [C.c_int]),
     "b200_set_sap_link12": (C.c_int, [C.c_int]),
     "b200_set_dw_staged": (C.c_int, [C.c_int]),
+    "Aweeinv_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Awooinv_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Awoe_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Aweo_dble": (None, [C.c_void_p, C.c_void_p]),
+    "Aw": (None, [C.c_void_p, C.c_void_p]),
+    "Awhat": (None, [C.c_void_p, C.c_void_p]),
+    "set_ltl_modes": (C.c_int, []),
+    "ltl_matrix": (C.c_void_p, []),
+    "dfl_Lvd": (None, [C.c_void_p]),
+    "dfl_LRvd": (None, [C.c_void_p, C.c_void_p]),
+    "dfl_RLvd": (None, [C.c_void_p, C.c_void_p]),
+    "dfl_Lv": (None, [C.c_void_p]),
+    "b200_set_ltl_solver": (C.c_int, [C.c_int]),
+    "b200_dfl_set_lmode": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_set_cuda_graphs": (C.c_int, [C.c_int]),
     "b200_graphs_cached": (C.c_int, []),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -619,6 +633,73 @@ def little(which, mu, v, w=None):
         f = check(lib().set_Awhat(mu))
         _void(lib().Awhat_dble, _ptr(v), _ptr(w))
     return w, f
+
+
+LITTLE_EO = {"Aweeinv_dble": 2, "Awooinv_dble": 3, "Awoe_dble": 4, "Aweo_dble": 5}
+
+
+def little_eo(name, mu, v, w=None):
+    """set_Awhat(mu), then one of Aweeinv_dble, Awooinv_dble, Awoe_dble,
+    Aweo_dble (little vectors of nv complex doubles)."""
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float64, copy=True)
+    f = check(lib().set_Awhat(mu))
+    _void(getattr(lib(), name), _ptr(v), _ptr(w))
+    return w, f
+
+
+def little32(which, mu, v, w=None):
+    """FP32 little operators: 0 set_Aw(mu), Aw; 1 set_Awhat(mu), Awhat
+    (little vectors of nv complex floats as float32 arrays)."""
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float32, copy=True)
+    if which == 0:
+        _void(lib().set_Aw, mu)
+        _void(lib().Aw, _ptr(v), _ptr(w))
+    else:
+        check(lib().set_Awhat(mu))
+        _void(lib().Awhat, _ptr(v), _ptr(w))
+    return w
+
+
+def set_ltl_modes():
+    return check(lib().set_ltl_modes())
+
+
+def ltl_matrix(ns):
+    p = lib().ltl_matrix()
+    if not p:
+        raise B200Error(_err_after() or "little modes are not set")
+    return np.ctypeslib.as_array((C.c_double * (2 * ns * ns)).from_address(p)).copy()
+
+
+def dfl_proj(which, v, w=None):
+    """0 dfl_Lvd(v), 1 dfl_LRvd(v, w), 2 dfl_RLvd(v, w); returns (v, w)"""
+    v = np.array(v, dtype=np.float64, copy=True)
+    w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float64, copy=True)
+    if which == 0:
+        _void(lib().dfl_Lvd, _ptr(v))
+    elif which == 1:
+        _void(lib().dfl_LRvd, _ptr(v), _ptr(w))
+    else:
+        _void(lib().dfl_RLvd, _ptr(v), _ptr(w))
+    return v, w
+
+
+def dfl_Lv(v):
+    v = np.array(v, dtype=np.float32, copy=True)
+    _void(lib().dfl_Lv, _ptr(v))
+    return v
+
+
+def set_ltl_solver(kind):
+    """0 the device GCR, 1 the reference's fgcr4vd + gcr4v with global-mode
+    deflation; returns the previous choice"""
+    return check(lib().b200_set_ltl_solver(int(kind)))
+
+
+def dfl_set_lmode(l, v):
+    return check(lib().b200_dfl_set_lmode(l, _ptr(np.ascontiguousarray(v, dtype=np.float32))))
 
 
 def ltl_gcr(mu, eta):

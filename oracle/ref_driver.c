@@ -538,12 +538,88 @@ int ref_little(int which, double mu, const double *v, double *w)
    else
    {
       ifail = set_Awhat(mu);
-      Awhat_dble(a, b);
+      if (which == 1) Awhat_dble(a, b);
+      else if (which == 2) Aweeinv_dble(a, b);
+      else if (which == 3) Awooinv_dble(a, b);
+      else if (which == 4) Awoe_dble(a, b);
+      else if (which == 5) Aweo_dble(a, b);
    }
    memcpy(w, b, (size_t)dfl_nv * sizeof(complex_dble));
    free(a);
    free(b);
    return ifail;
+}
+
+/* FP32 little operators (Aw.c:122, :361) on complex-float vectors, after
+ * set_Aw(mu) / set_Awhat(mu): which = 0 Aw, 1 Awhat. */
+int ref_little32(int which, double mu, const float *v, float *w)
+{
+   ENTER();
+   int ifail = 0;
+   size_t nb = (size_t)dfl_nv * sizeof(complex);
+   complex *a = malloc(nb), *b = malloc(nb);
+   memcpy(a, v, nb);
+   memcpy(b, w, nb);
+   if (which == 0)
+   {
+      set_Aw(mu);
+      Aw(a, b);
+   }
+   else
+   {
+      ifail = set_Awhat(mu);
+      Awhat(a, b);
+   }
+   memcpy(w, b, nb);
+   free(a);
+   free(b);
+   return ifail;
+}
+
+/* Little mode l of the last subspace: vflds()[Ns + l] (dfl_subspace.c:198). */
+void ref_dfl_get_lmode(int l, float *out)
+{
+   ENTER();
+   complex **vs = vflds();
+   dfl_parms_t dp = dfl_parms();
+   memcpy(out, vs[dp.Ns + l], (size_t)dfl_nv * sizeof(complex));
+}
+
+/* set_Awhat(mu) (which rebuilds the little modes, Aw_ops.c) and the inverse
+ * little-little matrix (ltl_modes.c:301) into m (Ns*Ns complex). */
+int ref_ltl_modes(double mu, double *m)
+{
+   ENTER();
+   int ifail = set_Awhat(mu);
+   dfl_parms_t dp = dfl_parms();
+   memcpy(m, ltl_matrix(), (size_t)dp.Ns * dp.Ns * sizeof(complex_dble));
+   return ifail;
+}
+
+/* ltl_modes.c projections on copies: which = 0 dfl_Lvd(v), 1 dfl_LRvd(v, w),
+ * 2 dfl_RLvd(v, w); the little modes must be up to date (ref_ltl_modes). */
+void ref_dfl_proj(int which, double *v, double *w)
+{
+   ENTER();
+   complex_dble *a = vd_copy(v), *b = vd_copy(w);
+   if (which == 0) dfl_Lvd(a);
+   else if (which == 1) dfl_LRvd(a, b);
+   else dfl_RLvd(a, b);
+   memcpy(v, a, (size_t)dfl_nv * sizeof(complex_dble));
+   memcpy(w, b, (size_t)dfl_nv * sizeof(complex_dble));
+   free(a);
+   free(b);
+}
+
+void ref_dfl_Lv(float *v)
+{
+   ENTER();
+   size_t nb = (size_t)dfl_nv * sizeof(complex);
+   complex *a = malloc(nb);
+   memcpy(a, v, nb);
+   dfl_Lv(a);
+   memcpy(v, a, nb);
+   free(a);
 }
 
 double ref_ltl_gcr(double mu, const double *eta, double *psi, int *ifail, int *status)

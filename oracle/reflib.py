@@ -277,6 +277,38 @@ class RefLib:
         f = self.lib.ref_little(which, mu, self._p(v), self._p(w))
         return w, f
 
+    def little32(self, which, mu, v, w=None):
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float32, copy=True)
+        self.lib.ref_little32.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        self.lib.ref_little32(which, mu, self._p(v), self._p(w))
+        return w
+
+    def dfl_get_lmode(self, l, nv):
+        out = np.zeros(2 * nv, dtype=np.float32)
+        self.lib.ref_dfl_get_lmode.argtypes = [C.c_int, C.c_void_p]
+        self.lib.ref_dfl_get_lmode(l, self._p(out))
+        return out
+
+    def ltl_modes(self, mu, ns):
+        m = np.zeros(2 * ns * ns)
+        self.lib.ref_ltl_modes.argtypes = [C.c_double, C.c_void_p]
+        f = self.lib.ref_ltl_modes(mu, self._p(m))
+        return m, f
+
+    def dfl_proj(self, which, v, w=None):
+        v = np.array(v, dtype=np.float64, copy=True)
+        w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float64, copy=True)
+        self.lib.ref_dfl_proj.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        self.lib.ref_dfl_proj(which, self._p(v), self._p(w))
+        return v, w
+
+    def dfl_Lv(self, v):
+        v = np.array(v, dtype=np.float32, copy=True)
+        self.lib.ref_dfl_Lv.argtypes = [C.c_void_p]
+        self.lib.ref_dfl_Lv(self._p(v))
+        return v
+
     def ltl_gcr(self, mu, eta):
         eta = np.ascontiguousarray(eta, dtype=np.float64)
         psi = np.zeros_like(eta)
