@@ -207,6 +207,16 @@ int b200_set_dw_staged(int mode);
  * b200_graphs_cached: the number of executable graphs held (no reference
  * counterpart). */
 int b200_set_cuda_graphs(int on);
+/* on != 0 (default): Dw_dble and Dw on page-locked host arrays run as a
+ * pipeline over x0-slabs (copy in, operator, copy out of different slabs
+ * overlap) when every slab of whole block rows is a contiguous range of
+ * each parity half of the caller's storage order, as openQCD's ipt[] makes
+ * slabs of L0_TRD planes; otherwise, or with 0, the fields are copied
+ * whole.  Returns the previous setting.  b200_pipeline_slabs: the number of
+ * slabs of the current geometry (0: no pipeline).  No reference
+ * counterpart. */
+int b200_set_pipeline(int on);
+int b200_pipeline_slabs(void);
 int b200_graphs_cached(void);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32, 16, or 12 for the 12-real links): index,

@@ -60,6 +60,80 @@ static int check_fields(const Ctx &c) {
 // Run a device-layout operator on reference-layout arrays (host or device):
 // copy in, convert, apply, convert back, copy out.  The output array is read
 // first because the even/odd pieces leave one parity of r unchanged.
+static bool pinned_host(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Dw on page-locked host arrays, pipelined over the x0-slabs of the slab
+// plan: the input slabs are copied and converted on one stream in the order
+// R-1, 0, 1, ..., R-2; as soon as a slab's neighbours are in, its Dw runs
+// on the library stream and its result is converted and copied back on a
+// third stream, so host-to-device and device-to-host transfers overlap.
+template <typename R>
+static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr, char *st_in, char *st_out) {
+  const int prec = sizeof(R) == 8 ? 64 : 32;
+  const size_t site = 24 * sizeof(R);
+  const int nsl = (int)c.slab.size();
+  if ((!c.st_in && cudaStreamCreateWithFlags(&c.st_in, cudaStreamNonBlocking) != cudaSuccess) ||
+      (!c.st_out && cudaStreamCreateWithFlags(&c.st_out, cudaStreamNonBlocking) != cudaSuccess))
+    return fail("no CUDA stream for the pipelined transfers");
+  while ((int)c.slab_ev.size() < 2 * nsl + 1) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail("no CUDA event");
+    c.slab_ev.push_back(e);
+  }
+  cudaEvent_t *ev_in = c.slab_ev.data(), *ev_out = ev_in + nsl, ev0 = ev_in[2 * nsl];
+  cudaEventRecord(ev0, c.stream);
+  cudaStreamWaitEvent(c.st_in, ev0, 0);
+  cudaStreamWaitEvent(c.st_out, ev0, 0);
+  auto h2d = [&](int k) {
+    const Slab &sb = c.slab[k];
+    for (int p = 0; p < 2; p++) {
+      const size_t o = (size_t)sb.q0[p] * site, n = (size_t)(sb.q1[p] - sb.q0[p]) * site;
+      cudaMemcpyAsync(st_in + o, (const char *)s + o, n, cudaMemcpyHostToDevice, c.st_in);
+    }
+    for (int p = 0; p < 2; p++) {
+      const int d0 = (p * c.g.nbl + sb.b0) * c.g.vbh, nd = (sb.b1 - sb.b0) * c.g.vbh;
+      spinor_from_ref_range(c, prec, st_in, fs, d0, nd, c.st_in);
+    }
+    cudaEventRecord(ev_in[k], c.st_in);
+  };
+  auto comp = [&](int k, int after) {
+    const Slab &sb = c.slab[k];
+    cudaStreamWaitEvent(c.stream, ev_in[after], 0);
+    qcd::dirac_dw_blocks<R>(c, mu, fs, fr, c.d_ident + sb.b0, sb.b1 - sb.b0, c.stream);
+    for (int p = 0; p < 2; p++) {
+      const int d0 = (p * c.g.nbl + sb.b0) * c.g.vbh, nd = (sb.b1 - sb.b0) * c.g.vbh;
+      spinor_to_ref_range(c, prec, fr, st_out, d0, nd, c.stream);
+    }
+    cudaEventRecord(ev_out[k], c.stream);
+    cudaStreamWaitEvent(c.st_out, ev_out[k], 0);
+    for (int p = 0; p < 2; p++) {
+      const size_t o = (size_t)sb.q0[p] * site, n = (size_t)(sb.q1[p] - sb.q0[p]) * site;
+      cudaMemcpyAsync((char *)r + o, st_out + o, n, cudaMemcpyDeviceToHost, c.st_out);
+    }
+  };
+  // slab j-1 has its neighbours j-2 (or nsl-1), j-1, j once slab j is in
+  h2d(nsl - 1);
+  h2d(0);
+  for (int j = 1; j <= nsl - 2; j++) {
+    h2d(j);
+    comp(j - 1, j);
+  }
+  comp(nsl - 2, nsl - 2);
+  comp(nsl - 1, nsl - 2);
+  const cudaError_t e1 = cudaStreamSynchronize(c.st_out), e2 = cudaStreamSynchronize(c.stream),
+                    e3 = cudaStreamSynchronize(c.st_in);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+    return fail(std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
+  return 0;
+}
+
 template <typename R>
 static void ref_layout_op(int op, R mu, const void *s, void *r) {
   Ctx &c = ctx();
@@ -77,6 +151,10 @@ static void ref_layout_op(int op, R mu, const void *s, void *r) {
   void *fr = prec == 64 ? c.ws64[1] : c.ws32[1];
   char *st_in = (char *)c.stage, *st_out = (char *)c.stage + nb;
   cudaStream_t st = c.stream;
+  if (op == 0 && c.pipeline && c.slab.size() >= 3 && pinned_host(s) && pinned_host(r)) {
+    dw_pipelined<R>(c, mu, s, r, fs, fr, st_in, st_out);
+    return;
+  }
   cudaMemcpyAsync(st_in, s, nb, cudaMemcpyDefault, st);
   spinor_from_ref(c, prec, st_in, fs, st);
   if (op != 0) {
@@ -350,6 +428,17 @@ int b200_set_cuda_graphs(int on) {
 }
 
 int b200_graphs_cached(void) { return (int)qcd::graphs_cached(); }
+
+// 1 (default): Dw_dble / Dw on page-locked host arrays overlap their
+// transfers over x0-slabs when the storage order allows; 0: whole-field copies
+int b200_set_pipeline(int on) {
+  Ctx &c = ctx();
+  const int prev = c.pipeline;
+  c.pipeline = on != 0;
+  return prev;
+}
+
+int b200_pipeline_slabs(void) { return (int)ctx().slab.size(); }
 
 int b200_set_dw_staged(int mode) {
   Ctx &c = ctx();

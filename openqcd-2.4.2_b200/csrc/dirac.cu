@@ -359,6 +359,34 @@ int dirac_op(const Ctx &c, int op, R mu, const void *s, void *r, void *tmp, cuda
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
+// Dw on all sites of the listed blocks (block indices in device memory):
+// the launches of dirac_op(0) with the block list as the traversal order
+template <typename R>
+int dirac_dw_blocks(const Ctx &c, R mu, const void *s, void *r, const int *blocks, int nblk, cudaStream_t st) {
+  const R muo = c.eoflg ? (R)0 : mu;
+  constexpr int OPS = OP_SW | OP_HOP;
+  if (sizeof(R) == 8 && c.dw_staged && c.d_kerr) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(dirac_staged_kernel<OPS, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DWT_SMEM);
+      attr = true;
+    }
+    const int tpc = (c.g.vbh + DWT_TS - 1) / DWT_TS;
+    dirac_staged_kernel<OPS, 2><<<2 * nblk * tpc, DWT_TS, DWT_SMEM, st>>>(
+        c.g, (const double2 *)s, (const double2 *)s, (double2 *)r, (const double2 *)c.ud, (const double2 *)c.swd,
+        (double)mu, (double)muo, blocks, tpc, c.d_kerr);
+  } else {
+    const void *u = sizeof(R) == 8 ? (const void *)c.ud : (const void *)c.u32;
+    const void *sw = sizeof(R) == 8 ? (const void *)c.swd : (const void *)c.sw32;
+    const int threads = 128, n = nblk * c.g.vb;
+    dirac_kernel<R, OPS, 2><<<(n + threads - 1) / threads, threads, 0, st>>>(c.g, s, s, r, u, sw, nullptr, mu, muo,
+                                                                            blocks);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+template int dirac_dw_blocks<double>(const Ctx &, double, const void *, void *, const int *, int, cudaStream_t);
+template int dirac_dw_blocks<float>(const Ctx &, float, const void *, void *, const int *, int, cudaStream_t);
+
 // Dwhat_dble with the odd intermediate in a caller-provided half-field
 // (odd chunks only, volh sites); used by the allocation-free entry point.
 int dwhat_dble_halfscratch(const Ctx &c, double mu, const void *s, void *r, void *odd_scratch, cudaStream_t st) {

@@ -114,14 +114,56 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
     c.h_dev2q = d2q;
     c.have_ipt = true;
   }
+  // x0-slab plan: the thinnest slabs (a whole number of block rows, at least
+  // three slabs) whose sites are contiguous in each parity half of the
+  // storage order.  openQCD's ipt orders the sites by the thread-local
+  // sub-lattices with x0 slowest (modules/lattice/geometry.c:200-240), so
+  // slabs of L0_TRD planes qualify.
+  c.slab.clear();
+  if (ipt) {
+    const int nb0 = g.nb[0], bs0 = g.bstr[0];
+    for (int rows = 1; rows <= nb0 / 3 && c.slab.empty(); rows++) {
+      if (nb0 % rows) continue;
+      const int R = nb0 / rows;
+      std::vector<Slab> sl(R);
+      bool ok = true;
+      for (int k = 0; k < R && ok; k++) {
+        Slab &sb = sl[k];
+        sb.b0 = k * rows * bs0;
+        sb.b1 = (k + 1) * rows * bs0;
+        for (int p = 0; p < 2 && ok; p++) {
+          const size_t d0 = (size_t)(p * g.nbl + sb.b0) * g.vbh, d1 = (size_t)(p * g.nbl + sb.b1) * g.vbh;
+          int lo = g.vol, hi = -1;
+          for (size_t d = d0; d < d1; d++) {
+            lo = std::min(lo, c.h_dev2q[d]);
+            hi = std::max(hi, c.h_dev2q[d]);
+          }
+          ok = (size_t)(hi - lo + 1) == d1 - d0;
+          sb.q0[p] = lo;
+          sb.q1[p] = hi + 1;
+        }
+      }
+      if (ok) c.slab = sl;
+    }
+  }
+  cudaFree(c.d_ident);
+  c.d_ident = nullptr;
+  {
+    std::vector<int> id(g.nbl);
+    for (int b = 0; b < g.nbl; b++) id[b] = b;
+    if (cudaMalloc(&c.d_ident, g.nbl * sizeof(int)) != cudaSuccess) return fail("geometry: device allocation failed");
+    cudaMemcpy(c.d_ident, id.data(), g.nbl * sizeof(int), cudaMemcpyHostToDevice);
+  }
   return cudaGetLastError() == cudaSuccess ? 0 : fail("geometry: CUDA error");
 }
 
 // ------------------------------------------------------------------ spinors
 template <typename R>
-__global__ void k_spinor_from_ref(Geom g, const int *__restrict__ d2q, const R *__restrict__ q, void *dev) {
-  int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= g.vol) return;
+__global__ void k_spinor_from_ref(Geom g, const int *__restrict__ d2q, const R *__restrict__ q, void *dev, int d0,
+                                  int nd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd) return;
+  const int d = d0 + i;
   int chunk = d / g.vbh, s = d - chunk * g.vbh;
   const R *src = q + (size_t)__ldg(d2q + d) * 24;
   spinor<R> v;
@@ -131,9 +173,10 @@ __global__ void k_spinor_from_ref(Geom g, const int *__restrict__ d2q, const R *
 }
 
 template <typename R>
-__global__ void k_spinor_to_ref(Geom g, const int *__restrict__ d2q, const void *dev, R *q) {
-  int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= g.vol) return;
+__global__ void k_spinor_to_ref(Geom g, const int *__restrict__ d2q, const void *dev, R *q, int d0, int nd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nd) return;
+  const int d = d0 + i;
   int chunk = d / g.vbh, s = d - chunk * g.vbh;
   R *dst = q + (size_t)__ldg(d2q + d) * 24;
   spinor<R> v = Store<R>::load_spinor_rw(dev, chunk, s, g.vbh);
@@ -141,20 +184,32 @@ __global__ void k_spinor_to_ref(Geom g, const int *__restrict__ d2q, const void 
   for (int k = 0; k < 12; k++) { dst[2 * k] = v.c[k / 3].c[k % 3].re; dst[2 * k + 1] = v.c[k / 3].c[k % 3].im; }
 }
 
-int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st) {
+int spinor_from_ref_range(const Ctx &c, int prec, const void *q, void *dev, int d0, int n, cudaStream_t st) {
   if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
-  int n = c.g.vol, t = 128;
-  if (prec == 64) k_spinor_from_ref<double><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const double *)q, dev);
-  else k_spinor_from_ref<float><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const float *)q, dev);
+  const int t = 128;
+  if (n <= 0) return 0;
+  if (prec == 64)
+    k_spinor_from_ref<double><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const double *)q, dev, d0, n);
+  else
+    k_spinor_from_ref<float><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, (const float *)q, dev, d0, n);
   return cudaGetLastError() == cudaSuccess ? 0 : fail("spinor_from_ref: launch failed");
 }
 
-int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st) {
+int spinor_to_ref_range(const Ctx &c, int prec, const void *dev, void *q, int d0, int n, cudaStream_t st) {
   if (!c.have_ipt) return fail("no reference site order: pass ipt[] to the geometry call");
-  int n = c.g.vol, t = 128;
-  if (prec == 64) k_spinor_to_ref<double><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, dev, (double *)q);
-  else k_spinor_to_ref<float><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, dev, (float *)q);
+  const int t = 128;
+  if (n <= 0) return 0;
+  if (prec == 64) k_spinor_to_ref<double><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, dev, (double *)q, d0, n);
+  else k_spinor_to_ref<float><<<(n + t - 1) / t, t, 0, st>>>(c.g, c.d_dev2q, dev, (float *)q, d0, n);
   return cudaGetLastError() == cudaSuccess ? 0 : fail("spinor_to_ref: launch failed");
+}
+
+int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st) {
+  return spinor_from_ref_range(c, prec, q, dev, 0, c.g.vol, st);
+}
+
+int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st) {
+  return spinor_to_ref_range(c, prec, dev, q, 0, c.g.vol, st);
 }
 
 // -------------------------------------------------------------------- links

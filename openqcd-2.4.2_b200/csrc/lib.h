@@ -13,6 +13,14 @@ namespace qcd {
 
 struct LtlRef;
 
+// An x0-slab of the lattice whose sites are contiguous ranges of the
+// reference's storage order in each parity half: device blocks [b0, b1)
+// (lexicographic block order, x0 slowest) and storage indices [q0[p], q1[p]).
+struct Slab {
+  int b0, b1;
+  int q0[2], q1[2];
+};
+
 // Deflation state (the reference's DFL block grid, little operator and
 // parameter sets dfl_parms, dfl_pro_parms, dfl_gen_parms).
 struct DflState {
@@ -82,6 +90,13 @@ struct Ctx {
   int *d_dev2q = nullptr;       // [vol] device site (chunk*vbh+s) -> reference index ix
   int *d_link2q = nullptr;      // [4*vol] (device site, mu) -> slot in the reference ud[4V]
   std::vector<int> h_dev2q;
+  // x0-slab plan for pipelined host transfers (empty if the storage order
+  // has no contiguous slabs), the identity block list, the copy streams
+  std::vector<Slab> slab;
+  int *d_ident = nullptr;
+  cudaStream_t st_in = nullptr, st_out = nullptr;
+  std::vector<cudaEvent_t> slab_ev;
+  int pipeline = 1;             // pipelined host transfers of Dw / Dw_dble when possible
 
   // parameters
   double csw = 0.0, m0 = 0.0;
@@ -155,11 +170,18 @@ size_t spinor_bytes(const Ctx &c, int prec);   // prec 64 or 32
 template <typename R>
 int dirac_op(const Ctx &c, int op, R mu, const void *s, void *r, void *tmp, cudaStream_t st);
 
+// Dw on all sites of the blocks blocks[0..nblk) (device block indices)
+template <typename R>
+int dirac_dw_blocks(const Ctx &c, R mu, const void *s, void *r, const int *blocks, int nblk, cudaStream_t st);
+
 int dwhat_dble_halfscratch(const Ctx &c, double mu, const void *s, void *r, void *odd_scratch, cudaStream_t st);
 
 // layout.cu
 int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt);
 int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st);   // q: reference AoS on device
+// the same for the device sites [d0, d0 + n) only
+int spinor_from_ref_range(const Ctx &c, int prec, const void *q, void *dev, int d0, int n, cudaStream_t st);
+int spinor_to_ref_range(const Ctx &c, int prec, const void *dev, void *q, int d0, int n, cudaStream_t st);
 int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st);
 int links_from_ref(Ctx &c, const void *qud, cudaStream_t st);                           // qud on device
 int links_to_ref(const Ctx &c, void *qud, cudaStream_t st);

@@ -117,6 +117,8 @@ _SIGS = {
     "b200_set_ltl_solver": (C.c_int, [C.c_int]),
     "b200_dfl_set_lmode": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_set_cuda_graphs": (C.c_int, [C.c_int]),
+    "b200_set_pipeline": (C.c_int, [C.c_int]),
+    "b200_pipeline_slabs": (C.c_int, []),
     "b200_graphs_cached": (C.c_int, []),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_void_p]),
@@ -274,6 +276,16 @@ def set_cuda_graphs(on):
     """SAP preconditioner as CUDA graphs (default on); returns the previous
     setting"""
     return lib().b200_set_cuda_graphs(1 if on else 0)
+
+
+def set_pipeline(on):
+    """pipelined host transfers of Dw / Dw_dble (default on); returns the
+    previous setting"""
+    return lib().b200_set_pipeline(1 if on else 0)
+
+
+def pipeline_slabs():
+    return lib().b200_pipeline_slabs()
 
 
 def graphs_cached():
