@@ -109,13 +109,18 @@ class Dist:
         self.world = env_int("WORLD_SIZE", 1)
         self.local = env_int("LOCAL_RANK", 0)
         self.pg = None
+        self.cuda = False
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            # NCCL between the GPUs; gloo where there is no GPU (the CPU
+            # tests of the rank logic)
+            self.cuda = torch.cuda.is_available()
+            if self.cuda:
+                torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl" if self.cuda else "gloo", timeout=datetime.timedelta(seconds=300))
             self.torch, self.dist = torch, dist
             self.pg = True
 
@@ -126,7 +131,7 @@ class Dist:
     def max(self, x):
         if not self.pg:
             return x
-        t = self.torch.tensor([float(x)], device="cuda")
+        t = self.torch.tensor([float(x)], device="cuda" if self.cuda else "cpu")
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
