@@ -181,9 +181,9 @@ double fgcr(int vol, void (*Dop)(spinor_dble *s, spinor_dble *r), void (*Mop)(in
  * block solver (no reference counterpart): 32 (default) as the reference;
  * 16 reads FP16 copies of them, with FP32 work vectors and arithmetic. */
 int b200_set_sap_prec(int bits);
-/* Dw (FP32, twisted mass mu) on n device fields at once, reading every link
- * and SW matrix once per four fields (no reference counterpart):
- * r[j] = Dw s[j], or r[j] = sub[j] - Dw s[j] when sub is not NULL. */
+/* Dw (FP32, twisted mass mu) on n device fields (no reference
+ * counterpart): r[j] = Dw s[j], or r[j] = sub[j] - Dw s[j] when sub is not
+ * NULL, the subtraction fused into the operator's store. */
 int b200_dev_dirac_multi(int n, float mu, void *const *s, void *const *r, void *const *sub);
 /* Start (on != 0) or stop profiler collection around a region of interest
  * (for ncu --profile-from-start off). */
