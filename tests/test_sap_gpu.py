@@ -6,7 +6,7 @@ SAP works in FP32, so its outputs agree with the reference's to FP32 rounding
 rho after ncy cycles, against the reference built from its plain-C code
 paths.  (The reference's AVX build computes the MR step length with the
 approximate reciprocal vrcpss, modules/sap/blk_solv.c:291-300, and agrees only
-to about 1e-4; the device code uses the exact reciprocal of the C path.)  The solver is judged on the FP64 true residual
+to about 1e-4; the device code uses the exact reciprocal of the C path.)  The solver is checked on the FP64 true residual
 |eta - Dw psi| / |eta| computed by the REFERENCE's Dw_dble, and on the
 solution itself: both solvers reach res = 1e-10, so their solutions agree to
 about cond(Dw) * 1e-10.

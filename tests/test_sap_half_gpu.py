@@ -1,6 +1,6 @@
 """SAP on FP16 copies of the links and SW matrices (FP32 work vectors and
 arithmetic; an option of this library with no reference counterpart).  It
-is a preconditioner, so it is judged by what the solver does with it: its
+is a preconditioner, so it is assessed by what the solver does with it: its
 cycles stay within a few 1e-2 of the FP32 cycles of the reference
 (modules/sap/sap.c:720) and of the identity rho = eta - Dw psi, and SAP+GCR
 reaches the same FP64 true residual 1e-10, checked with the reference's
