@@ -1151,14 +1151,12 @@ static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, vo
   else dfl_ltl_gcr(c, mu, vd, vd, &ifail, status, st);
   dfl_prolong(c, vd, ws0, st);
   dfl_mark(c, 3);
-  dirac_op<float>(c, 0, (float)mu, ws0, chi, c.tmp32, st);
-  la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - D ws0
-  la_zero(c, 32, phi, PAR_ALL, st);
+  void *const sv[1] = {ws0}, *const rv[1] = {chi}, *const bv[1] = {(void *)rho};
+  dirac_multi32(c, 1, (float)mu, sv, rv, bv, st);   // chi = rho - D ws0
   dfl_mark(c, 5);
-  sap_cycles(c, (float)mu, c.isolv, c.nmr, c.ncy, phi, chi, phib, st);
+  // SAP on chi, then chi = rho - (final residual), phi = SAP solution + ws0
+  sap_mop(c, (float)mu, c.isolv, c.nmr, c.ncy, chi, phi, chi, phib, st, rho, ws0);
   dfl_mark(c, 4);
-  la_diff(c, 32, rho, chi, PAR_ALL, st);       // chi = rho - chi
-  la_axpy(c, 32, phi, 1.0, 0.0, ws0, PAR_ALL, st);
   lstat[0] += status[0];
   lstat[1] += status[1];
 }

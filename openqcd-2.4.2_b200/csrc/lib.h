@@ -354,6 +354,6 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
                cudaStream_t st);
 // psi = ncy cycles on rho = rh, then rho = rh - rho (the sap_gcr preconditioner)
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
-            cudaStream_t st);
+            cudaStream_t st, const void *base = nullptr, const void *add = nullptr);
 
 }  // namespace qcd

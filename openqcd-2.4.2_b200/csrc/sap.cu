@@ -789,13 +789,20 @@ struct SapKey {
 };
 }  // namespace
 
-// ph = sap psi, ch = rh - sap rho: the output step of the preconditioner
+// ph = sap psi (+ add), ch = base - sap rho: the output step of the
+// preconditioner (base = rh, or the residual the caller's preconditioner
+// started from; add = the part of the solution applied before SAP)
 __global__ void k_sap_out(size_t n, const float4 *__restrict__ spsi, const float4 *__restrict__ srho,
-                          const float4 *__restrict__ rh, float4 *ph, float4 *ch) {
+                          const float4 *base, const float4 *__restrict__ add, float4 *ph, float4 *ch) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float4 a = rh[i], b = srho[i];
-  ph[i] = spsi[i];
+  const float4 a = base[i], b = srho[i];
+  float4 p = spsi[i];
+  if (add) {
+    const float4 q = add[i];
+    p = make_float4(p.x + q.x, p.y + q.y, p.z + q.z, p.w + q.w);
+  }
+  ph[i] = p;
   ch[i] = make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
 }
 
@@ -809,19 +816,24 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
 }
 
 // The preconditioner of sap_gcr (sap_gcr.c:126-134): psi = ncy SAP cycles
-// from psi = 0 on rho = rh, then rho = rh - rho (= D psi).  With CUDA graphs
+// from psi = 0 on rho = rh, then rho = rh - rho (= D psi); with base given,
+// rho = base - (final residual), and psi += add (the deflated
+// preconditioner of dfl_sap_gcr.c:212-241, where SAP runs on what the
+// deflation part left and base is the residual it started from).  With CUDA graphs
 // on, the cycles run on three library-owned fields (solution, residual,
 // block scratch) whose addresses never change, so the captured sequence
 // (zero the solution, ncy x [block solves, boundary updates] per colour) is
 // one graph per parameter set, replayed at every GCR step: rh is copied in
 // before the replay and the results copied out after it.
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
-            cudaStream_t st) {
+            cudaStream_t st, const void *base, const void *add) {
+  if (!base) base = rh;
   if (!c.use_graphs) {
     la_zero(c, 32, psi, PAR_ALL, st);
-    la_copy(c, 32, rh, 32, rho, PAR_ALL, st);
+    if (rho != rh) la_copy(c, 32, rh, 32, rho, PAR_ALL, st);
     if (sap_cycles(c, mu, isolv, nmr, ncy, psi, rho, phi_blk, st)) return -1;
-    la_diff(c, 32, rh, rho, PAR_ALL, st);
+    la_diff(c, 32, base, rho, PAR_ALL, st);
+    if (add) la_axpy(c, 32, psi, 1.0, 0.0, add, PAR_ALL, st);
     return 0;
   }
   for (int k = 0; k < 3; k++)
@@ -847,7 +859,8 @@ int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void 
   if (rc) return -1;
   const size_t n = (size_t)c.g.vol * 6;
   k_sap_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, (const float4 *)spsi, (const float4 *)srho,
-                                                           (const float4 *)rh, (float4 *)psi, (float4 *)rho);
+                                                           (const float4 *)base, (const float4 *)add,
+                                                           (float4 *)psi, (float4 *)rho);
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
 }
 

@@ -713,13 +713,10 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       for (int i = 0; i < na; i++) {
         SysState &y = S[A[i]];
         void *ph = y.phi[y.k], *ch = y.chi[y.k];
-        la_zero(c, 32, ph, PAR_ALL, st);
         dfl_mark(c, 2);
-        sap_cycles(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ph, ch, phib, st);
+        // SAP on ch = rho - D ws0, then ch = rho - (final residual), ph += ws0
+        sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ch, ph, ch, phib, st, y.rho, y.ws0);
         dfl_mark(c, 4);
-        la_diff(c, 32, y.rho, ch, PAR_ALL, st);        // ch = rho - ch
-        la_axpy(c, 32, ph, 1.0, 0.0, y.ws0, PAR_ALL, st);
-        dfl_mark(c, 2);
         y.lstat += ls[i];
       }
     } else {
