@@ -382,6 +382,7 @@ def batched_c4(qb):
                      "per_mass": per_mu, "setup_s": setup, "true_residual_max_checked": worst,
                      "solver": "deflated SAP+GCR, 4 batches of 12 (one per mass), Ns=28, nkv=8, ncy=2"}
     out["plain_s_per_rhs_mean"] = sum(p["s"] for p in plain) / len(plain)
+    out["rhs_tiles"] = qb.rhs_tiles()
     for f in srcs + P + [psi]:
         f.free()
     qb.release_workspace()

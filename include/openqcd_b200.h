@@ -324,6 +324,12 @@ int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status);
  * previous choice (no reference counterpart). */
 /* ltl_gcr.c:155 */ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int *status);
 int b200_set_ltl_solver(int kind);
+/* RHS-tile autotuner of the multi-right-hand-side restriction and
+ * prolongation (fields per pass: 1, 2 or 4, chosen by timing on the first
+ * call with four or more fields per geometry): tile[0] restriction, tile[1]
+ * prolongation (0: not tuned yet); ms[0..2] and ms[3..5] the times of four
+ * fields with tiles 1, 2 and 4.  No reference counterpart. */
+int b200_rhs_tiles(int tile[2], float ms[6]);
 /* Little mode l (nv complex floats) for a subspace uploaded as a basis with
  * b200_dfl_set_basis; dfl_subspace() and dfl_modes() set them themselves
  * (no reference counterpart). */

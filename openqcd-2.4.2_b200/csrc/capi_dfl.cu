@@ -322,6 +322,12 @@ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int 
   return rho;
 }
 
+// RHS tiles (fields per pass) the autotuner chose for the streamed
+// restriction (tile[0]) and prolongation (tile[1]), 0 if not tuned yet, and
+// the times of four fields with tiles 1, 2, 4 (ms[0..2] restriction,
+// ms[3..5] prolongation)
+int b200_rhs_tiles(int *tile, float *ms) { return qcd::rhs_tiles(ctx(), tile, ms); }
+
 int b200_set_ltl_solver(int kind) {
   Ctx &c = ctx();
   if (kind < 0 || kind > 1) return fail("set_ltl_solver: kind must be 0 or 1");

@@ -385,12 +385,91 @@ static void restrict_pass(Ctx &c, const void *const *x, double2 *const *vd, cuda
                                                                       ptrs<NRT>((const void *const *)vd));
 }
 
+// RHS tile autotuner: the number of fields per pass of the streamed
+// restriction and prolongation (1, 2 or 4), timed once per geometry on the
+// first call with four or more fields (on the caller's own data: every tile
+// computes the same result) and kept.
+namespace {
+struct TileTune {
+  int vbh = 0, nb = 0, Ns = 0;
+  int tile[2] = {BT, BT};            // restriction, prolongation
+  float ms[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  bool done[2] = {false, false};
+};
+TileTune g_tile;
+}  // namespace
+
+static bool tile_key_changed(const Ctx &c) {
+  const DflState &d = c.dfl;
+  if (g_tile.vbh == c.g.vbh && g_tile.nb == d.nb && g_tile.Ns == d.Ns) return false;
+  g_tile = TileTune();
+  g_tile.vbh = c.g.vbh;
+  g_tile.nb = d.nb;
+  g_tile.Ns = d.Ns;
+  return true;
+}
+
+template <class F>
+static float time_on(cudaStream_t st, F f) {
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  f();   // warm-up (attributes, caches)
+  cudaEventRecord(e0, st);
+  f();
+  cudaEventRecord(e1, st);
+  cudaEventSynchronize(e1);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms;
+}
+
+static void restrict_tiled(Ctx &c, int tile, int nr, const void *const *x, double2 *const *vd, cudaStream_t st) {
+  int r = 0;
+  if (tile >= 4)
+    for (; r + 4 <= nr; r += 4) restrict_pass<4>(c, x + r, vd + r, st);
+  if (tile >= 2)
+    for (; r + 2 <= nr; r += 2) restrict_pass<2>(c, x + r, vd + r, st);
+  for (; r < nr; r++) restrict_pass<1>(c, x + r, vd + r, st);
+}
+
+template <int NRT>
+static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st);
+
+static void prolong_tiled(Ctx &c, int tile, int nr, const double2 *const *vd, void *const *s, cudaStream_t st) {
+  int r = 0;
+  if (tile >= 4)
+    for (; r + 4 <= nr; r += 4) prolong_pass<4>(c, vd + r, s + r, st);
+  if (tile >= 2)
+    for (; r + 2 <= nr; r += 2) prolong_pass<2>(c, vd + r, s + r, st);
+  for (; r < nr; r++) prolong_pass<1>(c, vd + r, s + r, st);
+}
+
 // vd[r] = restriction of the FP32 fields x[r], r < nr
 void dfl_restrict_b(Ctx &c, int nr, const void *const *x, double2 *const *vd, cudaStream_t st) {
-  int r = 0;
-  for (; r + BT <= nr; r += BT) restrict_pass<BT>(c, x + r, vd + r, st);
-  for (; r + 2 <= nr; r += 2) restrict_pass<2>(c, x + r, vd + r, st);
-  for (; r < nr; r++) restrict_pass<1>(c, x + r, vd + r, st);
+  tile_key_changed(c);
+  if (nr >= 4 && !g_tile.done[0]) {
+    const int tiles[3] = {1, 2, 4};
+    int best = 2;
+    for (int i = 0; i < 3; i++) {
+      g_tile.ms[0][i] = time_on(st, [&]() { restrict_tiled(c, tiles[i], 4, x, vd, st); });
+      if (g_tile.ms[0][i] < g_tile.ms[0][best]) best = i;
+    }
+    g_tile.tile[0] = tiles[best];
+    g_tile.done[0] = true;
+  }
+  restrict_tiled(c, g_tile.tile[0], nr, x, vd, st);
+}
+
+int rhs_tiles(const Ctx &c, int *tile, float *ms) {
+  (void)c;
+  for (int k = 0; k < 2; k++) {
+    tile[k] = g_tile.done[k] ? g_tile.tile[k] : 0;
+    for (int i = 0; i < 3; i++) ms[3 * k + i] = g_tile.ms[k][i];
+  }
+  return 0;
 }
 
 template <int NRT>
@@ -407,10 +486,18 @@ static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaS
 
 // s[r] = prolongation of the little vectors vd[r], r < nr
 void dfl_prolong_b(Ctx &c, int nr, const double2 *const *vd, void *const *s, cudaStream_t st) {
-  int r = 0;
-  for (; r + BT <= nr; r += BT) prolong_pass<BT>(c, vd + r, s + r, st);
-  for (; r + 2 <= nr; r += 2) prolong_pass<2>(c, vd + r, s + r, st);
-  for (; r < nr; r++) prolong_pass<1>(c, vd + r, s + r, st);
+  tile_key_changed(c);
+  if (nr >= 4 && !g_tile.done[1]) {
+    const int tiles[3] = {1, 2, 4};
+    int best = 2;
+    for (int i = 0; i < 3; i++) {
+      g_tile.ms[1][i] = time_on(st, [&]() { prolong_tiled(c, tiles[i], 4, vd, s, st); });
+      if (g_tile.ms[1][i] < g_tile.ms[1][best]) best = i;
+    }
+    g_tile.tile[1] = tiles[best];
+    g_tile.done[1] = true;
+  }
+  prolong_tiled(c, g_tile.tile[1], nr, vd, s, st);
 }
 
 template <int NRT>

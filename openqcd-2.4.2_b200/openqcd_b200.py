@@ -115,6 +115,7 @@ _SIGS = {
     "dfl_RLvd": (None, [C.c_void_p, C.c_void_p]),
     "dfl_Lv": (None, [C.c_void_p]),
     "b200_set_ltl_solver": (C.c_int, [C.c_int]),
+    "b200_rhs_tiles": (C.c_int, [C.c_void_p, C.c_void_p]),
     "b200_dfl_set_lmode": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_set_cuda_graphs": (C.c_int, [C.c_int]),
     "b200_set_pipeline": (C.c_int, [C.c_int]),
@@ -702,6 +703,16 @@ def dfl_Lv(v):
     v = np.array(v, dtype=np.float32, copy=True)
     _void(lib().dfl_Lv, _ptr(v))
     return v
+
+
+def rhs_tiles():
+    """autotuned fields per pass of the batched restriction and prolongation
+    (0: not tuned yet) and the times of four fields with tiles 1, 2, 4"""
+    t = np.zeros(2, dtype=np.int32)
+    ms = np.zeros(6, dtype=np.float32)
+    check(lib().b200_rhs_tiles(_ptr(t), _ptr(ms)))
+    return {"restrict": int(t[0]), "prolong": int(t[1]), "restrict_ms": ms[:3].tolist(),
+            "prolong_ms": ms[3:].tolist()}
 
 
 def set_ltl_solver(kind):

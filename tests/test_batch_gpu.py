@@ -147,3 +147,12 @@ def test_dirac_multi(setup, n):
         assert site_rel_err(R[i].to_ref(setup.vol), ref, setup.vol) <= 2e-6
         diff = U[i].to_ref(setup.vol).astype(np.float64) - ref
         assert site_rel_err(Q[i].to_ref(setup.vol), diff, setup.vol) <= 2e-6
+
+
+def test_rhs_tile_autotuner(setup):
+    """After a deflated batched solve the RHS-tile autotuner has timed the
+    restriction and prolongation with 1, 2 and 4 fields per pass and kept
+    one of them."""
+    t = qb.rhs_tiles()
+    assert t["restrict"] in (1, 2, 4) and t["prolong"] in (1, 2, 4), t
+    assert all(m > 0 for m in t["restrict_ms"] + t["prolong_ms"]), t
