@@ -230,12 +230,21 @@ def main():
     ap.add_argument("--profile-solver", action="store_true",
                     help="run only the 48^3x96 solver comparison, with profiler collection around the chosen solve")
     ap.add_argument("--solver-lattice", default=None, help="L0,L1,L2,L3 for --profile-solver (smaller cases)")
+    ap.add_argument("--profile-setup", action="store_true",
+                    help="run only the deflation subspace generation of the solver workload, with profiler "
+                         "collection around it, and print its phase times")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     d = Dist()
     try:
         if args.impl == "reference":
             return run_reference(args, d)
+        if args.profile_setup:
+            import openqcd_b200 as qb
+            qb.set_device(d.local)
+            L = tuple(int(x) for x in args.solver_lattice.split(",")) if args.solver_lattice else None
+            print(json.dumps(setup_profile(qb, lattice=L)))
+            return 0
         if args.profile_solver:
             import openqcd_b200 as qb
             qb.set_device(d.local)
@@ -322,6 +331,29 @@ def solver_c3(qb, profile=False, lattice=None):
     psi.free()
     qb.release_workspace()
     return out
+
+
+def setup_profile(qb, lattice=None):
+    """Subspace generation of the solver workload (dfl_modes, Ns = 28, ninv =
+    10, on the solver's field) with profiler collection around it: seconds
+    and the phase timers of the deflation code."""
+    L, BSx, NS = (lattice or SOLVER_L), SOLVER_BS, 28
+    qb.geometry(L, BSx, qb.even_first_ipt(L))
+    qb.set_parms(CSW, M0, 0)
+    qb.random_ud(EPS, 20251204)
+    qb.sw_term()
+    qb.set_sap_parms(BSx, 1, 4, 5)
+    qb.set_dfl_parms(BSx, NS)
+    qb.set_dfl_pro_parms(24, 256, 1e-2, 24, 1e-2)
+    qb.set_dfl_gen_parms(1.0 / (2.0 * (4.0 + M0)), 0.0, 10, 4, 4)
+    qb.dfl_profile(True)
+    qb.check(qb.lib().b200_profiler(1))
+    t0 = time.time()
+    f, st = qb.dfl_modes(1)
+    qb.lib().b200_sync()
+    dt = time.time() - t0
+    qb.check(qb.lib().b200_profiler(0))
+    return {"lattice": list(L), "dfl_modes_s": dt, "ifail": f, "status": st, "phases_s": qb.dfl_profile(False)}
 
 
 def batched_c4(qb):

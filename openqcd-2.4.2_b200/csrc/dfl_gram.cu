@@ -262,7 +262,9 @@ __global__ void __launch_bounds__(256) k_blk_apply(Geom g, const int *__restrict
 }
 
 // ------------------------------------------------------------------ host
-static int gram_tile_sites(int Ns) { return Ns <= 32 ? 32 : 16; }
+// sites per shared-memory tile: 16 lets three CTAs share an SM for Ns = 28
+// (180 -> 161 ms per two-pass subspace at 48^3x96 against 32-site tiles)
+static int gram_tile_sites(int Ns) { return Ns <= 32 ? 16 : 8; }
 
 // shared memory of the Gram kernel: the tile with its rows padded to a
 // multiple of four, or the split-K partial sums, whichever is larger
