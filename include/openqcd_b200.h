@@ -77,6 +77,14 @@ int b200_set_lat_parms(double csw);
  * exponential form c exp{[csw/(4+m0)] (i/4) sigma F} (sw_term.c:46-49) */
 int b200_set_sw_type(int isw);
 int b200_set_bc_parms(int type);
+/* The spatial phase angles theta[0..2] of set_bc_parms (lat_parms.c:516):
+ * gauge fields made on the device (b200_random_ud) or read by import_cnfg
+ * get the phase of set_ud_phase (modules/uflds/uflds.c:249-355), U(x,k)
+ * times exp(i theta[k-1]/N[k]) besides the sign of the time links at
+ * x0 = N0-1, and export_cnfg takes it off again; a field loaded with
+ * b200_upload_ud is used as given (the caller has set its phase).  Default
+ * 0; set it before the field is made or read. */
+int b200_set_bc_theta(const double theta[3]);
 int b200_set_sw_parms(double m0);
 int b200_set_tm_parms(int eoflg);
 int b200_set_sap_parms(const int bs[4], int isolv, int nmr, int ncy);

@@ -116,7 +116,10 @@ int plaq_sum(Ctx &c, double *sum) {
 }
 
 // ---------------------------------------------------------- configurations
-// the antiperiodic phase of bc type 3 sits on U(x,0) with x0 = N0-1
+// the antiperiodic phase of bc type 3 sits on U(x,0) with x0 = N0-1; with
+// phase angles theta the spatial links carry exp(i theta[k-1]/N[k]) as well
+// (set_ud_phase, modules/uflds/uflds.c:249-355), put on after reading a
+// configuration and taken off before writing one
 static bool phase_link(const Ctx &c, const int x[4], int mu) { return c.bc == 3 && mu == 0 && x[0] == c.g.L[0] - 1; }
 
 int export_cnfg(Ctx &c, const char *out) {
@@ -135,6 +138,9 @@ int export_cnfg(Ctx &c, const char *out) {
   int32_t ls[4] = {L[0], L[1], L[2], L[3]};
   bool ok = fwrite(ls, sizeof(int32_t), 4, f) == 4 && fwrite(&plaq, sizeof(double), 1, f) == 1;
   std::vector<double> line((size_t)4 * L[3] * 18);
+  double pr[3], pi[3];
+  const bool phased = spatial_phases(c, pr, pi);
+  for (int k = 0; k < 3; k++) pi[k] = -pi[k];   // the phase is taken off (set_phase(-1))
   int x[4];
   for (x[0] = 0; x[0] < L[0] && ok; x[0]++)
     for (x[1] = 0; x[1] < L[1] && ok; x[1]++)
@@ -151,8 +157,13 @@ int export_cnfg(Ctx &c, const char *out) {
               const double sg = phase_link(c, y, mu) ? -1.0 : 1.0;
               for (int k = 0; k < 9; k++) {
                 const double2 v = hu[(((size_t)chunk * 4 + mu) * 9 + k) * c.g.vbh + s];
-                *q++ = sg * v.x;
-                *q++ = sg * v.y;
+                if (phased && mu > 0) {
+                  *q++ = v.x * pr[mu - 1] - v.y * pi[mu - 1];
+                  *q++ = v.x * pi[mu - 1] + v.y * pr[mu - 1];
+                } else {
+                  *q++ = sg * v.x;
+                  *q++ = sg * v.y;
+                }
               }
             }
         }
@@ -181,6 +192,8 @@ int import_cnfg(Ctx &c, const char *in, int mask) {
   const size_t nd = (size_t)c.g.vol * 36;
   std::vector<double2> hu(nd);
   std::vector<double> line((size_t)4 * L[3] * 18);
+  double pr[3], pi[3];
+  const bool phased = spatial_phases(c, pr, pi);
   int x[4];
   bool ok = true;
   for (x[0] = 0; x[0] < L[0] && ok; x[0]++)
@@ -198,7 +211,11 @@ int import_cnfg(Ctx &c, const char *in, int mask) {
               dev_site(c, y, chunk, s);
               const double sg = phase_link(c, y, mu) ? -1.0 : 1.0;
               for (int k = 0; k < 9; k++) {
-                hu[(((size_t)chunk * 4 + mu) * 9 + k) * c.g.vbh + s] = make_double2(sg * q[0], sg * q[1]);
+                double2 &d = hu[(((size_t)chunk * 4 + mu) * 9 + k) * c.g.vbh + s];
+                if (phased && mu > 0)
+                  d = make_double2(q[0] * pr[mu - 1] - q[1] * pi[mu - 1], q[0] * pi[mu - 1] + q[1] * pr[mu - 1]);
+                else
+                  d = make_double2(sg * q[0], sg * q[1]);
                 q += 2;
               }
             }

@@ -278,6 +278,11 @@ int b200_set_bc_parms(int type) {
   ctx().bc = type;
   return 0;
 }
+int b200_set_bc_theta(const double theta[3]) {
+  Ctx &c = ctx();
+  for (int k = 0; k < 3; k++) c.theta[k] = theta ? theta[k] : 0.0;
+  return 0;
+}
 int b200_set_sw_parms(double m0) { ctx().m0 = m0; ctx().have_sw = false; return 0; }
 int b200_set_tm_parms(int eoflg) { ctx().eoflg = eoflg != 0; return 0; }
 

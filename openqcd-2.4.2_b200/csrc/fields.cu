@@ -120,8 +120,26 @@ __device__ void su3_exp(const double *M, double *U) {
 // X_13 = x5+i x6, X_23 = x7+i x8 (anti-Hermitian).  U = exp(eps X).  With
 // antiperiodic fermion boundary conditions (type 3) the time links at
 // x0 = L0-1 get the factor -1, as the reference's set_ud_phase does
-// (modules/uflds/uflds.c:307-335).
-__global__ void k_gen_links(Geom g, double2 *ud, double eps, uint32_t k0, uint32_t k1, int antiperiodic) {
+// (modules/uflds/uflds.c:307-335), and with phase angles theta the spatial
+// links U(x,k) get the factor exp(i theta[k-1]/N[k]) (uflds.c:249-300).
+struct LinkPhase {
+  double re[3], im[3];
+  int on;
+};
+
+bool spatial_phases(const Ctx &c, double pr[3], double pi[3]) {
+  bool on = false;
+  for (int k = 0; k < 3; k++) {
+    const double p = c.theta[k] / (double)c.g.L[k + 1];
+    pr[k] = cos(p);
+    pi[k] = sin(p);
+    on |= p != 0.0;
+  }
+  return on;
+}
+
+__global__ void k_gen_links(Geom g, double2 *ud, double eps, uint32_t k0, uint32_t k1, int antiperiodic,
+                            LinkPhase ph) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 4 * g.vol) return;
   int d = i >> 2, mu = i & 3;
@@ -158,14 +176,23 @@ __global__ void k_gen_links(Geom g, double2 *ud, double eps, uint32_t k0, uint32
   su3_exp(M, U);
   double sg = (antiperiodic && mu == 0 && x0 == g.L[0] - 1) ? -1.0 : 1.0;
   double2 *dst = ud + ((size_t)chunk * 4 + mu) * 9 * g.vbh + s;
-  for (int k = 0; k < 9; k++) dst[(size_t)k * g.vbh] = make_double2(sg * U[2 * k], sg * U[2 * k + 1]);
+  if (ph.on && mu > 0) {
+    const double pr = ph.re[mu - 1], pi = ph.im[mu - 1];
+    for (int k = 0; k < 9; k++)
+      dst[(size_t)k * g.vbh] = make_double2(U[2 * k] * pr - U[2 * k + 1] * pi, U[2 * k] * pi + U[2 * k + 1] * pr);
+  } else {
+    for (int k = 0; k < 9; k++) dst[(size_t)k * g.vbh] = make_double2(sg * U[2 * k], sg * U[2 * k + 1]);
+  }
 }
 
 int gen_links(Ctx &c, double eps, uint64_t seed, cudaStream_t st) {
   size_t n = (size_t)c.g.vol * 36 * sizeof(double2);
   if (!c.ud && cudaMalloc(&c.ud, n) != cudaSuccess) return fail("out of device memory (gauge field)");
   int t = 128, m = 4 * c.g.vol;
-  k_gen_links<<<(m + t - 1) / t, t, 0, st>>>(c.g, c.ud, eps, (uint32_t)seed, (uint32_t)(seed >> 32), c.bc == 3);
+  LinkPhase ph;
+  ph.on = spatial_phases(c, ph.re, ph.im);
+  k_gen_links<<<(m + t - 1) / t, t, 0, st>>>(c.g, c.ud, eps, (uint32_t)seed, (uint32_t)(seed >> 32), c.bc == 3,
+                                              ph);
   if (cudaGetLastError() != cudaSuccess) return fail("gen_links: launch failed");
   c.have_ud = true;
   return links_refresh_f32(c, st);

@@ -101,6 +101,7 @@ struct Ctx {
   // parameters
   double csw = 0.0, m0 = 0.0;
   int bc = 3, eoflg = 0;
+  double theta[3] = {0.0, 0.0, 0.0};   // spatial phase angles of set_bc_parms
   int isw = 0;                  // SW term: 0 traditional, 1 exponential
   int isolv = 1, nmr = 4, ncy = 5;
   bool sap_set = false;
@@ -197,6 +198,9 @@ int apply_swinv_ref_layout(int vol, double mu, const void *m, const void *s, voi
                            cudaStream_t st);
 
 // fields.cu
+// exp(i theta[k]/N[k+1]) of the spatial links (set_phase, uflds.c:249-276);
+// true when an angle is non-zero
+bool spatial_phases(const Ctx &c, double pr[3], double pi[3]);
 int gen_links(Ctx &c, double eps, uint64_t seed, cudaStream_t st);
 int gen_spinor(const Ctx &c, int prec, void *dev, double sigma, uint64_t seed, cudaStream_t st);
 

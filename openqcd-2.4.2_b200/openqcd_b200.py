@@ -46,6 +46,7 @@ _SIGS = {
     "b200_set_lat_parms": (C.c_int, [C.c_double]),
     "b200_set_sw_type": (C.c_int, [C.c_int]),
     "b200_set_bc_parms": (C.c_int, [C.c_int]),
+    "b200_set_bc_theta": (C.c_int, [C.c_void_p]),
     "b200_set_sw_parms": (C.c_int, [C.c_double]),
     "b200_set_tm_parms": (C.c_int, [C.c_int]),
     "b200_set_sap_parms": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
@@ -258,6 +259,13 @@ def set_parms(csw, m0, eoflg=0, bc=3, isw=0):
     check(L.b200_set_bc_parms(bc))
     check(L.b200_set_sw_parms(m0))
     check(L.b200_set_tm_parms(eoflg))
+
+
+def set_bc_theta(theta):
+    """spatial phase angles of set_bc_parms (applied to fields made on the
+    device or read from files)"""
+    t = np.ascontiguousarray(theta, dtype=np.float64)
+    return check(lib().b200_set_bc_theta(_ptr(t)))
 
 
 def set_sap_parms(bs, isolv, nmr, ncy):

@@ -63,13 +63,24 @@ static void need_ws(int n, int nd)
    if (nd > nwsd) { alloc_wsd(nd); nwsd = nd; }
 }
 
+static double bc_theta[3] = {0.0, 0.0, 0.0};
+
+/* The spatial phase angles theta of set_bc_parms (flags/lat_parms.c), taken
+ * by the first ref_init call of the process; set_ud_phase() then multiplies
+ * U(x,k) by exp(i theta[k-1]/N[k]) (modules/uflds/uflds.c:249-300). */
+void ref_set_theta(double t0, double t1, double t2)
+{
+   bc_theta[0] = t0; bc_theta[1] = t1; bc_theta[2] = t2;
+}
+
 /* Geometry, parameter data base and random-number generator.  Must be called
  * once per process before any other ref_ function. */
 void ref_init_isw(int bc, int seed, double csw, double m0, int eoflg, int isw)
 {
    ENTER();
    int provided;
-   double phi[2] = {0.0, 0.0}, phip[2] = {0.0, 0.0}, theta[3] = {0.0, 0.0, 0.0};
+   double phi[2] = {0.0, 0.0}, phip[2] = {0.0, 0.0}, theta[3];
+   theta[0] = bc_theta[0]; theta[1] = bc_theta[1]; theta[2] = bc_theta[2];
 
    if (!initialised)
    {

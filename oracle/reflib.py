@@ -95,7 +95,12 @@ class RefLib:
     def _p(a):
         return a.ctypes.data_as(C.c_void_p)
 
-    def init(self, bc=3, seed=1234, csw=1.5, m0=0.0, eoflg=0, isw=0):
+    def init(self, bc=3, seed=1234, csw=1.5, m0=0.0, eoflg=0, isw=0, theta=None):
+        """theta: the spatial phase angles of set_bc_parms (taken by the
+        first init of a library instance only)"""
+        if theta is not None:
+            self.lib.ref_set_theta.argtypes = [C.c_double] * 3
+            self.lib.ref_set_theta(*[float(t) for t in theta])
         self.lib.ref_init_isw.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
         self.lib.ref_init_isw(bc, seed, csw, m0, eoflg, isw)
 

@@ -30,12 +30,14 @@ class Setup:
     """Reference fields on lattice L (links exp(eps X), SW term), and the
     device library loaded with the same fields."""
 
-    def __init__(self, L, bs=(4, 4, 4, 4), eps=0.4, csw=1.5, m0=0.0, seed=1234, eoflg=0, portable=False, isw=0):
+    def __init__(self, L, bs=(4, 4, 4, 4), eps=0.4, csw=1.5, m0=0.0, seed=1234, eoflg=0, portable=False, isw=0,
+                 theta=None):
         assert reflib.ensure_built(L, portable=portable), "reference oracle library missing for %s" % (L,)
-        # the exponential SW type needs its own instance of the reference
-        # (set_lat_parms is called once per instance)
-        self.ref = reflib.RefLib(L, portable=portable, private=isw != 0)
-        self.ref.init(bc=3, seed=seed, csw=csw, m0=m0, eoflg=eoflg, isw=isw)
+        # the exponential SW type and phase angles need their own instance
+        # of the reference (set_lat_parms and set_bc_parms are called once
+        # per instance)
+        self.ref = reflib.RefLib(L, portable=portable, private=isw != 0 or theta is not None)
+        self.ref.init(bc=3, seed=seed, csw=csw, m0=m0, eoflg=eoflg, isw=isw, theta=theta)
         self.ref.gen_links(eps, seed)
         assert self.ref.sw_term(0) == 0
         self.L = tuple(L)
@@ -46,6 +48,7 @@ class Setup:
         self.swd = self.ref.swd()
         qb.geometry(L, bs, self.ipt)
         qb.set_parms(csw, m0, eoflg, isw=isw)
+        qb.set_bc_theta(theta if theta is not None else (0.0, 0.0, 0.0))
         qb.upload_ud(self.ud)
         self.sw_fail = qb.upload_swd(self.swd)
 
