@@ -1151,11 +1151,14 @@ static void dfl_mop(Ctx &c, double mu, const void *rho, void *phi, void *chi, vo
   else dfl_ltl_gcr(c, mu, vd, vd, &ifail, status, st);
   dfl_prolong(c, vd, ws0, st);
   dfl_mark(c, 3);
-  void *const sv[1] = {ws0}, *const rv[1] = {chi}, *const bv[1] = {(void *)rho};
-  dirac_multi32(c, 1, (float)mu, sv, rv, bv, st);   // chi = rho - D ws0
+  // rho - D ws0, written where the SAP sequence reads its input
+  void *in = sap_input_field(c);
+  if (!in) in = chi;
+  void *const sv[1] = {ws0}, *const rv[1] = {in}, *const bv[1] = {(void *)rho};
+  dirac_multi32(c, 1, (float)mu, sv, rv, bv, st);
   dfl_mark(c, 5);
-  // SAP on chi, then chi = rho - (final residual), phi = SAP solution + ws0
-  sap_mop(c, (float)mu, c.isolv, c.nmr, c.ncy, chi, phi, chi, phib, st, rho, ws0);
+  // SAP on it, then chi = rho - (final residual), phi = SAP solution + ws0
+  sap_mop(c, (float)mu, c.isolv, c.nmr, c.ncy, in, phi, chi, phib, st, rho, ws0);
   dfl_mark(c, 4);
   lstat[0] += status[0];
   lstat[1] += status[1];

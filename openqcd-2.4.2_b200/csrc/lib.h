@@ -243,6 +243,10 @@ void flat_copy(Ctx &c, int pin, const void *x, int pout, void *y, size_t nsite);
 void flat_add_s2sd(Ctx &c, const void *s, void *sd, size_t nsite);
 void flat_diff_sd2s(Ctx &c, const void *a, const void *b, void *r, size_t nsite);
 void flat_diff(Ctx &c, int prec, const void *x, void *y, size_t nsite);
+// y = sum over l = 0..n-1 of (cre[l] + i cim[l]) x[l], FP32 fields, one pass
+// per 16 terms
+void la_lincomb32(const Ctx &c, void *y, int n, const float *cre, const float *cim, void *const *x,
+                  cudaStream_t st);
 
 // solver.cu: the GCR recursion over an abstract set of FP32/FP64 field
 // operations, so the same code serves device-layout fields (sap_gcr) and
@@ -257,6 +261,9 @@ struct KrylovOps {
   std::function<void(const void *, void *)> copy64to32;            // assign_sd2s
   std::function<void(const void *, void *)> add32to64;             // add_s2sd
   std::function<void(const void *, const void *, void *)> diff64to32;  // diff_sd2s
+  // y = sum of c[l] x[l], l = 0..n-1 in this order (optional: without it
+  // the recursion zeroes y and applies one axpy32 per term)
+  std::function<void(void *, int, const cplxf *, void *const *)> lincomb32;
 };
 double fgcr_core(const KrylovOps &o, int nkv, int nmx, int istop, double res, const void *eta, void *psi,
                  int *status, const std::function<void(const void *, void *)> &Dop,
@@ -357,6 +364,9 @@ int sap_storage_mode(Ctx &c);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
                cudaStream_t st);
+// field the captured SAP sequence reads its input from (null when CUDA
+// graphs are off); an rh written there is not copied again by sap_mop
+void *sap_input_field(Ctx &c);
 // psi = ncy cycles on rho = rh, then rho = rh - rho (the sap_gcr preconditioner)
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
             cudaStream_t st, const void *base = nullptr, const void *add = nullptr);

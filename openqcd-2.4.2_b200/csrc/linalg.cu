@@ -12,6 +12,7 @@
 // double (per thread, then a fixed tree in the block), then one block adds
 // the RB partials in double-double (Knuth's TwoSum), so results are
 // bit-identical from run to run.
+#include <cstring>
 #include "lib.h"
 
 namespace qcd {
@@ -347,6 +348,46 @@ void la_axpy(const Ctx &c, int prec, void *y, double ar, double ai, const void *
   Range r = range(c, prec, par);
   if (prec == 64) k_axpy_d<<<nblk(r.n), 256, 0, st>>>(r, (double2 *)y, ar, ai, (const double2 *)x);
   else k_axpy_f<<<nblk(r.n), 256, 0, st>>>(r, (float4 *)y, (float)ar, (float)ai, (const float4 *)x);
+}
+
+// y (+)= sum of c_l x_l over up to 16 terms, applied in the given order with
+// the arithmetic of k_axpy_f: the solution update of fgcr (update_psi,
+// fgcr.c:181) in one pass over the fields instead of one axpy per term
+struct LcTerms {
+  const float4 *x[16];
+  float2 c[16];
+};
+__global__ void k_lincomb_f(Range r, float4 *y, int nt, int acc, LcTerms t) {
+  const size_t i = blockIdx.x * (size_t)256 + threadIdx.x;
+  if (i >= r.n) return;
+  float4 b = acc ? y[r.beg + i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (int l = 0; l < nt; l++) {
+    const float4 a = t.x[l][r.beg + i];
+    const float ar = t.c[l].x, ai = t.c[l].y;
+    b.x += ar * a.x - ai * a.y;
+    b.y += ar * a.y + ai * a.x;
+    b.z += ar * a.z - ai * a.w;
+    b.w += ar * a.w + ai * a.z;
+  }
+  y[r.beg + i] = b;
+}
+void la_lincomb32(const Ctx &c, void *y, int n, const float *cre, const float *cim, void *const *x,
+                  cudaStream_t st) {
+  const Range r = range(c, 32, PAR_ALL);
+  if (n <= 0) {
+    la_zero(c, 32, y, PAR_ALL, st);
+    return;
+  }
+  for (int l0 = 0; l0 < n; l0 += 16) {
+    LcTerms t;
+    std::memset(&t, 0, sizeof(t));
+    const int nt = n - l0 < 16 ? n - l0 : 16;
+    for (int l = 0; l < nt; l++) {
+      t.x[l] = (const float4 *)x[l0 + l];
+      t.c[l] = make_float2(cre[l0 + l], cim[l0 + l]);
+    }
+    k_lincomb_f<<<nblk(r.n), 256, 0, st>>>(r, (float4 *)y, nt, l0 > 0, t);
+  }
 }
 
 // y = x - y

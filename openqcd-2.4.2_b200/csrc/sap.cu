@@ -825,6 +825,15 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
 // (zero the solution, ncy x [block solves, boundary updates] per colour) is
 // one graph per parameter set, replayed at every GCR step: rh is copied in
 // before the replay and the results copied out after it.
+// The field the captured SAP sequence reads its input from (null when CUDA
+// graphs are off): a caller that computes rh can write it there directly
+// and pass it as rh, which saves sap_mop the copy.
+void *sap_input_field(Ctx &c) {
+  if (!c.use_graphs) return nullptr;
+  if (!c.sap_fld[1] && cudaMalloc(&c.sap_fld[1], spinor_bytes(c, 32)) != cudaSuccess) return nullptr;
+  return c.sap_fld[1];
+}
+
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
             cudaStream_t st, const void *base, const void *add) {
   if (!base) base = rh;
@@ -850,7 +859,8 @@ int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void 
   key.variant = c.sap_variant[mode];
   key.ncy = ncy;
   key.a = sap_args(c, mu, nmr, mode, spsi, srho, sphi);
-  la_copy(c, 32, rh, 32, srho, PAR_ALL, st);
+  if (base == srho) return fail("sap_mop: an input in the SAP input field needs a separate base");
+  if (rh != srho) la_copy(c, 32, rh, 32, srho, PAR_ALL, st);
   const int rc = graph_run(c, &key, sizeof(key), st, [&]() {
     la_zero(c, 32, spsi, PAR_ALL, st);
     for (int n = 0; n < ncy; n++) sap_cycle_launch(c, key.a, isolv, mode, st);

@@ -75,8 +75,18 @@ double fgcr_core(const KrylovOps &o, int nkv, int nmx, int istop, double res, co
       cc[l].re = z.re * r;
       cc[l].im = z.im * r;
     }
-    o.zero32(rho);
-    for (int l = k; l >= 0; l--) o.axpy32(rho, cc[l].re, cc[l].im, phi[l]);
+    if (o.lincomb32) {
+      std::vector<cplxf> cl;
+      std::vector<void *> xl;
+      for (int l = k; l >= 0; l--) {
+        cl.push_back(cc[l]);
+        xl.push_back(phi[l]);
+      }
+      o.lincomb32(rho, k + 1, cl.data(), xl.data());
+    } else {
+      o.zero32(rho);
+      for (int l = k; l >= 0; l--) o.axpy32(rho, cc[l].re, cc[l].im, phi[l]);
+    }
     o.add32to64(rho, psi);
     Dop(psi, wrk);
     o.diff64to32(eta, wrk, rho);
@@ -116,6 +126,14 @@ KrylovOps dev_krylov_ops(Ctx &c) {
   };
   o.axpy32 = [&c, st](void *y, float ar, float ai, const void *x) { la_axpy(c, 32, y, ar, ai, x, PAR_ALL, st); };
   o.zero32 = [&c, st](void *x) { la_zero(c, 32, x, PAR_ALL, st); };
+  o.lincomb32 = [&c, st](void *y, int n, const cplxf *cl, void *const *x) {
+    std::vector<float> re(n), im(n);
+    for (int l = 0; l < n; l++) {
+      re[l] = cl[l].re;
+      im[l] = cl[l].im;
+    }
+    la_lincomb32(c, y, n, re.data(), im.data(), x, st);
+  };
   o.zero64 = [&c, st](void *x) { la_zero(c, 64, x, PAR_ALL, st); };
   o.copy64to32 = [&c, st](const void *x, void *y) { la_copy(c, 64, x, 32, y, PAR_ALL, st); };
   o.add32to64 = [&c, st](const void *s, void *d) { la_add_s2sd(c, s, d, PAR_ALL, st); };

@@ -701,21 +701,17 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       if (ltl_gcr_b(c, mu[0], na, (const double2 *const *)v.data(), v.data(), lf.data(), ls.data(), st)) return -1;
       dfl_prolong_b(c, na, (const double2 *const *)v.data(), w0.data(), st);
       dfl_mark(c, 3);
-      {
-        // ch = rho - D ws0 for all active systems, links and SW read once per four
-        std::vector<void *> chs(na), rhs(na);
-        for (int i = 0; i < na; i++) {
-          chs[i] = S[A[i]].chi[S[A[i]].k];
-          rhs[i] = S[A[i]].rho;
-        }
-        dirac_multi32(c, na, (float)mu[0], w0.data(), chs.data(), rhs.data(), st);
-      }
       for (int i = 0; i < na; i++) {
         SysState &y = S[A[i]];
         void *ph = y.phi[y.k], *ch = y.chi[y.k];
-        dfl_mark(c, 2);
-        // SAP on ch = rho - D ws0, then ch = rho - (final residual), ph += ws0
-        sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, ch, ph, ch, phib, st, y.rho, y.ws0);
+        // rho - D ws0, written where the SAP sequence reads its input
+        void *in = sap_input_field(c);
+        if (!in) in = ch;
+        void *const rv[1] = {in}, *const bv[1] = {y.rho};
+        dirac_multi32(c, 1, (float)mu[0], &w0[i], rv, bv, st);
+        dfl_mark(c, 3);
+        // SAP on it, then ch = rho - (final residual), ph += ws0
+        sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, in, ph, ch, phib, st, y.rho, y.ws0);
         dfl_mark(c, 4);
         y.lstat += ls[i];
       }
@@ -760,8 +756,15 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
           y.cc[l].re = z.re * rb;
           y.cc[l].im = z.im * rb;
         }
-        o.zero32(y.rho);
-        for (int l = k; l >= 0; l--) o.axpy32(y.rho, y.cc[l].re, y.cc[l].im, y.phi[l]);
+        {
+          std::vector<cplxf> cl;
+          std::vector<void *> xl;
+          for (int l = k; l >= 0; l--) {
+            cl.push_back(y.cc[l]);
+            xl.push_back(y.phi[l]);
+          }
+          o.lincomb32(y.rho, k + 1, cl.data(), xl.data());
+        }
         o.add32to64(y.rho, psi[r]);
         dirac_op<double>(c, 0, y.mu, psi[r], wrk, c.tmp64, st);
         o.diff64to32(y.rsd, wrk, y.rho);
