@@ -197,9 +197,13 @@ int b200_dev_dirac_multi(int n, float mu, void *const *s, void *const *r, void *
  * (for ncu --profile-from-start off). */
 int b200_profiler(int on);
 /* on != 0 (default): when every link satisfies the SU(3) relation
- * row3 = +-conj(row1 x row2), the even-odd SAP block solver reads FP32
- * links as their first two rows and rebuilds the third (no reference
- * counterpart; 2/3 of the link bytes, results equal to FP32 rounding). */
+ * row3 = conj(row1 x row2), with the sign flipped on the time links at
+ * x0 = N0-1 (the antiperiodic phase), the FP32 Dirac operators and the
+ * even-odd SAP solver (block solves and block-boundary hops) read FP32
+ * links as their first two rows and rebuild the third (no reference
+ * counterpart; 2/3 of the link bytes, results equal to FP32 rounding).
+ * Links with spatial phases (theta != 0) fail the check and are read in
+ * full. */
 int b200_set_sap_link12(int on);
 /* mode != 0 (default): the FP64 operators with an SW term (all but
  * Dwoe_dble and Dweo_dble) stage each tile's SW matrices in shared memory

@@ -108,7 +108,9 @@ __device__ __forceinline__ void store_spinor_cs(double2 *base, int chunk, int s,
 #endif
 constexpr int kDwUnroll = DW_UNROLL;
 
-template <typename R, int OPS, int PAR, int RHALF = 0, int THALF = 0>
+// L12 = 1 (FP32 only): the links are read as 12 reals (load_link12), the
+// time links at x0 = N0-1 with the boundary sign.
+template <typename R, int OPS, int PAR, int RHALF = 0, int THALF = 0, int L12 = 0>
 __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) dirac_kernel(Geom g, const void *__restrict__ s, const void *__restrict__ t,
                                                     void *r, const void *__restrict__ u,
                                                     const void *__restrict__ sw, const void *__restrict__ swinv,
@@ -145,19 +147,24 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
   if (OPS & (OP_HOP | OP_HOPSUB)) {
     spinor<R> h;
     szero(h);
+    const int x0 = x.n[0] * g.bs[0] + x.y[0];
 #pragma unroll kDwUnroll
     for (int mu = 0; mu < 4; mu++) {
       int c2, s2;
       site_nbr(g, x, mu, +1, c2, s2);
       {
         spinor<R> sp = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
-        su3<R> uu = Store<R>::load_link(u, chunk, mu, si, g.vbh);
+        su3<R> uu;
+        if constexpr (L12 != 0) uu = load_link12(u, chunk, mu, si, g.vbh, mu == 0 && x0 == g.L[0] - 1);
+        else uu = Store<R>::load_link(u, chunk, mu, si, g.vbh);
         hop_fwd<R>(mu, uu, sp, h);
       }
       site_nbr(g, x, mu, -1, c2, s2);
       {
         spinor<R> sm = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
-        su3<R> uu = Store<R>::load_link(u, c2, mu, s2, g.vbh);
+        su3<R> uu;
+        if constexpr (L12 != 0) uu = load_link12(u, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
+        else uu = Store<R>::load_link(u, c2, mu, s2, g.vbh);
         hop_bwd<R>(mu, uu, sm, h);
       }
     }
@@ -342,6 +349,13 @@ static void launch(const Ctx &c, const void *s, const void *t, void *r, R mu_e, 
   }
   int n = PAR == 2 ? c.g.vol : c.g.volh;
   int threads = 128;
+  if constexpr (sizeof(R) == 4 && (OPS & (OP_HOP | OP_HOPSUB)) != 0) {
+    if (const void *u12 = links12(const_cast<Ctx &>(c), st)) {
+      dirac_kernel<R, OPS, PAR, 0, 0, 1><<<(n + threads - 1) / threads, threads, 0, st>>>(
+          c.g, s, t, r, u12, sw, swinv, mu_e, mu_o, c.sched, nullptr);
+      return;
+    }
+  }
   dirac_kernel<R, OPS, PAR><<<(n + threads - 1) / threads, threads, 0, st>>>(c.g, s, t, r, u, sw, swinv, mu_e, mu_o,
                                                                            c.sched, nullptr);
 }
@@ -386,6 +400,13 @@ int dirac_dw_blocks(const Ctx &c, R mu, const void *s, void *r, const int *block
     const void *u = sizeof(R) == 8 ? (const void *)c.ud : (const void *)c.u32;
     const void *sw = sizeof(R) == 8 ? (const void *)c.swd : (const void *)c.sw32;
     const int threads = 128, n = nblk * c.g.vb;
+    if constexpr (sizeof(R) == 4) {
+      if (const void *u12 = links12(const_cast<Ctx &>(c), st)) {
+        dirac_kernel<R, OPS, 2, 0, 0, 1><<<(n + threads - 1) / threads, threads, 0, st>>>(
+            c.g, s, s, r, u12, sw, nullptr, mu, muo, blocks, nullptr);
+        return cudaGetLastError() == cudaSuccess ? 0 : -2;
+      }
+    }
     dirac_kernel<R, OPS, 2><<<(n + threads - 1) / threads, threads, 0, st>>>(c.g, s, s, r, u, sw, nullptr, mu, muo,
                                                                             blocks, nullptr);
   }
@@ -418,10 +439,17 @@ int dirac_multi32(const Ctx &c, int n, float mu, void *const *sv, void *const *r
   const float muo = c.eoflg ? 0.0f : mu;
   const int threads = 128, nn = c.g.vol;
   const unsigned nb = (unsigned)((nn + threads - 1) / threads);
+  const void *u12 = links12(const_cast<Ctx &>(c), st);
   for (int j = 0; j < n; j++) {
-    if (subv)
+    if (subv && u12)
+      dirac_kernel<float, OP_SW | OP_HOP | OP_SUB, 2, 0, 0, 1><<<nb, threads, 0, st>>>(
+          c.g, sv[j], sv[j], rv[j], u12, c.sw32, nullptr, mu, muo, c.sched, subv[j]);
+    else if (subv)
       dirac_kernel<float, OP_SW | OP_HOP | OP_SUB, 2><<<nb, threads, 0, st>>>(
           c.g, sv[j], sv[j], rv[j], c.u32, c.sw32, nullptr, mu, muo, c.sched, subv[j]);
+    else if (u12)
+      dirac_kernel<float, OP_SW | OP_HOP, 2, 0, 0, 1><<<nb, threads, 0, st>>>(c.g, sv[j], sv[j], rv[j], u12, c.sw32,
+                                                                             nullptr, mu, muo, c.sched, nullptr);
     else
       dirac_kernel<float, OP_SW | OP_HOP, 2><<<nb, threads, 0, st>>>(c.g, sv[j], sv[j], rv[j], c.u32, c.sw32, nullptr,
                                                                     mu, muo, c.sched, nullptr);

@@ -364,6 +364,9 @@ int sap_storage_mode(Ctx &c);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,
                cudaStream_t st);
+// the 12-real FP32 link copy (first two rows) when the 12-real reads are on
+// and every link passed the SU(3) check with its boundary sign, else null
+const void *links12(Ctx &c, cudaStream_t st);
 // field the captured SAP sequence reads its input from (null when CUDA
 // graphs are off); an rh written there is not copied again by sap_mop
 void *sap_input_field(Ctx &c);

@@ -279,6 +279,32 @@ template <> struct Store<float> {
   }
 };
 
+// FP32 link stored as its first two rows (12 reals, planes
+// ((chunk*4 + mu)*6 + k)*vbh + s); the third row is rebuilt as the complex
+// conjugate of the cross product of the first two, exact for SU(3), and
+// negated for a link that carries the antiperiodic time-boundary sign
+// (neg).  The library checks every link for this relation, with the sign
+// its position implies, before it reads 12-real links.
+__device__ __forceinline__ su3<float> load_link12(const void *base, int chunk, int mu, int s, int vbh, bool neg) {
+  const float2 *p = (const float2 *)base + ((size_t)chunk * 4 + mu) * 6 * vbh + s;
+  su3<float> r;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    const float2 v = __ldg(p + (size_t)k * vbh);
+    r.e[k] = mk<float>(v.x, v.y);
+  }
+  const float sg = neg ? -1.0f : 1.0f;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const int a = (j + 1) % 3, b = (j + 2) % 3;
+    const cpx<float> x1 = r.e[a], y2 = r.e[3 + b], x2 = r.e[b], y1 = r.e[3 + a];
+    const float re = x1.re * y2.re - x1.im * y2.im - (x2.re * y1.re - x2.im * y1.im);
+    const float im = x1.re * y2.im + x1.im * y2.re - (x2.re * y1.im + x2.im * y1.re);
+    r.e[6 + j] = mk<float>(sg * re, -sg * im);
+  }
+  return r;
+}
+
 // ---------------------------------------------------------------- Pauli 6x6
 // The Hermitian 6x6 matrix is packed as in the reference
 // (modules/sw_term/pauli_dble.c:1336-1442 and set_aa :1644-1675): u[0..5] the

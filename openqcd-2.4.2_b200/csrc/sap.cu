@@ -76,6 +76,10 @@ struct SapF32 {
   __device__ __forceinline__ static su3<float> link(const void *u, int chunk, int mu, int s, int vbh) {
     return Store<float>::load_link(u, chunk, mu, s, vbh);
   }
+  // a link of the block-boundary hops (18 reals: the time-boundary sign is stored)
+  __device__ __forceinline__ static su3<float> blink(const void *u, int chunk, int mu, int s, int vbh, bool) {
+    return link(u, chunk, mu, s, vbh);
+  }
   __device__ __forceinline__ static spinor<float> sw(const void *m, int chunk, int s, int vbh, float mu,
                                                      const spinor<float> &in) {
     return apply_sw_site<float>(m, chunk, s, vbh, mu, in);
@@ -100,6 +104,9 @@ struct SapF16 {
       r.e[k] = mk<float>(f.x, f.y);
     }
     return r;
+  }
+  __device__ __forceinline__ static su3<float> blink(const void *u, int chunk, int mu, int s, int vbh, bool) {
+    return link(u, chunk, mu, s, vbh);
   }
   __device__ __forceinline__ static spinor<float> sw(const void *m, int chunk, int s, int vbh, float mu,
                                                      const spinor<float> &in) {
@@ -128,8 +135,9 @@ struct SapF16 {
 // ((chunk*4 + mu)*6 + k)*vbh + s) and the third row rebuilt as the complex
 // conjugate of the cross product of the first two, exact for SU(3).  The
 // hops inside a block never use the time-boundary links that carry the
-// antiperiodic sign (a block does not wrap), and the library checks all
-// other links for the SU(3) relation before it selects this policy.
+// antiperiodic sign (a block does not wrap); the block-boundary hops give
+// the sign by position (load_link12).  The library checks every link for
+// the relation, with that sign, before it selects this policy.
 struct SapF32R {
   using T = float;
   static constexpr int NP = 24;
@@ -140,23 +148,11 @@ struct SapF32R {
     SapF32::sm_store(sm, ld, s, v);
   }
   __device__ __forceinline__ static su3<float> link(const void *u, int chunk, int mu, int s, int vbh) {
-    const float2 *p = (const float2 *)u + ((size_t)chunk * 4 + mu) * 6 * vbh + s;
-    su3<float> r;
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-      const float2 v = __ldg(p + (size_t)k * vbh);
-      r.e[k] = mk<float>(v.x, v.y);
-    }
-    // row 3 = conj(row 1 x row 2)
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      const int a = (j + 1) % 3, b = (j + 2) % 3;
-      const cpx<float> x1 = r.e[a], y2 = r.e[3 + b], x2 = r.e[b], y1 = r.e[3 + a];
-      const float re = x1.re * y2.re - x1.im * y2.im - (x2.re * y1.re - x2.im * y1.im);
-      const float im = x1.re * y2.im + x1.im * y2.re - (x2.re * y1.im + x2.im * y1.re);
-      r.e[6 + j] = mk<float>(re, -im);
-    }
-    return r;
+    return load_link12(u, chunk, mu, s, vbh, false);
+  }
+  // a link of the block-boundary hops, which may carry the time-boundary sign
+  __device__ __forceinline__ static su3<float> blink(const void *u, int chunk, int mu, int s, int vbh, bool neg) {
+    return load_link12(u, chunk, mu, s, vbh, neg);
   }
   __device__ __forceinline__ static spinor<float> sw(const void *m, int chunk, int s, int vbh, float mu,
                                                      const spinor<float> &in) {
@@ -496,6 +492,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
   Site x;
   site_decode(g, p, blk, s, x);
   const int chunk = p * g.nbl + blk;
+  const int x0 = x.n[0] * g.bs[0] + x.y[0];   // the time links at x0 = N0-1 carry the boundary sign
   spinor<float> hsum;
   szero(hsum);
   bool any = false;
@@ -505,7 +502,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
       int c2, s2;
       site_nbr(g, x, mu, +1, c2, s2);
       spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = P::link(a.ub, chunk, mu, s, g.vbh);
+      su3<float> uu = P::blink(a.ub, chunk, mu, s, g.vbh, mu == 0 && x0 == g.L[0] - 1);
       hop_fwd<float>(mu, uu, sp, hsum);
       any = true;
     }
@@ -513,7 +510,7 @@ __global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
       int c2, s2;
       site_nbr(g, x, mu, -1, c2, s2);
       spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = P::link(a.ub, c2, mu, s2, g.vbh);
+      su3<float> uu = P::blink(a.ub, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
       hop_bwd<float>(mu, uu, sm, hsum);
       any = true;
     }
@@ -568,12 +565,19 @@ static int sap_half_fields(Ctx &c, cudaStream_t st) {
 }
 
 // 12-real copies of the FP32 links (first two rows) and a check that every
-// link satisfies row3 = +-conj(row1 x row2) to FP32 accuracy (the sign is
-// the antiperiodic boundary phase); bad[0] counts links that do not.
-__global__ void k_links12(size_t nlink, const float2 *__restrict__ u32, float2 *u12, int vbh, int *bad) {
+// link satisfies row3 = conj(row1 x row2) to FP32 accuracy, with the sign
+// flipped on the time links at x0 = N0-1 (the antiperiodic boundary phase
+// of bc type 3); bad[0] counts links that do not.
+__global__ void k_links12(Geom g, size_t nlink, const float2 *__restrict__ u32, float2 *u12, int *bad) {
+  const int vbh = g.vbh;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= nlink) return;
   const size_t cm = i / vbh, s = i - cm * vbh;   // cm = chunk*4 + mu
+  const int chunk = (int)(cm >> 2), mu = (int)(cm & 3);
+  const int par = chunk >= g.nbl;
+  Site x;
+  site_decode(g, par, chunk - par * g.nbl, (int)s, x);
+  const bool neg = mu == 0 && x.n[0] * g.bs[0] + x.y[0] == g.L[0] - 1;
   const float2 *p = u32 + cm * 9 * vbh + s;
   float2 e[9];
 #pragma unroll
@@ -590,7 +594,7 @@ __global__ void k_links12(size_t nlink, const float2 *__restrict__ u32, float2 *
     dp = fmaxf(dp, fabsf(re - e[6 + j].x) + fabsf(im - e[6 + j].y));
     dm = fmaxf(dm, fabsf(re + e[6 + j].x) + fabsf(im + e[6 + j].y));
   }
-  if (fminf(dp, dm) > 1e-5f) atomicAdd(bad, 1);
+  if ((neg ? dm : dp) > 1e-5f) atomicAdd(bad, 1);
 }
 
 static int sap_link12_fields(Ctx &c, cudaStream_t st) {
@@ -601,7 +605,7 @@ static int sap_link12_fields(Ctx &c, cudaStream_t st) {
   int *bad = nullptr;
   if (cudaMallocAsync(&bad, sizeof(int), st) != cudaSuccess) return fail("out of device memory");
   cudaMemsetAsync(bad, 0, sizeof(int), st);
-  k_links12<<<(unsigned)((nlink + 255) / 256), 256, 0, st>>>(nlink, c.u32, (float2 *)c.u12, c.g.vbh, bad);
+  k_links12<<<(unsigned)((nlink + 255) / 256), 256, 0, st>>>(c.g, nlink, c.u32, (float2 *)c.u12, bad);
   int h = 0;
   cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(bad, st);
@@ -609,6 +613,14 @@ static int sap_link12_fields(Ctx &c, cudaStream_t st) {
   c.u12_ok = h == 0;
   c.u12_valid = true;
   return 0;
+}
+
+// The 12-real FP32 links when they may be read (on, and every link passed
+// the check), else null: the FP32 Dirac operators read them too.
+const void *links12(Ctx &c, cudaStream_t st) {
+  if (!c.sap_link12 || !c.u32) return nullptr;
+  if (sap_link12_fields(c, st)) return nullptr;
+  return c.u12_ok ? c.u12 : nullptr;
 }
 
 // storage mode of the even-odd block solver: 0 FP32, 1 FP16, 2 FP32 with
@@ -673,7 +685,7 @@ static SapArgs sap_args(Ctx &c, float mu, int nmr, int mode, void *psi, void *rh
   a.rho = (float4 *)rho;
   a.phi = (float4 *)phi;
   a.u = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
-  a.ub = half ? (const void *)c.u16 : (const void *)c.u32;
+  a.ub = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
   a.sw = half ? (const void *)c.sw16 : (const void *)c.sw32;
   a.swinv = half ? (const void *)c.sw16_inv : (const void *)c.sw32_inv;
   return a;
@@ -778,6 +790,7 @@ static void sap_cycle_launch(Ctx &c, SapArgs a, int isolv, int mode, cudaStream_
     a.colour = ic;
     launch_blocks(c, a, isolv, mode, st);
     if (mode == 1) k_sap_bnd<SapF16><<<nbnd, 128, 0, st>>>(a);
+    else if (mode == 2) k_sap_bnd<SapF32R><<<nbnd, 128, 0, st>>>(a);
     else k_sap_bnd<SapF32><<<nbnd, 128, 0, st>>>(a);
   }
 }
