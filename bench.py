@@ -537,8 +537,11 @@ def run_b200(args, d):
     r32 = qb.DevField(32)
     qb.time_dirac(32, "Dw", MU, s32, r32, 3)
     ms32 = qb.time_dirac(32, "Dw", MU, s32, r32, args.steps) / args.steps
-    extra["dw_f32"] = {"ms": ms32, "GBs": BYTES_PER_SITE[32] * vol / (ms32 / 1e3) / 1e9,
-                       "frac_of_peak": BYTES_PER_SITE[32] * vol / (ms32 / 1e3) / 1e9 / peak}
+    # 672 algorithmic bytes per site when the links are read as 12 reals
+    # (two rows, the third rebuilt), 768 with all 18
+    b32 = 672 if qb.links12_active() else BYTES_PER_SITE[32]
+    extra["dw_f32"] = {"ms": ms32, "GBs": b32 * vol / (ms32 / 1e3) / 1e9, "bytes_per_site": b32,
+                       "frac_of_peak": b32 * vol / (ms32 / 1e3) / 1e9 / peak}
     for op, bps in (("Dwhat", 1344), ):
         qb.time_dirac(64, op, MU, s, r, 3)
         m = qb.time_dirac(64, op, MU, s, r, args.steps) / args.steps

@@ -205,6 +205,9 @@ int b200_profiler(int on);
  * Links with spatial phases (theta != 0) fail the check and are read in
  * full. */
 int b200_set_sap_link12(int on);
+/* 1 when the FP32 operators read 12-real links for the current gauge field
+ * (on, and every link passed the check), 0 when they read 18 reals. */
+int b200_links12_active(void);
 /* mode != 0 (default): the FP64 operators with an SW term (all but
  * Dwoe_dble and Dweo_dble) stage each tile's SW matrices in shared memory
  * with bulk asynchronous copies; 0 reads them directly.  Same arithmetic,

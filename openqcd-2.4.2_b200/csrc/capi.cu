@@ -452,6 +452,12 @@ int b200_set_dw_staged(int mode) {
   return prev;
 }
 
+int b200_links12_active(void) {
+  Ctx &c = ctx();
+  if (check_ready(c) || need(c.have_ud, "no gauge field on the device")) return -1;
+  return qcd::links12(c, c.stream) != nullptr;
+}
+
 int b200_sap_tuning(int prec, int *variant, int *threads, float *ms) {
   Ctx &c = ctx();
   if (check_ready(c)) return -1;

@@ -47,6 +47,7 @@ _SIGS = {
     "b200_set_sw_type": (C.c_int, [C.c_int]),
     "b200_set_bc_parms": (C.c_int, [C.c_int]),
     "b200_set_bc_theta": (C.c_int, [C.c_void_p]),
+    "b200_links12_active": (C.c_int, []),
     "b200_set_sw_parms": (C.c_int, [C.c_double]),
     "b200_set_tm_parms": (C.c_int, [C.c_int]),
     "b200_set_sap_parms": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
@@ -279,6 +280,11 @@ def set_sap_prec(bits):
 
 def set_sap_link12(on):
     return check(lib().b200_set_sap_link12(1 if on else 0))
+
+
+def links12_active():
+    """True when the FP32 operators read 12-real links for the current field"""
+    return check(lib().b200_links12_active()) == 1
 
 
 def set_cuda_graphs(on):

@@ -66,6 +66,7 @@ def test_dirac_multi_link12(setup):
     r18, r12 = both(run)
     assert site_rel_err(r12, r18, setup.vol) <= 1e-6
     assert not np.array_equal(r12, r18)     # the 12-real reads were used
+    assert qb.links12_active()
 
 
 def test_sap_gcr_link12(setup):
@@ -88,6 +89,7 @@ def test_link12_check_rejects(setup):
         s = setup.source(26)
         r18, r12 = both(lambda: qb.dirac_ref("Dw", 32, MU, s))
         assert np.array_equal(r12, r18)
+        assert not qb.links12_active()
     finally:
         qb.upload_ud(setup.ud)
         qb.upload_swd(setup.swd)
