@@ -385,6 +385,12 @@ int b200_net_apply(const void *in, void *out, int half);
 /* loss |M r - e|^2/|e|^2 of one pair and its gradient with respect to the
  * real and imaginary parts of the weights (packed like the weights) */
 int b200_net_grad(const void *r, const void *e, double *loss, float *grad);
+/* mean loss and mean gradient over npairs pairs (one minibatch), and one
+ * Adam step with a given gradient: the two halves of a training step, for
+ * data-parallel training where the ranks sum their gradients in between
+ * (openqcd_b200.net_train_data_parallel) */
+int b200_net_batch_grad(int npairs, void *const *r, void *const *e, double *loss, float *grad);
+int b200_net_adam_step(const float *grad, float lr);
 /* steps of Adam on minibatches of `batch` of the npairs (r, e) pairs,
  * on the device; loss_hist[step] = minibatch loss (may be NULL) */
 int b200_net_train(int npairs, void *const *r, void *const *e, int steps, int batch, float lr,

@@ -43,6 +43,18 @@ int b200_net_train(int npairs, void *const *r, void *const *e, int steps, int ba
   return qcd::net_train(c, npairs, (const void *const *)r, (const void *const *)e, steps, batch, lr, seed, loss_hist);
 }
 
+int b200_net_batch_grad(int npairs, void *const *r, void *const *e, double *loss, float *grad) {
+  Ctx &c = ctx();
+  if (!c.ready) return fail("geometry not set (call b200_geometry first)");
+  return qcd::net_batch_grad(c, npairs, (const void *const *)r, (const void *const *)e, loss, grad);
+}
+
+int b200_net_adam_step(const float *grad, float lr) {
+  Ctx &c = ctx();
+  if (!c.ready) return fail("geometry not set (call b200_geometry first)");
+  return qcd::net_adam(c, grad, lr);
+}
+
 // Training pairs from the plain solver: r[k] a Gaussian source (FP32 copy),
 // e[k] = Dw(mu)^-1 r[k] from sap_gcr to relative residual res (FP32 copy).
 int b200_net_make_pairs(int npairs, void *const *r, void *const *e, double mu, double res,

@@ -316,6 +316,8 @@ int net_nweights();
 int net_init(Ctx &c, uint64_t seed, float scale);
 int net_apply(Ctx &c, const void *in, void *out, bool half, cudaStream_t st);
 int net_grad(Ctx &c, const void *r, const void *e, double *loss, float *grad);
+int net_batch_grad(Ctx &c, int npairs, const void *const *r, const void *const *e, double *loss, float *grad);
+int net_adam(Ctx &c, const float *grad, float lr);
 int net_train(Ctx &c, int npairs, const void *const *r, const void *const *e, int steps, int batch, float lr,
               uint64_t seed, float *loss_hist);
 void net_release(Ctx &c);

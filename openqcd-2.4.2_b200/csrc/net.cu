@@ -401,6 +401,32 @@ int net_grad(Ctx &c, const void *r, const void *e, double *loss, float *grad) {
   return 0;
 }
 
+// mean loss and mean gradient over npairs pairs (one minibatch; a rank of a
+// data-parallel training sums these over ranks before the Adam step)
+int net_batch_grad(Ctx &c, int npairs, const void *const *r, const void *const *e, double *loss, float *grad) {
+  NetState &n = c.net;
+  if (!n.ready) return fail("network: no weights");
+  if (!c.have_ud) return fail("network: no gauge field on the device");
+  if (npairs < 1) return fail("network: no pairs");
+  if (net_fields(c)) return -1;
+  cudaStream_t st = c.stream;
+  grad_zero(c, st);
+  double tot = 0.0;
+  for (int k = 0; k < npairs; k++) {
+    double l = 0.0;
+    if (net_pair_grad(c, r[k], e[k], 1.0 / npairs, &l, st)) return -1;
+    tot += l;
+  }
+  cudaStreamSynchronize(st);
+  std::vector<double> g[NLAY];
+  grad_read(c, g);
+  float *p = grad;
+  for (int l = 0; l < NLAY; l++)
+    for (size_t k = 0; k < g[l].size(); k++) *p++ = (float)g[l][k];
+  *loss = tot;
+  return 0;
+}
+
 // Adam (Kingma & Ba, 2015) on the real parameters
 static void adam_step(NetState &n, const std::vector<double> *g, float lr) {
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
@@ -413,6 +439,21 @@ static void adam_step(NetState &n, const std::vector<double> *g, float lr) {
       n.v[l][k] = b2 * n.v[l][k] + (1.0f - b2) * gk * gk;
       n.w[l][k] -= lr * (n.m[l][k] / c1) / (std::sqrt(n.v[l][k] / c2) + eps);
     }
+}
+
+// one Adam step with a given gradient (packed like the weights), then the
+// device copies of the weights
+int net_adam(Ctx &c, const float *grad, float lr) {
+  NetState &n = c.net;
+  if (!n.ready) return fail("network: no weights");
+  std::vector<double> g[NLAY];
+  const float *p = grad;
+  for (int l = 0; l < NLAY; l++) {
+    g[l].resize(n.w[l].size());
+    for (size_t k = 0; k < g[l].size(); k++) g[l][k] = *p++;
+  }
+  adam_step(n, g, lr);
+  return net_upload(c);
 }
 
 // steps of Adam on minibatches of `batch` pairs drawn from the npairs

@@ -156,6 +156,8 @@ _SIGS = {
     "b200_net_get_weights": (C.c_int, [C.c_void_p]),
     "b200_net_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "b200_net_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_net_batch_grad": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_net_adam_step": (C.c_int, [C.c_void_p, C.c_float]),
     "b200_net_train": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_ulonglong,
                                  C.c_void_p]),
     "b200_net_make_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_ulonglong]),
@@ -804,6 +806,74 @@ def net_grad(r, e):
     g = np.zeros(net_nweights(), dtype=np.float32)
     check(lib().b200_net_grad(r.ptr, e.ptr, C.byref(loss), _ptr(g)))
     return loss.value, g
+
+
+def net_batch_grad(rs, es):
+    """mean loss and mean gradient over the pairs (rs[k], es[k])"""
+    n = len(rs)
+    rp = (C.c_void_p * n)(*[x.ptr for x in rs])
+    ep = (C.c_void_p * n)(*[x.ptr for x in es])
+    loss = C.c_double(0.0)
+    g = np.zeros(net_nweights(), dtype=np.float32)
+    check(lib().b200_net_batch_grad(n, rp, ep, C.byref(loss), _ptr(g)))
+    return loss.value, g
+
+
+def net_adam_step(grad, lr):
+    g = np.ascontiguousarray(grad, dtype=np.float32)
+    return check(lib().b200_net_adam_step(_ptr(g), lr))
+
+
+def data_parallel_steps(grad_fn, step_fn, npairs, steps, batch, lr, seed, allreduce, world):
+    """The loop of data-parallel training, independent of where the
+    gradients come from.  Per step this rank draws `batch` of its own
+    npairs pairs (generator seeded with `seed`, which differs between
+    ranks), grad_fn(indices) -> (mean loss, mean gradient); the loss and
+    gradient are summed over the ranks by allreduce (a float64 vector in,
+    the sum out) and divided by `world`, and step_fn(gradient, lr) applies
+    the same optimiser step on every rank, so the weights stay identical.
+    Returns the per-step mean loss over all ranks."""
+    rng = np.random.default_rng(seed)
+    hist = []
+    for _ in range(steps):
+        idx = rng.integers(0, npairs, size=batch)
+        loss, g = grad_fn(idx)
+        buf = np.concatenate([[loss], np.asarray(g, dtype=np.float64)])
+        buf = np.asarray(allreduce(buf), dtype=np.float64) / world
+        step_fn(buf[1:].astype(np.float32), lr)
+        hist.append(float(buf[0]))
+    return hist
+
+
+def net_train_data_parallel(rs, es, steps, batch, lr, seed=1, group=None):
+    """Data-parallel training of the network over the ranks of a
+    torch.distributed process group (one process per GPU): every rank holds
+    its own training pairs (e.g. from its own gauge field) and draws its
+    minibatches with the seed seed + rank; the gradients are all-reduced
+    (SUM, then divided by the number of ranks) and every rank applies the
+    same Adam step.  Without an initialised process group it is plain
+    training on this rank's pairs.  Returns the per-step mean loss."""
+    try:
+        import torch
+        import torch.distributed as dist
+        on = dist.is_available() and dist.is_initialized()
+    except ImportError:
+        on = False
+    rank = dist.get_rank(group) if on else 0
+    world = dist.get_world_size(group) if on else 1
+
+    def allreduce(v):
+        if not on:
+            return v
+        dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+        t = torch.from_numpy(np.ascontiguousarray(v)).to(dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return t.cpu().numpy()
+
+    def grad_fn(idx):
+        return net_batch_grad([rs[i] for i in idx], [es[i] for i in idx])
+
+    return data_parallel_steps(grad_fn, net_adam_step, len(rs), steps, batch, lr, seed + rank, allreduce, world)
 
 
 def net_train(rs, es, steps, batch, lr, seed=1):
