@@ -31,12 +31,12 @@ class Setup:
     device library loaded with the same fields."""
 
     def __init__(self, L, bs=(4, 4, 4, 4), eps=0.4, csw=1.5, m0=0.0, seed=1234, eoflg=0, portable=False, isw=0,
-                 theta=None):
+                 theta=None, private=False):
         assert reflib.ensure_built(L, portable=portable), "reference oracle library missing for %s" % (L,)
         # the exponential SW type and phase angles need their own instance
         # of the reference (set_lat_parms and set_bc_parms are called once
         # per instance)
-        self.ref = reflib.RefLib(L, portable=portable, private=isw != 0 or theta is not None)
+        self.ref = reflib.RefLib(L, portable=portable, private=private or isw != 0 or theta is not None)
         self.ref.init(bc=3, seed=seed, csw=csw, m0=m0, eoflg=eoflg, isw=isw, theta=theta)
         self.ref.gen_links(eps, seed)
         assert self.ref.sw_term(0) == 0
