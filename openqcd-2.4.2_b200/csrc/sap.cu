@@ -37,7 +37,7 @@ struct SapArgs {
   int eoflg;
   float4 *psi, *rho, *phi;
   const void *u;        // links as the block solver's policy reads them
-  const void *ub;       // links for the block-boundary hops (FP32 or FP16, 18 reals)
+  const void *ub;       // links for the block-boundary hops (as u, but 18-real FP32 in the FP32 mode)
   const void *sw, *swinv;
 };
 
