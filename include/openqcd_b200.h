@@ -319,6 +319,12 @@ int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status);
 /* Aw_dble.c:306 */ void Aweo_dble(complex_dble *v, complex_dble *w);
 /* Aw.c:122 */ void Aw(complex *v, complex *w);
 /* Aw.c:361 */ void Awhat(complex *v, complex *w);
+/* Aw.c:202-359, the FP32 even-odd pieces (after set_Awhat): w_e = Aee^-1 v_e,
+ * w_o = Aoo^-1 v_o, w_o = Aoe v_e, w_e = w_e - Aeo v_o */
+/* Aw.c:202 */ void Aweeinv(complex *v, complex *w);
+/* Aw.c:234 */ void Awooinv(complex *v, complex *w);
+/* Aw.c:266 */ void Awoe(complex *v, complex *w);
+/* Aw.c:306 */ void Aweo(complex *v, complex *w);
 /* Global-mode ("little-little") deflation of the even-odd little system:
  * the little modes are the modes of the last dfl_subspace()/dfl_modes()
  * call in the block basis; set_ltl_modes returns 1 if the little-little

@@ -287,7 +287,10 @@ static void little_apply(int which, complex_dble *v, complex_dble *w) {
   Ctx &c = ctx();
   if (qcd::dfl_ready(c)) return;
   qcd::DflState &d = c.dfl;
-  if (!d.aw_valid || (which == 1 && !d.awhat_valid)) { fail("Aw: the little operator is not set (set_Aw / set_Awhat)"); return; }
+  // Aw, Awoe, Aweo need the little operator, Awhat, Aweeinv, Awooinv the
+  // even-odd preconditioned one (Aw.c:44-48)
+  const bool hat = which >= 1 && which <= 3;
+  if (!d.aw_valid || (hat && !d.awhat_valid)) { fail("Aw: the little operator is not set (set_Aw / set_Awhat)"); return; }
   double2 *a = qcd::lbuf(c, 0), *b = qcd::lbuf(c, 1), *t = qcd::lbuf(c, 2);
   if (!a || !b || !t) return;
   size_t nb = (size_t)d.nv * sizeof(double2);
@@ -377,6 +380,10 @@ static void little_f32(int which, complex *v, complex *w) {
 
 void Aw(complex *v, complex *w) { little_f32(0, v, w); }
 void Awhat(complex *v, complex *w) { little_f32(1, v, w); }
+void Aweeinv(complex *v, complex *w) { little_f32(2, v, w); }
+void Awooinv(complex *v, complex *w) { little_f32(3, v, w); }
+void Awoe(complex *v, complex *w) { little_f32(4, v, w); }
+void Aweo(complex *v, complex *w) { little_f32(5, v, w); }
 
 // ---- global-mode deflation (ltl_modes.c)
 int set_ltl_modes(void) {

@@ -893,17 +893,27 @@ const double *ltl_matrix_host(Ctx &c) {
 }
 
 // FP32 little operators on device little vectors (complex floats): Aw
-// (Aw.c:122, all blocks) and Awhat (Aw.c:361, even blocks)
+// (Aw.c:122, all blocks), Awhat (Aw.c:361, even blocks) and the even-odd
+// pieces of Aw.c:202-359 -- 2 Aweeinv (w_e = Aee^-1 v_e), 3 Awooinv
+// (w_o = Aoo^-1 v_o), 4 Awoe (w_o = Aoe v_e), 5 Aweo (w_e -= Aeo v_o)
 int little32_apply(Ctx &c, int which, const float2 *v, float2 *w) {
   DflState &d = c.dfl;
   if (ensure_base(c)) return -1;
   LtlRef &r = *lr(c);
+  const int nbh = d.nb / 2;
   if (which == 0) {
     little32(0, c, 0, d.nb, d.Ablk, d.Ahop, false, v, nullptr, w);
-  } else {
-    const int nbh = d.nb / 2;
+  } else if (which == 1) {
     little32(1, c, nbh, nbh, nullptr, d.Mhop, false, v, nullptr, r.t32);
     little32(2, c, 0, nbh, nullptr, d.Mhop, false, v, r.t32, w);
+  } else if (which == 2) {
+    little32(3, c, 0, nbh, d.Ainv, nullptr, false, v, nullptr, w);
+  } else if (which == 3) {
+    little32(3, c, nbh, nbh, d.Ainv, nullptr, false, v, nullptr, w);
+  } else if (which == 4) {
+    little32(1, c, nbh, nbh, nullptr, d.Ahop, false, v, nullptr, w);
+  } else {
+    little32(2, c, 0, nbh, nullptr, d.Ahop, false, w, v, w);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : fail("little operator: launch failed");
 }

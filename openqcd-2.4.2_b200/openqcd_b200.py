@@ -110,6 +110,10 @@ _SIGS = {
     "Aweo_dble": (None, [C.c_void_p, C.c_void_p]),
     "Aw": (None, [C.c_void_p, C.c_void_p]),
     "Awhat": (None, [C.c_void_p, C.c_void_p]),
+    "Aweeinv": (None, [C.c_void_p, C.c_void_p]),
+    "Awooinv": (None, [C.c_void_p, C.c_void_p]),
+    "Awoe": (None, [C.c_void_p, C.c_void_p]),
+    "Aweo": (None, [C.c_void_p, C.c_void_p]),
     "set_ltl_modes": (C.c_int, []),
     "ltl_matrix": (C.c_void_p, []),
     "dfl_Lvd": (None, [C.c_void_p]),
@@ -677,17 +681,20 @@ def little_eo(name, mu, v, w=None):
     return w, f
 
 
+LITTLE32 = ["Aw", "Awhat", "Aweeinv", "Awooinv", "Awoe", "Aweo"]
+
+
 def little32(which, mu, v, w=None):
-    """FP32 little operators: 0 set_Aw(mu), Aw; 1 set_Awhat(mu), Awhat
-    (little vectors of nv complex floats as float32 arrays)."""
+    """FP32 little operators: 0 set_Aw(mu), Aw; 1..5 set_Awhat(mu), then
+    Awhat, Aweeinv, Awooinv, Awoe, Aweo (little vectors of nv complex floats
+    as float32 arrays)."""
     v = np.ascontiguousarray(v, dtype=np.float32)
     w = np.zeros_like(v) if w is None else np.array(w, dtype=np.float32, copy=True)
     if which == 0:
         _void(lib().set_Aw, mu)
-        _void(lib().Aw, _ptr(v), _ptr(w))
     else:
         check(lib().set_Awhat(mu))
-        _void(lib().Awhat, _ptr(v), _ptr(w))
+    _void(getattr(lib(), LITTLE32[which]), _ptr(v), _ptr(w))
     return w
 
 

@@ -579,7 +579,11 @@ int ref_little32(int which, double mu, const float *v, float *w)
    else
    {
       ifail = set_Awhat(mu);
-      Awhat(a, b);
+      if (which == 1) Awhat(a, b);
+      else if (which == 2) Aweeinv(a, b);
+      else if (which == 3) Awooinv(a, b);
+      else if (which == 4) Awoe(a, b);
+      else Aweo(a, b);
    }
    memcpy(w, b, nb);
    free(a);

@@ -57,7 +57,7 @@ def test_little_eo_pieces(setup, name):
     assert rel_norm_err(dev, ref) <= 1e-12
 
 
-@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("which", [0, 1, 2, 3, 4, 5], ids=["Aw", "Awhat", "Aweeinv", "Awooinv", "Awoe", "Aweo"])
 def test_little_fp32(setup, which):
     v, w0 = rvec(setup, np.float32), rvec(setup, np.float32)
     ref = setup.ref.little32(which, MU, v, w0)
