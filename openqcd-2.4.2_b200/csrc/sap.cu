@@ -481,8 +481,14 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
 // rho(y) -= D_{y,x} phi(x) for every site y of a block of colour 1-c and every
 // neighbour x of y in a (colour c) block: the block-boundary hop of the
 // reference's Dw_bnd/sap_com, as a gather.
+// 8 resident CTAs per SM (64 registers): two SAP cycles at 48^3x96 with 6^4
+// blocks 17.86 ms against 17.99 ms with the compiler's choice (80-87
+// registers, 6 CTAs); 12 CTAs (40 registers) spilled
+#ifndef SAP_BND_MINB
+#define SAP_BND_MINB 8
+#endif
 template <class P>
-__global__ void __launch_bounds__(128) k_sap_bnd(SapArgs a) {
+__global__ void __launch_bounds__(128, SAP_BND_MINB) k_sap_bnd(SapArgs a) {
   const Geom &g = a.g;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= (size_t)(g.nbl / 2) * g.vb) return;
