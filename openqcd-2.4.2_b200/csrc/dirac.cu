@@ -96,12 +96,14 @@ __device__ __forceinline__ void store_spinor_cs(double2 *base, int chunk, int s,
 // only the odd chunks (chunk index counted from the first odd chunk).
 // Resident CTAs per SM asked of the compiler: the FP64 kernel keeps 255
 // registers (more CTAs made it spill and run slower), the FP32 kernel runs
-// 3 CTAs per SM (14 % faster than 2 on B200).
+// 4 CTAs per SM at 128 registers (3 CTAs were 14 % faster than 2 on B200;
+// with the 12-real link reads 4 are 5-7 % faster than 3: Dw 0.3006 against
+// 0.3218 ms at 32^3x64, 1.58 against 1.67 ms at 48^3x96).
 #ifndef DW_MINB64
 #define DW_MINB64 1
 #endif
 #ifndef DW_MINB32
-#define DW_MINB32 3
+#define DW_MINB32 4
 #endif
 #ifndef DW_UNROLL
 #define DW_UNROLL 4
