@@ -209,8 +209,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
 // latency at the CTA start is exposed and the L2 traffic hardly fell, L1
 // already caught those reads); three CTAs per SM (168 registers, 0.91 ms);
 // an L2 bulk prefetch (cp.async.bulk.prefetch.L2) of the tile's links and
-// other-parity spinors at the CTA start (0.72 ms against 0.66 ms).
-constexpr int DWT_TS = 128;
+// other-parity spinors at the CTA start (0.72 ms against 0.66 ms); 64-site
+// tiles at four CTAs per SM (the same warps per SM: 0.670 against 0.667 ms,
+// and the same under the power cap).
+#ifndef DWT_TILE
+#define DWT_TILE 128
+#endif
+constexpr int DWT_TS = DWT_TILE;
 #ifndef DWT_MINB
 #define DWT_MINB 2
 #endif
