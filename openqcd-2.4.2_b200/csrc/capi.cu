@@ -80,28 +80,34 @@ static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr
   const size_t site = 24 * sizeof(R);
   const int nsl = (int)c.slab.size();
   if ((!c.st_in && cudaStreamCreateWithFlags(&c.st_in, cudaStreamNonBlocking) != cudaSuccess) ||
-      (!c.st_out && cudaStreamCreateWithFlags(&c.st_out, cudaStreamNonBlocking) != cudaSuccess))
+      (!c.st_out && cudaStreamCreateWithFlags(&c.st_out, cudaStreamNonBlocking) != cudaSuccess) ||
+      (!c.st_cv && cudaStreamCreateWithFlags(&c.st_cv, cudaStreamNonBlocking) != cudaSuccess))
     return fail("no CUDA stream for the pipelined transfers");
-  while ((int)c.slab_ev.size() < 2 * nsl + 1) {
+  while ((int)c.slab_ev.size() < 3 * nsl + 1) {
     cudaEvent_t e;
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail("no CUDA event");
     c.slab_ev.push_back(e);
   }
-  cudaEvent_t *ev_in = c.slab_ev.data(), *ev_out = ev_in + nsl, ev0 = ev_in[2 * nsl];
+  cudaEvent_t *ev_in = c.slab_ev.data(), *ev_out = ev_in + nsl, *ev_cp = ev_in + 2 * nsl, ev0 = ev_in[3 * nsl];
   cudaEventRecord(ev0, c.stream);
   cudaStreamWaitEvent(c.st_in, ev0, 0);
+  cudaStreamWaitEvent(c.st_cv, ev0, 0);
   cudaStreamWaitEvent(c.st_out, ev0, 0);
+  // the host-to-device copies run back to back on st_in; each slab's
+  // conversion to the device layout follows on st_cv
   auto h2d = [&](int k) {
     const Slab &sb = c.slab[k];
     for (int p = 0; p < 2; p++) {
       const size_t o = (size_t)sb.q0[p] * site, n = (size_t)(sb.q1[p] - sb.q0[p]) * site;
       cudaMemcpyAsync(st_in + o, (const char *)s + o, n, cudaMemcpyHostToDevice, c.st_in);
     }
+    cudaEventRecord(ev_cp[k], c.st_in);
+    cudaStreamWaitEvent(c.st_cv, ev_cp[k], 0);
     for (int p = 0; p < 2; p++) {
       const int d0 = (p * c.g.nbl + sb.b0) * c.g.vbh, nd = (sb.b1 - sb.b0) * c.g.vbh;
-      spinor_from_ref_range(c, prec, st_in, fs, d0, nd, c.st_in);
+      spinor_from_ref_range(c, prec, st_in, fs, d0, nd, c.st_cv);
     }
-    cudaEventRecord(ev_in[k], c.st_in);
+    cudaEventRecord(ev_in[k], c.st_cv);
   };
   auto comp = [&](int k, int after) {
     const Slab &sb = c.slab[k];
@@ -128,8 +134,8 @@ static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr
   comp(nsl - 2, nsl - 2);
   comp(nsl - 1, nsl - 2);
   const cudaError_t e1 = cudaStreamSynchronize(c.st_out), e2 = cudaStreamSynchronize(c.stream),
-                    e3 = cudaStreamSynchronize(c.st_in);
-  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+                    e3 = cudaStreamSynchronize(c.st_in), e4 = cudaStreamSynchronize(c.st_cv);
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
     return fail(std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError()));
   return 0;
 }

@@ -94,7 +94,7 @@ struct Ctx {
   // has no contiguous slabs), the identity block list, the copy streams
   std::vector<Slab> slab;
   int *d_ident = nullptr;
-  cudaStream_t st_in = nullptr, st_out = nullptr;
+  cudaStream_t st_in = nullptr, st_out = nullptr, st_cv = nullptr;
   std::vector<cudaEvent_t> slab_ev;
   int pipeline = 1;             // pipelined host transfers of Dw / Dw_dble when possible
 
