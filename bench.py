@@ -140,6 +140,130 @@ class Dist:
             self.dist.destroy_process_group()
 
 
+FIELD_SEED, SOURCE_SEED = 20251203, 7
+
+
+def expiq(Q):
+    """exp(iQ) for traceless Hermitian 3x3 matrices Q[..., 3, 3], by the
+    Cayley-Hamilton closed form of Morningstar and Peardon (Phys. Rev. D 69
+    (2004) 054501, eqs. 19-34): exp(iQ) = f0 + f1 Q + f2 Q^2 with the f_j from
+    the invariants c0 = det Q, c1 = tr Q^2 / 2; c0 < 0 through
+    f_j(-c0) = (-1)^j conj(f_j(c0))."""
+    Q2 = Q @ Q
+    c1 = 0.5 * np.einsum("...ii->...", Q2).real
+    c0 = np.einsum("...ij,...ji->...", Q, Q2).real / 3.0
+    neg = c0 < 0
+    c0 = np.abs(c0)
+    c1s = np.maximum(c1, 1e-300)
+    c0max = 2.0 * (c1s / 3.0) ** 1.5
+    theta = np.arccos(np.clip(c0 / c0max, -1.0, 1.0))
+    u = np.sqrt(c1s / 3.0) * np.cos(theta / 3.0)
+    w = np.sqrt(c1s) * np.sin(theta / 3.0)
+    w2 = w * w
+    small = np.abs(w) < 0.05
+    xi0 = np.where(small, 1.0 - w2 / 6.0 * (1.0 - w2 / 20.0 * (1.0 - w2 / 42.0)),
+                   np.sin(w) / np.where(small, 1.0, w))
+    u2 = u * u
+    e2iu = np.exp(2j * u)
+    emiu = np.exp(-1j * u)
+    cw = np.cos(w)
+    h0 = (u2 - w2) * e2iu + emiu * (8.0 * u2 * cw + 2j * u * (3.0 * u2 + w2) * xi0)
+    h1 = 2.0 * u * e2iu - emiu * (2.0 * u * cw - 1j * (3.0 * u2 - w2) * xi0)
+    h2 = e2iu - emiu * (cw + 3j * u * xi0)
+    den = 9.0 * u2 - w2
+    f0, f1, f2 = h0 / den, h1 / den, h2 / den
+    f0 = np.where(neg, np.conj(f0), f0)
+    f1 = np.where(neg, -np.conj(f1), f1)
+    f2 = np.where(neg, np.conj(f2), f2)
+    U = f1[..., None, None] * Q + f2[..., None, None] * Q2
+    for i in range(3):
+        U[..., i, i] += f0
+    return U
+
+
+def synthetic_links(L, eps, seed):
+    """U(x, mu) = exp(i eps H), H = sum_a c_a T_a with c_a ~ N(0, 1) (a
+    Gaussian traceless Hermitian matrix, unit variance per su(3) generator),
+    for every site x (lexicographic, x3 fastest) and direction mu; the time
+    links at x0 = L0 - 1 carry the factor -1 of the antiperiodic quark
+    boundary (bc type 3, as set_ud_phase leaves the field).  Returns
+    complex128 [V, 4, 3, 3].  Built in numpy so that both bench arms run
+    on the same field."""
+    V = int(np.prod(L))
+    rng = np.random.default_rng(seed)
+    U = np.empty((V, 4, 3, 3), dtype=np.complex128)
+    chunk = 1 << 19
+    for a in range(0, V, chunk):
+        b = min(V, a + chunk)
+        c = rng.standard_normal((8, b - a, 4)) * (0.5 * eps)
+        H = np.empty((b - a, 4, 3, 3), dtype=np.complex128)
+        d8 = c[7] / np.sqrt(3.0)
+        H[..., 0, 0] = c[2] + d8
+        H[..., 1, 1] = -c[2] + d8
+        H[..., 2, 2] = -2.0 * d8
+        H[..., 0, 1] = c[0] - 1j * c[1]
+        H[..., 0, 2] = c[3] - 1j * c[4]
+        H[..., 1, 2] = c[5] - 1j * c[6]
+        H[..., 1, 0] = np.conj(H[..., 0, 1])
+        H[..., 2, 0] = np.conj(H[..., 0, 2])
+        H[..., 2, 1] = np.conj(H[..., 1, 2])
+        U[a:b] = expiq(H)
+    U.reshape(L[0], -1, 4, 3, 3)[L[0] - 1, :, 0] *= -1.0
+    return U
+
+
+def synthetic_source(L, seed):
+    """Gaussian spinor field, unit variance per real component, [V, 24]
+    (lexicographic sites)."""
+    return np.random.default_rng(seed).standard_normal((int(np.prod(L)), 24))
+
+
+def links_storage(U, L, ipt):
+    """The reference's gauge-field array for storage order ipt[] (ipt[lex] =
+    storage index, even sites first): U(x, mu) at slot 8 (ix - V/2) + 2 mu of
+    the odd site x with index ix, U(x - mu, mu) at slot 8 (ix - V/2) + 2 mu + 1
+    (main/README.global)."""
+    V = U.shape[0]
+    x = np.indices(L).reshape(4, -1)
+    odd = np.nonzero(x.sum(axis=0) & 1)[0]
+    base = 8 * (ipt[odd].astype(np.int64) - V // 2)
+    out = np.empty((4 * V, 3, 3), dtype=np.complex128)
+    xo = x[:, odd]
+    for mu in range(4):
+        y = xo.copy()
+        y[mu] = (y[mu] - 1) % L[mu]
+        lex_m = np.ravel_multi_index(tuple(y), L)
+        out[base + 2 * mu] = U[odd, mu]
+        out[base + 2 * mu + 1] = U[lex_m, mu]
+    return out.view(np.float64).reshape(-1)
+
+
+def spinor_storage(s_lex, ipt):
+    out = np.empty_like(s_lex)
+    out[ipt] = s_lex
+    return out.reshape(-1)
+
+
+def max_site_err(a_store, b_store, ipt_a, ipt_b):
+    """max over sites of |a(x) - b(x)| / |b(x)| for two spinor fields in
+    the storage orders ipt_a, ipt_b"""
+    a = np.asarray(a_store, dtype=np.float64).reshape(-1, 24)[ipt_a]
+    b = np.asarray(b_store, dtype=np.float64).reshape(-1, 24)[ipt_b]
+    return float((np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)).max())
+
+
+DATA = "synthetic: links exp(i 0.3 H), H Gaussian traceless Hermitian, and a Gaussian source, made in numpy"
+
+
+def bench_config(ngpus):
+    """the workload description both arms print"""
+    return {"workload": WORKLOAD, "lattice": list(LATTICE), "block": list(BS), "global_batch": 1,
+            "parallelism": "single" if ngpus <= 1 else "replicas%d" % ngpus,
+            "field": "numpy links exp(i 0.3 H), H Gaussian traceless Hermitian (seed %d), Gaussian source (seed %d)"
+                     % (FIELD_SEED, SOURCE_SEED),
+            "l2": "inputs larger than L2 (3.2 GB per application), no flush"}
+
+
 def ref_lattice_threads():
     """Thread-local lattice for the reference build: as many OpenMP threads as
     host cores allow (NTHREAD = V / V_TRD, a power of two up to 64)."""
@@ -165,27 +289,52 @@ def reference_lib(L):
         T = {32: (16, 16, 16, 16), 16: (32, 16, 16, 16), 8: (32, 16, 16, 32)}[nt]
 
 
-def cpu_reference_timing(L, mu, seconds=12.0, warm=1, ud_ref=None):
+def bench_inputs(ipt):
+    """the bench's gauge field and source in storage order ipt[]"""
+    U = synthetic_links(LATTICE, EPS, FIELD_SEED)
+    ud = links_storage(U, LATTICE, ipt)
+    del U
+    s = spinor_storage(synthetic_source(LATTICE, SOURCE_SEED), ipt)
+    return ud, s
+
+
+def reference_on_bench_field(ref):
+    """load the bench's field into the reference library (its own storage
+    order) and build its SW term; returns (ipt, source)"""
+    ref.init(bc=3, seed=4321, csw=CSW, m0=M0, eoflg=0)
+    ipt = ref.ipt()
+    ud, s = bench_inputs(ipt)
+    ref.set_ud(ud)
+    del ud
+    ref.sw_term(0)
+    return ipt, s
+
+
+def cpu_reference_timing(seconds=12.0, check=None):
     """Time the reference's Dw_dble (its own CPU code, OpenMP) on the bench
-    lattice.  Returns (GB/s, threads, sample description)."""
-    ref, nt = reference_lib(L)
+    field and source.  check = (device-order ipt, device result of Dw_dble
+    on that source): the result is compared site by site.  Returns the
+    cpu_baseline object."""
+    ref, nt = reference_lib(LATTICE)
     if ref is None:
         return None
-    ref.init(bc=3, seed=4321, csw=CSW, m0=M0, eoflg=0)
-    if ud_ref is not None:
-        ref.set_ud(ud_ref)
-    else:
-        ref.lib.ref_random_ud(4321)
-    ref.sw_term(0)
-    ref.time_dirac(0, mu, warm)
-    t1 = ref.time_dirac(0, mu, 1)
+    ipt, s = reference_on_bench_field(ref)
+    t1, r = ref.time_dirac_src(MU, s, 1)
     n = max(2, int(seconds / max(t1, 1e-3)))
-    t = ref.time_dirac(0, mu, n)
-    vol = ref.vol
-    gbs = BYTES_PER_SITE[64] * vol * n / t / 1e9
-    return {"value": gbs, "unit": "GB/s", "cores": nt, "kind": "reference",
-            "sample": "%d applications of the reference Dw_dble (AVX/FMA3 build, NPROC=1, NTHREAD=%d) on 32^3x64, %.1f s"
-                      % (n, nt, t)}
+    t, r = ref.time_dirac_src(MU, s, n)
+    gbs = BYTES_PER_SITE[64] * ref.vol * n / t / 1e9
+    out = {"value": gbs, "unit": "GB/s", "cores": nt, "kind": "reference",
+           "sample": "%d applications of the reference Dw_dble (AVX/FMA3 build, NPROC=1, NTHREAD=%d) on the bench's "
+                     "32^3x64 field and source, %.1f s" % (n, nt, t)}
+    if check is not None:
+        # the device's Dw_dble and Dw results on the same source, against
+        # the reference's (bars 1e-13 and 2e-6 per site)
+        ipt_dev, r_dev, r32_dev = check
+        out["max_site_rel_err_vs_device"] = max_site_err(r_dev, r, ipt_dev, ipt)
+        if r32_dev is not None:
+            r32 = ref.dirac(0, MU, s.astype(np.float32))
+            out["max_site_rel_err_vs_device_f32"] = max_site_err(r32_dev, r32, ipt_dev, ipt)
+    return out
 
 
 def run_reference(args, d):
@@ -195,22 +344,19 @@ def run_reference(args, d):
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference oracle library for 32^3x64 is not built"}))
         return 0
-    ref.init(bc=3, seed=4321, csw=CSW, m0=M0, eoflg=0)
-    ref.gen_links(EPS, 4321)
-    ref.sw_term(0)
-    ref.time_dirac(0, MU, max(1, args.warmup))
-    times = [ref.time_dirac(0, MU, 1) for _ in range(args.steps)]
+    ipt, s = reference_on_bench_field(ref)
+    ref.time_dirac_src(MU, s, max(1, args.warmup))
+    times = [ref.time_dirac_src(MU, s, 1)[0] for _ in range(args.steps)]
     tot = sum(times)
-    vol = ref.vol
-    gbs = BYTES_PER_SITE[64] * vol * args.steps / tot / 1e9
+    gbs = BYTES_PER_SITE[64] * ref.vol * args.steps / tot / 1e9
     out = {
         "impl": "reference", "metric": "Dw_dble GB/s", "value": gbs, "unit": "GB/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD + " -- reference CPU implementation", "lattice": list(LATTICE),
-                   "l2": "inputs larger than L2 (3.2 GB per application)"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": DATA, "config": bench_config(args.gpus),
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": nt, "kind": "reference",
-                         "sample": "%d single applications of the reference Dw_dble, NTHREAD=%d" % (args.steps, nt)},
+                         "sample": "%d single applications of the reference Dw_dble (AVX/FMA3 build, NPROC=1, "
+                                   "NTHREAD=%d) on the bench's field and source" % (args.steps, nt)},
         "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -509,10 +655,18 @@ def run_b200(args, d):
     ipt = qb.even_first_ipt(L)
     qb.geometry(L, BS, ipt)
     qb.set_parms(CSW, M0, 0)
-    qb.random_ud(EPS, 20251203 + d.rank)
+    s_host = None
+    if L == LATTICE:
+        # the field and source the reference arm uses (both arms make them
+        # in numpy from the same seeds); the SW term is built on the device
+        ud, s_host = bench_inputs(ipt)
+        qb.upload_ud(ud)
+        del ud
+    else:
+        qb.random_ud(EPS, FIELD_SEED + d.rank)
     qb.sw_term()
     vol = qb.lib().b200_volume()
-    s = qb.DevField(64).random(1.0, 7 + d.rank)
+    s = qb.DevField(64).from_ref(s_host) if s_host is not None else qb.DevField(64).random(1.0, SOURCE_SEED)
     r = qb.DevField(64)
 
     for _ in range(args.warmup):
@@ -531,12 +685,17 @@ def run_b200(args, d):
     peak, peak_kind = peaks()
     achieved = bytes_step / (per_launch_ms / 1e3) / 1e9
 
+    # the result of the timed launches, for the comparison with the reference
+    r_host = r.to_ref(vol) if s_host is not None else None
+
     extra = {}
-    # FP32 operator (Dw, modules/dirac/Dw.c:973)
-    s32 = qb.DevField(32).random(1.0, 8)
+    # FP32 operator (Dw, modules/dirac/Dw.c:973) on the same source
+    s32 = qb.DevField(32).from_ref(s_host.astype(np.float32)) if s_host is not None else \
+        qb.DevField(32).random(1.0, 8)
     r32 = qb.DevField(32)
     qb.time_dirac(32, "Dw", MU, s32, r32, 3)
     ms32 = qb.time_dirac(32, "Dw", MU, s32, r32, args.steps) / args.steps
+    r32_host = r32.to_ref(vol) if s_host is not None else None
     # 672 algorithmic bytes per site when the links are read as 12 reals
     # (two rows, the third rebuilt), 768 with all 18
     b32 = 672 if qb.links12_active() else BYTES_PER_SITE[32]
@@ -587,7 +746,7 @@ def run_b200(args, d):
     cpu = None
     if not args.no_cpu_baseline and d.rank == 0 and d.world == 1 and L == LATTICE:
         try:
-            cpu = cpu_reference_timing(L, MU)
+            cpu = cpu_reference_timing(check=(ipt, r_host, r32_host))
         except Exception as e:  # the baseline is reported, not required
             cpu = {"unavailable": str(e)[:200]}
 
@@ -604,10 +763,9 @@ def run_b200(args, d):
             "metric": "Dw_dble GB/s", "value": value, "unit": "GB/s", "n_gpus": d.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (device-generated links exp(0.3 X), Gaussian source)",
-            "config": {"workload": WORKLOAD, "lattice": list(L), "block": list(BS), "global_batch": 1,
-                       "parallelism": "replicas%d" % d.world if d.world > 1 else "single",
-                       "l2": "inputs larger than L2 (3.2 GB per application), no flush"},
+            "data": DATA if L == LATTICE else "synthetic (device-generated links exp(0.3 X), Gaussian source)",
+            "config": bench_config(d.world) if L == LATTICE else {"workload": "Dw_dble profiling case",
+                                                                  "lattice": list(L)},
             "roofline": {"bound": "hbm", "kernel": "dirac_staged_kernel<OP_SW|OP_HOP, all sites> (Dw_dble, SW staged)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,

@@ -127,8 +127,16 @@ const char *b200_last_error(void);
  * clearing it before and reading it after). */
 void b200_clear_error(void);
 void b200_set_fatal(int on);
+/* Wait for the library's stream; fails when a kernel gave up one of its
+ * bounded waits for bulk copies (the flag is cleared by the call). */
 int b200_sync(void);
 int b200_volume(void);
+/* No counterpart in the reference.  Self-check of that failure path: one CTA
+ * waits, with at most `limit` polls (1 .. 2^22), on an mbarrier that nothing
+ * completes, records the error and returns with nothing in flight.  Returns
+ * -1 with the bounded-wait message when the path works; the context stays
+ * usable. */
+int b200_selfcheck_bounded_wait(int limit);
 
 /* --------------------------------------- drop-in operators (dirac.h:24-52) */
 /* Dw_dble.c:1377 */ void Dw_dble(double mu, spinor_dble *s, spinor_dble *r);
@@ -214,6 +222,17 @@ int b200_links12_active(void);
  * identical results.  Returns the previous mode (no reference
  * counterpart). */
 int b200_set_dw_staged(int mode);
+/* Traversal order of the blocks in the full-lattice operator kernels (no
+ * reference counterpart; results do not depend on it, only how long a
+ * block's face data wait in L2 between uses): 0 Morton order of the block
+ * coordinates (default), 1 lexicographic with x0 slowest, 2 lexicographic
+ * with x0 fastest, 3 columns along x0 in Morton order of the spatial block
+ * coordinates, 4 slabs of two block rows along x0, Morton order inside.
+ * Returns the previous kind.  b200_tune_block_order times Dw_dble on the
+ * resident fields under each kind (ms[kind], if ms is not null: 5 floats),
+ * keeps the fastest and returns it. */
+int b200_set_block_order(int kind);
+int b200_tune_block_order(float *ms);
 /* on != 0 (default): the SAP preconditioner's launch sequence (ncy cycles of
  * block solves and boundary updates with the copies around them) is
  * captured as a CUDA graph on its first use with a given set of fields and
@@ -429,14 +448,15 @@ double b200_dev_norm2(int prec, const void *f);
 /* No counterpart in the reference.  Dwhat_dble (even-odd preconditioned FP64
  * operator, as b200_dev_dirac(64, 5, ...)) on device-resident fields in the
  * library's layout, without allocating anything: for callers that cannot let
- * a library call cudaMalloc -- during CUDA graph capture, with a device memory
- * pool that already holds all memory, or in loops that must avoid
- * cudaMalloc's implicit synchronisation.  The odd-site intermediate lives in
- * a static device array of 12 MiB (held by every GPU that loads the library
- * until exit), so lattices larger than 131072 sites are rejected with an
- * error.  The first call on a device looks up the array's device address;
- * make that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (other streams or host threads) race. */
+ * a library call cudaMalloc -- applications whose own memory pool already
+ * holds the device (a further cudaMalloc would fail or fragment it) and
+ * services whose device footprint must stay fixed after start-up.  The
+ * odd-site intermediate lives in a static device array of 12 MiB (held by
+ * every GPU that loads the library until exit), so lattices larger than
+ * 131072 sites are rejected with an error.  The first call on a device looks
+ * up the array's device address; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams or host threads) race.  Returns when the result is complete. */
 int b200_dev_Dwhat_dble_noalloc(double mu, const void *s, void *r);
 /* Device time of n back-to-back operator applications, measured with CUDA
  * events on the library's stream; returns total milliseconds in *ms. */

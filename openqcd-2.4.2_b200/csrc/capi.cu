@@ -458,6 +458,50 @@ int b200_set_dw_staged(int mode) {
   return prev;
 }
 
+int b200_set_block_order(int kind) {
+  Ctx &c = ctx();
+  if (check_ready(c)) return -1;
+  const int prev = c.block_order;
+  if (qcd::set_block_order(c, kind)) return -1;
+  return prev;
+}
+
+int b200_tune_block_order(float *ms) {
+  Ctx &c = ctx();
+  if (check_fields(c) || ensure_tmp(c)) return -1;
+  const size_t nb = qcd::spinor_bytes(c, 64);
+  void *s = nullptr, *r = nullptr;
+  if (cudaMalloc(&s, nb) != cudaSuccess || cudaMalloc(&r, nb) != cudaSuccess) {
+    cudaFree(s);
+    return fail("tune_block_order: out of device memory");
+  }
+  qcd::gen_spinor(c, 64, s, 1.0, 4711, c.stream);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int best = -1;
+  float tbest = 0.0f;
+  for (int kind = 0; kind < qcd::kBlockOrders; kind++) {
+    if (qcd::set_block_order(c, kind)) { best = -2; break; }
+    for (int i = 0; i < 2; i++) dirac_op<double>(c, 0, 0.0, s, r, c.tmp64, c.stream);
+    cudaEventRecord(e0, c.stream);
+    for (int i = 0; i < 10; i++) dirac_op<double>(c, 0, 0.0, s, r, c.tmp64, c.stream);
+    cudaEventRecord(e1, c.stream);
+    cudaEventSynchronize(e1);
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) ms[kind] = t / 10.0f;
+    if (best < 0 || t < tbest) { best = kind; tbest = t; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(s);
+  cudaFree(r);
+  if (best < 0) return -1;
+  if (qcd::set_block_order(c, best)) return -1;
+  return b200_sync() ? -1 : best;
+}
+
 int b200_links12_active(void) {
   Ctx &c = ctx();
   if (check_ready(c) || need(c.have_ud, "no gauge field on the device")) return -1;

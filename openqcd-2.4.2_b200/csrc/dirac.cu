@@ -319,7 +319,9 @@ __global__ void __launch_bounds__(DWT_TS, DWT_MINB)
     }
     if (OPS & OP_HOP) sadd(acc, h);
     else if (OPS & OP_HOPSUB) ssub(acc, h);
-    store_spinor_cs(r, chunk, si, g.vbh, acc);
+    // a site whose SW matrices did not arrive keeps its old output (the
+    // error flag tells the host the result is invalid)
+    if (ok) store_spinor_cs(r, chunk, si, g.vbh, acc);
   }
   // a thread whose wait gave up waits once more (bounded) for the copies
   // still addressed to this CTA's shared memory before the CTA exits (thread

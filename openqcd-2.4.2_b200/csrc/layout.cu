@@ -19,6 +19,50 @@ namespace qcd {
 
 static int pack4(const int a[4]) { return a[0] | (a[1] << 8) | (a[2] << 16) | (a[3] << 24); }
 
+static uint64_t interleave(const int *n, int dims, int first) {
+  uint64_t k = 0;
+  for (int bit = 0; bit < 8; bit++)
+    for (int d = 0; d < dims; d++) k |= (uint64_t)((n[first + d] >> bit) & 1) << (dims * bit + dims - 1 - d);
+  return k;
+}
+
+// Traversal order of the blocks in the full-lattice operator kernels (the
+// sched table).  The order decides how long the face data of a block (the
+// neighbour spinors and backward links its neighbours read) waits in L2
+// between its uses.  Kinds:
+//   0  Morton order of the four block coordinates (bits interleaved)
+//   1  lexicographic, n0 slowest (neighbours along x0 nb1*nb2*nb3 blocks apart)
+//   2  lexicographic with n0 fastest (neighbours along x3 nb0 blocks apart ...)
+//   3  columns along x0 (n0 fastest) in Morton order of (n1, n2, n3)
+//   4  slabs of two block rows along x0, Morton order of (n1, n2, n3) inside
+//      each slab, the two rows of a column together
+int set_block_order(Ctx &c, int kind) {
+  const Geom &g = c.g;
+  if (kind < 0 || kind >= kBlockOrders) return fail("block order: unknown kind");
+  std::vector<std::pair<uint64_t, int>> key(g.nbl);
+  for (int b = 0; b < g.nbl; b++) {
+    int n[4], r = b;
+    for (int mu = 3; mu >= 0; mu--) { n[mu] = r % g.nb[mu]; r /= g.nb[mu]; }
+    uint64_t k = 0;
+    switch (kind) {
+      case 0: k = interleave(n, 4, 0); break;
+      case 1: k = (uint64_t)b; break;
+      case 2: k = ((uint64_t)((n[1] * g.nb[2] + n[2]) * g.nb[3] + n[3])) * g.nb[0] + n[0]; break;
+      case 3: k = interleave(n, 3, 1) * g.nb[0] + n[0]; break;
+      default: k = ((uint64_t)(n[0] / 2) << 40) | (interleave(n, 3, 1) << 1) | (uint64_t)(n[0] & 1); break;
+    }
+    key[b] = {k, b};
+  }
+  std::sort(key.begin(), key.end());
+  std::vector<int> sch(g.nbl);
+  for (int b = 0; b < g.nbl; b++) sch[b] = key[b].second;
+  if (!c.sched && cudaMalloc(&c.sched, g.nbl * sizeof(int)) != cudaSuccess)
+    return fail("block order: device allocation failed");
+  cudaMemcpy(c.sched, sch.data(), g.nbl * sizeof(int), cudaMemcpyHostToDevice);
+  c.block_order = kind;
+  return 0;
+}
+
 int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
   Geom &g = c.g;
   for (int mu = 0; mu < 4; mu++) {
@@ -36,27 +80,12 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
   g.lstr[3] = 1; g.lstr[2] = bs[3]; g.lstr[1] = bs[3] * bs[2]; g.lstr[0] = bs[3] * bs[2] * bs[1];
   g.bstr[3] = 1; g.bstr[2] = g.nb[3]; g.bstr[1] = g.nb[3] * g.nb[2]; g.bstr[0] = g.nb[3] * g.nb[2] * g.nb[1];
 
-  std::vector<int> bco(g.nbl), lco(g.vb), sch(g.nbl);
-  std::vector<std::pair<uint64_t, int>> key(g.nbl);
+  std::vector<int> bco(g.nbl), lco(g.vb);
   for (int b = 0; b < g.nbl; b++) {
     int n[4], r = b;
     for (int mu = 3; mu >= 0; mu--) { n[mu] = r % g.nb[mu]; r /= g.nb[mu]; }
     bco[b] = pack4(n);
-    // Morton key: the bits of the four block coordinates interleaved
-    uint64_t k = 0;
-    for (int bit = 0; bit < 8; bit++)
-      for (int mu = 0; mu < 4; mu++) k |= (uint64_t)((n[mu] >> bit) & 1) << (4 * bit + 3 - mu);
-    key[b] = {k, b};
   }
-  // Traversal order of the full-lattice operator kernels: blocks sorted by
-  // Morton key, so that the neighbours of a block in every direction are
-  // visited a short time before or after it and their face data are still
-  // in L2 (in lexicographic order the neighbours along x0 are
-  // nb1*nb2*nb3 blocks away, more than the L2 holds on large lattices).
-#ifndef BLOCK_ORDER_LEX
-  std::sort(key.begin(), key.end());
-#endif
-  for (int b = 0; b < g.nbl; b++) sch[b] = key[b].second;
   for (int l = 0; l < g.vb; l++) {
     int y[4], r = l;
     for (int mu = 3; mu >= 0; mu--) { y[mu] = r % bs[mu]; r /= bs[mu]; }
@@ -64,13 +93,13 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
     lco[p * g.vbh + l / 2] = pack4(y);
   }
   cudaFree(c.d_bcoord); cudaFree(c.d_lcoord); cudaFree(c.sched);
+  c.sched = nullptr;
   if (cudaMalloc(&c.d_bcoord, g.nbl * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c.d_lcoord, g.vb * sizeof(int)) != cudaSuccess ||
-      cudaMalloc(&c.sched, g.nbl * sizeof(int)) != cudaSuccess)
+      cudaMalloc(&c.d_lcoord, g.vb * sizeof(int)) != cudaSuccess)
     return fail("geometry: device allocation failed");
   cudaMemcpy(c.d_bcoord, bco.data(), g.nbl * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemcpy(c.d_lcoord, lco.data(), g.vb * sizeof(int), cudaMemcpyHostToDevice);
-  cudaMemcpy(c.sched, sch.data(), g.nbl * sizeof(int), cudaMemcpyHostToDevice);
+  if (set_block_order(c, c.block_order)) return -1;
   g.bcoord = c.d_bcoord;
   g.lcoord = c.d_lcoord;
 

@@ -85,6 +85,7 @@ struct Ctx {
   Geom g{};                     // device pointers inside point to the tables below
   int *d_bcoord = nullptr, *d_lcoord = nullptr;
   int *sched = nullptr;         // block traversal order for full-lattice kernels
+  int block_order = 0;          // its kind (set_block_order in layout.cu)
   // reference (openQCD) storage order, when the caller supplied its ipt[]
   bool have_ipt = false;
   int *d_dev2q = nullptr;       // [vol] device site (chunk*vbh+s) -> reference index ix
@@ -179,6 +180,8 @@ int dwhat_dble_halfscratch(const Ctx &c, double mu, const void *s, void *r, void
 
 // layout.cu
 int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt);
+constexpr int kBlockOrders = 5;
+int set_block_order(Ctx &c, int kind);   // block traversal order of the full-lattice kernels
 int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream_t st);   // q: reference AoS on device
 // the same for the device sites [d0, d0 + n) only
 int spinor_from_ref_range(const Ctx &c, int prec, const void *q, void *dev, int d0, int n, cudaStream_t st);

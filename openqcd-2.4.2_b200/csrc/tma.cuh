@@ -73,12 +73,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *e
 }
 
 // the same with the error recorded by a plain store (for a flag in mapped
-// host memory, where device atomics are not guaranteed)
-__device__ __forceinline__ bool mbar_wait_st(uint64_t *bar, unsigned parity, int *err) {
-  for (int it = 0; it < (1 << 22); it++)
+// host memory, where device atomics are not guaranteed), and an explicit
+// iteration limit
+__device__ __forceinline__ bool mbar_wait_st_lim(uint64_t *bar, unsigned parity, int *err, int limit) {
+  for (int it = 0; it < limit; it++)
     if (mbar_try_wait(bar, parity)) return true;
   *(volatile int *)err = 1;
   return false;
+}
+__device__ __forceinline__ bool mbar_wait_st(uint64_t *bar, unsigned parity, int *err) {
+  return mbar_wait_st_lim(bar, parity, err, 1 << 22);
 }
 
 }  // namespace qcd

@@ -199,6 +199,9 @@ _SIGS = {
     "b200_dev_time_dirac": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "b200_dev_time_sap": (C.c_int, [C.c_float, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                     C.c_void_p]),
+    "b200_set_block_order": (C.c_int, [C.c_int]),
+    "b200_tune_block_order": (C.c_int, [C.c_void_p]),
+    "b200_selfcheck_bounded_wait": (C.c_int, [C.c_int]),
     "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 }
 
@@ -317,6 +320,20 @@ def set_dw_staged(mode):
     """FP64 operators: 1 SW matrices staged in shared memory (default), 0
     read directly; returns the previous mode"""
     return lib().b200_set_dw_staged(int(mode))
+
+
+def set_block_order(kind):
+    """traversal order of the blocks in the full-lattice kernels; returns the
+    previous kind"""
+    return check(lib().b200_set_block_order(int(kind)))
+
+
+def tune_block_order():
+    """time Dw_dble under every block order, keep the fastest; returns
+    (kind, [ms per launch for each kind])"""
+    ms = np.zeros(5, dtype=np.float32)
+    k = check(lib().b200_tune_block_order(_ptr(ms)))
+    return k, [float(x) for x in ms]
 
 
 def sap_tuning(prec):

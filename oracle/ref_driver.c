@@ -324,6 +324,27 @@ double ref_time_dirac(int op, double mu, int n)
    return t1 - t0;
 }
 
+/* The same timing of Dw_dble on the caller's source s (reference storage
+ * order); the last application's result is copied to r. */
+double ref_time_dirac_src(double mu, const double *s, double *r, int n)
+{
+   ENTER();
+   int i;
+   double t0, t1;
+   spinor_dble **wsd;
+
+   wsd = reserve_wsd(2);
+   memcpy(wsd[0], s, VOLUME * sizeof(spinor_dble));
+   Dw_dble(mu, wsd[0], wsd[1]);
+   t0 = MPI_Wtime();
+   for (i = 0; i < n; i++)
+      Dw_dble(mu, wsd[0], wsd[1]);
+   t1 = MPI_Wtime();
+   memcpy(r, wsd[1], VOLUME * sizeof(spinor_dble));
+   release_wsd();
+   return t1 - t0;
+}
+
 /* Site-local SW term of the reference on caller arrays
  * (modules/sw_term/pauli_dble.c:1840, :1860; pauli.c:1107).  The reference's
  * AVX code needs 32-byte aligned matrices and spinors, so the caller's arrays

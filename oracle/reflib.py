@@ -173,6 +173,16 @@ class RefLib:
     def time_dirac(self, op, mu, n):
         return self.lib.ref_time_dirac(op, mu, n)
 
+    def time_dirac_src(self, mu, s, n):
+        """seconds for n applications of Dw_dble to s; returns (seconds, Dw_dble s)"""
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        r = np.zeros_like(s)
+        f = self.lib.ref_time_dirac_src
+        f.argtypes = [C.c_double, C.c_void_p, C.c_void_p, C.c_int]
+        f.restype = C.c_double
+        t = f(mu, self._p(s), self._p(r), n)
+        return t, r
+
     def apply_sw_dble(self, vol, mu, m, s):
         m = np.ascontiguousarray(m, dtype=np.float64)
         s = np.ascontiguousarray(s, dtype=np.float64)
