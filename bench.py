@@ -70,13 +70,22 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(dev), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "20"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        # nvidia-smi needs a moment before its first sample: wait for it, so
+        # that a short timed region started after this falls between samples
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 3.0:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.p is None:
             return None
+        time.sleep(0.1)      # one more sample after the timed region
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
@@ -669,11 +678,11 @@ def run_b200(args, d):
     s = qb.DevField(64).from_ref(s_host) if s_host is not None else qb.DevField(64).random(1.0, SOURCE_SEED)
     r = qb.DevField(64)
 
+    clk = Clocks(d.local)      # sampling from before the warm-up to just after the timed launches
     for _ in range(args.warmup):
         qb.time_dirac(64, "Dw", MU, s, r, 1)
     d.barrier()
     qb.lib().b200_sync()
-    clk = Clocks(d.local)
     ms = qb.time_dirac(64, "Dw", MU, s, r, args.steps)
     clocks = clk.stop()
     qb.lib().b200_sync()

@@ -40,7 +40,52 @@ struct Geom {
   int lstr[4], bstr[4];
   const int *bcoord;   // [nbl]    packed n0 | n1<<8 | n2<<16 | n3<<24
   const int *lcoord;   // [2*vbh]  packed y0 | y1<<8 | y2<<16 | y3<<24 for (p, s)
+  // Domain decomposition along x0 (dd.cu): the local lattice starts at
+  // global time x0off of a global extent N0 (x0off = 0, N0 = L[0] on one
+  // rank).  dd != 0: the local x0-faces are rank boundaries, and the hops
+  // across them read the half-spinor faces hup (neighbour at x0 + 1, for
+  // the forward hop at the last local plane) and hdn (neighbour at x0 - 1,
+  // for the backward hop at the first plane) instead of wrapping around.
+  int x0off, N0, dd;
+  const void *hup, *hdn;
 };
+
+// Sites of one x0-face: F = L1 L2 L3.  Face index of a site (its spatial
+// coordinates): parity q of y1 + y2 + y3, then the block (n1, n2, n3)
+// lexicographically, then half the in-block spatial index
+// (y1 bs2 + y2) bs3 + y3, so that consecutive sites of a chunk on the face
+// have consecutive face indices.
+__device__ __forceinline__ int face_sites(const Geom &g) { return g.L[1] * g.L[2] * g.L[3]; }
+__device__ __forceinline__ int face_index_of(const Geom &g, const int n[4], const int y[4]) {
+  const int vb3h = g.bs[1] * g.bs[2] * g.bs[3] / 2;
+  const int q = (y[1] + y[2] + y[3]) & 1;
+  const int b3 = (n[1] * g.nb[2] + n[2]) * g.nb[3] + n[3];
+  const int l3 = (y[1] * g.bs[2] + y[2]) * g.bs[3] + y[3];
+  return (q * (g.nb[1] * g.nb[2] * g.nb[3]) + b3) * vb3h + (l3 >> 1);
+}
+// the site of face index f on the local plane x0 = 0 (side 0) or
+// x0 = L0 - 1 (side 1): chunk and in-chunk index
+__device__ __forceinline__ void face_site(const Geom &g, int side, int f, int &chunk, int &s, int n[4], int y[4]) {
+  const int vb3h = g.bs[1] * g.bs[2] * g.bs[3] / 2;
+  const int nb3 = g.nb[1] * g.nb[2] * g.nb[3];
+  const int s3 = f % vb3h, qb = f / vb3h;
+  const int q = qb / nb3, b3 = qb - q * nb3;
+  n[3] = b3 % g.nb[3];
+  n[2] = (b3 / g.nb[3]) % g.nb[2];
+  n[1] = b3 / (g.nb[3] * g.nb[2]);
+  n[0] = side ? g.nb[0] - 1 : 0;
+  const int hb3 = g.bs[3] / 2;
+  const int t = s3 / hb3;
+  y[2] = t % g.bs[2];
+  y[1] = t / g.bs[2];
+  y[3] = 2 * (s3 - t * hb3) + ((q + y[1] + y[2]) & 1);
+  y[0] = side ? g.bs[0] - 1 : 0;
+  const int blk = ((n[0] * g.nb[1] + n[1]) * g.nb[2] + n[2]) * g.nb[3] + n[3];
+  const int l = y[0] * g.lstr[0] + y[1] * g.lstr[1] + y[2] * g.lstr[2] + y[3];
+  const int p = (y[0] + y[1] + y[2] + y[3]) & 1;
+  chunk = p * g.nbl + blk;
+  s = l >> 1;
+}
 
 __device__ __forceinline__ void unpack4(int v, int a[4]) {
   a[0] = v & 255; a[1] = (v >> 8) & 255; a[2] = (v >> 16) & 255; a[3] = (v >> 24) & 255;
@@ -406,6 +451,73 @@ __device__ __forceinline__ void hop_bwd(int mu, const su3<R> &u, const spinor<R>
       h = viadd(sm.c[1], sm.c[3]); c = udagmul(u, h); vacc(acc.c[1], c); videc(acc.c[3], c);
       break;
   }
+}
+
+// ------------------------------------------------- half-spinor x0-faces
+// Planes of F face sites: FP64 as 6 double2 planes, FP32 as 3 float4 planes
+// (two complex components each); h0 = components 0..2, h1 = 3..5.
+template <typename R> struct Half;
+template <> struct Half<double> {
+  __device__ __forceinline__ static void load(const void *b, int F, int f, vec3<double> &h0, vec3<double> &h1) {
+    const double2 *p = (const double2 *)b + f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double2 a = __ldg(p + (size_t)k * F), c = __ldg(p + (size_t)(k + 3) * F);
+      h0.c[k] = mk<double>(a.x, a.y);
+      h1.c[k] = mk<double>(c.x, c.y);
+    }
+  }
+  __device__ __forceinline__ static void store(void *b, int F, int f, const vec3<double> &h0, const vec3<double> &h1) {
+    double2 *p = (double2 *)b + f;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      p[(size_t)k * F] = make_double2(h0.c[k].re, h0.c[k].im);
+      p[(size_t)(k + 3) * F] = make_double2(h1.c[k].re, h1.c[k].im);
+    }
+  }
+};
+template <> struct Half<float> {
+  __device__ __forceinline__ static void load(const void *b, int F, int f, vec3<float> &h0, vec3<float> &h1) {
+    const float4 *p = (const float4 *)b + f;
+    const float4 a = __ldg(p), c = __ldg(p + F), d = __ldg(p + 2 * (size_t)F);
+    h0.c[0] = mk<float>(a.x, a.y); h0.c[1] = mk<float>(a.z, a.w); h0.c[2] = mk<float>(c.x, c.y);
+    h1.c[0] = mk<float>(c.z, c.w); h1.c[1] = mk<float>(d.x, d.y); h1.c[2] = mk<float>(d.z, d.w);
+  }
+  __device__ __forceinline__ static void store(void *b, int F, int f, const vec3<float> &h0, const vec3<float> &h1) {
+    float4 *p = (float4 *)b + f;
+    p[0] = make_float4(h0.c[0].re, h0.c[0].im, h0.c[1].re, h0.c[1].im);
+    p[F] = make_float4(h0.c[2].re, h0.c[2].im, h1.c[0].re, h1.c[0].im);
+    p[2 * (size_t)F] = make_float4(h1.c[1].re, h1.c[1].im, h1.c[2].re, h1.c[2].im);
+  }
+};
+
+// The x0 hops across a rank boundary, split where the two ranks meet.  The
+// forward hop U(x,0)(1 - g0) s(x+0) needs the neighbour's projection
+// h = (s1 + s3, s2 + s4) (the same sums hop_fwd forms); the backward hop
+// U(x-0,0)^dag (1 + g0) s(x-0) needs c = U^dag (s1 - s3, s2 - s4), which the
+// rank holding the link forms.  Same operations in the same order as
+// hop_fwd / hop_bwd with mu = 0, so the results are bit-identical.
+template <typename R>
+__device__ __forceinline__ void dd_proj_fwd(const spinor<R> &s, vec3<R> &h0, vec3<R> &h1) {
+  h0 = vadd(s.c[0], s.c[2]);
+  h1 = vadd(s.c[1], s.c[3]);
+}
+template <typename R>
+__device__ __forceinline__ void dd_proj_bwd(const su3<R> &u, const spinor<R> &s, vec3<R> &c0, vec3<R> &c1) {
+  c0 = udagmul(u, vsub(s.c[0], s.c[2]));
+  c1 = udagmul(u, vsub(s.c[1], s.c[3]));
+}
+template <typename R>
+__device__ __forceinline__ void dd_hop_fwd(const su3<R> &u, const vec3<R> &h0, const vec3<R> &h1, spinor<R> &acc) {
+  vec3<R> c = umul(u, h0);
+  vacc(acc.c[0], c); vacc(acc.c[2], c);
+  c = umul(u, h1);
+  vacc(acc.c[1], c); vacc(acc.c[3], c);
+}
+template <typename R>
+__device__ __forceinline__ void dd_hop_bwd(const vec3<R> &c0, const vec3<R> &c1, spinor<R> &acc) {
+  vacc(acc.c[0], c0); vdec(acc.c[2], c0);
+  vacc(acc.c[1], c1); vdec(acc.c[3], c1);
 }
 
 template <typename R> __device__ __forceinline__ void sscale(spinor<R> &s, R c) {

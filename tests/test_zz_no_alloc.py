@@ -46,7 +46,7 @@ def test_noalloc_allocates_nothing():
     # first call on this device in a throwaway geometry: it loads the
     # array's module and looks up its address, which is set-up, not a
     # per-call allocation
-    qb.geometry((8, 8, 8, 8), (4, 4, 4, 4))
+    qb.geometry((8, 8, 8, 8), (4, 4, 4, 4), qb.even_first_ipt((8, 8, 8, 8)))
     qb.set_parms(1.5, -0.05)
     qb.random_ud(0.4, 3)
     qb.sw_term()
@@ -55,7 +55,7 @@ def test_noalloc_allocates_nothing():
     qb.check(L.b200_dev_Dwhat_dble_noalloc(0.1, a.ptr, b.ptr))
     a.free(); b.free()
 
-    qb.geometry((8, 8, 8, 16), (4, 4, 4, 4))
+    qb.geometry((8, 8, 8, 16), (4, 4, 4, 4), qb.even_first_ipt((8, 8, 8, 16)))
     qb.set_parms(1.7, -0.05)
     qb.random_ud(0.3, 4)
     qb.sw_term()
