@@ -19,10 +19,13 @@ e2e     : the drop-in C entry point Dw_dble(mu, s, r) on page-locked host
 Extra keys report the FP32 operator and the plain GPU SAP+GCR solve
 (seconds per right-hand side to FP64 relative residual 1e-10).
 
-With N GPUs (torchrun) every rank holds its own lattice (independent
-replicas, weak scaling); the only collective is the max-over-ranks of the
-timings.  --impl reference times the reference's own CPU Dw_dble (built from
-its sources, OpenMP on the host cores) on the same workload, on rank 0.
+With N GPUs (torchrun) the ranks hold consecutive 32^3x64 slabs along x0
+of one (64 N) x 32^3 lattice (the reference's NPROC0 = N process grid, weak
+scaling): every application packs the half-spinor x0-faces, exchanges them
+with the neighbour ranks (NCCL point-to-point, or through the host with
+--dd-transport host) and then runs the operator; the timings are maxed over
+the ranks.  --impl reference times the reference's own CPU Dw_dble (built
+from its sources, OpenMP on the host cores) on one slab, on rank 0.
 """
 import argparse
 import json
@@ -113,10 +116,14 @@ class Clocks:
 
 
 class Dist:
-    def __init__(self):
+    """backend "nccl" (one GPU per rank) or "gloo" (host transport of the
+    faces: ranks may share a GPU, and the CPU tests of the rank logic)"""
+
+    def __init__(self, backend="nccl"):
         self.rank = env_int("RANK", 0)
         self.world = env_int("WORLD_SIZE", 1)
         self.local = env_int("LOCAL_RANK", 0)
+        self.device = self.local
         self.pg = None
         self.cuda = False
         if self.world > 1:
@@ -124,11 +131,12 @@ class Dist:
 
             import torch
             import torch.distributed as dist
-            # NCCL between the GPUs; gloo where there is no GPU (the CPU
-            # tests of the rank logic)
-            self.cuda = torch.cuda.is_available()
-            if self.cuda:
-                torch.cuda.set_device(self.local)
+            has_gpu = torch.cuda.is_available()
+            self.cuda = has_gpu and backend == "nccl"
+            if has_gpu:
+                self.device = self.local % torch.cuda.device_count()
+                torch.cuda.set_device(self.device)
+            # a short timeout: ranks waiting for a failed one end with an error
             dist.init_process_group("nccl" if self.cuda else "gloo", timeout=datetime.timedelta(seconds=300))
             self.torch, self.dist = torch, dist
             self.pg = True
@@ -190,22 +198,23 @@ def expiq(Q):
     return U
 
 
-def synthetic_links(L, eps, seed):
+def synthetic_links(L, eps, seed, planes=None):
     """U(x, mu) = exp(i eps H), H = sum_a c_a T_a with c_a ~ N(0, 1) (a
-    Gaussian traceless Hermitian matrix, unit variance per su(3) generator),
-    for every site x (lexicographic, x3 fastest) and direction mu; the time
-    links at x0 = L0 - 1 carry the factor -1 of the antiperiodic quark
-    boundary (bc type 3, as set_ud_phase leaves the field).  Returns
-    complex128 [V, 4, 3, 3].  Built in numpy so that both bench arms run
-    on the same field."""
-    V = int(np.prod(L))
-    rng = np.random.default_rng(seed)
-    U = np.empty((V, 4, 3, 3), dtype=np.complex128)
-    chunk = 1 << 19
-    for a in range(0, V, chunk):
-        b = min(V, a + chunk)
-        c = rng.standard_normal((8, b - a, 4)) * (0.5 * eps)
-        H = np.empty((b - a, 4, 3, 3), dtype=np.complex128)
+    Gaussian traceless Hermitian matrix, unit variance per su(3) generator,
+    T_a the Gell-Mann matrices / 2), for every site x of the time planes
+    `planes` (default all) of the lattice L (lexicographic, x3 fastest) and
+    every direction mu; the time links at x0 = L0 - 1 carry the factor -1
+    of the antiperiodic quark boundary (bc type 3, as set_ud_phase leaves
+    the field).  Every time plane has its own random stream (seed, x0), so a
+    rank can make its slab of a large lattice alone.  Returns complex128
+    [len(planes) * L1 L2 L3, 4, 3, 3].  Built in numpy so that both bench
+    arms run on the same field."""
+    planes = list(range(L[0])) if planes is None else list(planes)
+    F = int(np.prod(L[1:]))
+    U = np.empty((len(planes), F, 4, 3, 3), dtype=np.complex128)
+    for k, x0 in enumerate(planes):
+        c = np.random.default_rng([seed, x0]).standard_normal((8, F, 4)) * (0.5 * eps)
+        H = np.empty((F, 4, 3, 3), dtype=np.complex128)
         d8 = c[7] / np.sqrt(3.0)
         H[..., 0, 0] = c[2] + d8
         H[..., 1, 1] = -c[2] + d8
@@ -216,34 +225,47 @@ def synthetic_links(L, eps, seed):
         H[..., 1, 0] = np.conj(H[..., 0, 1])
         H[..., 2, 0] = np.conj(H[..., 0, 2])
         H[..., 2, 1] = np.conj(H[..., 1, 2])
-        U[a:b] = expiq(H)
-    U.reshape(L[0], -1, 4, 3, 3)[L[0] - 1, :, 0] *= -1.0
-    return U
+        U[k] = expiq(H)
+        if x0 == L[0] - 1:
+            U[k, :, 0] *= -1.0
+    return U.reshape(-1, 4, 3, 3)
 
 
-def synthetic_source(L, seed):
+def synthetic_source(L, seed, planes=None):
     """Gaussian spinor field, unit variance per real component, [V, 24]
-    (lexicographic sites)."""
-    return np.random.default_rng(seed).standard_normal((int(np.prod(L)), 24))
+    (lexicographic sites of the time planes `planes`, one random stream
+    per plane)."""
+    planes = list(range(L[0])) if planes is None else list(planes)
+    F = int(np.prod(L[1:]))
+    return np.concatenate([np.random.default_rng([seed, x0]).standard_normal((F, 24)) for x0 in planes])
 
 
-def links_storage(U, L, ipt):
-    """The reference's gauge-field array for storage order ipt[] (ipt[lex] =
-    storage index, even sites first): U(x, mu) at slot 8 (ix - V/2) + 2 mu of
-    the odd site x with index ix, U(x - mu, mu) at slot 8 (ix - V/2) + 2 mu + 1
-    (main/README.global)."""
-    V = U.shape[0]
-    x = np.indices(L).reshape(4, -1)
+def slab_links_storage(Lg, x0a, L0, eps, seed, ipt):
+    """The reference's gauge-field array, storage order ipt[] (ipt[lex] =
+    storage index, even sites first), of the slab x0a <= x0 < x0a + L0 of the
+    global lattice Lg: U(x, mu) at slot 8 (ix - V/2) + 2 mu of the odd site x
+    with index ix, U(x - mu, mu) at slot 8 (ix - V/2) + 2 mu + 1
+    (main/README.global); for the first plane's odd sites U(x - 0, 0) is a
+    link of the plane below the slab, as openQCD's local fields hold it."""
+    Ll = (L0,) + tuple(Lg[1:])
+    V = int(np.prod(Ll))
+    below = synthetic_links(Lg, eps, seed, [(x0a - 1) % Lg[0]])          # the plane below
+    U = synthetic_links(Lg, eps, seed, range(x0a, x0a + L0))
+    x = np.indices(Ll).reshape(4, -1)
     odd = np.nonzero(x.sum(axis=0) & 1)[0]
     base = 8 * (ipt[odd].astype(np.int64) - V // 2)
     out = np.empty((4 * V, 3, 3), dtype=np.complex128)
     xo = x[:, odd]
     for mu in range(4):
-        y = xo.copy()
-        y[mu] = (y[mu] - 1) % L[mu]
-        lex_m = np.ravel_multi_index(tuple(y), L)
         out[base + 2 * mu] = U[odd, mu]
-        out[base + 2 * mu + 1] = U[lex_m, mu]
+        y = xo.copy()
+        y[mu] = (y[mu] - 1) % Ll[mu]
+        lex_m = np.ravel_multi_index(tuple(y), Ll)
+        bw = U[lex_m, mu]
+        if mu == 0:
+            first = xo[0] == 0
+            bw[first] = below[np.ravel_multi_index(tuple(xo[1:, first]), Lg[1:]), 0]
+        out[base + 2 * mu + 1] = bw
     return out.view(np.float64).reshape(-1)
 
 
@@ -265,9 +287,11 @@ DATA = "synthetic: links exp(i 0.3 H), H Gaussian traceless Hermitian, and a Gau
 
 
 def bench_config(ngpus):
-    """the workload description both arms print"""
+    """the workload description both arms print: with N GPUs, N slabs of
+    32^3x64 along x0 (global lattice (64 N) x 32^3, weak scaling)"""
     return {"workload": WORKLOAD, "lattice": list(LATTICE), "block": list(BS), "global_batch": 1,
-            "parallelism": "single" if ngpus <= 1 else "replicas%d" % ngpus,
+            "parallelism": "single" if ngpus <= 1 else "x0-slabs%d (global %dx%dx%dx%d)" % (
+                ngpus, ngpus * LATTICE[0], LATTICE[1], LATTICE[2], LATTICE[3]),
             "field": "numpy links exp(i 0.3 H), H Gaussian traceless Hermitian (seed %d), Gaussian source (seed %d)"
                      % (FIELD_SEED, SOURCE_SEED),
             "l2": "inputs larger than L2 (3.2 GB per application), no flush"}
@@ -298,12 +322,14 @@ def reference_lib(L):
         T = {32: (16, 16, 16, 16), 16: (32, 16, 16, 16), 8: (32, 16, 16, 32)}[nt]
 
 
-def bench_inputs(ipt):
-    """the bench's gauge field and source in storage order ipt[]"""
-    U = synthetic_links(LATTICE, EPS, FIELD_SEED)
-    ud = links_storage(U, LATTICE, ipt)
-    del U
-    s = spinor_storage(synthetic_source(LATTICE, SOURCE_SEED), ipt)
+def bench_inputs(ipt, nproc=1, rank=0):
+    """the bench's gauge field and source in storage order ipt[]: the slab of
+    rank `rank` of nproc ranks along x0 (each holding a 32^3x64 slab of the
+    global (64 nproc) x 32^3 lattice); nproc = 1 is the 32^3x64 lattice"""
+    L0 = LATTICE[0]
+    Lg = (nproc * L0,) + tuple(LATTICE[1:])
+    ud = slab_links_storage(Lg, rank * L0, L0, EPS, FIELD_SEED, ipt)
+    s = spinor_storage(synthetic_source(Lg, SOURCE_SEED, range(rank * L0, (rank + 1) * L0)), ipt)
     return ud, s
 
 
@@ -379,6 +405,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--lattice", default=None, help="L0,L1,L2,L3 (profiling runs)")
+    ap.add_argument("--dd-transport", default="nccl", choices=["nccl", "host"],
+                    help="N > 1: faces between the GPUs with NCCL, or through the host with gloo (ranks sharing "
+                         "a GPU)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-solver", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -390,7 +419,7 @@ def main():
                          "collection around it, and print its phase times")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
-    d = Dist()
+    d = Dist("gloo" if args.dd_transport == "host" else "nccl")
     try:
         if args.impl == "reference":
             return run_reference(args, d)
@@ -660,19 +689,24 @@ def learned_c5(qb):
 def run_b200(args, d):
     import openqcd_b200 as qb
     L = tuple(int(x) for x in args.lattice.split(",")) if args.lattice else LATTICE
-    qb.set_device(d.local)
+    qb.set_device(d.device)
     ipt = qb.even_first_ipt(L)
+    if d.world > 1:
+        # the ranks hold consecutive x0-slabs of one lattice (the reference's
+        # NPROC0 = N process grid), faces exchanged at every application
+        dd = qb.DomainDecomposition(transport=args.dd_transport)
+        dd.install()
     qb.geometry(L, BS, ipt)
     qb.set_parms(CSW, M0, 0)
     s_host = None
     if L == LATTICE:
         # the field and source the reference arm uses (both arms make them
         # in numpy from the same seeds); the SW term is built on the device
-        ud, s_host = bench_inputs(ipt)
+        ud, s_host = bench_inputs(ipt, d.world, d.rank)
         qb.upload_ud(ud)
         del ud
     else:
-        qb.random_ud(EPS, FIELD_SEED + d.rank)
+        qb.random_ud(EPS, FIELD_SEED)
     qb.sw_term()
     vol = qb.lib().b200_volume()
     s = qb.DevField(64).from_ref(s_host) if s_host is not None else qb.DevField(64).random(1.0, SOURCE_SEED)
@@ -718,6 +752,7 @@ def run_b200(args, d):
 
     e2e = None
     if not args.no_e2e:
+        d.barrier()
         sh = qb.HostArray(vol * 24)
         rh = qb.HostArray(vol * 24)
         qb.check(qb.lib().b200_dev_to_ref(64, s.ptr, sh.a.ctypes.data))

@@ -67,6 +67,45 @@ int b200_set_device(int dev);
  * (modules/lattice/geometry.c:273) for this library. */
 int b200_geometry(const int L[4], const int bs[4], const int *ipt);
 
+/* Domain decomposition along x0, as the reference's process grid with
+ * NPROC0 > 1 (include/global.h:18-36): nproc0 ranks, this one at position
+ * cpr0, each holding an L0 x L1 x L2 x L3 slab (L as given to b200_geometry,
+ * the local lattice; the global time extent is nproc0 * L0).  Takes effect
+ * at the next b200_geometry call; nproc0 = 1 switches it off.  L0 / bs0
+ * must be even.  The transport is the caller's:
+ *
+ *  - xchg moves, per operator application, the x0-faces: send_dn (this
+ *    rank's first time plane) to rank cpr0 - 1, where it arrives in
+ *    recv_up, and send_up (the last plane) to rank cpr0 + 1, arriving in
+ *    recv_dn (periodic in the rank index).  All four are device buffers of
+ *    the library, `bytes` long.  The send buffers are written by work
+ *    already enqueued on `stream` (a cudaStream_t); work the library
+ *    enqueues on it after the call returns reads the receive buffers, so
+ *    the callback either enqueues the transfers on that stream (NCCL) or
+ *    synchronises it, copies, and returns when the data are in place.
+ *  - gather is an all-gather of n doubles from every rank into out[nproc0 *
+ *    n] (rank-major, host memory), used for the global sums, which every
+ *    rank then adds in rank order in double-double (the reference's
+ *    global_qsum, modules/utils/qsum.c:389).
+ *
+ * Available with it: the Dirac operators (device and drop-in entry
+ * points), gauge and SW uploads/downloads, the SW term from the links,
+ * apply_sw, the SAP cycle, sap_gcr, fgcr on device fields, the CG solvers
+ * and the BLAS-1 reductions on device fields.  Not available (an error):
+ * deflation, batched solves, the learned preconditioner, field files and
+ * the plaquette, the allocation-free entry point.  Returns 0 or -1. */
+typedef int (*b200_dd_exchange_fn)(void *send_dn, void *send_up, void *recv_up, void *recv_dn, size_t bytes,
+                                   void *stream, void *user);
+typedef int (*b200_dd_allgather_fn)(const double *in, double *out, int n, void *user);
+int b200_dd_setup(int nproc0, int cpr0, b200_dd_exchange_fn xchg, b200_dd_allgather_fn gather, void *user);
+/* The exchange buffers (send_dn, send_up, recv_up, recv_dn) and their size,
+ * and the number of exchanges so far; returns nproc0. */
+int b200_dd_info(void **bufs, size_t *bytes, long long *nexchange);
+/* The global sum the reductions use: n (hi, lo) double-double pairs of this
+ * rank (in[2k], in[2k+1]) summed over the ranks in rank order with TwoSum,
+ * the same on every rank, into out (host code only, no device work). */
+int b200_dd_global_sum(const double *in, double *out, int n);
+
 /* Parameter data base: the values the reference reads from
  * set_lat_parms (modules/flags/lat_parms.c:216, csw), set_bc_parms (:516,
  * only type 3 = periodic gauge / antiperiodic quark fields is supported),
@@ -118,7 +157,8 @@ int b200_random_ud(double eps, unsigned long long seed);
 void *b200_host_alloc(size_t bytes);
 void b200_host_free(void *p);
 /* Device-memory buffer of the given size, and a copy between any two
- * host/device addresses (cudaMemcpyDefault semantics). */
+ * host/device addresses (cudaMemcpyDefault semantics), ordered on the
+ * library's stream and complete when the call returns. */
 void *b200_dev_alloc(size_t bytes);
 int b200_memcpy(void *dst, const void *src, size_t bytes);
 
@@ -232,6 +272,11 @@ int b200_set_dw_staged(int mode);
  * resident fields under each kind (ms[kind], if ms is not null: 5 floats),
  * keeps the fastest and returns it. */
 int b200_set_block_order(int kind);
+/* Fix the launch variant of the even-odd SAP block kernel for the current
+ * block size (the index of the autotuner's candidate list, 0..3), so that
+ * separate runs use the same arithmetic; -1 lets the autotuner choose again
+ * (no reference counterpart). */
+int b200_set_sap_variant(int variant);
 int b200_tune_block_order(float *ms);
 /* on != 0 (default): the SAP preconditioner's launch sequence (ncy cycles of
  * block solves and boundary updates with the copies around them) is

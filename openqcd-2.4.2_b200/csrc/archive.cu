@@ -101,6 +101,7 @@ static double ksum(const std::vector<double> &v) {
 }
 
 int plaq_sum(Ctx &c, double *sum) {
+  if (dd_unsupported(c, "plaq_sum")) return -1;
   if (!c.have_ud) return fail("plaq_sum: no gauge field on the device");
   const int t = 256, nb = (c.g.vol + t - 1) / t;
   double *part = nullptr;
@@ -123,6 +124,7 @@ int plaq_sum(Ctx &c, double *sum) {
 static bool phase_link(const Ctx &c, const int x[4], int mu) { return c.bc == 3 && mu == 0 && x[0] == c.g.L[0] - 1; }
 
 int export_cnfg(Ctx &c, const char *out) {
+  if (dd_unsupported(c, "export_cnfg")) return -1;
   if (!c.ready) return fail("geometry not set (call b200_geometry first)");
   if (!c.have_ud) return fail("export_cnfg: no gauge field on the device");
   const int *L = c.g.L;
@@ -174,6 +176,7 @@ int export_cnfg(Ctx &c, const char *out) {
 }
 
 int import_cnfg(Ctx &c, const char *in, int mask) {
+  if (dd_unsupported(c, "import_cnfg")) return -1;
   if (!c.ready) return fail("geometry not set (call b200_geometry first)");
   const int *L = c.g.L;
   FILE *f = fopen(in, "rb");
@@ -261,6 +264,7 @@ static double norm_sq(const double *sd, size_t n) {
 }
 
 int export_sfld(Ctx &c, const char *out, int eo, const void *sd) {
+  if (dd_unsupported(c, "export_sfld")) return -1;
   if (!c.ready) return fail("geometry not set (call b200_geometry first)");
   if (!c.have_ipt) return fail("export_sfld: no reference site order (pass ipt[] to the geometry call)");
   if (eo < 0 || eo > 1) return fail("export_sfld: parameter eo is out of range");
@@ -292,6 +296,7 @@ int export_sfld(Ctx &c, const char *out, int eo, const void *sd) {
 }
 
 int import_sfld(Ctx &c, const char *in, int eo, void *sd) {
+  if (dd_unsupported(c, "import_sfld")) return -1;
   if (!c.ready) return fail("geometry not set (call b200_geometry first)");
   if (!c.have_ipt) return fail("import_sfld: no reference site order (pass ipt[] to the geometry call)");
   if (eo < 0 || eo > 1) return fail("import_sfld: parameter eo is out of range");

@@ -157,7 +157,7 @@ static void ref_layout_op(int op, R mu, const void *s, void *r) {
   void *fr = prec == 64 ? c.ws64[1] : c.ws32[1];
   char *st_in = (char *)c.stage, *st_out = (char *)c.stage + nb;
   cudaStream_t st = c.stream;
-  if (op == 0 && c.pipeline && c.slab.size() >= 3 && pinned_host(s) && pinned_host(r)) {
+  if (op == 0 && c.pipeline && !qcd::dd_on(c) && c.slab.size() >= 3 && pinned_host(s) && pinned_host(r)) {
     dw_pipelined<R>(c, mu, s, r, fs, fr, st_in, st_out);
     return;
   }
@@ -216,8 +216,14 @@ void *b200_dev_alloc(size_t bytes) {
   return p;
 }
 
+// Ordered on the library's stream and complete on return (a plain
+// cudaMemcpy from pageable host memory may return before its DMA reaches
+// device memory, and the library's stream does not wait for the legacy
+// default stream).
 int b200_memcpy(void *dst, const void *src, size_t bytes) {
-  return cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) == cudaSuccess ? 0 : fail("memcpy failed");
+  cudaStream_t st = ctx().stream;
+  if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, st) != cudaSuccess) return fail("memcpy failed");
+  return cudaStreamSynchronize(st) == cudaSuccess ? 0 : fail("memcpy failed");
 }
 void b200_set_fatal(int on) { g_fatal = on != 0; }
 int b200_sync(void) {
@@ -267,7 +273,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   qcd::net_fields_release(c);
   qcd::graphs_release();
   c.ready = false;
-  if (geometry_init(c, L, bs, ipt)) return -1;
+  if (geometry_init(c, L, bs, ipt) || qcd::dd_buffers(c)) return -1;
   c.ready = true;
   return 0;
 }
@@ -458,6 +464,12 @@ int b200_set_dw_staged(int mode) {
   return prev;
 }
 
+int b200_set_sap_variant(int variant) {
+  Ctx &c = ctx();
+  if (check_fields(c)) return -1;
+  return qcd::sap_set_variant(c, variant);
+}
+
 int b200_set_block_order(int kind) {
   Ctx &c = ctx();
   if (check_ready(c)) return -1;
@@ -527,6 +539,8 @@ int b200_upload_ud(const su3_dble *ud) {
   if (ensure_stage(c, n)) return -1;
   cudaMemcpyAsync(c.stage, ud, 4 * (size_t)c.g.vol * sizeof(su3_dble), cudaMemcpyDefault, c.stream);
   if (links_from_ref(c, c.stage, c.stream)) return -1;
+  // the forward time links of the last plane's even sites are at the rank above
+  if (qcd::dd_on(c) && qcd::dd_links_after_upload(c, c.stage, c.stream)) return -1;
   c.have_ud = true;
   if (links_refresh_f32(c, c.stream)) return -1;
   return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("upload_ud: CUDA error");
@@ -538,6 +552,7 @@ int b200_download_ud(su3_dble *ud) {
   size_t n = 4 * (size_t)c.g.vol * sizeof(su3_dble);
   if (ensure_stage(c, n)) return -1;
   if (links_to_ref(c, c.stage, c.stream)) return -1;
+  if (qcd::dd_on(c) && qcd::dd_links_after_download(c, c.stage, c.stream)) return -1;
   cudaMemcpyAsync(ud, c.stage, n, cudaMemcpyDefault, c.stream);
   return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("download_ud: CUDA error");
 }

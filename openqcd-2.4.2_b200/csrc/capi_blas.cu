@@ -6,7 +6,8 @@
 // reference's fields span vol sites per OpenMP thread, NTHREAD threads
 // (sflds/README.icom), so the library covers vol * nthread sites with
 // nthread set by b200_set_nthread() (default 1).  icom & 0x1 (sum over MPI
-// processes) is a no-op in this single-process library.  Arrays may be in
+// processes) sums over the ranks of the domain decomposition (b200_dd_setup)
+// in rank order in double-double, and is a no-op on one rank.  Arrays may be in
 // device memory (used in place) or in host memory (staged through device
 // buffers, written back when the call modifies them).
 #include "lib.h"
@@ -70,7 +71,9 @@ static int dd_dot(int prec, int vol, int icom, const void *s, const void *r, dou
   if (flat_scratch(c, &scr, &od)) return -1;
   View vs(c, s, b, 0, false), vr(c, r, b, 1, false);
   if (!vs.dev || !vr.dev) return -1;
-  return flat_dot(c, prec, vs.dev, vr.dev, n, out4, scr, od);
+  if (flat_dot(c, prec, vs.dev, vr.dev, n, out4, scr, od)) return -1;
+  // icom & 0x1: the sum over the ranks (domain decomposition)
+  return ((icom & 1) && dd_on(c)) ? dd_global(c, out4, 2, false) : 0;
 }
 
 static int dd_norm(int prec, int vol, int icom, const void *s, double *out2) {
@@ -81,7 +84,8 @@ static int dd_norm(int prec, int vol, int icom, const void *s, double *out2) {
   if (flat_scratch(c, &scr, &od)) return -1;
   View vs(c, s, b, 0, false);
   if (!vs.dev) return -1;
-  return flat_norm2(c, prec, vs.dev, n, out2, scr, od);
+  if (flat_norm2(c, prec, vs.dev, n, out2, scr, od)) return -1;
+  return ((icom & 1) && dd_on(c)) ? dd_global(c, out2, 1, false) : 0;
 }
 
 static void axpy(int prec, int vol, int icom, void *s, const void *r, double ar, double ai) {
@@ -211,17 +215,24 @@ double fgcr(int vol, void (*Dop)(spinor_dble *s, spinor_dble *r), void (*Mop)(in
       double m;
       View v(c, x, b32, 0, false);
       qcd::flat_umax(c, 32, v.dev, n, &m, scr, od);
+      if (qcd::dd_on(c)) {
+        double mm[2] = {m, 0.0};
+        qcd::dd_global(c, mm, 1, true);
+        m = mm[0];
+      }
       return (double)(float)sqrt(m);
     }
     double d[2];
     View v(c, x, b32, 0, false);
     qcd::flat_norm2(c, 32, v.dev, n, d, scr, od);
+    if (qcd::dd_on(c)) qcd::dd_global(c, d, 1, false);
     return sqrt((double)(float)(d[0] + d[1]));
   };
   o.dot32 = [&](const void *x, const void *y) {
     double d[4];
     View vx(c, x, b32, 0, false), vy(c, y, b32, 1, false);
     qcd::flat_dot(c, 32, vx.dev, vy.dev, n, d, scr, od);
+    if (qcd::dd_on(c)) qcd::dd_global(c, d, 2, false);
     return cplxf{(float)(d[0] + d[1]), (float)(d[2] + d[3])};
   };
   o.normalize32 = [&](void *x) { return normalize((int)n, 0, (spinor *)x); };

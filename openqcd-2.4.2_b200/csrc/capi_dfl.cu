@@ -82,6 +82,7 @@ extern "C" {
 int b200_set_dfl_parms(const int bs[4], int Ns) {
   Ctx &c = ctx();
   if (!c.ready) return fail("geometry not set (call b200_geometry first)");
+  if (qcd::dd_unsupported(c, "deflation")) return -1;
   return qcd::dfl_set_parms(c, bs, Ns);
 }
 
@@ -193,7 +194,7 @@ int b200_dev_gcr_batch(int nrhs, int dfl, int nkv, int nmx, int istop, double re
                        void *const *eta, void *const *psi, double *rho, int *ifail, int *status) {
   Ctx &c = ctx();
   if (!c.ready) return fail("geometry not set (call b200_geometry first)");
-  if (qcd::fields_ready(c)) return -1;
+  if (qcd::fields_ready(c) || qcd::dd_unsupported(c, "batched solves")) return -1;
   return qcd::gcr_batch(c, nrhs, dfl, nkv, nmx, istop, res, mu, (const void *const *)eta, psi, rho, ifail, status);
 }
 

@@ -17,9 +17,15 @@ extern "C" {
 
 int b200_net_nweights(void) { return qcd::net_nweights(); }
 
-int b200_net_init(unsigned long long seed, float scale) { return qcd::net_init(ctx(), seed, scale); }
+int b200_net_init(unsigned long long seed, float scale) {
+  if (qcd::dd_unsupported(ctx(), "the learned preconditioner")) return -1;
+  return qcd::net_init(ctx(), seed, scale);
+}
 
-int b200_net_set_weights(const float *w) { return qcd::net_set_weights(ctx(), w); }
+int b200_net_set_weights(const float *w) {
+  if (qcd::dd_unsupported(ctx(), "the learned preconditioner")) return -1;
+  return qcd::net_set_weights(ctx(), w);
+}
 
 int b200_net_get_weights(float *w) { return qcd::net_get_weights(ctx(), w); }
 

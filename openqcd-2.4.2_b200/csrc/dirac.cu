@@ -113,12 +113,11 @@ constexpr int kDwUnroll = DW_UNROLL;
 
 // L12 = 1 (FP32 only): the links are read as 12 reals (load_link12), the
 // time links at x0 = N0-1 with the boundary sign.
-template <typename R, int OPS, int PAR, int RHALF = 0, int THALF = 0, int L12 = 0, int DD = 0>
-__global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) dirac_kernel(Geom g, const void *__restrict__ s, const void *__restrict__ t,
-                                                    void *r, const void *__restrict__ u,
-                                                    const void *__restrict__ sw, const void *__restrict__ swinv,
-                                                    R mu_e, R mu_o, const int *__restrict__ sched,
-                                                    const void *__restrict__ sub) {
+template <typename R, int OPS, int PAR, int RHALF, int THALF, int L12, int DD>
+__device__ __forceinline__ void dirac_body(const Geom &g, const DDGeom &dg, const void *__restrict__ s,
+                                           const void *__restrict__ t, void *r, const void *__restrict__ u,
+                                           const void *__restrict__ sw, const void *__restrict__ swinv, R mu_e,
+                                           R mu_o, const int *__restrict__ sched, const void *__restrict__ sub) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   int p, blk, si;
   if (PAR == 2) {
@@ -150,38 +149,61 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
   if (OPS & (OP_HOP | OP_HOPSUB)) {
     spinor<R> h;
     szero(h);
-    const int x0 = g.x0off + x.n[0] * g.bs[0] + x.y[0];   // global time coordinate
-    // DD: the x0-neighbours across the rank boundary come from the faces
-    const bool dd_up = DD && x.n[0] + 1 == g.nb[0] && x.y[0] + 1 == g.bs[0];
-    const bool dd_dn = DD && x.n[0] == 0 && x.y[0] == 0;
+    if constexpr (DD == 0) {
+      const int x0 = x.n[0] * g.bs[0] + x.y[0];
 #pragma unroll kDwUnroll
-    for (int mu = 0; mu < 4; mu++) {
-      int c2, s2;
-      site_nbr(g, x, mu, +1, c2, s2);
-      {
+      for (int mu = 0; mu < 4; mu++) {
+        int c2, s2;
+        site_nbr(g, x, mu, +1, c2, s2);
+        {
+          spinor<R> sp = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
+          su3<R> uu;
+          if constexpr (L12 != 0) uu = load_link12(u, chunk, mu, si, g.vbh, mu == 0 && x0 == g.L[0] - 1);
+          else uu = Store<R>::load_link(u, chunk, mu, si, g.vbh);
+          hop_fwd<R>(mu, uu, sp, h);
+        }
+        site_nbr(g, x, mu, -1, c2, s2);
+        {
+          spinor<R> sm = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
+          su3<R> uu;
+          if constexpr (L12 != 0) uu = load_link12(u, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
+          else uu = Store<R>::load_link(u, c2, mu, s2, g.vbh);
+          hop_bwd<R>(mu, uu, sm, h);
+        }
+      }
+    } else {
+      // domain decomposition: global time coordinate, and the x0-neighbours
+      // across the rank boundary from the faces
+      const int x0 = dg.x0off + x.n[0] * g.bs[0] + x.y[0];
+      const bool up = x.n[0] + 1 == g.nb[0] && x.y[0] + 1 == g.bs[0];
+      const bool dn = x.n[0] == 0 && x.y[0] == 0;
+#pragma unroll kDwUnroll
+      for (int mu = 0; mu < 4; mu++) {
+        int c2, s2;
         su3<R> uu;
-        if constexpr (L12 != 0) uu = load_link12(u, chunk, mu, si, g.vbh, mu == 0 && x0 == g.N0 - 1);
+        if constexpr (L12 != 0) uu = load_link12(u, chunk, mu, si, g.vbh, mu == 0 && x0 == dg.N0 - 1);
         else uu = Store<R>::load_link(u, chunk, mu, si, g.vbh);
-        if (mu == 0 && dd_up) {
+        if (mu == 0 && up) {
           vec3<R> h0, h1;
-          Half<R>::load(g.hup, face_sites(g), face_index_of(g, x.n, x.y), h0, h1);
+          Half<R>::load(dg.hup, face_sites(g), face_index_of(g, x.n, x.y), h0, h1);
           dd_hop_fwd<R>(uu, h0, h1, h);
         } else {
+          site_nbr(g, x, mu, +1, c2, s2);
           spinor<R> sp = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
           hop_fwd<R>(mu, uu, sp, h);
         }
-      }
-      if (mu == 0 && dd_dn) {
-        vec3<R> c0, c1;
-        Half<R>::load(g.hdn, face_sites(g), face_index_of(g, x.n, x.y), c0, c1);
-        dd_hop_bwd<R>(c0, c1, h);
-      } else {
-        site_nbr(g, x, mu, -1, c2, s2);
-        spinor<R> sm = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
-        su3<R> uu;
-        if constexpr (L12 != 0) uu = load_link12(u, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
-        else uu = Store<R>::load_link(u, c2, mu, s2, g.vbh);
-        hop_bwd<R>(mu, uu, sm, h);
+        if (mu == 0 && dn) {
+          vec3<R> c0, c1;
+          Half<R>::load(dg.hdn, face_sites(g), face_index_of(g, x.n, x.y), c0, c1);
+          dd_hop_bwd<R>(c0, c1, h);
+        } else {
+          site_nbr(g, x, mu, -1, c2, s2);
+          spinor<R> sm = Store<R>::load_spinor(t, THALF ? c2 - g.nbl : c2, s2, g.vbh);
+          su3<R> ub;
+          if constexpr (L12 != 0) ub = load_link12(u, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
+          else ub = Store<R>::load_link(u, c2, mu, s2, g.vbh);
+          hop_bwd<R>(mu, ub, sm, h);
+        }
       }
     }
     sscale<R>(h, (R)-0.5);
@@ -204,6 +226,25 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32) d
   }
 }
 
+
+// The operator kernels: without domain decomposition the parameter list of
+// the single-GPU kernel stays as it was (a larger one made the compiler
+// spill in the FP32 operator); the DD twin takes the slab's geometry.
+template <typename R, int OPS, int PAR, int RHALF = 0, int THALF = 0, int L12 = 0>
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32)
+    dirac_kernel(Geom g, const void *__restrict__ s, const void *__restrict__ t, void *r, const void *__restrict__ u,
+                 const void *__restrict__ sw, const void *__restrict__ swinv, R mu_e, R mu_o,
+                 const int *__restrict__ sched, const void *__restrict__ sub) {
+  dirac_body<R, OPS, PAR, RHALF, THALF, L12, 0>(g, DDGeom{0, 0, nullptr, nullptr}, s, t, r, u, sw, swinv, mu_e, mu_o,
+                                                sched, sub);
+}
+template <typename R, int OPS, int PAR, int L12>
+__global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32)
+    dirac_dd_kernel(Geom g, DDGeom dg, const void *__restrict__ s, const void *__restrict__ t, void *r,
+                    const void *__restrict__ u, const void *__restrict__ sw, const void *__restrict__ swinv, R mu_e,
+                    R mu_o, const int *__restrict__ sched) {
+  dirac_body<R, OPS, PAR, 0, 0, L12, 1>(g, dg, s, t, r, u, sw, swinv, mu_e, mu_o, sched, nullptr);
+}
 
 // ------------------------------------------------------------------------
 // FP64 operator with the SW matrices staged in shared memory.  A CTA owns a
@@ -282,14 +323,12 @@ __device__ __forceinline__ void staged_tile(const Geom &g, int PAR_, int t, int 
 // with bulk prefetches while the current tile was computed: 0.90 ms against
 // 0.69 ms at 32^3x64, DRAM reads 4.35 GB against 3.36 GB per launch (the
 // prefetched lines were partly evicted before use).
-template <int OPS, int PAR, int DD = 0>
-__global__ void __launch_bounds__(DWT_TS, DWT_MINB)
-    dirac_staged_kernel(Geom g, const double2 *__restrict__ s, const double2 *__restrict__ t, double2 *r,
-                        const double2 *__restrict__ u, const double2 *__restrict__ swm, double mu_e, double mu_o,
-                        const int *__restrict__ sched, int tpc, int ntiles, int *err) {
-  extern __shared__ __align__(128) unsigned char dwt_smem[];
-  double2 *sw_s = (double2 *)dwt_smem;          // [36][DWT_TS]
-  __shared__ uint64_t bar[1];
+template <int OPS, int PAR, int DD>
+__device__ __forceinline__ void staged_body(const Geom &g, const DDGeom &dg, const double2 *__restrict__ s,
+                                            const double2 *__restrict__ t, double2 *r, const double2 *__restrict__ u,
+                                            const double2 *__restrict__ swm, double mu_e, double mu_o,
+                                            const int *__restrict__ sched, int tpc, int ntiles, int *err,
+                                            double2 *sw_s, uint64_t *bar) {
   constexpr bool HAS_SW = (OPS & (OP_SW | OP_INV)) != 0;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -322,26 +361,33 @@ __global__ void __launch_bounds__(DWT_TS, DWT_MINB)
       site_decode(g, p, blk, si, x);
       spinor<double> h;
       szero(h);
-      const bool dd_up = DD && x.n[0] + 1 == g.nb[0] && x.y[0] + 1 == g.bs[0];
-      const bool dd_dn = DD && x.n[0] == 0 && x.y[0] == 0;
 #pragma unroll
       for (int mu = 0; mu < 4; mu++) {
         int c2, s2;
-        const su3<double> uu = Store<double>::load_link(u, chunk, mu, si, g.vbh);
-        if (mu == 0 && dd_up) {
-          vec3<double> h0, h1;
-          Half<double>::load(g.hup, face_sites(g), face_index_of(g, x.n, x.y), h0, h1);
-          dd_hop_fwd<double>(uu, h0, h1, h);
-        } else {
+        bool fwd_done = false, bwd_done = false;
+        if constexpr (DD != 0) {
+          // the x0-neighbours across the rank boundary come from the faces
+          if (mu == 0 && x.n[0] + 1 == g.nb[0] && x.y[0] + 1 == g.bs[0]) {
+            vec3<double> h0, h1;
+            Half<double>::load(dg.hup, face_sites(g), face_index_of(g, x.n, x.y), h0, h1);
+            const su3<double> uu = Store<double>::load_link(u, chunk, mu, si, g.vbh);
+            dd_hop_fwd<double>(uu, h0, h1, h);
+            fwd_done = true;
+          }
+          if (mu == 0 && x.n[0] == 0 && x.y[0] == 0) {
+            vec3<double> c0, c1;
+            Half<double>::load(dg.hdn, face_sites(g), face_index_of(g, x.n, x.y), c0, c1);
+            dd_hop_bwd<double>(c0, c1, h);
+            bwd_done = true;
+          }
+        }
+        if (!fwd_done) {
           site_nbr(g, x, mu, +1, c2, s2);
           const spinor<double> sp = Store<double>::load_spinor(t, c2, s2, g.vbh);
+          const su3<double> uu = Store<double>::load_link(u, chunk, mu, si, g.vbh);
           hop_fwd<double>(mu, uu, sp, h);
         }
-        if (mu == 0 && dd_dn) {
-          vec3<double> c0, c1;
-          Half<double>::load(g.hdn, face_sites(g), face_index_of(g, x.n, x.y), c0, c1);
-          dd_hop_bwd<double>(c0, c1, h);
-        } else {
+        if (!bwd_done) {
           site_nbr(g, x, mu, -1, c2, s2);
           const spinor<double> sm = Store<double>::load_spinor(t, c2, s2, g.vbh);
           const su3<double> ub = Store<double>::load_link(u, c2, mu, s2, g.vbh);
@@ -382,44 +428,94 @@ __global__ void __launch_bounds__(DWT_TS, DWT_MINB)
 }
 
 template <int OPS, int PAR>
-static void launch_staged(const Ctx &c, const void *s, const void *t, void *r, double mu_e, double mu_o,
-                          cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(dirac_staged_kernel<OPS, PAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DWT_SMEM);
-    attr = true;
-  }
-  const int tpc = (c.g.vbh + DWT_TS - 1) / DWT_TS;
-  const int nchunk = PAR == 2 ? 2 * c.g.nbl : c.g.nbl;
-  const void *swm = (OPS & OP_INV) ? (const void *)c.swd_inv : (const void *)c.swd;
-  const int ntiles = nchunk * tpc;
-  dirac_staged_kernel<OPS, PAR><<<ntiles, DWT_TS, DWT_SMEM, st>>>(
-      c.g, (const double2 *)s, (const double2 *)t, (double2 *)r, (const double2 *)c.ud, (const double2 *)swm, mu_e,
-      mu_o, c.sched, tpc, ntiles, c.d_kerr);
+__global__ void __launch_bounds__(DWT_TS, DWT_MINB)
+    dirac_staged_kernel(Geom g, const double2 *__restrict__ s, const double2 *__restrict__ t, double2 *r,
+                        const double2 *__restrict__ u, const double2 *__restrict__ swm, double mu_e, double mu_o,
+                        const int *__restrict__ sched, int tpc, int ntiles, int *err) {
+  extern __shared__ __align__(128) unsigned char dwt_smem[];
+  __shared__ uint64_t bar[1];
+  staged_body<OPS, PAR, 0>(g, DDGeom{0, 0, nullptr, nullptr}, s, t, r, u, swm, mu_e, mu_o, sched, tpc, ntiles, err,
+                           (double2 *)dwt_smem, bar);
+}
+template <int OPS, int PAR>
+__global__ void __launch_bounds__(DWT_TS, DWT_MINB)
+    dirac_staged_dd_kernel(Geom g, DDGeom dg, const double2 *__restrict__ s, const double2 *__restrict__ t,
+                           double2 *r, const double2 *__restrict__ u, const double2 *__restrict__ swm, double mu_e,
+                           double mu_o, const int *__restrict__ sched, int tpc, int ntiles, int *err) {
+  extern __shared__ __align__(128) unsigned char dwt_smem[];
+  __shared__ uint64_t bar[1];
+  staged_body<OPS, PAR, 1>(g, dg, s, t, r, u, swm, mu_e, mu_o, sched, tpc, ntiles, err, (double2 *)dwt_smem, bar);
 }
 
+template <int OPS, int PAR, int DD>
+static void launch_staged(const Ctx &c, const DDGeom &dg, const void *s, const void *t, void *r, double mu_e,
+                          double mu_o, cudaStream_t st) {
+  const Geom &g = c.g;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(DD ? (const void *)dirac_staged_dd_kernel<OPS, PAR> : (const void *)dirac_staged_kernel<OPS, PAR>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DWT_SMEM);
+    attr = true;
+  }
+  const int tpc = (g.vbh + DWT_TS - 1) / DWT_TS;
+  const int nchunk = PAR == 2 ? 2 * g.nbl : g.nbl;
+  const void *swm = (OPS & OP_INV) ? (const void *)c.swd_inv : (const void *)c.swd;
+  const int ntiles = nchunk * tpc;
+  if (DD)
+    dirac_staged_dd_kernel<OPS, PAR><<<ntiles, DWT_TS, DWT_SMEM, st>>>(
+        g, dg, (const double2 *)s, (const double2 *)t, (double2 *)r, (const double2 *)c.ud, (const double2 *)swm,
+        mu_e, mu_o, c.sched, tpc, ntiles, c.d_kerr);
+  else
+    dirac_staged_kernel<OPS, PAR><<<ntiles, DWT_TS, DWT_SMEM, st>>>(
+        g, (const double2 *)s, (const double2 *)t, (double2 *)r, (const double2 *)c.ud, (const double2 *)swm, mu_e,
+        mu_o, c.sched, tpc, ntiles, c.d_kerr);
+}
+
+template <typename R, int OPS, int PAR, int L12, int DD>
+static void launch_plain(const Ctx &c, const DDGeom &dg, const void *s, const void *t, void *r, const void *u,
+                         R mu_e, R mu_o, cudaStream_t st) {
+  const Geom &g = c.g;
+  const void *sw = sizeof(R) == 8 ? (const void *)c.swd : (const void *)c.sw32;
+  const void *swinv = sizeof(R) == 8 ? (const void *)c.swd_inv : (const void *)c.sw32_inv;
+  const int n = PAR == 2 ? g.vol : g.volh, threads = 128;
+  if (DD)
+    dirac_dd_kernel<R, OPS, PAR, L12><<<(n + threads - 1) / threads, threads, 0, st>>>(g, dg, s, t, r, u, sw, swinv,
+                                                                                      mu_e, mu_o, c.sched);
+  else
+    dirac_kernel<R, OPS, PAR, 0, 0, L12><<<(n + threads - 1) / threads, threads, 0, st>>>(
+        g, s, t, r, u, sw, swinv, mu_e, mu_o, c.sched, nullptr);
+}
+
+// With domain decomposition the operators that hop (all but Dwee, Dwoo)
+// first exchange the x0-faces of the field they hop on.
 template <typename R, int OPS, int PAR>
 static void launch(const Ctx &c, const void *s, const void *t, void *r, R mu_e, R mu_o, bool inv,
                    cudaStream_t st) {
-  const void *u = sizeof(R) == 8 ? (const void *)c.ud : (const void *)c.u32;
-  const void *sw = sizeof(R) == 8 ? (const void *)c.swd : (const void *)c.sw32;
-  const void *swinv = sizeof(R) == 8 ? (const void *)c.swd_inv : (const void *)c.sw32_inv;
   (void)inv;
+  constexpr bool HOPS = (OPS & (OP_HOP | OP_HOPSUB)) != 0;
+  const void *u = sizeof(R) == 8 ? (const void *)c.ud : (const void *)c.u32;
+  const void *u12 = nullptr;
+  if constexpr (sizeof(R) == 4 && HOPS) u12 = links12(const_cast<Ctx &>(c), st);
+  DDGeom g = c.ddg;
+  const bool dd = HOPS && dd_on(c);
+  if (dd && dd_faces(const_cast<Ctx &>(c), sizeof(R) == 8 ? 64 : 32, t, u12 ? u12 : u, u12 != nullptr, st, g))
+    return;
   if (sizeof(R) == 8 && !(OPS & OP_ACC) && (OPS & (OP_SW | OP_INV)) && c.dw_staged && c.d_kerr) {
-    launch_staged<OPS, PAR>(c, s, t, r, (double)mu_e, (double)mu_o, st);
+    if (dd) launch_staged<OPS, PAR, 1>(c, g, s, t, r, (double)mu_e, (double)mu_o, st);
+    else launch_staged<OPS, PAR, 0>(c, g, s, t, r, (double)mu_e, (double)mu_o, st);
     return;
   }
-  int n = PAR == 2 ? c.g.vol : c.g.volh;
-  int threads = 128;
-  if constexpr (sizeof(R) == 4 && (OPS & (OP_HOP | OP_HOPSUB)) != 0) {
-    if (const void *u12 = links12(const_cast<Ctx &>(c), st)) {
-      dirac_kernel<R, OPS, PAR, 0, 0, 1><<<(n + threads - 1) / threads, threads, 0, st>>>(
-          c.g, s, t, r, u12, sw, swinv, mu_e, mu_o, c.sched, nullptr);
+  if constexpr (sizeof(R) == 4) {
+    if (u12) {
+      if (dd) launch_plain<R, OPS, PAR, 1, 1>(c, g, s, t, r, u12, mu_e, mu_o, st);
+      else launch_plain<R, OPS, PAR, 1, 0>(c, g, s, t, r, u12, mu_e, mu_o, st);
       return;
     }
   }
-  dirac_kernel<R, OPS, PAR><<<(n + threads - 1) / threads, threads, 0, st>>>(c.g, s, t, r, u, sw, swinv, mu_e, mu_o,
-                                                                           c.sched, nullptr);
+  {
+    if (dd) launch_plain<R, OPS, PAR, 0, 1>(c, g, s, t, r, u, mu_e, mu_o, st);
+    else launch_plain<R, OPS, PAR, 0, 0>(c, g, s, t, r, u, mu_e, mu_o, st);
+  }
 }
 
 // op: 0 Dw, 1 Dwee, 2 Dwoo, 3 Dwoe, 4 Dweo, 5 Dwhat.  tmp: a scratch field

@@ -138,8 +138,8 @@ bool spatial_phases(const Ctx &c, double pr[3], double pi[3]) {
   return on;
 }
 
-__global__ void k_gen_links(Geom g, double2 *ud, double eps, uint32_t k0, uint32_t k1, int antiperiodic,
-                            LinkPhase ph) {
+__global__ void k_gen_links(Geom g, DDGeom dg, double2 *ud, double eps, uint32_t k0, uint32_t k1,
+                            int antiperiodic, LinkPhase ph) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= 4 * g.vol) return;
   int d = i >> 2, mu = i & 3;
@@ -147,10 +147,11 @@ __global__ void k_gen_links(Geom g, double2 *ud, double eps, uint32_t k0, uint32
   int p = chunk >= g.nbl, blk = chunk - p * g.nbl;
   Site xs;
   site_decode(g, p, blk, s, xs);
-  int x0 = xs.n[0] * g.bs[0] + xs.y[0];
-  // global counter: lexicographic site index, so the field does not depend on the block size
-  uint32_t lex = 0;
-  for (int m = 0; m < 4; m++) lex = lex * g.L[m] + (xs.n[m] * g.bs[m] + xs.y[m]);
+  int x0 = dg.x0off + xs.n[0] * g.bs[0] + xs.y[0];     // global time coordinate
+  // global counter: lexicographic index of the site in the global lattice,
+  // so the field depends neither on the block size nor on the ranks
+  uint32_t lex = (uint32_t)x0;
+  for (int m = 1; m < 4; m++) lex = lex * g.L[m] + (xs.n[m] * g.bs[m] + xs.y[m]);
   double gg[8];
   for (int r = 0; r < 2; r++) {
     P4 c = {lex, (uint32_t)mu, (uint32_t)r, 0x4c494e4bu};
@@ -174,7 +175,7 @@ __global__ void k_gen_links(Geom g, double2 *ud, double eps, uint32_t k0, uint32
   M[14] = -M[10]; M[15] = M[11];        // X_32
   double U[18];
   su3_exp(M, U);
-  double sg = (antiperiodic && mu == 0 && x0 == g.L[0] - 1) ? -1.0 : 1.0;
+  double sg = (antiperiodic && mu == 0 && x0 == dg.N0 - 1) ? -1.0 : 1.0;
   double2 *dst = ud + ((size_t)chunk * 4 + mu) * 9 * g.vbh + s;
   if (ph.on && mu > 0) {
     const double pr = ph.re[mu - 1], pi = ph.im[mu - 1];
@@ -191,7 +192,7 @@ int gen_links(Ctx &c, double eps, uint64_t seed, cudaStream_t st) {
   int t = 128, m = 4 * c.g.vol;
   LinkPhase ph;
   ph.on = spatial_phases(c, ph.re, ph.im);
-  k_gen_links<<<(m + t - 1) / t, t, 0, st>>>(c.g, c.ud, eps, (uint32_t)seed, (uint32_t)(seed >> 32), c.bc == 3,
+  k_gen_links<<<(m + t - 1) / t, t, 0, st>>>(c.g, c.ddg, c.ud, eps, (uint32_t)seed, (uint32_t)(seed >> 32), c.bc == 3,
                                               ph);
   if (cudaGetLastError() != cudaSuccess) return fail("gen_links: launch failed");
   c.have_ud = true;
@@ -200,15 +201,15 @@ int gen_links(Ctx &c, double eps, uint64_t seed, cudaStream_t st) {
 
 // Gaussian spinor field: every real component normal with variance sigma^2/2.
 template <typename R>
-__global__ void k_gen_spinor(Geom g, void *dst, double sigma, uint32_t k0, uint32_t k1) {
+__global__ void k_gen_spinor(Geom g, DDGeom dg, void *dst, double sigma, uint32_t k0, uint32_t k1) {
   int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= g.vol) return;
   int chunk = d / g.vbh, s = d - chunk * g.vbh;
   int p = chunk >= g.nbl, blk = chunk - p * g.nbl;
   Site xs;
   site_decode(g, p, blk, s, xs);
-  uint32_t lex = 0;
-  for (int m = 0; m < 4; m++) lex = lex * g.L[m] + (xs.n[m] * g.bs[m] + xs.y[m]);
+  uint32_t lex = (uint32_t)(dg.x0off + xs.n[0] * g.bs[0] + xs.y[0]);
+  for (int m = 1; m < 4; m++) lex = lex * g.L[m] + (xs.n[m] * g.bs[m] + xs.y[m]);
   spinor<R> v;
   for (int k = 0; k < 6; k++) {
     P4 o = philox({lex, (uint32_t)k, 0x53504e52u, 0u}, k0, k1);
@@ -226,9 +227,9 @@ __global__ void k_gen_spinor(Geom g, void *dst, double sigma, uint32_t k0, uint3
 int gen_spinor(const Ctx &c, int prec, void *dev, double sigma, uint64_t seed, cudaStream_t st) {
   int t = 128;
   if (prec == 64)
-    k_gen_spinor<double><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, dev, sigma, (uint32_t)seed, (uint32_t)(seed >> 32));
+    k_gen_spinor<double><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ddg, dev, sigma, (uint32_t)seed, (uint32_t)(seed >> 32));
   else
-    k_gen_spinor<float><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, dev, sigma, (uint32_t)seed, (uint32_t)(seed >> 32));
+    k_gen_spinor<float><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ddg, dev, sigma, (uint32_t)seed, (uint32_t)(seed >> 32));
   return cudaGetLastError() == cudaSuccess ? 0 : fail("gen_spinor: launch failed");
 }
 

@@ -78,6 +78,10 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
   g.vb = bs[0] * bs[1] * bs[2] * bs[3];
   g.vbh = g.vb / 2;
   g.lstr[3] = 1; g.lstr[2] = bs[3]; g.lstr[1] = bs[3] * bs[2]; g.lstr[0] = bs[3] * bs[2] * bs[1];
+  // domain decomposition along x0: this rank's slab of the global lattice
+  c.ddg.x0off = c.dd.rank * L[0];
+  c.ddg.N0 = c.dd.np * L[0];
+  c.ddg.hup = c.ddg.hdn = nullptr;
   g.bstr[3] = 1; g.bstr[2] = g.nb[3]; g.bstr[1] = g.nb[3] * g.nb[2]; g.bstr[0] = g.nb[3] * g.nb[2] * g.nb[1];
 
   std::vector<int> bco(g.nbl), lco(g.vb);

@@ -9,9 +9,28 @@
 #include <vector>
 #include "qcd.cuh"
 
+// Transport callbacks of the domain decomposition (declared for callers in
+// include/openqcd_b200.h with the same signatures).
+typedef int (*b200_dd_exchange_fn)(void *send_dn, void *send_up, void *recv_up, void *recv_dn, size_t bytes,
+                                   void *stream, void *user);
+typedef int (*b200_dd_allgather_fn)(const double *in, double *out, int n, void *user);
+
 namespace qcd {
 
 struct LtlRef;
+
+// Domain decomposition along x0 (dd.cu): ranks, the caller's transport and
+// the four face buffers (send to the rank below, send to the rank above,
+// received from above, received from below).
+struct DDState {
+  int np = 1, rank = 0;
+  b200_dd_exchange_fn xchg = nullptr;
+  b200_dd_allgather_fn gather = nullptr;
+  void *user = nullptr;
+  void *buf[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t bytes = 0;
+  long long nxchg = 0;
+};
 
 // An x0-slab of the lattice whose sites are contiguous ranges of the
 // reference's storage order in each parity half: device blocks [b0, b1)
@@ -157,16 +176,35 @@ struct Ctx {
   std::vector<void *> ws32, ws64;   // solver workspaces (reserve_ws / reserve_wsd)
   DflState dfl;
   NetState net;
+  DDState dd;
+  DDGeom ddg{0, 0, nullptr, nullptr};   // this rank's slab (x0off, N0) for the kernels
   // preconditioner of sap_gcr: 0 SAP, 1 network (SAP when the residual
   // stalls), 2 network then SAP on the remainder, 3 none
   int precond = 0;
 };
+
+inline bool dd_on(const Ctx &c) { return c.dd.np > 1; }
 
 Ctx &ctx();
 void set_error(const std::string &msg);
 int fail(const std::string &msg);   // records msg, returns -1 (or aborts in fatal mode)
 
 size_t spinor_bytes(const Ctx &c, int prec);   // prec 64 or 32
+
+// dd.cu: domain decomposition along x0
+int dd_buffers(Ctx &c);
+int dd_exchange(Ctx &c, size_t bytes, cudaStream_t st);
+// pack the half-spinor faces of field t (links u: FP64, FP32 or 12-real
+// FP32 with l12), exchange them, and return in g the geometry with the
+// received faces attached
+int dd_faces(Ctx &c, int prec, const void *t, const void *u, int l12, cudaStream_t st, DDGeom &dg);
+int dd_links_after_upload(Ctx &c, const void *qud, cudaStream_t st);
+int dd_links_after_download(Ctx &c, void *qud, cudaStream_t st);
+// n (hi, lo) pairs summed (or maxed) over the ranks, in rank order
+int dd_global(Ctx &c, double *res, int n, bool is_max);
+int dd_all(Ctx &c, int flag);                       // 1 when flag is non-zero on every rank
+int dd_rank0(Ctx &c, int value);                    // rank 0's value on every rank
+int dd_unsupported(const Ctx &c, const char *what);  // fails under domain decomposition
 
 // dirac.cu
 template <typename R>
@@ -365,6 +403,7 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status);
 // sap.cu
 int sap_prepare(Ctx &c, cudaStream_t st);
 int sap_variant_threads(const Ctx &c, int slot);
+int sap_set_variant(Ctx &c, int v);
 int sap_storage_mode(Ctx &c);
 int sap_cycle(Ctx &c, float mu, int isolv, int nmr, void *psi, void *rho, void *phi_blk, cudaStream_t st);
 int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *rho, void *phi_blk,

@@ -168,11 +168,13 @@ static int ensure_red(Ctx &c) {
   return 0;
 }
 
-static int finish(Ctx &c, int nc, double *res) {
+// the nc (hi, lo) results of this rank, then (domain decomposition) their
+// sum or maximum over the ranks, the same on every rank
+static int finish(Ctx &c, int nc, double *res, bool is_max = false) {
   cudaMemcpyAsync(c.h_red, c.red_out, 2 * nc * sizeof(double), cudaMemcpyDeviceToHost, c.stream);
   if (cudaStreamSynchronize(c.stream) != cudaSuccess) return fail("reduction: CUDA error");
   for (int k = 0; k < 2 * nc; k++) res[k] = c.h_red[k];
-  return 0;
+  return dd_on(c) ? dd_global(c, res, nc, is_max) : 0;
 }
 
 int la_norm2(Ctx &c, int prec, const void *x, int par, double *res) {
@@ -257,7 +259,7 @@ int la_unorm(Ctx &c, int prec, const void *x, int par, double *res) {
   if (prec == 64) k_unorm<double><<<RB, RT, 0, c.stream>>>(c.g, x, c0, nch, c.red);
   else k_unorm<float><<<RB, RT, 0, c.stream>>>(c.g, x, c0, nch, c.red);
   k_max_finish<<<1, 32, 0, c.stream>>>(c.red, RB, c.red_out);
-  return finish(c, 1, res);
+  return finish(c, 1, res, true);
 }
 
 // ------------------------------------------------------------- elementwise

@@ -59,6 +59,7 @@ extern "C" int b200_dev_Dwhat_dble_noalloc(double mu, const void *s, void *r) {
     return qcd::fail("Dwhat_dble_noalloc: the lattice has " + std::to_string(c.g.vol) +
                      " sites, the static scratch serves at most " + std::to_string(qcd::NOALLOC_MAX_SITES));
   if (!c.have_ud || !c.have_sw) return qcd::fail("Dwhat_dble_noalloc: gauge or SW field missing on the device");
+  if (qcd::dd_unsupported(c, "Dwhat_dble_noalloc")) return -1;
   void *scratch = nullptr;
   if (qcd::scratch_address(c.dev, &scratch)) return -1;
   // the first kernel writes every odd site the second one reads: nothing to clear

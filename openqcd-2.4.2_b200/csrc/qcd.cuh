@@ -40,13 +40,17 @@ struct Geom {
   int lstr[4], bstr[4];
   const int *bcoord;   // [nbl]    packed n0 | n1<<8 | n2<<16 | n3<<24
   const int *lcoord;   // [2*vbh]  packed y0 | y1<<8 | y2<<16 | y3<<24 for (p, s)
-  // Domain decomposition along x0 (dd.cu): the local lattice starts at
-  // global time x0off of a global extent N0 (x0off = 0, N0 = L[0] on one
-  // rank).  dd != 0: the local x0-faces are rank boundaries, and the hops
-  // across them read the half-spinor faces hup (neighbour at x0 + 1, for
-  // the forward hop at the last local plane) and hdn (neighbour at x0 - 1,
-  // for the backward hop at the first plane) instead of wrapping around.
-  int x0off, N0, dd;
+};
+
+// Domain decomposition along x0 (dd.cu): the local lattice starts at global
+// time x0off of a global extent N0 (x0off = 0, N0 = L[0] on one rank).  The
+// kernels built for it hop across the local x0-faces with the half-spinor
+// faces hup (neighbour at x0 + 1, for the forward hop at the last local
+// plane) and hdn (neighbour at x0 - 1, for the backward hop at the first
+// plane) instead of wrapping around.  Kept apart from Geom, which every
+// kernel takes: a larger Geom made the compiler spill in the FP32 operator.
+struct DDGeom {
+  int x0off, N0;
   const void *hup, *hdn;
 };
 

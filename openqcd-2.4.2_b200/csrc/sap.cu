@@ -487,8 +487,8 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
 #ifndef SAP_BND_MINB
 #define SAP_BND_MINB 8
 #endif
-template <class P>
-__global__ void __launch_bounds__(128, SAP_BND_MINB) k_sap_bnd(SapArgs a) {
+template <class P, int DD>
+__device__ __forceinline__ void sap_bnd_body(const SapArgs &a, const DDGeom &dg) {
   const Geom &g = a.g;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= (size_t)(g.nbl / 2) * g.vb) return;
@@ -498,26 +498,44 @@ __global__ void __launch_bounds__(128, SAP_BND_MINB) k_sap_bnd(SapArgs a) {
   Site x;
   site_decode(g, p, blk, s, x);
   const int chunk = p * g.nbl + blk;
-  const int x0 = x.n[0] * g.bs[0] + x.y[0];   // the time links at x0 = N0-1 carry the boundary sign
+  // global time coordinate: the time links at x0 = N0-1 carry the boundary sign
+  const int x0 = (DD ? dg.x0off : 0) + x.n[0] * g.bs[0] + x.y[0];
+  const int xlast = (DD ? dg.N0 : g.L[0]) - 1;
+  // DD: the x0-neighbour blocks across the rank boundary are on the other
+  // ranks; their hops come from the exchanged faces of phi
+  const bool dd_up = DD && x.n[0] + 1 == g.nb[0] && x.y[0] + 1 == g.bs[0];
+  const bool dd_dn = DD && x.n[0] == 0 && x.y[0] == 0;
   spinor<float> hsum;
   szero(hsum);
   bool any = false;
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
     if (crosses_block(g, x, mu, +1)) {
-      int c2, s2;
-      site_nbr(g, x, mu, +1, c2, s2);
-      spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = P::blink(a.ub, chunk, mu, s, g.vbh, mu == 0 && x0 == g.L[0] - 1);
-      hop_fwd<float>(mu, uu, sp, hsum);
+      su3<float> uu = P::blink(a.ub, chunk, mu, s, g.vbh, mu == 0 && x0 == xlast);
+      if (mu == 0 && dd_up) {
+        vec3<float> h0, h1;
+        Half<float>::load(dg.hup, face_sites(g), face_index_of(g, x.n, x.y), h0, h1);
+        dd_hop_fwd<float>(uu, h0, h1, hsum);
+      } else {
+        int c2, s2;
+        site_nbr(g, x, mu, +1, c2, s2);
+        spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
+        hop_fwd<float>(mu, uu, sp, hsum);
+      }
       any = true;
     }
     if (crosses_block(g, x, mu, -1)) {
-      int c2, s2;
-      site_nbr(g, x, mu, -1, c2, s2);
-      spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
-      su3<float> uu = P::blink(a.ub, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
-      hop_bwd<float>(mu, uu, sm, hsum);
+      if (mu == 0 && dd_dn) {
+        vec3<float> c0, c1;
+        Half<float>::load(dg.hdn, face_sites(g), face_index_of(g, x.n, x.y), c0, c1);
+        dd_hop_bwd<float>(c0, c1, hsum);
+      } else {
+        int c2, s2;
+        site_nbr(g, x, mu, -1, c2, s2);
+        spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
+        su3<float> uu = P::blink(a.ub, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
+        hop_bwd<float>(mu, uu, sm, hsum);
+      }
       any = true;
     }
   }
@@ -526,6 +544,57 @@ __global__ void __launch_bounds__(128, SAP_BND_MINB) k_sap_bnd(SapArgs a) {
   spinor<float> rr = Store<float>::load_spinor_rw(a.rho, chunk, s, g.vbh);
   sadd(rr, hsum);
   Store<float>::store_spinor(a.rho, chunk, s, g.vbh, rr);
+}
+
+// the single-GPU kernel keeps its parameter list; the DD twin takes the
+// slab's geometry with the received faces
+template <class P>
+__global__ void __launch_bounds__(128, SAP_BND_MINB) k_sap_bnd(SapArgs a) {
+  sap_bnd_body<P, 0>(a, DDGeom{0, 0, nullptr, nullptr});
+}
+template <class P>
+__global__ void __launch_bounds__(128, SAP_BND_MINB) k_sap_bnd_dd(SapArgs a, DDGeom dg) {
+  sap_bnd_body<P, 1>(a, dg);
+}
+
+// DD: the x0-faces of the block solutions phi (FP32 half spinors, as
+// k_dd_pack in dd.cu, with the links as the boundary hops read them)
+template <class P>
+__global__ void k_sap_dd_pack(SapArgs a, DDGeom dg, void *dn, void *up) {
+  const Geom &g = a.g;
+  const int F = face_sites(g);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * F) return;
+  const int side = i >= F, f = i - side * F;
+  int chunk, s, n[4], y[4];
+  face_site(g, side, f, chunk, s, n, y);
+  const spinor<float> v = Store<float>::load_spinor(a.phi, chunk, s, g.vbh);
+  vec3<float> h0, h1;
+  if (side == 0) {
+    dd_proj_fwd<float>(v, h0, h1);
+    Half<float>::store(dn, F, f, h0, h1);
+  } else {
+    const su3<float> uu = P::blink(a.ub, chunk, 0, s, g.vbh, dg.x0off + g.L[0] - 1 == dg.N0 - 1);
+    dd_proj_bwd<float>(uu, v, h0, h1);
+    Half<float>::store(up, F, f, h0, h1);
+  }
+}
+
+template <class P>
+static void sap_bnd_launch(Ctx &c, SapArgs a, cudaStream_t st) {
+  const size_t nb_sites = (size_t)(c.g.nbl / 2) * c.g.vb;
+  const unsigned nbnd = (unsigned)((nb_sites + 127) / 128);
+  DDGeom dg = c.ddg;
+  if (!dd_on(c)) {
+    k_sap_bnd<P><<<nbnd, 128, 0, st>>>(a);
+    return;
+  }
+  const int F = c.g.L[1] * c.g.L[2] * c.g.L[3];
+  k_sap_dd_pack<P><<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(a, dg, c.dd.buf[0], c.dd.buf[1]);
+  if (dd_exchange(c, (size_t)F * 48, st)) return;
+  dg.hup = c.dd.buf[2];
+  dg.hdn = c.dd.buf[3];
+  k_sap_bnd_dd<P><<<nbnd, 128, 0, st>>>(a, dg);
 }
 
 // dynamic shared memory a block kernel may use (of 227 KB per CTA)
@@ -574,7 +643,7 @@ static int sap_half_fields(Ctx &c, cudaStream_t st) {
 // link satisfies row3 = conj(row1 x row2) to FP32 accuracy, with the sign
 // flipped on the time links at x0 = N0-1 (the antiperiodic boundary phase
 // of bc type 3); bad[0] counts links that do not.
-__global__ void k_links12(Geom g, size_t nlink, const float2 *__restrict__ u32, float2 *u12, int *bad) {
+__global__ void k_links12(Geom g, DDGeom dg, size_t nlink, const float2 *__restrict__ u32, float2 *u12, int *bad) {
   const int vbh = g.vbh;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= nlink) return;
@@ -583,7 +652,7 @@ __global__ void k_links12(Geom g, size_t nlink, const float2 *__restrict__ u32, 
   const int par = chunk >= g.nbl;
   Site x;
   site_decode(g, par, chunk - par * g.nbl, (int)s, x);
-  const bool neg = mu == 0 && x.n[0] * g.bs[0] + x.y[0] == g.L[0] - 1;
+  const bool neg = mu == 0 && dg.x0off + x.n[0] * g.bs[0] + x.y[0] == dg.N0 - 1;
   const float2 *p = u32 + cm * 9 * vbh + s;
   float2 e[9];
 #pragma unroll
@@ -611,12 +680,12 @@ static int sap_link12_fields(Ctx &c, cudaStream_t st) {
   int *bad = nullptr;
   if (cudaMallocAsync(&bad, sizeof(int), st) != cudaSuccess) return fail("out of device memory");
   cudaMemsetAsync(bad, 0, sizeof(int), st);
-  k_links12<<<(unsigned)((nlink + 255) / 256), 256, 0, st>>>(c.g, nlink, c.u32, (float2 *)c.u12, bad);
+  k_links12<<<(unsigned)((nlink + 255) / 256), 256, 0, st>>>(c.g, c.ddg, nlink, c.u32, (float2 *)c.u12, bad);
   int h = 0;
   cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(bad, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return fail("sap: 12-real link conversion failed");
-  c.u12_ok = h == 0;
+  c.u12_ok = dd_all(c, h == 0) != 0;   // the same choice on every rank
   c.u12_valid = true;
   return 0;
 }
@@ -746,6 +815,7 @@ static int sap_autotune(Ctx &c, int mode, cudaStream_t st) {
   cudaFreeAsync(rho, st);
   cudaFreeAsync(phi, st);
   if (best < 0) return fail("sap: no block-kernel variant fits this block size");
+  best = dd_rank0(c, best);   // every rank runs rank 0's choice (the same arithmetic everywhere)
   c.sap_variant[mode] = best;
   c.sap_tuned_vbh[mode] = c.g.vbh;
   c.sap_tuned_ms[mode] = best_ms / 3.0f;
@@ -753,6 +823,24 @@ static int sap_autotune(Ctx &c, int mode, cudaStream_t st) {
 }
 
 int sap_variant_threads(const Ctx &c, int slot) { return eo_threads(kEo[c.sap_variant[slot]], c.g.vbh); }
+
+// Fix the launch variant of the even-odd block kernel for the current block
+// size and storage mode (-1: tune again on the next use).
+int sap_set_variant(Ctx &c, int v) {
+  const int mode = sap_mode(c, 1, c.stream);
+  if (mode < 0) return -1;
+  if (v < 0) {
+    c.sap_tuned_vbh[mode] = 0;
+    return 0;
+  }
+  if (v >= kNEo || !eo_threads(kEo[v], c.g.vbh)) return fail("sap: this launch variant does not fit the block size");
+  for (int m = 0; m < 3; m++)
+    cudaFuncSetAttribute(kEo[v].k[m], cudaFuncAttributeMaxDynamicSharedMemorySize, SAP_SMEM_MAX);
+  c.sap_variant[mode] = v;
+  c.sap_tuned_vbh[mode] = c.g.vbh;
+  c.sap_tuned_ms[mode] = 0.0f;
+  return 0;
+}
 
 int sap_prepare(Ctx &c, cudaStream_t st) {
   int ns;
@@ -790,14 +878,12 @@ static int sap_ready(Ctx &c, int isolv, cudaStream_t st) {
 // the launches of one cycle: block solves and boundary updates, colour 0
 // then colour 1 (sap.c:720)
 static void sap_cycle_launch(Ctx &c, SapArgs a, int isolv, int mode, cudaStream_t st) {
-  const size_t nb_sites = (size_t)(c.g.nbl / 2) * c.g.vb;
-  const unsigned nbnd = (unsigned)((nb_sites + 127) / 128);
   for (int ic = 0; ic < 2; ic++) {
     a.colour = ic;
     launch_blocks(c, a, isolv, mode, st);
-    if (mode == 1) k_sap_bnd<SapF16><<<nbnd, 128, 0, st>>>(a);
-    else if (mode == 2) k_sap_bnd<SapF32R><<<nbnd, 128, 0, st>>>(a);
-    else k_sap_bnd<SapF32><<<nbnd, 128, 0, st>>>(a);
+    if (mode == 1) sap_bnd_launch<SapF16>(c, a, st);
+    else if (mode == 2) sap_bnd_launch<SapF32R>(c, a, st);
+    else sap_bnd_launch<SapF32>(c, a, st);
   }
 }
 
@@ -848,7 +934,7 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
 // graphs are off): a caller that computes rh can write it there directly
 // and pass it as rh, which saves sap_mop the copy.
 void *sap_input_field(Ctx &c) {
-  if (!c.use_graphs) return nullptr;
+  if (!c.use_graphs || dd_on(c)) return nullptr;
   if (!c.sap_fld[1] && cudaMalloc(&c.sap_fld[1], spinor_bytes(c, 32)) != cudaSuccess) return nullptr;
   return c.sap_fld[1];
 }
@@ -856,7 +942,9 @@ void *sap_input_field(Ctx &c) {
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
             cudaStream_t st, const void *base, const void *add) {
   if (!base) base = rh;
-  if (!c.use_graphs) {
+  // with domain decomposition the cycles call the exchange between their
+  // launches, so they are not captured
+  if (!c.use_graphs || dd_on(c)) {
     la_zero(c, 32, psi, PAR_ALL, st);
     if (rho != rh) la_copy(c, 32, rh, 32, rho, PAR_ALL, st);
     if (sap_cycles(c, mu, isolv, nmr, ncy, psi, rho, phi_blk, st)) return -1;

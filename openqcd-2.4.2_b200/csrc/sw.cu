@@ -176,6 +176,25 @@ __device__ __forceinline__ su3<double> link_at(const Geom &g, const double2 *ud,
   return Store<double>::load_link(ud, chunk, mu, s, g.vbh);
 }
 
+// With domain decomposition x[0] runs from -1 to L0: the planes x0 = -1 and
+// x0 = L0 are the neighbour ranks' last and first planes, whose four links
+// per site arrived in the faces dg.hdn, dg.hup (18 doubles per link, four
+// links per face site).
+__device__ __forceinline__ su3<double> link_dd(const Geom &g, const DDGeom &dg, const double2 *ud, const int x[4],
+                                               int mu) {
+  if (x[0] >= 0 && x[0] < g.L[0]) return link_at(g, ud, x, mu);
+  int n[4], y[4];
+  for (int k = 1; k < 4; k++) {
+    n[k] = x[k] / g.bs[k];
+    y[k] = x[k] - n[k] * g.bs[k];
+  }
+  n[0] = y[0] = 0;
+  const double *p = (const double *)(x[0] < 0 ? dg.hdn : dg.hup) + ((size_t)face_index_of(g, n, y) * 4 + mu) * 18;
+  su3<double> u;
+  for (int k = 0; k < 9; k++) u.e[k] = mk<double>(p[2 * k], p[2 * k + 1]);
+  return u;
+}
+
 __device__ __forceinline__ su3<double> mm(const su3<double> &a, const su3<double> &b) {
   su3<double> r;
 #pragma unroll
@@ -219,13 +238,21 @@ __device__ __forceinline__ void add_antiherm(const su3<double> &m, double X[9]) 
 // Clover field tensor F_{mu nu}(x) = (1/8) sum over the four plaquettes with a
 // corner at x of (P - P^dag), each plaquette read in the orientation the
 // reference uses (modules/tcharge/ftensor.c:141-192, periodic case).
-__device__ void ftensor_site(const Geom &g, const double2 *ud, const int x[4], int mu, int nu, double X[9]) {
+template <int DD>
+__device__ void ftensor_site(const Geom &g, const DDGeom &dg, const double2 *ud, const int x[4], int mu, int nu,
+                             double X[9]) {
   for (int k = 0; k < 9; k++) X[k] = 0.0;
   int c[4], a[4], b[4], ab[4];
+  // periodic shifts; with domain decomposition x0 is not wrapped (the
+  // planes -1 and L0 come from the neighbour ranks)
   auto sh = [&](const int *in, int *o, int dm, int sm, int dn, int sn) {
     for (int k = 0; k < 4; k++) o[k] = in[k];
-    if (sm) o[dm] = (o[dm] + sm + g.L[dm]) % g.L[dm];
-    if (sn) o[dn] = (o[dn] + sn + g.L[dn]) % g.L[dn];
+    if (sm) o[dm] = (DD && dm == 0) ? o[dm] + sm : (o[dm] + sm + g.L[dm]) % g.L[dm];
+    if (sn) o[dn] = (DD && dn == 0) ? o[dn] + sn : (o[dn] + sn + g.L[dn]) % g.L[dn];
+  };
+  auto link_at = [&](const Geom &gg, const double2 *u, const int *xx, int m) {
+    if constexpr (DD != 0) return link_dd(gg, dg, u, xx, m);
+    else return qcd::link_at(gg, u, xx, m);
   };
   // corner c = x : leaf = w1 w2,  w1 = U(c,mu)U(c+mu,nu), w2 = U(c+nu,mu)^dag U(c,nu)^dag
   sh(x, c, mu, 0, nu, 0);
@@ -430,9 +457,9 @@ static int sw_exp_order(double csw, double m0) {
   return -1;
 }
 
-template <bool ISW>
-__global__ void k_sw_term(Geom g, const double2 *__restrict__ ud, double2 *swd, double2 *swd_inv, double c1,
-                          double c2, ExpCoef ec) {
+template <bool ISW, int DD>
+__global__ void k_sw_term(Geom g, DDGeom dg, const double2 *__restrict__ ud, double2 *swd, double2 *swd_inv,
+                          double c1, double c2, ExpCoef ec) {
   int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= g.vol) return;
   int chunk = d / g.vbh, s = d - chunk * g.vbh;
@@ -444,7 +471,7 @@ __global__ void k_sw_term(Geom g, const double2 *__restrict__ ud, double2 *swd, 
   for (int mu = 0; mu < 4; mu++) x[mu] = xs.n[mu] * g.bs[mu] + xs.y[mu];
   const int planes[6][2] = {{0, 1}, {0, 2}, {0, 3}, {2, 3}, {3, 1}, {1, 2}};
   double F[6][9];
-  for (int n = 0; n < 6; n++) ftensor_site(g, ud, x, planes[n][0], planes[n][1], F[n]);
+  for (int n = 0; n < 6; n++) ftensor_site<DD>(g, dg, ud, x, planes[n][0], planes[n][1], F[n]);
   for (int half = 0; half < 2; half++) {
     double u[36], X[9];
     const double sg = half == 0 ? -1.0 : 1.0;
@@ -470,11 +497,41 @@ __global__ void k_sw_term(Geom g, const double2 *__restrict__ ud, double2 *swd, 
   }
 }
 
+// the four links of each site of the first (side 0) and last (side 1)
+// local planes, for the neighbour ranks' clover leaves
+__global__ void k_sw_dd_pack(Geom g, const double2 *__restrict__ ud, double *dn, double *up) {
+  const int F = face_sites(g);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 2 * F) return;
+  const int side = i >= F, f = i - side * F;
+  int chunk, s, n[4], y[4];
+  face_site(g, side, f, chunk, s, n, y);
+  double *dst = (side ? up : dn) + (size_t)f * 72;
+  for (int mu = 0; mu < 4; mu++) {
+    const su3<double> u = Store<double>::load_link(ud, chunk, mu, s, g.vbh);
+    for (int k = 0; k < 9; k++) {
+      dst[mu * 18 + 2 * k] = u.e[k].re;
+      dst[mu * 18 + 2 * k + 1] = u.e[k].im;
+    }
+  }
+}
+
 int sw_compute(Ctx &c, cudaStream_t st) {
   if (!c.have_ud) return fail("sw_term: no gauge field on the device");
   if (c.bc != 3) return fail("sw_term: only periodic boundary conditions (type 3) are supported");
   if (alloc_sw(c)) return -1;
   int t = 64;
+  DDGeom dg = c.ddg;
+  const bool dd = dd_on(c);
+  if (dd) {
+    // the neighbours' link planes: x0 = -1 (from below) and x0 = L0 (from above)
+    const int F = c.g.L[1] * c.g.L[2] * c.g.L[3];
+    k_sw_dd_pack<<<(unsigned)((2 * F + 127) / 128), 128, 0, st>>>(c.g, c.ud, (double *)c.dd.buf[0],
+                                                                   (double *)c.dd.buf[1]);
+    if (dd_exchange(c, (size_t)F * 576, st)) return -1;
+    dg.hup = c.dd.buf[2];
+    dg.hdn = c.dd.buf[3];
+  }
   const double c1 = 4.0 + c.m0;
   ExpCoef ec{};
   if (c.isw) {
@@ -482,9 +539,11 @@ int sw_compute(Ctx &c, cudaStream_t st) {
     if (ec.n < 0) return fail("sw_order: SW parameters are out of range");
     ec.c[0] = 1.0;
     for (int k = 1; k <= ec.n; k++) ec.c[k] = ec.c[k - 1] / (double)k;
-    k_sw_term<true><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw / c1, ec);
+    if (dd) k_sw_term<true, 1><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, dg, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw / c1, ec);
+    else k_sw_term<true, 0><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, dg, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw / c1, ec);
   } else {
-    k_sw_term<false><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw, ec);
+    if (dd) k_sw_term<false, 1><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, dg, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw, ec);
+    else k_sw_term<false, 0><<<(c.g.vol + t - 1) / t, t, 0, st>>>(c.g, dg, c.ud, c.swd, c.swd_inv, c1, -0.5 * c.csw, ec);
   }
   if (cudaGetLastError() != cudaSuccess) return fail("sw_term: launch failed");
   // the exponential form brings its exact inverse (1/c) exp(-A): no

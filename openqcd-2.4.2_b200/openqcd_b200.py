@@ -18,6 +18,11 @@ LIB_PATH = os.environ.get("B200_LIB", os.path.join(HERE, "libopenqcd_b200.so"))
 
 _lib = None
 
+# transport callbacks of the domain decomposition (b200_dd_setup)
+DD_EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                             C.c_void_p)
+DD_ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int, C.c_void_p)
+
 
 class Qflt(C.Structure):
     _fields_ = [("q", C.c_double * 2)]
@@ -201,6 +206,10 @@ _SIGS = {
                                     C.c_void_p]),
     "b200_set_block_order": (C.c_int, [C.c_int]),
     "b200_tune_block_order": (C.c_int, [C.c_void_p]),
+    "b200_dd_setup": (C.c_int, [C.c_int, C.c_int, DD_EXCHANGE_FN, DD_ALLGATHER_FN, C.c_void_p]),
+    "b200_dd_info": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_dd_global_sum": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "b200_set_sap_variant": (C.c_int, [C.c_int]),
     "b200_selfcheck_bounded_wait": (C.c_int, [C.c_int]),
     "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 }
@@ -960,3 +969,129 @@ def tmcg(nmx, istop, res, mu, eta, eo=False, psi0=None):
     if rho < 0:
         raise B200Error(_err_after())
     return psi, rho, ifail.value, status.value
+
+
+# ------------------------------------------------------------------------
+# Domain decomposition along x0: the transport the library calls back.
+
+class DomainDecomposition:
+    """Ranks of a torch.distributed group holding consecutive x0-slabs
+    (b200_dd_setup).  transport "host": the exchange synchronises the
+    library's stream, copies the two send faces to host memory, moves them
+    with point-to-point messages of the group's backend (gloo) and copies
+    the received faces back; "nccl": the faces move between the device
+    buffers with NCCL (torch's batch_isend_irecv), no host copy.  The
+    all-gather of the reduction partials goes through the same group.
+
+    memcpy(dst, src, nbytes) moves bytes between the library's buffers and
+    host memory (default: the library's own b200_memcpy); a test on CPU can
+    pass a host-only copy.  Call install() before b200_geometry."""
+
+    def __init__(self, group=None, transport="host", memcpy=None):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist, self.group = torch, dist, group
+        self.np = dist.get_world_size(group)
+        self.rank = dist.get_rank(group)
+        self.transport = transport
+        self.memcpy = memcpy or (lambda dst, src, n: check(lib().b200_memcpy(dst, src, n)))
+        self.sync_stream = memcpy is None      # a host-only copy (CPU test) has no stream to wait for
+        self._xfn = DD_EXCHANGE_FN(self._exchange)
+        self._gfn = DD_ALLGATHER_FN(self._allgather)
+        self.error = None
+
+    def install(self):
+        return check(lib().b200_dd_setup(self.np, self.rank, self._xfn, self._gfn, None))
+
+    def _peer(self, d):
+        return self.dist.get_global_rank(self.group, (self.rank + d) % self.np) if self.group is not None \
+            else (self.rank + d) % self.np
+
+    def _exchange(self, send_dn, send_up, recv_up, recv_dn, nbytes, stream, user):
+        try:
+            self.exchange(send_dn, send_up, recv_up, recv_dn, nbytes)
+            return 0
+        except Exception as e:          # reported to the library, which fails the call
+            self.error = e
+            return -1
+
+    def exchange(self, send_dn, send_up, recv_up, recv_dn, nbytes):
+        torch, dist = self.torch, self.dist
+        dn, up = self._peer(-1), self._peer(+1)
+        if self.transport == "nccl":
+            lib().b200_sync()
+            t = {k: _device_bytes(torch, p, nbytes) for k, p in
+                 (("sd", send_dn), ("su", send_up), ("ru", recv_up), ("rd", recv_dn))}
+            ops = [dist.P2POp(dist.isend, t["sd"], dn, self.group), dist.P2POp(dist.irecv, t["ru"], up, self.group),
+                   dist.P2POp(dist.isend, t["su"], up, self.group), dist.P2POp(dist.irecv, t["rd"], dn, self.group)]
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+            torch.cuda.current_stream().synchronize()
+            return
+        hs = [torch.empty(nbytes, dtype=torch.uint8) for _ in range(4)]
+        if self.sync_stream:
+            lib().b200_sync()
+        self.memcpy(hs[0].data_ptr(), send_dn, nbytes)
+        self.memcpy(hs[1].data_ptr(), send_up, nbytes)
+        # tag 1: faces moving down (send_dn -> the lower rank's recv_up);
+        # tag 2: faces moving up (send_up -> the upper rank's recv_dn)
+        reqs = [dist.isend(hs[0], dn, self.group, tag=1), dist.isend(hs[1], up, self.group, tag=2),
+                dist.irecv(hs[2], up, self.group, tag=1), dist.irecv(hs[3], dn, self.group, tag=2)]
+        for r in reqs:
+            r.wait()
+        self.memcpy(recv_up, hs[2].data_ptr(), nbytes)
+        self.memcpy(recv_dn, hs[3].data_ptr(), nbytes)
+
+    def _allgather(self, inp, out, n, user):
+        try:
+            torch, dist = self.torch, self.dist
+            x = torch.tensor([inp[k] for k in range(n)], dtype=torch.float64)
+            if self.transport == "nccl":
+                x = x.cuda()
+            parts = [torch.empty_like(x) for _ in range(self.np)]
+            dist.all_gather(parts, x, group=self.group)
+            k = 0
+            for p in parts:
+                for v in p.cpu().tolist():
+                    out[k] = v
+                    k += 1
+            return 0
+        except Exception as e:
+            self.error = e
+            return -1
+
+
+class _CudaBytes:
+    """A device byte range torch can wrap without copying."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (int(ptr), False), "version": 3}
+
+
+def _device_bytes(torch, ptr, n):
+    return torch.as_tensor(_CudaBytes(ptr, n), device="cuda")
+
+
+def dd_info():
+    bufs = (C.c_void_p * 4)()
+    nb = C.c_size_t(0)
+    nx = C.c_longlong(0)
+    npr = lib().b200_dd_info(bufs, C.byref(nb), C.byref(nx))
+    return npr, [b for b in bufs], nb.value, nx.value
+
+
+def dd_global_sum(pairs):
+    """the library's global double-double sum of (hi, lo) pairs over the ranks"""
+    a = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1)
+    out = np.zeros_like(a)
+    check(lib().b200_dd_global_sum(_ptr(a), _ptr(out), a.size // 2))
+    return out
+
+
+def dd_off():
+    """back to one rank (takes effect at the next geometry call)"""
+    return check(lib().b200_dd_setup(1, 0, DD_EXCHANGE_FN(0), DD_ALLGATHER_FN(0), None))
+
+
+def set_sap_variant(v):
+    return check(lib().b200_set_sap_variant(int(v)))
