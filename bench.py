@@ -609,11 +609,13 @@ def learned_c5(qb):
     """The learned preconditioner: a gauge-equivariant parallel-transport
     network (4-8-8-4 colour-triplet channels, FP16 weights at inference)
     trained on the device on 2048 (source, solution) pairs from the plain
-    solver on a 16^4 field (links exp(0.3 X), m0 = -0.05, csw = 1.7), then
-    used as the flexible-GCR preconditioner on a 32^3x64 field and on a
-    48^3x96 field (6^4 SAP blocks): GCR steps and seconds to FP64 residual
-    1e-10 with no preconditioner (32^3x64 only), the network (SAP when it
-    stalls), SAP, and the network followed by SAP."""
+    solver on a 16^4 field (links exp(0.3 X), m0 = -0.05, csw = 1.7), and a
+    second one trained on 512 (residual, SAP-error) pairs (the error
+    Dw^-1 r - M_sap r that five SAP cycles leave), then used as the
+    flexible-GCR preconditioner on a 32^3x64 field and on a 48^3x96 field
+    (6^4 SAP blocks): GCR steps and seconds to FP64 residual 1e-10 with no
+    preconditioner (32^3x64 only), the network (SAP when it stalls), SAP,
+    the network followed by SAP, and SAP plus the SAP-error network."""
     out = {"data": "synthetic"}
     L16 = (16, 16, 16, 16)
     qb.geometry(L16, BS, qb.even_first_ipt(L16))
@@ -634,6 +636,19 @@ def learned_c5(qb):
     out["training"] = {"steps": 1200, "batch": 8, "lr": 3e-3, "s": time.time() - t0,
                        "loss_first": float(hist[:10].mean()), "loss_last": float(hist[-50:].mean())}
     w = qb.net_get_weights()
+    # a second network, trained on (residual, SAP-error) pairs, added to SAP
+    # (M = M_sap + N): it learns what SAP leaves rather than the whole inverse
+    nsap = 512
+    t0 = time.time()
+    qb.net_make_sap_pairs(rs[:nsap], es[:nsap], 0.0, 1e-6, seed=4)
+    out["sap_error_pairs"] = {"n": nsap, "s": time.time() - t0}
+    qb.net_init(2, 0.1)
+    t0 = time.time()
+    hist2 = qb.net_train(rs[:nsap], es[:nsap], 600, 8, 3e-3, seed=10)
+    qb.lib().b200_sync()
+    out["sap_error_training"] = {"steps": 600, "batch": 8, "lr": 3e-3, "s": time.time() - t0,
+                                 "loss_first": float(hist2[:10].mean()), "loss_last": float(hist2[-50:].mean())}
+    w_sap = qb.net_get_weights()
     for f in rs + es:
         f.free()
     qb.release_workspace()
@@ -646,7 +661,8 @@ def learned_c5(qb):
     eta = qb.DevField(64).random(1.0, 31)
     psi = qb.DevField(64)
     res = {}
-    for kind, name in ((0, "sap"), (1, "network"), (2, "network+sap"), (3, "none")):
+    for kind, name in ((0, "sap"), (1, "network"), (2, "network+sap"), (3, "none"), (4, "sap+error-network")):
+        qb.net_set_weights(w_sap if kind == 4 else w)
         qb.set_precond(kind)
         qb.dev_sap_gcr(16, 8192, 0, 1e-10, 0.0, eta, psi) if kind != 3 else None
         qb.lib().b200_sync()
@@ -671,7 +687,8 @@ def learned_c5(qb):
     qb.set_precond(0)
     qb.dev_sap_gcr(16, 2, 0, 1e-10, 0.0, eta, psi)      # SAP autotuning for the 6^4 blocks, untimed
     res = {}
-    for kind, name in ((0, "sap"), (1, "network"), (2, "network+sap")):
+    for kind, name in ((0, "sap"), (1, "network"), (2, "network+sap"), (4, "sap+error-network")):
+        qb.net_set_weights(w_sap if kind == 4 else w)
         qb.set_precond(kind)
         qb.lib().b200_sync()
         t0 = time.time()

@@ -367,6 +367,12 @@ int b200_dfl_set_basis(int l, const spinor *field);
 int b200_dfl_get_basis(int l, spinor *field);
 /* dfl_modes.c:423 */ void dfl_modes(int *ifail, int *status);
 int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status);
+/* No reference counterpart.  The start fields of the next dfl_modes call
+ * (Ns FP32 fields in the reference's storage order, one after another),
+ * in place of the library's own random fields: with the fields the
+ * reference draws (random_fields, dfl_modes.c:248) the two generate the
+ * same subspace up to rounding.  Used once. */
+int b200_dfl_set_start_fields(const spinor *fields);
 /* dfl_subspace.c:171 */ void dfl_subspace(spinor **mds);
 /* dfl_subspace.c:83  */ void dfl_s2vd(spinor *s, complex_dble *vd);
 /* dfl_subspace.c:126 */ void dfl_vd2s(complex_dble *vd, spinor *s);
@@ -468,9 +474,15 @@ int b200_net_train(int npairs, void *const *r, void *const *e, int steps, int ba
 /* training pairs from the plain solver: r Gaussian, e = Dw(mu)^-1 r */
 int b200_net_make_pairs(int npairs, void *const *r, void *const *e, double mu, double res,
                         unsigned long long seed);
+/* (residual, SAP-error) pairs: r Gaussian, e = Dw(mu)^-1 r - M_sap r, the
+ * error that ncy SAP cycles from zero (current SAP parameters) leave */
+int b200_net_make_sap_pairs(int npairs, void *const *r, void *const *e, double mu, double res,
+                            unsigned long long seed);
 /* preconditioner of sap_gcr: 0 SAP (default), 1 the network (SAP once a
  * step reduces the residual by less than 10 %), 2 the network followed by
- * SAP on its residual, 3 none */
+ * SAP on its residual, 3 none, 4 SAP plus the network's correction
+ * M_sap r + N r (a network trained on SAP-error pairs; SAP alone once a
+ * step reduces the residual by less than 10 %) */
 int b200_set_precond(int kind);
 
 /* ------------------------------------ device-resident fields (own layout) */

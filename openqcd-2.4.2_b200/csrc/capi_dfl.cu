@@ -458,6 +458,23 @@ int b200_dev_dfl_modes(unsigned long long seed, int *ifail, int *status) {
   return qcd::dfl_modes_dev(c, seed, ifail, status);
 }
 
+// Start fields of the next dfl_modes call: Ns FP32 fields in the reference's
+// storage order, one after another (host or device memory).
+int b200_dfl_set_start_fields(const spinor *fields) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return -1;
+  qcd::DflState &d = c.dfl;
+  while ((int)d.start.size() < d.Ns) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, qcd::spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory");
+    d.start.push_back(p);
+  }
+  for (int l = 0; l < d.Ns; l++)
+    if (qcd::ref32_in(c, fields + (size_t)l * c.g.vol, d.start[l])) return -1;
+  d.use_start = true;
+  return cudaStreamSynchronize(c.stream) == cudaSuccess ? 0 : fail("CUDA error");
+}
+
 // dfl_modes.c:423 with the library's generator seeded by 1
 void dfl_modes(int *ifail, int *status) {
   if (b200_dev_dfl_modes(1ull, ifail, status) < 0 && ifail[0] == 0) ifail[0] = -2;

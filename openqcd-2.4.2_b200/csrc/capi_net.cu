@@ -92,8 +92,39 @@ int b200_net_make_pairs(int npairs, void *const *r, void *const *e, double mu, d
   return rc;
 }
 
+// Training pairs for a network that corrects SAP: r[k] a Gaussian residual
+// (FP32 copy), e[k] = Dw(mu)^-1 r[k] - M_sap r[k], the error the SAP
+// preconditioner (ncy cycles from zero with the current SAP parameters)
+// leaves, with Dw^-1 r from sap_gcr to relative residual res.
+int b200_net_make_sap_pairs(int npairs, void *const *r, void *const *e, double mu, double res,
+                            unsigned long long seed) {
+  Ctx &c = ctx();
+  if (b200_net_make_pairs(npairs, r, e, mu, res, seed)) return -1;
+  void *psi = nullptr, *rho = nullptr, *phi = nullptr;
+  const size_t nb = qcd::spinor_bytes(c, 32);
+  if (cudaMalloc(&psi, nb) != cudaSuccess || cudaMalloc(&rho, nb) != cudaSuccess ||
+      cudaMalloc(&phi, nb) != cudaSuccess) {
+    cudaFree(psi);
+    cudaFree(rho);
+    return fail("out of device memory");
+  }
+  int rc = 0;
+  for (int k = 0; k < npairs && rc == 0; k++) {
+    qcd::la_zero(c, 32, psi, qcd::PAR_ALL, c.stream);
+    qcd::la_copy(c, 32, r[k], 32, rho, qcd::PAR_ALL, c.stream);
+    if (qcd::sap_cycles(c, (float)mu, c.isolv, c.nmr, c.ncy, psi, rho, phi, c.stream)) rc = -1;
+    else qcd::la_axpy(c, 32, e[k], -1.0, 0.0, psi, qcd::PAR_ALL, c.stream);   // e = Dw^-1 r - M_sap r
+  }
+  cudaStreamSynchronize(c.stream);
+  cudaFree(psi);
+  cudaFree(rho);
+  cudaFree(phi);
+  return rc;
+}
+
 int b200_set_precond(int kind) {
-  if (kind < 0 || kind > 3) return fail("set_precond: kind must be 0 (SAP), 1 (network), 2 (network + SAP), 3 (none)");
+  if (kind < 0 || kind > 4)
+    return fail("set_precond: kind must be 0 (SAP), 1 (network), 2 (network + SAP), 3 (none), 4 (SAP + network)");
   ctx().precond = kind;
   return 0;
 }

@@ -806,6 +806,7 @@ void dfl_release(Ctx &c) {
   DflState &d = c.dfl;
   for (void *p : d.basis) cudaFree(p);
   for (void *p : d.modes) cudaFree(p);
+  for (void *p : d.start) cudaFree(p);
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
   void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop,
@@ -1284,7 +1285,13 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   if (c.sw_inv_fail & 2) ifail[0] = -3;
   void *ws0 = c.ws32[0], *phib = c.ws32[8];
   const float mug = (float)d.gen_mu;
-  for (int l = 0; l < d.Ns; l++) gen_uniform_spinor32(c, d.modes[l], seed * 1000003ull + l, st);
+  if (d.use_start) {
+    // the caller's start fields (e.g. the reference's ranlxs fields)
+    for (int l = 0; l < d.Ns; l++) la_copy(c, 32, d.start[l], 32, d.modes[l], PAR_ALL, st);
+    d.use_start = false;
+  } else {
+    for (int l = 0; l < d.Ns; l++) gen_uniform_spinor32(c, d.modes[l], seed * 1000003ull + l, st);
+  }
   dfl_mark(c, -1);
   if (ifail[0] == 0) {
     int n;

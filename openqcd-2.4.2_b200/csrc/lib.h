@@ -55,6 +55,10 @@ struct DflState {
   double2 *bpart = nullptr;                          // the same for batched restriction
   int *kerr = nullptr;                               // error flag of bounded waits in kernels
   std::vector<void *> basis, modes;
+  // start fields of the next dfl_modes (b200_dfl_set_start_fields), used
+  // instead of the library's own random fields, once
+  std::vector<void *> start;
+  bool use_start = false;
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
   bool aw_valid = false, awhat_valid = false;

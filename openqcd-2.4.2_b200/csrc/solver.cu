@@ -174,11 +174,13 @@ double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, c
       const int isolv = c.isolv, nmr = c.nmr, ncy = c.ncy;
       DopFn Dop = [&](const void *s, void *r) { dirac_op<double>(c, 0, mu, s, r, c.tmp64, c.stream); };
       const int kind = c.precond;
-      if (kind == 1 || kind == 2) {
+      const bool net = kind == 1 || kind == 2 || kind == 4;
+      if (net) {
         if (!c.net.ready) { fail("sap_gcr: the network preconditioner has no weights"); return -1.0; }
-        if (reserve(c, c.ws32, 2 * nkv + 3, 32)) return -1.0;
+        if (reserve(c, c.ws32, 2 * nkv + 4, 32)) return -1.0;
       }
-      void *ws2 = (kind == 1 || kind == 2) ? c.ws32[2 * nkv + 2] : nullptr;
+      void *ws2 = net ? c.ws32[2 * nkv + 2] : nullptr;
+      void *ws3 = kind == 4 ? c.ws32[2 * nkv + 3] : nullptr;
       bool fallback = false;
       double rn_prev = -1.0;
       auto sap_mop = [&](const void *rh, void *ph, void *ch) {
@@ -187,6 +189,23 @@ double sap_gcr_dev(Ctx &c, int nkv, int nmx, int istop, double res, double mu, c
       MopFn Mop = [&](int, const void *rh, void *ph, void *ch) {
         if (kind == 0) {
           sap_mop(rh, ph, ch);
+        } else if (kind == 4) {
+          // SAP plus the network's estimate of the error SAP leaves (a
+          // network trained on (residual, SAP-error) pairs):
+          // ph = M_sap rh + N rh, ch = D ph; the network part is dropped
+          // once a step reduces the residual by less than 10 %
+          double r2[2];
+          la_norm2(c, 32, rh, PAR_ALL, r2);
+          const double rn = sqrt(r2[0] + r2[1]);
+          if (rn_prev > 0.0 && rn > 0.9 * rn_prev) fallback = true;
+          rn_prev = rn;
+          sap_mop(rh, ph, ch);
+          if (!fallback) {
+            net_apply(c, rh, ws2, true, c.stream);
+            dirac_op<float>(c, 0, muf, ws2, ws3, c.tmp32, c.stream);
+            la_axpy(c, 32, ph, 1.0, 0.0, ws2, PAR_ALL, c.stream);
+            la_axpy(c, 32, ch, 1.0, 0.0, ws3, PAR_ALL, c.stream);
+          }
         } else if (kind == 3) {
           la_copy(c, 32, rh, 32, ph, PAR_ALL, c.stream);
           dirac_op<float>(c, 0, muf, ph, ch, c.tmp32, c.stream);

@@ -210,6 +210,9 @@ _SIGS = {
     "b200_dd_info": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_dd_global_sum": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "b200_set_sap_variant": (C.c_int, [C.c_int]),
+    "b200_net_make_sap_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                          C.c_ulonglong]),
+    "b200_dfl_set_start_fields": (C.c_int, [C.c_void_p]),
     "b200_selfcheck_bounded_wait": (C.c_int, [C.c_int]),
     "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 }
@@ -660,6 +663,12 @@ def dfl_modes(seed=1):
     return ifail.value, list(status)
 
 
+def dfl_set_start_fields(fields):
+    """start fields of the next dfl_modes (Ns FP32 reference-layout fields)"""
+    f = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float32).reshape(-1) for x in fields]))
+    return check(lib().b200_dfl_set_start_fields(_ptr(f)))
+
+
 def dfl_subspace(modes):
     arrs = [np.ascontiguousarray(m, dtype=np.float32) for m in modes]
     ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
@@ -925,7 +934,16 @@ def net_make_pairs(rs, es, mu, res, seed=1):
     return check(lib().b200_net_make_pairs(n, rp, ep, mu, res, seed))
 
 
+def net_make_sap_pairs(rs, es, mu, res, seed=1):
+    """(residual, SAP-error) training pairs: es[k] = Dw^-1 rs[k] - M_sap rs[k]"""
+    n = len(rs)
+    rp = (C.c_void_p * n)(*[x.ptr for x in rs])
+    ep = (C.c_void_p * n)(*[x.ptr for x in es])
+    return check(lib().b200_net_make_sap_pairs(n, rp, ep, mu, res, seed))
+
+
 def set_precond(kind):
+    """0 SAP, 1 network, 2 network then SAP, 3 none, 4 SAP plus the network"""
     return check(lib().b200_set_precond(kind))
 
 

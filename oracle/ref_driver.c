@@ -497,6 +497,33 @@ int ref_dfl_modes(int seed, int *status)
    return ifail;
 }
 
+/* The Ns start fields dfl_modes() draws after start_ranlux(0, seed)
+ * (random_fields, modules/dfl/dfl_modes.c:248-264): every real component
+ * uniform in [-0.5, 0.5), drawn with ranlxs by each OpenMP thread for its
+ * VOLUME_TRD sites in turn, field after field.  Written one field after
+ * another in ipt order. */
+void ref_dfl_random_fields(int seed, int Ns, float *out)
+{
+   ENTER();
+   int l;
+   start_ranlux(0, seed);
+   for (l = 0; l < Ns; l++)
+   {
+      float *f = out + (size_t)l * VOLUME * 24;
+#pragma omp parallel
+      {
+         int k = omp_get_thread_num(), i, j;
+         float *p = f + (size_t)k * VOLUME_TRD * 24;
+         for (i = 0; i < VOLUME_TRD; i++, p += 24)
+         {
+            ranlxs(p, 24);
+            for (j = 0; j < 24; j++)
+               p[j] -= 0.5f;
+         }
+      }
+   }
+}
+
 /* dfl_subspace() (modules/dfl/dfl_subspace.c:171) on Ns FP32 fields given
  * one after another in ipt order. */
 void ref_dfl_subspace(int Ns, const float *modes)

@@ -260,6 +260,13 @@ class RefLib:
         f = self.lib.ref_dfl_modes(seed, status)
         return f, list(status)
 
+    def dfl_random_fields(self, seed, Ns):
+        """the start fields of dfl_modes after start_ranlux(0, seed), [Ns, V*24] FP32"""
+        out = np.zeros((Ns, self.vol * 24), dtype=np.float32)
+        self.lib.ref_dfl_random_fields.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        self.lib.ref_dfl_random_fields(seed, Ns, self._p(out))
+        return out
+
     def dfl_subspace(self, modes):
         m = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float32) for x in modes]))
         self.lib.ref_dfl_subspace.argtypes = [C.c_int, C.c_void_p]

@@ -105,3 +105,49 @@ def test_train_and_precondition(setup):
           % (it_none, it_net, it_sap, it_both, hist[:5].mean(), hist[-30:].mean()))
     assert it_net < it_none
     assert it_both <= it_sap + 2
+
+
+def test_sap_error_pairs_and_sap_plus_network(setup):
+    """(residual, SAP-error) pairs: e + M_sap r solves D x = r (to the
+    solver's residual); a network trained on them, added to SAP (kind 4),
+    reaches the FP64 residual in no more steps than SAP alone plus two"""
+    n = 32
+    rs = [qb.DevField(32) for _ in range(n)]
+    es = [qb.DevField(32) for _ in range(n)]
+    qb.set_precond(0)
+    qb.net_make_sap_pairs(rs, es, 0.0, 1e-6, seed=13)
+    # check one pair: D (e + M_sap r) = r
+    r = rs[0].to_ref(setup.vol).astype(np.float64)
+    e = es[0].to_ref(setup.vol).astype(np.float64)
+    psi, rho = qb.sap_ref(0.0, 1, 4, np.zeros_like(r, dtype=np.float32), r.astype(np.float32))
+    for _ in range(4):   # ncy = 5 cycles in all, as the pairs were made
+        psi, rho = qb.sap_ref(0.0, 1, 4, psi, rho)
+    x = e + psi.astype(np.float64)
+    res = np.linalg.norm(setup.ref.dirac_dble(0, 0.0, x) - r) / np.linalg.norm(r)
+    assert res < 1e-4, res
+    qb.net_init(5, 0.1)
+    hist = qb.net_train(rs, es, 200, 4, 3e-3, seed=6)
+    assert np.isfinite(hist).all()
+    eta = setup.source(79)
+    it_sap = iterations(setup, 0, eta)
+    it_4 = iterations(setup, 4, eta)
+    assert it_4 <= it_sap + 2, (it_4, it_sap)
+
+
+def test_poisoned_network_falls_back_to_sap(setup):
+    """a network with garbage weights: the network preconditioner (kind 1)
+    and SAP plus network (kind 4) stall, drop the network after one step
+    that reduces the residual by less than 10 %, and still reach the FP64
+    residual 1e-10 through SAP"""
+    w = qb.net_get_weights()
+    rng = np.random.default_rng(3)
+    try:
+        qb.net_set_weights((50.0 * rng.standard_normal(w.size)).astype(np.float32))
+        eta = setup.source(81)
+        it_sap = iterations(setup, 0, eta)
+        for kind in (1, 4):
+            it = iterations(setup, kind, eta)     # asserts the true residual
+            assert it <= 4 * it_sap + 8, (kind, it, it_sap)
+    finally:
+        qb.net_set_weights(w)
+        qb.set_precond(0)
