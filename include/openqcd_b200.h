@@ -277,6 +277,18 @@ int b200_set_block_order(int kind);
  * separate runs use the same arithmetic; -1 lets the autotuner choose again
  * (no reference counterpart). */
 int b200_set_sap_variant(int variant);
+/* Block-shape autotuner (no reference counterpart).  For each candidate
+ * SAP block shape cand[4 i .. 4 i + 3] (i < ncand) that fits the lattice,
+ * the resident gauge and SW fields are laid out again with it, and nsteps
+ * steps of the SAP-preconditioned GCR (current isolv, nmr, ncy) on a
+ * Gaussian source are timed: score[i] = ln(|eta| / |residual|) / seconds
+ * (-1 for shapes that do not fit).  Ns > 0: the shape is also the DFL
+ * block; every candidate gets an Ns-mode subspace (dfl_modes with the
+ * current generation parameters, not timed) and the deflated solver's
+ * steps are timed.  The best shape stays in force (the geometry and the SAP
+ * parameters now use it; deflation must be set up again); returns its
+ * index.  Needs the ipt[] of the geometry call. */
+int b200_tune_block_shape(const int *cand, int ncand, int nsteps, double mu, int Ns, float *score);
 int b200_tune_block_order(float *ms);
 /* on != 0 (default): the SAP preconditioner's launch sequence (ncy cycles of
  * block solves and boundary updates with the copies around them) is

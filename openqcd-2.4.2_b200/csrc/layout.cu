@@ -145,6 +145,7 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
     cudaMemcpy(c.d_dev2q, d2q.data(), g.vol * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(c.d_link2q, l2q.data(), 4 * (size_t)g.vol * sizeof(int), cudaMemcpyHostToDevice);
     c.h_dev2q = d2q;
+    c.h_ipt.assign(ipt, ipt + g.vol);
     c.have_ipt = true;
   }
   // x0-slab plan: the thinnest slabs (a whole number of block rows, at least

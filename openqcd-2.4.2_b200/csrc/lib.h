@@ -114,6 +114,7 @@ struct Ctx {
   int *d_dev2q = nullptr;       // [vol] device site (chunk*vbh+s) -> reference index ix
   int *d_link2q = nullptr;      // [4*vol] (device site, mu) -> slot in the reference ud[4V]
   std::vector<int> h_dev2q;
+  std::vector<int> h_ipt;       // the caller's ipt[] (for a change of block shape)
   // x0-slab plan for pipelined host transfers (empty if the storage order
   // has no contiguous slabs), the identity block list, the copy streams
   std::vector<Slab> slab;

@@ -15,6 +15,7 @@
 // ltl_gcr_b is the little solver of ltl_gcr.c:155 for nr little systems in
 // lock step, with per-system convergence.
 #include "lib.h"
+#include <array>
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -592,6 +593,64 @@ static int bw_reserve(Ctx &c, std::vector<void *> &v, size_t n, int prec) {
   return 0;
 }
 
+// The little operators of the masses of a deflated batch: the first lives
+// in the deflation state's own arrays, the others in arrays of the same
+// sizes; use(j) points the state at set j.  The state's own arrays hold
+// set 0 again when the batch ends (the destructor), marked stale.
+struct LittleSets {
+  Ctx *c = nullptr;
+  double2 *own[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<std::array<double2 *, 4>> set;
+  std::vector<double> mu;
+  std::vector<int> fail;
+  int build(Ctx &cc, const std::vector<double> &umu, cudaStream_t st) {
+    c = &cc;
+    DflState &d = cc.dfl;
+    own[0] = d.Ablk; own[1] = d.Ainv; own[2] = d.Ahop; own[3] = d.Mhop;
+    const size_t m = (size_t)d.nb * d.Ns * d.Ns * sizeof(double2);
+    const size_t sz[4] = {m, m, 8 * m, 8 * m};
+    mu = umu;
+    set.assign(umu.size(), {nullptr, nullptr, nullptr, nullptr});
+    fail.assign(umu.size(), 0);
+    for (size_t j = 0; j < umu.size(); j++) {
+      for (int k = 0; k < 4; k++) {
+        if (j == 0) set[j][k] = own[k];
+        else if (cudaMalloc(&set[j][k], sz[k]) != cudaSuccess) return qcd::fail("gcr_batch: out of device memory (little operators)");
+      }
+      point(j);
+      if (umu.size() > 1) d.aw_valid = d.awhat_valid = false;
+      const int f = dfl_set_Awhat(cc, umu[j], st);
+      if (f < 0) return -1;
+      fail[j] = f;
+    }
+    return 0;
+  }
+  void point(size_t j) {
+    DflState &d = c->dfl;
+    d.Ablk = set[j][0]; d.Ainv = set[j][1]; d.Ahop = set[j][2]; d.Mhop = set[j][3];
+  }
+  void use(Ctx &cc, size_t j) {
+    if (set.size() <= 1) return;
+    DflState &d = cc.dfl;
+    point(j);
+    d.aw_valid = d.awhat_valid = true;
+    d.aw_mu = mu[j];
+    d.aw_eo = cc.eoflg;
+    d.awhat_fail = fail[j];
+    d.awhat_ver++;
+  }
+  ~LittleSets() {
+    if (!c || set.size() <= 1) return;
+    DflState &d = c->dfl;
+    cudaStreamSynchronize(c->stream);
+    for (size_t j = 1; j < set.size(); j++)
+      for (int k = 0; k < 4; k++) cudaFree(set[j][k]);
+    d.Ablk = own[0]; d.Ainv = own[1]; d.Ahop = own[2]; d.Mhop = own[3];
+    d.aw_valid = d.awhat_valid = false;   // set 0's arrays hold the first mass; recompute on demand
+    d.awhat_ver++;
+  }
+};
+
 // nr systems Dw(mu[r]) psi[r] = eta[r] (FP64 device fields), flexible GCR
 // with SAP (dfl = 0) or deflated SAP (dfl = 1) preconditioning as in
 // sap_gcr / dfl_sap_gcr.  rho[r] = residual norm, ifail[r], status[r] as
@@ -605,10 +664,20 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
   if (nkv < 1 || nmx < 1 || res <= DBL_EPSILON || istop < 0 || istop > 1) return fail("gcr_batch: parameters are out of range");
   if (!c.sap_set) return fail("gcr_batch: SAP parameters are not set");
   if (!c.have_ud || !c.have_sw) return fail("gcr_batch: gauge or SW field missing on the device");
+  // the distinct twisted masses of the batch and each system's group; the
+  // little operator depends on the mass, so each group has its own
+  // (restriction, prolongation and SAP are shared by all systems)
+  std::vector<double> umu;
+  std::vector<int> grp(nr);
+  for (int r = 0; r < nr; r++) {
+    int j = 0;
+    while (j < (int)umu.size() && umu[j] != mu[r]) j++;
+    if (j == (int)umu.size()) umu.push_back(mu[r]);
+    grp[r] = j;
+  }
+  LittleSets lsets;
   if (dfl) {
     if (!d.ready || !d.have_basis) return fail("gcr_batch: the deflation subspace is not set");
-    for (int r = 1; r < nr; r++)
-      if (mu[r] != mu[0]) return fail("gcr_batch: deflation needs the same twisted mass for all systems");
     if (dfl_batch_alloc(c)) return -1;
   }
   if (sap_prepare(c, st) || ortho_alloc()) return -1;
@@ -670,12 +739,13 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
     }
   }
   if (dfl) {
-    if (dfl_set_Awhat(c, mu[0], st)) {
-      for (int r = 0; r < nr; r++) {
+    // one little operator per mass (set_Awhat, dfl_modes.c / Aw_ops.c:223)
+    if (lsets.build(c, umu, st)) return -1;
+    for (int r = 0; r < nr; r++)
+      if (lsets.fail[grp[r]]) {
         ifail[r] = -2;
         S[r].active = false;
       }
-    }
   }
   for (;;) {
     std::vector<int> A;
@@ -698,7 +768,26 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
         w0[i] = S[A[i]].ws0;
       }
       dfl_restrict_b(c, na, rh.data(), v.data(), st);
-      if (ltl_gcr_b(c, mu[0], na, (const double2 *const *)v.data(), v.data(), lf.data(), ls.data(), st)) return -1;
+      // the little systems, one batch per mass
+      for (int j = 0; j < (int)umu.size(); j++) {
+        std::vector<double2 *> vj;
+        std::vector<int> ij;
+        for (int i = 0; i < na; i++)
+          if (grp[A[i]] == j) {
+            vj.push_back(v[i]);
+            ij.push_back(i);
+          }
+        if (vj.empty()) continue;
+        lsets.use(c, j);
+        std::vector<int> lfj(vj.size()), lsj(vj.size());
+        if (ltl_gcr_b(c, umu[j], (int)vj.size(), (const double2 *const *)vj.data(), vj.data(), lfj.data(),
+                      lsj.data(), st))
+          return -1;
+        for (size_t q = 0; q < ij.size(); q++) {
+          lf[ij[q]] = lfj[q];
+          ls[ij[q]] = lsj[q];
+        }
+      }
       dfl_prolong_b(c, na, (const double2 *const *)v.data(), w0.data(), st);
       dfl_mark(c, 3);
       for (int i = 0; i < na; i++) {
@@ -708,7 +797,7 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
         void *in = sap_input_field(c);
         if (!in) in = ch;
         void *const rv[1] = {in}, *const bv[1] = {y.rho};
-        dirac_multi32(c, 1, (float)mu[0], &w0[i], rv, bv, st);
+        dirac_multi32(c, 1, (float)y.mu, &w0[i], rv, bv, st);
         dfl_mark(c, 3);
         // SAP on it, then ch = rho - (final residual), ph += ws0
         sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, in, ph, ch, phib, st, y.rho, y.ws0);

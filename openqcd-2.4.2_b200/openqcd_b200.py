@@ -213,6 +213,7 @@ _SIGS = {
     "b200_net_make_sap_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                           C.c_ulonglong]),
     "b200_dfl_set_start_fields": (C.c_int, [C.c_void_p]),
+    "b200_tune_block_shape": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p]),
     "b200_selfcheck_bounded_wait": (C.c_int, [C.c_int]),
     "b200_time_Dw_dble_host": (C.c_int, [C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
 }
@@ -1109,6 +1110,17 @@ def dd_global_sum(pairs):
 def dd_off():
     """back to one rank (takes effect at the next geometry call)"""
     return check(lib().b200_dd_setup(1, 0, DD_EXCHANGE_FN(0), DD_ALLGATHER_FN(0), None))
+
+
+def tune_block_shape(candidates, nsteps=8, mu=0.0, Ns=0):
+    """the block-shape autotuner: returns (the best shape, the score of every
+    candidate: residual reduction ln(|eta|/|r|) per second, -1 if it does
+    not fit); Ns > 0 scores the deflated solver with an Ns-mode subspace per
+    candidate; the best shape stays in force"""
+    c = np.ascontiguousarray(np.asarray(candidates, dtype=np.int32).reshape(-1, 4))
+    sc = np.zeros(len(c), dtype=np.float32)
+    k = check(lib().b200_tune_block_shape(_ptr(c), len(c), nsteps, mu, Ns, _ptr(sc)))
+    return tuple(int(v) for v in c[k]), [float(v) for v in sc]
 
 
 def set_sap_variant(v):

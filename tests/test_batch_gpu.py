@@ -7,7 +7,8 @@ single-system solver give or take one, with a solution equal to the
 single-system one to 1e-8 (the batched solver orthogonalises by classical
 Gram-Schmidt in fused passes, and its restriction and little solver sum in
 another order).  Systems of different twisted masses and a zero source
-share a batch; systems leave it as they converge."""
+share a batch (with deflation, one little operator per mass); systems
+leave it as they converge."""
 import numpy as np
 import pytest
 
@@ -106,11 +107,27 @@ def test_dfl_batch_matches_single(dfl, nr):
         assert true_res(dfl, mu, psi, etas[i]) <= 1.5e-10
 
 
-def test_dfl_batch_needs_one_mass(dfl):
-    E = [dev(64, dfl.source(60)), dev(64, dfl.source(61))]
-    P = [dev(64), dev(64)]
-    with pytest.raises(qb.B200Error):
-        qb.dev_gcr_batch(16, 256, 0, 1e-10, [0.0, 0.01], E, P, dfl=True)
+def test_dfl_batch_mixed_masses(dfl):
+    """systems of different twisted masses share one deflated batch: each
+    mass gets its own little operator, the restriction, prolongation and
+    SAP are shared; every system equals its single-system solve"""
+    mus = [0.0, 0.01, 0.0, 0.03]
+    etas = [dfl.source(60 + i) for i in range(len(mus))]
+    singles = []
+    for mu, eta in zip(mus, etas):
+        e, p = dev(64, eta), dev(64)
+        rho, ifail, st = qb.dev_dfl_sap_gcr(16, 256, 0, 1e-10, mu, e, p)
+        assert ifail == 0
+        singles.append((p.to_ref(dfl.vol), st[0]))
+    E = [dev(64, e) for e in etas]
+    P = [dev(64) for _ in etas]
+    rho, ifail, st, lst = qb.dev_gcr_batch(16, 256, 0, 1e-10, mus, E, P, dfl=True)
+    assert ifail == [0] * len(mus)
+    for i, mu in enumerate(mus):
+        psi = P[i].to_ref(dfl.vol)
+        assert abs(st[i] - singles[i][1]) <= 1, (st, [x[1] for x in singles])
+        assert rel_norm_err(psi, singles[i][0]) <= 1e-8
+        assert true_res(dfl, mu, psi, etas[i]) <= 1.5e-10
     qb.release_workspace()
 
 
