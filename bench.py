@@ -414,6 +414,9 @@ def main():
     ap.add_argument("--profile-solver", action="store_true",
                     help="run only the 48^3x96 solver comparison, with profiler collection around the chosen solve")
     ap.add_argument("--solver-lattice", default=None, help="L0,L1,L2,L3 for --profile-solver (smaller cases)")
+    ap.add_argument("--scan-block-orders", action="store_true",
+                    help="run only Dw_dble under each block traversal order (timings; the first 10 launches "
+                         "are the ones an ncu traffic capture takes)")
     ap.add_argument("--profile-setup", action="store_true",
                     help="run only the deflation subspace generation of the solver workload, with profiler "
                          "collection around it, and print its phase times")
@@ -423,6 +426,11 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, d)
+        if args.scan_block_orders:
+            import openqcd_b200 as qb
+            qb.set_device(d.local)
+            print(json.dumps(scan_block_orders(qb)))
+            return 0
         if args.profile_setup:
             import openqcd_b200 as qb
             qb.set_device(d.local)
@@ -510,10 +518,39 @@ def solver_c3(qb, profile=False, lattice=None):
                                "dfl_modes, ninv=10), nkv=8, isolv=1, nmr=3, ncy=2, FP32 SAP/Krylov, FP64 "
                                "residual, multi-RHS restriction/prolongation/little solver"}
     out["speedup_per_rhs"] = t_plain / t_chosen
+    # right-hand sides per gauge field after which the subspace generation
+    # has paid for itself
+    out["break_even_rhs"] = t_setup / (t_plain - t_chosen) if t_plain > t_chosen else None
     for fld in E + P:
         fld.free()
     psi.free()
     qb.release_workspace()
+    return out
+
+
+def scan_block_orders(qb):
+    """Dw_dble on 32^3x64 under each block traversal order: first two
+    launches per order (the launches a 10-launch ncu capture of
+    dirac_staged sees), then 3 x 20 timed launches per order."""
+    L = LATTICE
+    qb.geometry(L, BS, qb.even_first_ipt(L))
+    qb.set_parms(CSW, M0, 0)
+    qb.random_ud(EPS, FIELD_SEED)
+    qb.sw_term()
+    s = qb.DevField(64).random(1.0, SOURCE_SEED)
+    r = qb.DevField(64)
+    vol = qb.lib().b200_volume()
+    for k in range(5):
+        qb.set_block_order(k)
+        qb.dev_dirac("Dw", 0.0, s, r)
+        qb.dev_dirac("Dw", 0.0, s, r)
+    out = {}
+    for k in range(5):
+        qb.set_block_order(k)
+        qb.time_dirac(64, "Dw", 0.0, s, r, 5)
+        ms = [qb.time_dirac(64, "Dw", 0.0, s, r, 20) / 20 for _ in range(3)]
+        out[k] = {"ms": ms, "GBs": BYTES_PER_SITE[64] * vol / (min(ms) / 1e3) / 1e9}
+    qb.set_block_order(0)
     return out
 
 
@@ -629,6 +666,11 @@ def batched_c4(qb):
                                "mass), Ns=28, nkv=8, nmr=4, ncy=2, autotuned block shape and RHS tile"}
     out["plain_s_per_rhs_mean"] = sum(p["s"] for p in plain) / len(plain)
     out["speedup_per_rhs"] = out["plain_s_per_rhs_mean"] / out["chosen"]["s_per_rhs"]
+    gain = out["plain_s_per_rhs_mean"] - out["chosen"]["s_per_rhs"]
+    # right-hand sides per gauge field that pay for the subspace (and, once
+    # per lattice and parameter set, for the block-shape tuning as well)
+    out["break_even_rhs"] = setup / gain if gain > 0 else None
+    out["break_even_rhs_with_tuning"] = (setup + out["block_shape"]["s"]) / gain if gain > 0 else None
     out["rhs_tiles"] = qb.rhs_tiles()
     for f in srcs + P:
         f.free()
