@@ -374,6 +374,14 @@ int b200_dfl_profile(int on, double *out);
  * vector (its: GCR steps of the last solve), 5-7 the batched restriction,
  * prolongation and little solver on four right-hand sides. */
 int b200_dfl_time(int what, int n, float *ms, int *its);
+/* dfl_s2vd (dfl_subspace.c:83) and dfl_vd2s (:126) of nr fields at once
+ * (1 <= nr <= 16; the batching has no reference counterpart): fields in the
+ * reference layout, little vectors in the reference's block order, host or
+ * device memory.  Four fields per pass run on the tensor cores (TF32
+ * head/tail split products, FP32 accumulation, block sums in FP64), the rest
+ * on the CUDA cores; the results are rounded to FP32 as the reference's. */
+int b200_dfl_s2vd_multi(int nr, spinor *const *s, complex_dble *const *vd);
+int b200_dfl_vd2s_multi(int nr, complex_dble *const *vd, spinor *const *s);
 /* Basis vector l of every block as one global FP32 field, reference layout. */
 int b200_dfl_set_basis(int l, const spinor *field);
 int b200_dfl_get_basis(int l, spinor *field);
@@ -428,11 +436,18 @@ int b200_dfl_set_start_fields(const spinor *fields);
 /* ltl_gcr.c:155 */ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int *status);
 int b200_set_ltl_solver(int kind);
 /* RHS-tile autotuner of the multi-right-hand-side restriction and
- * prolongation (fields per pass: 1, 2 or 4, chosen by timing on the first
- * call with four or more fields per geometry): tile[0] restriction, tile[1]
- * prolongation (0: not tuned yet); ms[0..2] and ms[3..5] the times of four
- * fields with tiles 1, 2 and 4.  No reference counterpart. */
-int b200_rhs_tiles(int tile[2], float ms[6]);
+ * prolongation: one, two or four fields per pass on the CUDA cores, or four
+ * fields on the tensor cores, chosen by timing on the first call with four
+ * or more fields per geometry and deflation set-up.  tile[0] restriction,
+ * tile[1] prolongation (fields per pass, 0: not tuned yet), tc[k] = 1 when
+ * the four-field pass of k runs on the tensor cores; ms[0..3] and ms[4..7]
+ * the times of four fields with the kinds (1, 2, 4 on the CUDA cores, 4 on
+ * the tensor cores).  No reference counterpart. */
+int b200_rhs_tiles(int tile[2], int tc[2], float ms[8]);
+/* Fixes the RHS tiles of the current geometry and deflation set-up
+ * (tile[k] in {1, 2, 4}, tc[k] for four fields on the tensor cores; tile[k]
+ * = 0 hands k back to the autotuner).  No reference counterpart. */
+int b200_set_rhs_tiles(const int tile[2], const int tc[2]);
 /* Little mode l (nv complex floats) for a subspace uploaded as a basis with
  * b200_dfl_set_basis; dfl_subspace() and dfl_modes() set them themselves
  * (no reference counterpart). */

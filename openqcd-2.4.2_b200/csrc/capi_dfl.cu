@@ -272,6 +272,43 @@ void dfl_vd2s(complex_dble *vd, spinor *s) {
   qcd::ref32_out(c, f, s);
 }
 
+// dfl_s2vd / dfl_vd2s of nr fields at once through the batched kernels
+// (four fields per pass on the tensor cores, the rest on the CUDA cores)
+int b200_dfl_s2vd_multi(int nr, spinor *const *s, complex_dble *const *vd) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || !c.dfl.have_basis) return c.dfl.ready ? fail("dfl_s2vd_multi: no deflation subspace") : -1;
+  if (nr < 1 || nr > 16) return fail("dfl_s2vd_multi: nr must be in [1, 16]");
+  if (qcd::dfl_batch_alloc(c) || qcd::ensure_lvd_n(c, nr)) return -1;
+  std::vector<const void *> f(nr);
+  for (int r = 0; r < nr; r++) {
+    void *p = qcd::spinor_stage(c, 32, r);
+    if (!p || qcd::ref32_in(c, s[r], p)) return -1;
+    f[r] = p;
+  }
+  qcd::dfl_restrict_b(c, nr, f.data(), c.dfl.lvd.data(), c.stream);
+  for (int r = 0; r < nr; r++)
+    cudaMemcpyAsync(vd[r], c.dfl.lvd[r], (size_t)c.dfl.nv * sizeof(double2), cudaMemcpyDefault, c.stream);
+  if (b200_sync()) return -1;
+  return qcd::dfl_batch_check(c);
+}
+
+int b200_dfl_vd2s_multi(int nr, complex_dble *const *vd, spinor *const *s) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c) || !c.dfl.have_basis) return c.dfl.ready ? fail("dfl_vd2s_multi: no deflation subspace") : -1;
+  if (nr < 1 || nr > 16) return fail("dfl_vd2s_multi: nr must be in [1, 16]");
+  if (qcd::dfl_batch_alloc(c) || qcd::ensure_lvd_n(c, nr)) return -1;
+  std::vector<void *> f(nr);
+  for (int r = 0; r < nr; r++) {
+    f[r] = qcd::spinor_stage(c, 32, r);
+    if (!f[r]) return -1;
+    cudaMemcpyAsync(c.dfl.lvd[r], vd[r], (size_t)c.dfl.nv * sizeof(double2), cudaMemcpyDefault, c.stream);
+  }
+  qcd::dfl_prolong_b(c, nr, (const double2 *const *)c.dfl.lvd.data(), f.data(), c.stream);
+  for (int r = 0; r < nr; r++)
+    if (qcd::ref32_out(c, f[r], s[r])) return -1;
+  return qcd::dfl_batch_check(c);
+}
+
 void set_Aw(double mu) {
   Ctx &c = ctx();
   if (qcd::dfl_ready(c) || qcd::fields_ready(c)) return;
@@ -330,7 +367,8 @@ double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int 
 // restriction (tile[0]) and prolongation (tile[1]), 0 if not tuned yet, and
 // the times of four fields with tiles 1, 2, 4 (ms[0..2] restriction,
 // ms[3..5] prolongation)
-int b200_rhs_tiles(int *tile, float *ms) { return qcd::rhs_tiles(ctx(), tile, ms); }
+int b200_rhs_tiles(int *tile, int *tc, float *ms) { return qcd::rhs_tiles(ctx(), tile, tc, ms); }
+int b200_set_rhs_tiles(const int *tile, const int *tc) { return qcd::set_rhs_tiles(ctx(), tile, tc); }
 
 int b200_set_ltl_solver(int kind) {
   Ctx &c = ctx();

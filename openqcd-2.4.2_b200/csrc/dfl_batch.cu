@@ -6,6 +6,7 @@
 // keeps its own arithmetic: the results equal those of the single-system
 // routines of dfl.cu up to the summation order.
 #include "lib.h"
+#include "mma.cuh"
 #include "tma.cuh"
 #include <algorithm>
 #include <cmath>
@@ -26,59 +27,6 @@ constexpr int BSPLIT_T = 352;    // threads of a restriction/prolongation CTA
 static int chunk_split(int vbh) { return (vbh + BSPLIT_T - 1) / BSPLIT_T; }
 
 // ------------------------------------------------------------- restriction
-// part[(n, y, r, l)] = (basis_l, x_r) over the sites of CTA y of block n
-template <int NRT>
-__global__ void __launch_bounds__(BSPLIT_T) k_restrict_b(Geom g, const int *__restrict__ vd2lex,
-                                                         const float4 *const *__restrict__ basis, int Ns,
-                                                         Ptrs<NRT> x, int nsplit, double2 *part) {
-  extern __shared__ double2 red[];   // [Ns][NRT][nw]
-  const int n = blockIdx.x, y = blockIdx.y, p = y / nsplit, h = y - p * nsplit;
-  const int blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
-  const int per = (g.vbh + nsplit - 1) / nsplit, si = h * per + threadIdx.x;
-  const bool ok = (int)threadIdx.x < per && si < g.vbh;
-  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  spinor<float> xs[NRT];
-#pragma unroll
-  for (int r = 0; r < NRT; r++) {
-    szero(xs[r]);
-    if (ok) xs[r] = Store<float>::load_spinor(x.p[r], chunk, si, g.vbh);
-  }
-  for (int l = 0; l < Ns; l++) {
-    spinor<float> b;
-    szero(b);
-    if (ok) b = Store<float>::load_spinor(basis[l], chunk, si, g.vbh);
-#pragma unroll
-    for (int r = 0; r < NRT; r++) {
-      float sr = 0.0f, sim = 0.0f;
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          const cpx<float> bb = b.c[a].c[k], xx = xs[r].c[a].c[k];
-          sr += bb.re * xx.re + bb.im * xx.im;
-          sim += bb.re * xx.im - bb.im * xx.re;
-        }
-      double re = sr, im = sim;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_down_sync(0xffffffffu, re, o);
-        im += __shfl_down_sync(0xffffffffu, im, o);
-      }
-      if (lane == 0) red[((size_t)l * NRT + r) * nw + wp] = make_double2(re, im);
-    }
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < Ns * NRT; q += blockDim.x) {
-    double re = 0.0, im = 0.0;
-    for (int w = 0; w < nw; w++) {
-      re += red[(size_t)q * nw + w].x;
-      im += red[(size_t)q * nw + w].y;
-    }
-    const int l = q / NRT, r = q - l * NRT;
-    part[(((size_t)n * gridDim.y + y) * NRT + r) * Ns + l] = make_double2(re, im);
-  }
-}
-
 // vd_r[n*Ns + l] = sum_y part[(n, y, r, l)], rounded to float
 template <int NRT>
 __global__ void k_restrict_b_fin(const double2 *__restrict__ part, int Ns, int nb, int ny, Ptrs<NRT> vd) {
@@ -92,44 +40,6 @@ __global__ void k_restrict_b_fin(const double2 *__restrict__ part, int Ns, int n
     im += a.y;
   }
   ((double2 *)vd.p[r])[i] = make_double2((double)(float)re, (double)(float)im);
-}
-
-// ------------------------------------------------------------ prolongation
-// s_r = sum_l vd_r[n, l] basis_l on every block n, float coefficients
-template <int NRT>
-__global__ void __launch_bounds__(BSPLIT_T) k_prolong_b(Geom g, const int *__restrict__ vd2lex,
-                                                        const float4 *const *__restrict__ basis, int Ns,
-                                                        Ptrs<NRT> vd, int nsplit, Ptrs<NRT> s) {
-  __shared__ float2 z[NRT][64];
-  const int n = blockIdx.x, y = blockIdx.y, p = y / nsplit, h = y - p * nsplit;
-  const int blk = __ldg(vd2lex + n), chunk = p * g.nbl + blk;
-  for (int q = threadIdx.x; q < NRT * Ns; q += blockDim.x) {
-    const int r = q / Ns, l = q - r * Ns;
-    const double2 v = ((const double2 *)vd.p[r])[(size_t)n * Ns + l];
-    z[r][l] = make_float2((float)v.x, (float)v.y);
-  }
-  __syncthreads();
-  const int per = (g.vbh + nsplit - 1) / nsplit, si = h * per + threadIdx.x;
-  if ((int)threadIdx.x >= per || si >= g.vbh) return;
-  spinor<float> acc[NRT];
-#pragma unroll
-  for (int r = 0; r < NRT; r++) szero(acc[r]);
-  for (int l = 0; l < Ns; l++) {
-    const spinor<float> b = Store<float>::load_spinor(basis[l], chunk, si, g.vbh);
-#pragma unroll
-    for (int r = 0; r < NRT; r++) {
-      const float zr = z[r][l].x, zi = z[r][l].y;
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-          acc[r].c[a].c[k].re += zr * b.c[a].c[k].re - zi * b.c[a].c[k].im;
-          acc[r].c[a].c[k].im += zr * b.c[a].c[k].im + zi * b.c[a].c[k].re;
-        }
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < NRT; r++) Store<float>::store_spinor(s.p[r], chunk, si, g.vbh, acc[r]);
 }
 
 // -------------------------------------------------- little operator, NR vectors
@@ -185,8 +95,8 @@ __global__ void __launch_bounds__(288) k_little_b(int mode, int Ns, int b0, cons
 
 // ----------------------------------------------- TMA-staged variants
 constexpr int NSTAGE = 3;        // depth of the shared-memory copy ring
-// The same restriction and prolongation with the basis planes of the
-// CTA's sites streamed into shared memory by bulk asynchronous copies
+// Restriction and prolongation of NRT fields on the CUDA cores, one site
+// per thread, with the basis planes of the CTA's sites streamed into shared memory by bulk asynchronous copies
 // (cp.async.bulk, one per plane and basis vector, issued by one thread),
 // in a ring of NSTAGE buffers so that the copies of basis vectors l+1 ..
 // l+NSTAGE-1 overlap the arithmetic on vector l.  A plane segment is cnt consecutive float4 at
@@ -340,6 +250,241 @@ __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__re
   }
 }
 
+// ------------------------------------- tensor-core restriction / prolongation
+// Four fields at a time as real matrix products on the tensor cores
+// (mma.sync m16n8k8, TF32 head/tail operands; mma.cuh).  Each lane copies
+// the operand values it will use (the fields, the basis and, for the
+// prolongation, nothing else) from global memory into its own slots of a
+// per-warp shared-memory ring with cp.async, RD - 1 stages ahead of the
+// arithmetic: no registers are tied up by loads in flight and no barrier is
+// needed, since every lane reads only what it copied itself.
+constexpr int TC_W = 4;          // warps of a CTA; one CTA per (DFL block, parity)
+
+__device__ __forceinline__ float f4c(const float4 &v, int q) {
+  return q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ void *pick4(const Ptrs<4> &a, int i) {
+  return i == 0 ? a.p[0] : i == 1 ? a.p[1] : i == 2 ? a.p[2] : a.p[3];
+}
+
+// Restriction: C[l][2r] = Re (b_l, x_r), C[l][2r+1] = Im (b_l, x_r) with
+//   Re = sum_k B_l[k] X_r[k],  Im = sum_k B_l[k] Xh_r[k],
+// k over the 24 reals of each site (re, im interleaved) and Xh = (x_im,
+// -x_re) per complex component.  M = 16 basis vectors (MT tiles cover Ns),
+// N = 4 fields x (re, im), K = one real component at 8 sites (K row t <->
+// site 8 gi + t, row t+4 <-> site 8 gi + t + 4).  A stage of the ring is
+// one plane (4 real components) of one group of 8 sites: NV float4 per lane.
+// The sums of a warp over a group are added into FP64, the warps' sums in
+// FP64; part[(n, p, r, l)] as the CUDA-core kernel writes it (two parities).
+template <int MT> struct RestrictTc {
+  static constexpr int NV = 2 + 4 * MT;
+  static constexpr int RD = MT <= 2 ? 4 : 3;
+  static constexpr size_t smem = (size_t)TC_W * RD * NV * 32 * sizeof(float4);
+};
+
+template <int MT>
+__global__ void __launch_bounds__(32 * TC_W) k_restrict_tc(Geom g, const int *__restrict__ vd2lex,
+                                                          const float4 *const *__restrict__ basis, int Ns,
+                                                          Ptrs<4> fld, double2 *part) {
+  constexpr int NV = RestrictTc<MT>::NV, RD = RestrictTc<MT>::RD;
+  extern __shared__ float4 ring[];
+  __shared__ double2 red[TC_W][16 * MT][4];
+  const int n = blockIdx.x, p = blockIdx.y, chunk = p * g.nbl + __ldg(vd2lex + n);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
+  const bool imc = gq & 1;
+  const size_t off = (size_t)chunk * 6 * g.vbh;
+  const float4 *xf = (const float4 *)pick4(fld, gq >> 1) + off;
+  const float4 *bp[MT][2];
+#pragma unroll
+  for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int l = 16 * mt + gq + 8 * h;
+      bp[mt][h] = l < Ns ? basis[l] + off : nullptr;
+    }
+  float4 *my = ring + (size_t)w * RD * NV * 32 + lane;
+  const int ngrp = (g.vbh + 7) >> 3;
+  const int T = w < ngrp ? 6 * ((ngrp - 1 - w) / TC_W + 1) : 0;   // stages of this warp
+  auto issue = [&](int t) {
+    if (t < T) {
+      const int gq6 = t / 6, j = t - 6 * gq6, gi = w + TC_W * gq6;
+      const int s0 = 8 * gi + tq, s1 = s0 + 4;
+      const bool ok0 = s0 < g.vbh, ok1 = s1 < g.vbh;
+      const size_t pj = (size_t)j * g.vbh;
+      float4 *dst = my + (size_t)(t % RD) * NV * 32;
+      cp_async16(dst, ok0 ? xf + pj + s0 : xf, ok0);
+      cp_async16(dst + 32, ok1 ? xf + pj + s1 : xf, ok1);
+#pragma unroll
+      for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const float4 *b = bp[mt][h];
+          // slots 2 + 4 mt + k: k = 0 (row g, K row t), 1 (row g+8, t), 2 (g, t+4), 3 (g+8, t+4)
+          cp_async16(dst + (2 + 4 * mt + h) * 32, (b && ok0) ? b + pj + s0 : xf, b && ok0);
+          cp_async16(dst + (4 + 4 * mt + h) * 32, (b && ok1) ? b + pj + s1 : xf, b && ok1);
+        }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int t = 0; t < RD - 1; t++) issue(t);
+  double dacc[MT][4];
+  float acc[MT][4];
+#pragma unroll
+  for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      dacc[mt][i] = 0.0;
+      acc[mt][i] = 0.0f;
+    }
+  for (int t = 0; t < T; t++) {
+    issue(t + RD - 1);
+    cp_async_wait<RD - 1>();
+    const float4 *src = my + (size_t)(t % RD) * NV * 32;
+    const float4 x0 = src[0], x1 = src[32];
+    const float4 y0 = imc ? make_float4(x0.y, -x0.x, x0.w, -x0.z) : x0;
+    const float4 y1 = imc ? make_float4(x1.y, -x1.x, x1.w, -x1.z) : x1;
+    float4 a[MT][4];
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) a[mt][k] = src[(2 + 4 * mt + k) * 32];
+    // the 4 components of the plane (12 products) summed on the tensor
+    // cores, then added to acc with round-to-nearest
+    float d[MT][4];
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) d[mt][i] = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const Tf32x2 bs[2] = {tf32_split(f4c(y0, q)), tf32_split(f4c(y1, q))};
+#pragma unroll
+      for (int mt = 0; mt < MT; mt++) {
+        const Tf32x2 as[4] = {tf32_split(f4c(a[mt][0], q)), tf32_split(f4c(a[mt][1], q)),
+                              tf32_split(f4c(a[mt][2], q)), tf32_split(f4c(a[mt][3], q))};
+        mma_tf32x3(d[mt], as, bs);
+      }
+    }
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+      for (int i = 0; i < 4; i++) acc[mt][i] += d[mt][i];
+    if (t % 6 == 5) {   // end of a group of 8 sites
+#pragma unroll
+      for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          dacc[mt][i] += (double)acc[mt][i];
+          acc[mt][i] = 0.0f;
+        }
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int mt = 0; mt < MT; mt++) {
+    red[w][16 * mt + gq][tq] = make_double2(dacc[mt][0], dacc[mt][1]);
+    red[w][16 * mt + gq + 8][tq] = make_double2(dacc[mt][2], dacc[mt][3]);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < 4 * Ns; q += blockDim.x) {
+    const int r = q / Ns, l = q - r * Ns;
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int v = 0; v < TC_W; v++) {
+      re += red[v][l][r].x;
+      im += red[v][l][r].y;
+    }
+    part[(((size_t)n * 2 + p) * 4 + r) * Ns + l] = make_double2(re, im);
+  }
+}
+
+// Prolongation: s_r = sum_l z_{r,l} b_l with z the FP32-rounded little
+// vectors.  M = 16 complex components of 8 sites x one plane j (row g <->
+// site 8 gi + g, component 2 j; row g+8 <-> the same site, component 2 j +
+// 1), N = 4 fields x (re, im), K = 4 basis vectors x (re, im) (K row t <->
+// (l = 4 ks + t, re), row t+4 <-> (l, im)):
+//   B[(l, re)][(r, re)] = Re z,  B[(l, im)][(r, re)] = -Im z,
+//   B[(l, re)][(r, im)] = Im z,  B[(l, im)][(r, im)] = Re z.
+// The A fragment of a lane is one float4 of basis vector l at its site
+// (a0, a2, a1, a3), its C fragment one float4 of field t there.  The B
+// fragments depend only on the block: they are split once per CTA into
+// shared memory.  A stage of the ring is one tile with all its k-steps: KS
+// float4 per lane.  KS >= (Ns + 3) / 4.
+template <int KS> struct ProlongTc {
+  static constexpr int RD = 3;
+  static constexpr size_t smem = (size_t)TC_W * RD * KS * 32 * sizeof(float4);
+};
+
+template <int KS>
+__global__ void __launch_bounds__(32 * TC_W) k_prolong_tc(Geom g, const int *__restrict__ vd2lex,
+                                                         const float4 *const *__restrict__ basis, int Ns,
+                                                         Ptrs<4> vd, Ptrs<4> s) {
+  constexpr int RD = ProlongTc<KS>::RD;
+  extern __shared__ float4 pring[];
+  __shared__ uint4 zf[KS][32];
+  __shared__ const float4 *bq[4 * KS];
+  const int n = blockIdx.x, p = blockIdx.y, chunk = p * g.nbl + __ldg(vd2lex + n);
+  const size_t off = (size_t)chunk * 6 * g.vbh;
+  for (int i = threadIdx.x; i < 32 * KS; i += blockDim.x) {
+    const int ks = i >> 5, ln = i & 31, gg = ln >> 2, l = 4 * ks + (ln & 3);
+    float zr = 0.0f, zi = 0.0f;
+    if (l < Ns) {
+      const double2 v = ((const double2 *)pick4(vd, gg >> 1))[(size_t)n * Ns + l];
+      zr = (float)v.x;
+      zi = (float)v.y;
+    }
+    const Tf32x2 b0 = tf32_split((gg & 1) ? zi : zr), b1 = tf32_split((gg & 1) ? zr : -zi);
+    zf[ks][ln] = make_uint4(b0.hi, b0.lo, b1.hi, b1.lo);
+  }
+  for (int i = threadIdx.x; i < 4 * KS; i += blockDim.x) bq[i] = i < Ns ? basis[i] + off : nullptr;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
+  float4 *out = (float4 *)pick4(s, tq) + off;
+  float4 *my = pring + (size_t)w * RD * KS * 32 + lane;
+  const int ntile = ((g.vbh + 7) >> 3) * 6, nks = (Ns + 3) >> 2;
+  const int T = w < ntile ? (ntile - 1 - w) / TC_W + 1 : 0;   // tiles of this warp
+  const float4 *dummy = bq[0];
+  Tf32x2 bs[KS][2];   // this lane's B fragments, the same for every tile
+#pragma unroll
+  for (int ks = 0; ks < KS; ks++) {
+    const uint4 z = zf[ks][lane];
+    bs[ks][0] = {z.x, z.y};
+    bs[ks][1] = {z.z, z.w};
+  }
+  auto issue = [&](int t) {
+    if (t < T) {
+      const int ti = w + TC_W * t, gi = ti / 6, j = ti - 6 * gi, si = 8 * gi + gq;
+      const bool ok = si < g.vbh;
+      const size_t ia = (size_t)j * g.vbh + si;
+      float4 *dst = my + (size_t)(t % RD) * KS * 32;
+      for (int ks = 0; ks < nks; ks++) {
+        const float4 *b = bq[4 * ks + tq];
+        cp_async16(dst + ks * 32, (b && ok) ? b + ia : dummy, b && ok);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int t = 0; t < RD - 1; t++) issue(t);
+  for (int t = 0; t < T; t++) {
+    issue(t + RD - 1);
+    cp_async_wait<RD - 1>();
+    const float4 *src = my + (size_t)(t % RD) * KS * 32;
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++)
+      if (ks < nks) {
+        const float4 v = src[ks * 32];
+        const Tf32x2 as[4] = {tf32_split(v.x), tf32_split(v.z), tf32_split(v.y), tf32_split(v.w)};
+        mma_tf32x3_add(acc, as, bs[ks]);
+      }
+    const int ti = w + TC_W * t, gi = ti / 6, j = ti - 6 * gi, si = 8 * gi + gq;
+    if (si < g.vbh) out[(size_t)j * g.vbh + si] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+  }
+  cp_async_wait<0>();
+}
+
 // ------------------------------------------------------------ host wrappers
 template <int N> static Ptrs<N> ptrs(const void *const *a) {
   Ptrs<N> q;
@@ -371,29 +516,83 @@ int dfl_batch_check(Ctx &c) {
   return 0;
 }
 
-template <int NRT>
-static void restrict_pass(Ctx &c, const void *const *x, double2 *const *vd, cudaStream_t st) {
+template <int MT>
+static void restrict_tc(Ctx &c, const void *const *x, cudaStream_t st) {
   DflState &d = c.dfl;
+  const size_t shm = RestrictTc<MT>::smem;
+  cudaFuncSetAttribute(k_restrict_tc<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  k_restrict_tc<MT><<<dim3(d.nb, 2), 32 * TC_W, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
+                                                            ptrs<4>(x), d.bpart);
+}
+
+// four fields (TC) or NRT fields on the CUDA cores
+template <int NRT>
+static void restrict_pass(Ctx &c, const void *const *x, double2 *const *vd, bool tc, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int nn = d.nb * d.Ns;
+  if (NRT == 4 && tc) {
+    const int mt = (d.Ns + 15) / 16;
+    if (mt == 1) restrict_tc<1>(c, x, st);
+    else if (mt == 2) restrict_tc<2>(c, x, st);
+    else if (mt == 3) restrict_tc<3>(c, x, st);
+    else restrict_tc<4>(c, x, st);
+    k_restrict_b_fin<4><<<dim3((nn + 255) / 256, 4), 256, 0, st>>>(d.bpart, d.Ns, d.nb, 2,
+                                                                    ptrs<4>((const void *const *)vd));
+    return;
+  }
   const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
   const size_t shm = (size_t)NSTAGE * 6 * per * sizeof(float4) + (size_t)d.Ns * NRT * (t / 32) * sizeof(double2);
   cudaFuncSetAttribute(k_dfl_stream<NRT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
   k_dfl_stream<NRT, true><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
                                                                d.Ns, ptrs<NRT>(x), ptrs<NRT>(nullptr), ns, d.bpart,
                                                                d.kerr);
-  const int nn = d.nb * d.Ns;
   k_restrict_b_fin<NRT><<<dim3((nn + 255) / 256, NRT), 256, 0, st>>>(d.bpart, d.Ns, d.nb, 2 * ns,
                                                                       ptrs<NRT>((const void *const *)vd));
 }
 
-// RHS tile autotuner: the number of fields per pass of the streamed
-// restriction and prolongation (1, 2 or 4), timed once per geometry on the
-// first call with four or more fields (on the caller's own data: every tile
-// computes the same result) and kept.
+template <int KS>
+static void prolong_tc(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const size_t shm = ProlongTc<KS>::smem;
+  cudaFuncSetAttribute(k_prolong_tc<KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  k_prolong_tc<KS><<<dim3(d.nb, 2), 32 * TC_W, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis, d.Ns,
+                                                           ptrs<4>((const void *const *)vd),
+                                                           ptrs<4>((const void *const *)s));
+}
+
+template <int NRT>
+static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, bool tc, cudaStream_t st) {
+  DflState &d = c.dfl;
+  if (NRT == 4 && tc) {
+    const int ks = (d.Ns + 3) / 4;
+    if (ks <= 4) prolong_tc<4>(c, vd, s, st);
+    else if (ks <= 8) prolong_tc<8>(c, vd, s, st);
+    else if (ks <= 12) prolong_tc<12>(c, vd, s, st);
+    else prolong_tc<16>(c, vd, s, st);
+    return;
+  }
+  const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
+  const size_t shm = (size_t)NSTAGE * 6 * per * sizeof(float4);
+  cudaFuncSetAttribute(k_dfl_stream<NRT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+  k_dfl_stream<NRT, false><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
+                                                                d.Ns, ptrs<NRT>((const void *const *)s),
+                                                                ptrs<NRT>((const void *const *)vd), ns, nullptr,
+                                                                d.kerr);
+}
+
+// RHS tile autotuner of the restriction and the prolongation (k = 0, 1):
+// one, two or four fields per pass on the CUDA cores, or four on the tensor
+// cores (kinds 0..3), timed once per geometry and deflation set-up on the
+// first call with four or more fields (on the caller's own data: every kind
+// computes the same result up to rounding) and kept.
 namespace {
+constexpr int NKIND = 4;
+constexpr int kKindTile[NKIND] = {1, 2, 4, 4};
+constexpr bool kKindTc[NKIND] = {false, false, false, true};
 struct TileTune {
   int vbh = 0, nb = 0, Ns = 0;
-  int tile[2] = {BT, BT};            // restriction, prolongation
-  float ms[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  int kind[2] = {3, 3};
+  float ms[2][NKIND] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
   bool done[2] = {false, false};
 };
 TileTune g_tile;
@@ -426,78 +625,75 @@ static float time_on(cudaStream_t st, F f) {
   return ms;
 }
 
-static void restrict_tiled(Ctx &c, int tile, int nr, const void *const *x, double2 *const *vd, cudaStream_t st) {
+static void restrict_kind(Ctx &c, int kind, int nr, const void *const *x, double2 *const *vd, cudaStream_t st) {
+  const int tile = kKindTile[kind];
+  const bool tc = kKindTc[kind];
   int r = 0;
   if (tile >= 4)
-    for (; r + 4 <= nr; r += 4) restrict_pass<4>(c, x + r, vd + r, st);
+    for (; r + 4 <= nr; r += 4) restrict_pass<4>(c, x + r, vd + r, tc, st);
   if (tile >= 2)
-    for (; r + 2 <= nr; r += 2) restrict_pass<2>(c, x + r, vd + r, st);
-  for (; r < nr; r++) restrict_pass<1>(c, x + r, vd + r, st);
+    for (; r + 2 <= nr; r += 2) restrict_pass<2>(c, x + r, vd + r, false, st);
+  for (; r < nr; r++) restrict_pass<1>(c, x + r, vd + r, false, st);
 }
 
-template <int NRT>
-static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st);
-
-static void prolong_tiled(Ctx &c, int tile, int nr, const double2 *const *vd, void *const *s, cudaStream_t st) {
+static void prolong_kind(Ctx &c, int kind, int nr, const double2 *const *vd, void *const *s, cudaStream_t st) {
+  const int tile = kKindTile[kind];
+  const bool tc = kKindTc[kind];
   int r = 0;
   if (tile >= 4)
-    for (; r + 4 <= nr; r += 4) prolong_pass<4>(c, vd + r, s + r, st);
+    for (; r + 4 <= nr; r += 4) prolong_pass<4>(c, vd + r, s + r, tc, st);
   if (tile >= 2)
-    for (; r + 2 <= nr; r += 2) prolong_pass<2>(c, vd + r, s + r, st);
-  for (; r < nr; r++) prolong_pass<1>(c, vd + r, s + r, st);
+    for (; r + 2 <= nr; r += 2) prolong_pass<2>(c, vd + r, s + r, false, st);
+  for (; r < nr; r++) prolong_pass<1>(c, vd + r, s + r, false, st);
+}
+
+template <class F>
+static void tune_kind(int k, cudaStream_t st, F run) {
+  for (int i = 0; i < NKIND; i++) g_tile.ms[k][i] = time_on(st, [&]() { run(i); });
+  int best = NKIND - 1;
+  for (int i = 0; i < NKIND; i++)
+    if (g_tile.ms[k][i] < g_tile.ms[k][best]) best = i;
+  g_tile.kind[k] = best;
+  g_tile.done[k] = true;
 }
 
 // vd[r] = restriction of the FP32 fields x[r], r < nr
 void dfl_restrict_b(Ctx &c, int nr, const void *const *x, double2 *const *vd, cudaStream_t st) {
   tile_key_changed(c);
-  if (nr >= 4 && !g_tile.done[0]) {
-    const int tiles[3] = {1, 2, 4};
-    int best = 2;
-    for (int i = 0; i < 3; i++) {
-      g_tile.ms[0][i] = time_on(st, [&]() { restrict_tiled(c, tiles[i], 4, x, vd, st); });
-      if (g_tile.ms[0][i] < g_tile.ms[0][best]) best = i;
-    }
-    g_tile.tile[0] = tiles[best];
-    g_tile.done[0] = true;
-  }
-  restrict_tiled(c, g_tile.tile[0], nr, x, vd, st);
-}
-
-int rhs_tiles(const Ctx &c, int *tile, float *ms) {
-  (void)c;
-  for (int k = 0; k < 2; k++) {
-    tile[k] = g_tile.done[k] ? g_tile.tile[k] : 0;
-    for (int i = 0; i < 3; i++) ms[3 * k + i] = g_tile.ms[k][i];
-  }
-  return 0;
-}
-
-template <int NRT>
-static void prolong_pass(Ctx &c, const double2 *const *vd, void *const *s, cudaStream_t st) {
-  DflState &d = c.dfl;
-  const int ns = chunk_split(c.g.vbh), per = (c.g.vbh + ns - 1) / ns, t = (per + 31) / 32 * 32;
-  const size_t shm = (size_t)NSTAGE * 6 * per * sizeof(float4);
-  cudaFuncSetAttribute(k_dfl_stream<NRT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-  k_dfl_stream<NRT, false><<<dim3(d.nb, 2 * ns), t, shm, st>>>(c.g, d.vd2lex, (const float4 *const *)d.d_basis,
-                                                                d.Ns, ptrs<NRT>((const void *const *)s),
-                                                                ptrs<NRT>((const void *const *)vd), ns, nullptr,
-                                                                d.kerr);
+  if (nr >= 4 && !g_tile.done[0]) tune_kind(0, st, [&](int i) { restrict_kind(c, i, 4, x, vd, st); });
+  restrict_kind(c, g_tile.kind[0], nr, x, vd, st);
 }
 
 // s[r] = prolongation of the little vectors vd[r], r < nr
 void dfl_prolong_b(Ctx &c, int nr, const double2 *const *vd, void *const *s, cudaStream_t st) {
   tile_key_changed(c);
-  if (nr >= 4 && !g_tile.done[1]) {
-    const int tiles[3] = {1, 2, 4};
-    int best = 2;
-    for (int i = 0; i < 3; i++) {
-      g_tile.ms[1][i] = time_on(st, [&]() { prolong_tiled(c, tiles[i], 4, vd, s, st); });
-      if (g_tile.ms[1][i] < g_tile.ms[1][best]) best = i;
-    }
-    g_tile.tile[1] = tiles[best];
-    g_tile.done[1] = true;
+  if (nr >= 4 && !g_tile.done[1]) tune_kind(1, st, [&](int i) { prolong_kind(c, i, 4, vd, s, st); });
+  prolong_kind(c, g_tile.kind[1], nr, vd, s, st);
+}
+
+// fixes the tiles of the current geometry and deflation set-up (tile 1, 2
+// or 4, tc for four fields on the tensor cores; tile 0 hands the choice back
+// to the autotuner)
+int set_rhs_tiles(Ctx &c, const int *tile, const int *tc) {
+  for (int k = 0; k < 2; k++)
+    if (tile[k] != 0 && tile[k] != 1 && tile[k] != 2 && tile[k] != 4)
+      return fail("set_rhs_tiles: tiles must be 0, 1, 2 or 4");
+  tile_key_changed(c);
+  for (int k = 0; k < 2; k++) {
+    g_tile.done[k] = tile[k] != 0;
+    g_tile.kind[k] = tile[k] == 1 ? 0 : tile[k] == 2 ? 1 : (tile[k] == 4 && !tc[k]) ? 2 : 3;
   }
-  prolong_tiled(c, g_tile.tile[1], nr, vd, s, st);
+  return 0;
+}
+
+int rhs_tiles(const Ctx &c, int *tile, int *tc, float *ms) {
+  (void)c;
+  for (int k = 0; k < 2; k++) {
+    tile[k] = g_tile.done[k] ? kKindTile[g_tile.kind[k]] : 0;
+    tc[k] = g_tile.done[k] && kKindTc[g_tile.kind[k]];
+    for (int i = 0; i < NKIND; i++) ms[NKIND * k + i] = g_tile.ms[k][i];
+  }
+  return 0;
 }
 
 template <int NRT>

@@ -375,7 +375,8 @@ int dirac_multi32(const Ctx &c, int n, float mu, void *const *sv, void *const *r
 void dfl_mark(Ctx &c, int k);
 int ensure_lvd_n(Ctx &c, int n);
 int dfl_batch_check(Ctx &c);
-int rhs_tiles(const Ctx &c, int *tile, float *ms);   // autotuned RHS tiles (restrict, prolong) and their times
+int set_rhs_tiles(Ctx &c, const int *tile, const int *tc);   // fixed RHS tiles (0: autotune)
+int rhs_tiles(const Ctx &c, int *tile, int *tc, float *ms);   // RHS tiles (restrict, prolong) and the kinds' times
 // solver_batch.cu
 int ltl_gcr_b(Ctx &c, double mu, int nr, const double2 *const *eta, double2 *const *psi, int *ifail, int *status,
               cudaStream_t st);

@@ -126,7 +126,8 @@ _SIGS = {
     "dfl_RLvd": (None, [C.c_void_p, C.c_void_p]),
     "dfl_Lv": (None, [C.c_void_p]),
     "b200_set_ltl_solver": (C.c_int, [C.c_int]),
-    "b200_rhs_tiles": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "b200_rhs_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "b200_set_rhs_tiles": (C.c_int, [C.c_void_p, C.c_void_p]),
     "b200_dfl_set_lmode": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_set_cuda_graphs": (C.c_int, [C.c_int]),
     "b200_set_pipeline": (C.c_int, [C.c_int]),
@@ -172,6 +173,8 @@ _SIGS = {
     "b200_net_make_pairs": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_ulonglong]),
     "b200_set_precond": (C.c_int, [C.c_int]),
     "b200_dfl_time": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_dfl_s2vd_multi": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_dfl_vd2s_multi": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "dfl_modes": (None, [C.c_void_p, C.c_void_p]),
@@ -683,6 +686,26 @@ def dfl_s2vd(s, nv):
     return vd
 
 
+def dfl_s2vd_multi(fields, nv):
+    """batched dfl_s2vd of several FP32 fields (reference layout)"""
+    fs = [np.ascontiguousarray(f, dtype=np.float32) for f in fields]
+    vds = [np.zeros(2 * nv) for _ in fs]
+    pf = (C.c_void_p * len(fs))(*[f.ctypes.data for f in fs])
+    pv = (C.c_void_p * len(fs))(*[v.ctypes.data for v in vds])
+    check(lib().b200_dfl_s2vd_multi(len(fs), pf, pv))
+    return vds
+
+
+def dfl_vd2s_multi(vds, vol):
+    """batched dfl_vd2s of several little vectors"""
+    vs = [np.ascontiguousarray(v, dtype=np.float64) for v in vds]
+    fs = [np.zeros(vol * 24, dtype=np.float32) for _ in vs]
+    pv = (C.c_void_p * len(vs))(*[v.ctypes.data for v in vs])
+    pf = (C.c_void_p * len(vs))(*[f.ctypes.data for f in fs])
+    check(lib().b200_dfl_vd2s_multi(len(vs), pv, pf))
+    return fs
+
+
 def dfl_vd2s(vd, vol):
     vd = np.ascontiguousarray(vd, dtype=np.float64)
     s = np.zeros(vol * 24, dtype=np.float32)
@@ -766,12 +789,24 @@ def dfl_Lv(v):
 
 def rhs_tiles():
     """autotuned fields per pass of the batched restriction and prolongation
-    (0: not tuned yet) and the times of four fields with tiles 1, 2, 4"""
+    (0: not tuned yet), whether the four-field pass runs on the tensor cores,
+    and the times of four fields with 1, 2, 4 fields per pass on the CUDA
+    cores and 4 on the tensor cores"""
     t = np.zeros(2, dtype=np.int32)
-    ms = np.zeros(6, dtype=np.float32)
-    check(lib().b200_rhs_tiles(_ptr(t), _ptr(ms)))
-    return {"restrict": int(t[0]), "prolong": int(t[1]), "restrict_ms": ms[:3].tolist(),
-            "prolong_ms": ms[3:].tolist()}
+    tc = np.zeros(2, dtype=np.int32)
+    ms = np.zeros(8, dtype=np.float32)
+    check(lib().b200_rhs_tiles(_ptr(t), _ptr(tc), _ptr(ms)))
+    return {"restrict": int(t[0]), "prolong": int(t[1]), "restrict_tc": bool(tc[0]), "prolong_tc": bool(tc[1]),
+            "restrict_ms": ms[:4].tolist(), "prolong_ms": ms[4:].tolist()}
+
+
+def set_rhs_tiles(restrict, prolong, restrict_tc=True, prolong_tc=True):
+    """fix the fields per pass of the batched restriction and prolongation
+    (1, 2 or 4; 0 hands the choice back to the autotuner) and whether four
+    fields run on the tensor cores"""
+    t = np.array([restrict, prolong], dtype=np.int32)
+    tc = np.array([int(restrict_tc), int(prolong_tc)], dtype=np.int32)
+    check(lib().b200_set_rhs_tiles(_ptr(t), _ptr(tc)))
 
 
 def set_ltl_solver(kind):

@@ -168,8 +168,11 @@ def test_dirac_multi(setup, n):
 
 def test_rhs_tile_autotuner(setup):
     """After a deflated batched solve the RHS-tile autotuner has timed the
-    restriction and prolongation with 1, 2 and 4 fields per pass and kept
-    one of them."""
+    restriction and prolongation with 1, 2 and 4 fields per pass on the CUDA
+    cores and 4 on the tensor cores, and kept the fastest."""
     t = qb.rhs_tiles()
     assert t["restrict"] in (1, 2, 4) and t["prolong"] in (1, 2, 4), t
     assert all(m > 0 for m in t["restrict_ms"] + t["prolong_ms"]), t
+    for k in ("restrict", "prolong"):
+        kind = {1: 0, 2: 1, 4: 3 if t[k + "_tc"] else 2}[t[k]]
+        assert t[k + "_ms"][kind] == min(t[k + "_ms"]), t
