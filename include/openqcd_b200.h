@@ -381,6 +381,13 @@ int b200_dfl_time(int what, int n, float *ms, int *its);
  * head/tail split products, FP32 accumulation, block sums in FP64), the rest
  * on the CUDA cores; the results are rounded to FP32 as the reference's. */
 int b200_dfl_s2vd_multi(int nr, spinor *const *s, complex_dble *const *vd);
+/* Awhat_dble (Aw_dble.c:361) of nr little vectors at once (1 <= nr <= 16;
+ * the batching has no reference counterpart), after set_Awhat: the path of
+ * the batched little solver, four vectors per pass with the preconditioned
+ * hop matrices rounded to FP32 on the tensor cores (TF32 head/tail split
+ * products, FP32 sums per matrix, FP64 across matrices), the rest in FP64.
+ * Only the even blocks of w are written, as by Awhat_dble. */
+int b200_Awhat_dble_multi(int nr, complex_dble *const *v, complex_dble *const *w);
 int b200_dfl_vd2s_multi(int nr, complex_dble *const *vd, spinor *const *s);
 /* Basis vector l of every block as one global FP32 field, reference layout. */
 int b200_dfl_set_basis(int l, const spinor *field);

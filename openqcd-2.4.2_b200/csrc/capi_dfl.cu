@@ -341,6 +341,29 @@ static void little_apply(int which, complex_dble *v, complex_dble *w) {
 }
 
 void Aw_dble(complex_dble *v, complex_dble *w) { little_apply(0, v, w); }
+
+// Awhat_dble of nr little vectors at once (the batched path: four vectors
+// per pass on the tensor cores with FP32 matrices, the rest in FP64)
+int b200_Awhat_dble_multi(int nr, complex_dble *const *v, complex_dble *const *w) {
+  Ctx &c = ctx();
+  if (qcd::dfl_ready(c)) return -1;
+  qcd::DflState &d = c.dfl;
+  if (!d.aw_valid || !d.awhat_valid) return fail("Awhat_dble_multi: the little operator is not set (set_Awhat)");
+  if (nr < 1 || nr > 16) return fail("Awhat_dble_multi: nr must be in [1, 16]");
+  if (qcd::ensure_lvd_n(c, 3 * nr)) return -1;
+  const size_t nb = (size_t)d.nv * sizeof(double2);
+  std::vector<double2 *> a(nr), b(nr), t(nr);
+  for (int r = 0; r < nr; r++) {
+    a[r] = d.lvd[r];
+    b[r] = d.lvd[nr + r];
+    t[r] = d.lvd[2 * nr + r];
+    cudaMemcpyAsync(a[r], v[r], nb, cudaMemcpyDefault, c.stream);
+    cudaMemcpyAsync(b[r], w[r], nb, cudaMemcpyDefault, c.stream);
+  }
+  qcd::dfl_Awhat_b(c, nr, (const double2 *const *)a.data(), b.data(), t.data(), c.stream);
+  for (int r = 0; r < nr; r++) cudaMemcpyAsync(w[r], b[r], nb, cudaMemcpyDefault, c.stream);
+  return b200_sync();
+}
 void Awhat_dble(complex_dble *v, complex_dble *w) { little_apply(1, v, w); }
 
 double ltl_gcr(double mu, complex_dble *eta, complex_dble *psi, int *ifail, int *status) {

@@ -120,6 +120,8 @@ static int dfl_alloc(Ctx &c) {
     cudaFree(*mats[i]);
     if (cudaMalloc(mats[i], sz[i]) != cudaSuccess) return fail("out of device memory (little operator)");
   }
+  cudaFree(d.Mhop32);
+  if (cudaMalloc(&d.Mhop32, 4 * m) != cudaSuccess) return fail("out of device memory (little operator)");
   d.aw_valid = d.awhat_valid = false;
   d.have_basis = false;
   d.ready = true;
@@ -615,6 +617,12 @@ __global__ void k_cinv(int Ns, const double2 *__restrict__ A, double2 *B, int *f
   }
 }
 
+// b = a rounded to FP32
+static __global__ void k_round32(const double2 *__restrict__ a, float2 *b, size_t n) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = make_float2((float)a[i].x, (float)a[i].y);
+}
+
 // M[n][ifc] = Ainv[n] * Ahop[n][ifc]  (column-major products)
 __global__ void k_cmatmul8(int Ns, const double2 *__restrict__ Ainv, const double2 *__restrict__ Ahop, double2 *M) {
   const int n = blockIdx.x >> 3, ifc = blockIdx.x & 7;
@@ -809,7 +817,7 @@ void dfl_release(Ctx &c) {
   for (void *p : d.start) cudaFree(p);
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
-  void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop,
+  void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop, d.Mhop32,
                   d.lvtab, d.ldots, d.lpart, d.rpart, d.bpart, d.kerr, d.gram, d.tri, d.gfail};
   if (d.h_ldots) cudaFreeHost(d.h_ldots);
   for (void *p : bufs) cudaFree(p);
@@ -944,6 +952,8 @@ int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st) {
   cudaFuncSetAttribute(k_cinv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   k_cinv<<<d.nb, 256, shm, st>>>(d.Ns, d.Ablk, d.Ainv, dfail);
   k_cmatmul8<<<8 * d.nb, 256, 0, st>>>(d.Ns, d.Ainv, d.Ahop, d.Mhop);
+  const size_t nm = (size_t)8 * d.nb * d.Ns * d.Ns;
+  k_round32<<<(unsigned)((nm + 255) / 256), 256, 0, st>>>(d.Mhop, d.Mhop32, nm);
   int hf = 0;
   cudaMemcpyAsync(&hf, dfail, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaFreeAsync(dfail, st);

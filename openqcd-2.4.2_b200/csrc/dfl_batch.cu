@@ -485,6 +485,78 @@ __global__ void __launch_bounds__(32 * TC_W) k_prolong_tc(Geom g, const int *__r
   cp_async_wait<0>();
 }
 
+// ----------------------------- preconditioned little hops on the tensor cores
+// The hop part of Awhat (modes 1 and 2 of k_little_b) for four vectors
+// with the FP32 copy of the matrices H = Ablk^-1 Ahop (Mhop32) on the
+// tensor cores (mma.sync m16n8k8, TF32 head/tail operands, FP32 sums per
+// matrix, FP64 across the 8 matrices of a block).  One warp per matrix; for
+// matrix A and the vectors x_r (rounded to FP32)
+//   W[k][(r, re)] = sum_l Re A[k][l] Re x_r[l] - Im A[k][l] Im x_r[l]
+//   W[k][(r, im)] = sum_l Re A[k][l] Im x_r[l] + Im A[k][l] Re x_r[l]
+// is a real product with M = 16 rows k per tile (MT tiles), N = 4 vectors
+// x (re, im), K = 4 columns l x (re, im): K row t <-> (l = 4 ks + t, re),
+// row t+4 <-> (l, im), A[k][(l, re)] = Re A, A[k][(l, im)] = -Im A,
+// B[(l, re)][(r, re)] = Re x, B[(l, im)][(r, re)] = Im x,
+// B[(l, re)][(r, im)] = Im x, B[(l, im)][(r, im)] = -Re x.
+template <int MT>
+__global__ void __launch_bounds__(256) k_little_hop_tc(int mode, int Ns, int b0, const float2 *__restrict__ H,
+                                                       const int *__restrict__ nbr, Ptrs<4> v, Ptrs<4> u,
+                                                       Ptrs<4> w) {
+  __shared__ double2 part[8][16 * MT][4];
+  const int n = b0 + blockIdx.x, wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float2 *a = H + ((size_t)8 * n + wp) * Ns * Ns;
+  const size_t xoff = (size_t)__ldg(nbr + 8 * n + wp) * Ns;
+  const Ptrs<4> &src = mode == 2 ? u : v;
+  const int gq = lane >> 2, tq = lane & 3;
+  const bool imcol = gq & 1;
+  const double2 *x = (const double2 *)pick4(src, gq >> 1) + xoff;
+  float acc[MT][4];
+#pragma unroll
+  for (int mt = 0; mt < MT; mt++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) acc[mt][i] = 0.0f;
+  const int nks = (Ns + 3) >> 2;
+#pragma unroll 2
+  for (int ks = 0; ks < nks; ks++) {
+    const int l = 4 * ks + tq;
+    const bool lok = l < Ns;
+    const double2 xv = lok ? __ldg(x + l) : make_double2(0.0, 0.0);
+    const float xr = (float)xv.x, xi = (float)xv.y;
+    const Tf32x2 bs[2] = {tf32_split(imcol ? xi : xr), tf32_split(imcol ? -xr : xi)};
+    const float2 *al = a + (size_t)l * Ns;
+#pragma unroll
+    for (int mt = 0; mt < MT; mt++) {
+      const int k = 16 * mt + gq;
+      const float2 m0 = (lok && k < Ns) ? __ldg(al + k) : make_float2(0.0f, 0.0f);
+      const float2 m1 = (lok && k + 8 < Ns) ? __ldg(al + k + 8) : make_float2(0.0f, 0.0f);
+      const Tf32x2 as[4] = {tf32_split(m0.x), tf32_split(m1.x), tf32_split(-m0.y), tf32_split(-m1.y)};
+      mma_tf32x3_add(acc[mt], as, bs);
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < MT; mt++) {
+    part[wp][16 * mt + gq][tq] = make_double2(acc[mt][0], acc[mt][1]);
+    part[wp][16 * mt + gq + 8][tq] = make_double2(acc[mt][2], acc[mt][3]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < Ns * 4; i += blockDim.x) {
+    const int k = i >> 2, r = i & 3;
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      re += part[j][k][r].x;
+      im += part[j][k][r].y;
+    }
+    double2 *wr = (double2 *)pick4(w, r) + (size_t)n * Ns + k;
+    if (mode == 2) {
+      const double2 vv = ((const double2 *)pick4(v, r))[(size_t)n * Ns + k];
+      *wr = make_double2(vv.x - re, vv.y - im);
+    } else {
+      *wr = make_double2(re, im);
+    }
+  }
+}
+
 // ------------------------------------------------------------ host wrappers
 template <int N> static Ptrs<N> ptrs(const void *const *a) {
   Ptrs<N> q;
@@ -712,12 +784,37 @@ void little_b(Ctx &c, int nr, int mode, int b0, int nblk, const double2 *A, cons
   for (; r < nr; r++) little_pass<1>(c, mode, b0, nblk, A, H, v + r, u ? u + r : nullptr, w + r, st);
 }
 
+template <int MT>
+static void hop_tc(Ctx &c, int mode, int b0, int nblk, const double2 *const *v, const double2 *const *u,
+                   double2 *const *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  k_little_hop_tc<MT><<<nblk, 256, 0, st>>>(mode, d.Ns, b0, d.Mhop32, d.nbr, ptrs<4>((const void *const *)v),
+                                            ptrs<4>((const void *const *)u), ptrs<4>((const void *const *)w));
+}
+
+// modes 1 and 2 with H = Mhop: four vectors at a time on the tensor cores
+// (FP32 matrices), the rest on the CUDA cores (FP64 matrices)
+static void awhat_hops(Ctx &c, int nr, int mode, int b0, int nblk, const double2 *const *v,
+                       const double2 *const *u, double2 *const *w, cudaStream_t st) {
+  DflState &d = c.dfl;
+  const int mt = (d.Ns + 15) / 16;
+  int r = 0;
+  for (; r + 4 <= nr; r += 4) {
+    const double2 *const *ur = u ? u + r : nullptr;
+    if (mt == 1) hop_tc<1>(c, mode, b0, nblk, v + r, ur, w + r, st);
+    else if (mt == 2) hop_tc<2>(c, mode, b0, nblk, v + r, ur, w + r, st);
+    else if (mt == 3) hop_tc<3>(c, mode, b0, nblk, v + r, ur, w + r, st);
+    else hop_tc<4>(c, mode, b0, nblk, v + r, ur, w + r, st);
+  }
+  for (; r < nr; r++) little_pass<1>(c, mode, b0, nblk, nullptr, d.Mhop, v + r, u ? u + r : nullptr, w + r, st);
+}
+
 // w_r = Awhat v_r (even halves), t_r odd intermediates
 void dfl_Awhat_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, double2 *const *t, cudaStream_t st) {
   DflState &d = c.dfl;
   const int nbh = d.nb / 2;
-  little_b(c, nr, 1, nbh, nbh, nullptr, d.Mhop, v, nullptr, t, st);
-  little_b(c, nr, 2, 0, nbh, nullptr, d.Mhop, v, (const double2 *const *)t, w, st);
+  awhat_hops(c, nr, 1, nbh, nbh, v, nullptr, t, st);
+  awhat_hops(c, nr, 2, 0, nbh, v, (const double2 *const *)t, w, st);
 }
 
 void dfl_Aw_b(Ctx &c, int nr, const double2 *const *v, double2 *const *w, cudaStream_t st) {

@@ -61,6 +61,7 @@ struct DflState {
   bool use_start = false;
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
+  float2 *Mhop32 = nullptr;     // FP32 copy of Mhop (the batched little hops on the tensor cores)
   bool aw_valid = false, awhat_valid = false;
   int awhat_fail = 0, aw_eo = 0;
   double aw_mu = 0.0;

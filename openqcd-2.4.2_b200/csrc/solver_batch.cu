@@ -599,21 +599,21 @@ static int bw_reserve(Ctx &c, std::vector<void *> &v, size_t n, int prec) {
 // set 0 again when the batch ends (the destructor), marked stale.
 struct LittleSets {
   Ctx *c = nullptr;
-  double2 *own[4] = {nullptr, nullptr, nullptr, nullptr};
-  std::vector<std::array<double2 *, 4>> set;
+  void *own[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  std::vector<std::array<void *, 5>> set;
   std::vector<double> mu;
   std::vector<int> fail;
   int build(Ctx &cc, const std::vector<double> &umu, cudaStream_t st) {
     c = &cc;
     DflState &d = cc.dfl;
-    own[0] = d.Ablk; own[1] = d.Ainv; own[2] = d.Ahop; own[3] = d.Mhop;
+    own[0] = d.Ablk; own[1] = d.Ainv; own[2] = d.Ahop; own[3] = d.Mhop; own[4] = d.Mhop32;
     const size_t m = (size_t)d.nb * d.Ns * d.Ns * sizeof(double2);
-    const size_t sz[4] = {m, m, 8 * m, 8 * m};
+    const size_t sz[5] = {m, m, 8 * m, 8 * m, 4 * m};
     mu = umu;
-    set.assign(umu.size(), {nullptr, nullptr, nullptr, nullptr});
+    set.assign(umu.size(), {nullptr, nullptr, nullptr, nullptr, nullptr});
     fail.assign(umu.size(), 0);
     for (size_t j = 0; j < umu.size(); j++) {
-      for (int k = 0; k < 4; k++) {
+      for (int k = 0; k < 5; k++) {
         if (j == 0) set[j][k] = own[k];
         else if (cudaMalloc(&set[j][k], sz[k]) != cudaSuccess) return qcd::fail("gcr_batch: out of device memory (little operators)");
       }
@@ -627,7 +627,8 @@ struct LittleSets {
   }
   void point(size_t j) {
     DflState &d = c->dfl;
-    d.Ablk = set[j][0]; d.Ainv = set[j][1]; d.Ahop = set[j][2]; d.Mhop = set[j][3];
+    d.Ablk = (double2 *)set[j][0]; d.Ainv = (double2 *)set[j][1]; d.Ahop = (double2 *)set[j][2];
+    d.Mhop = (double2 *)set[j][3]; d.Mhop32 = (float2 *)set[j][4];
   }
   void use(Ctx &cc, size_t j) {
     if (set.size() <= 1) return;
@@ -644,8 +645,9 @@ struct LittleSets {
     DflState &d = c->dfl;
     cudaStreamSynchronize(c->stream);
     for (size_t j = 1; j < set.size(); j++)
-      for (int k = 0; k < 4; k++) cudaFree(set[j][k]);
-    d.Ablk = own[0]; d.Ainv = own[1]; d.Ahop = own[2]; d.Mhop = own[3];
+      for (int k = 0; k < 5; k++) cudaFree(set[j][k]);
+    d.Ablk = (double2 *)own[0]; d.Ainv = (double2 *)own[1]; d.Ahop = (double2 *)own[2];
+    d.Mhop = (double2 *)own[3]; d.Mhop32 = (float2 *)own[4];
     d.aw_valid = d.awhat_valid = false;   // set 0's arrays hold the first mass; recompute on demand
     d.awhat_ver++;
   }

@@ -174,6 +174,7 @@ _SIGS = {
     "b200_set_precond": (C.c_int, [C.c_int]),
     "b200_dfl_time": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_s2vd_multi": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
+    "b200_Awhat_dble_multi": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_vd2s_multi": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
     "b200_dfl_set_basis": (C.c_int, [C.c_int, C.c_void_p]),
     "b200_dfl_get_basis": (C.c_int, [C.c_int, C.c_void_p]),
@@ -694,6 +695,16 @@ def dfl_s2vd_multi(fields, nv):
     pv = (C.c_void_p * len(fs))(*[v.ctypes.data for v in vds])
     check(lib().b200_dfl_s2vd_multi(len(fs), pf, pv))
     return vds
+
+
+def Awhat_multi(vs, ws=None):
+    """batched Awhat_dble of several little vectors (set_Awhat done before)"""
+    vs = [np.ascontiguousarray(v, dtype=np.float64) for v in vs]
+    ws = [np.zeros_like(v) for v in vs] if ws is None else [np.array(w, dtype=np.float64, copy=True) for w in ws]
+    pv = (C.c_void_p * len(vs))(*[v.ctypes.data for v in vs])
+    pw = (C.c_void_p * len(ws))(*[w.ctypes.data for w in ws])
+    check(lib().b200_Awhat_dble_multi(len(vs), pv, pw))
+    return ws
 
 
 def dfl_vd2s_multi(vds, vol):

@@ -8,12 +8,19 @@ must meet the bar of
 the single-field routines: 2e-6 relative to the largest component (the
 reference computes in FP32 and rounds its inner products to FP32).  Ns = 8,
 20, 28 and 40 cover one, two (with padded rows) and three row tiles of 16
-basis vectors, and one to ten k-steps of the prolongation."""
+basis vectors, and one to ten k-steps of the prolongation.
+
+The batched Awhat_dble (the little operator of the batched little solver:
+four vectors per pass on the tensor cores with the hop matrices rounded to
+FP32) against the reference's Awhat_dble (modules/little/Aw_dble.c:361):
+1e-6 relative in norm (FP32 matrices; the reference's own FP32 little
+operators are held to 1e-5), and the FP64 passes of the same call to
+1e-12."""
 import numpy as np
 import pytest
 
 import openqcd_b200 as qb
-from helpers import Setup
+from helpers import Setup, rel_norm_err
 
 pytestmark = pytest.mark.gpu
 
@@ -84,3 +91,20 @@ def test_tiles_back_to_autotuner(st):
     assert qb.rhs_tiles()["restrict"] in (1, 2, 4)
     ref = st.ref.dfl_s2vd(fields[2])
     assert np.abs(vds[2] - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("nr", [4, 5])
+def test_awhat_multi(st, nr):
+    rng = np.random.default_rng(31 + nr)
+    vs = [rng.standard_normal(2 * st.nv) for _ in range(nr)]
+    w0 = [rng.standard_normal(2 * st.nv) for _ in range(nr)]
+    mu = 0.01
+    qb.little(1, mu, vs[0])                 # set_Awhat(mu) on the device
+    ws = qb.Awhat_multi(vs, w0)
+    for r in range(nr):
+        ref, f = st.ref.little(1, mu, vs[r], w0[r])
+        assert f == 0
+        err = rel_norm_err(ws[r], ref)
+        print("Ns %d nr %d vector %d: relative error %.2e" % (st.Ns, nr, r, err))
+        assert err <= (1e-6 if r < 4 else 1e-12), (r, err)
+
