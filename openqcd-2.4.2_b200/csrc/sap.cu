@@ -50,8 +50,10 @@ __device__ __forceinline__ int block_of_colour(const Geom &g, int h, int colour)
   return q + (((n[0] + n[1] + n[2] + n[3]) & 1) != colour);
 }
 
-// Storage policies of the block solver.  Both keep the block work vectors
-// in shared memory as 24 float planes (plane k at sm[k*ld + s]); SapF32
+// Storage policies of the block solver.  All keep the block work vectors
+// in shared memory as 6 float4 planes (plane j at sm[4*(j*ld + s)], the
+// complex components 2j and 2j+1 of site s: one 16-byte access per pair);
+// SapF32
 // reads the FP32 links and Pauli matrices, SapF16 FP16 copies of them (links
 // as __half2 planes, Pauli matrices as uint2 planes of four halves), with
 // all arithmetic in FP32.  (FP16 work vectors were tried: their rounding,
@@ -61,16 +63,24 @@ struct SapF32 {
   using T = float;
   static constexpr int NP = 24;
   __device__ __forceinline__ static spinor<float> sm_load(const float *sm, int ld, int s) {
+    const float4 *p = reinterpret_cast<const float4 *>(sm);
     spinor<float> r;
 #pragma unroll
-    for (int k = 0; k < 12; k++) r.c[k / 3].c[k % 3] = mk<float>(sm[(2 * k) * ld + s], sm[(2 * k + 1) * ld + s]);
+    for (int j = 0; j < 6; j++) {
+      const float4 v = p[j * ld + s];
+      const int k = 2 * j;
+      r.c[k / 3].c[k % 3] = mk<float>(v.x, v.y);
+      r.c[(k + 1) / 3].c[(k + 1) % 3] = mk<float>(v.z, v.w);
+    }
     return r;
   }
   __device__ __forceinline__ static void sm_store(float *sm, int ld, int s, const spinor<float> &v) {
+    float4 *p = reinterpret_cast<float4 *>(sm);
 #pragma unroll
-    for (int k = 0; k < 12; k++) {
-      sm[(2 * k) * ld + s] = v.c[k / 3].c[k % 3].re;
-      sm[(2 * k + 1) * ld + s] = v.c[k / 3].c[k % 3].im;
+    for (int j = 0; j < 6; j++) {
+      const int k = 2 * j;
+      const cpx<float> a = v.c[k / 3].c[k % 3], b = v.c[(k + 1) / 3].c[(k + 1) % 3];
+      p[j * ld + s] = make_float4(a.re, a.im, b.re, b.im);
     }
   }
   __device__ __forceinline__ static su3<float> link(const void *u, int chunk, int mu, int s, int vbh) {
@@ -191,6 +201,10 @@ __device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int 
   return h;
 }
 
+// v = the block's sums of v, the same in every thread (the warps' partial
+// sums added in warp order by each thread), with one barrier.  The callers
+// separate two reductions by other barriers, so red is never overwritten
+// while a thread still reads it.
 template <int NC>
 __device__ __forceinline__ void block_allreduce(double v[NC], double *red) {
   int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -199,7 +213,6 @@ __device__ __forceinline__ void block_allreduce(double v[NC], double *red) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
   }
-  __syncthreads();
   if (lane == 0)
 #pragma unroll
     for (int k = 0; k < NC; k++) red[k * 32 + w] = v[k];
@@ -231,13 +244,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
   const int ld = g.vbh;
   T *S1 = smem, *W = smem + P::NP * ld, *S0 = smem + 2 * P::NP * ld;
   __shared__ double red[3 * 32];
-  __shared__ float zsh[2];
-  __shared__ int stop;
   const int blk = block_of_colour(g, blockIdx.x, a.colour);
   const int ce = blk, co = g.nbl + blk;
   const int T_ = blockDim.x;
   const int nmr = a.nmr;
-  if (threadIdx.x == 0) stop = 0;
   for (int step = 0; step <= nmr + 1; step++) {
     const bool last = step == nmr + 1;
     // ---- odd sites
@@ -331,24 +341,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
       __syncthreads();
       continue;
     }
-    // MR coefficient (blk_solv.c:1153-1188): stop if |s2|^2 < 2 FLT_MIN
+    // MR coefficient (blk_solv.c:1153-1188): stop if |s2|^2 < 2 FLT_MIN;
+    // every thread has the same sums and computes the same coefficient
     block_allreduce<3>(v, red);
-    if (threadIdx.x == 0) {
-      float r = (float)v[0];
-      if (r < 2.0f * 1.17549435e-38f) {
-        stop = 1;
-      } else {
-        float ri = 1.0f / r;
-        zsh[0] = (float)v[1] * ri;
-        zsh[1] = (float)v[2] * ri;
-      }
-    }
-    __syncthreads();
-    if (stop) {
+    const float rr = (float)v[0];
+    if (rr < 2.0f * 1.17549435e-38f) {
       step = nmr;   // go to the reconstruction step
       continue;
     }
-    const float zr = zsh[0], zi = zsh[1];
+    const float ri = 1.0f / rr, zr = (float)v[1] * ri, zi = (float)v[2] * ri;
 #pragma unroll
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T_;
@@ -385,8 +386,6 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
   // planes: S1 even, S1 odd; the solution S0 accumulates in phi
   float *S1[2] = {smem, smem + 24 * ld};
   __shared__ double red[3 * 32];
-  __shared__ float zsh[2];
-  __shared__ int stop;
   const int blk = block_of_colour(g, blockIdx.x, a.colour);
   const int T = blockDim.x;
   const float muo = a.eoflg ? 0.0f : a.mu;
@@ -402,7 +401,6 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         Store<float>::store_spinor(a.phi, p * g.nbl + blk, s, g.vbh, z);
       }
     }
-  if (threadIdx.x == 0) stop = 0;
   __syncthreads();
 
   for (int imr = 0; imr < a.nmr; imr++) {
@@ -428,18 +426,9 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         }
       }
     block_allreduce<3>(v, red);
-    if (threadIdx.x == 0) {
-      float r = (float)v[0];
-      if (r < 2.0f * 1.17549435e-38f) stop = 1;
-      else {
-        float ri = 1.0f / r;
-        zsh[0] = (float)v[1] * ri;
-        zsh[1] = (float)v[2] * ri;
-      }
-    }
-    __syncthreads();
-    if (stop) break;
-    const float zr = zsh[0], zi = zsh[1];
+    const float rr = (float)v[0];
+    if (rr < 2.0f * 1.17549435e-38f) break;
+    const float ri = 1.0f / rr, zr = (float)v[1] * ri, zi = (float)v[2] * ri;
     for (int p = 0; p < 2; p++)
 #pragma unroll
       for (int k = 0; k < NS; k++) {
