@@ -497,6 +497,7 @@ def solver_c3(qb, profile=False, lattice=None):
     f, stm = qb.dfl_modes(1)
     qb.lib().b200_sync()
     t_setup = time.time() - t0
+    qb.release_workspace()      # the generation's work fields
     nr = 4
     qb.set_sap_parms(BSx, 1, 3, 2)
     E = [eta] + [qb.DevField(64).random(1.0, 100 + i) for i in range(nr - 1)]
@@ -643,7 +644,10 @@ def batched_c4(qb):
     # two batches of 24 systems, two masses each (48 systems at once would
     # need 48 x (2 nkv + 2) FP32 Krylov fields of 201 MB, more than the 180 GB)
     P = [qb.DevField(64) for _ in range(24)]
-    qb.dev_gcr_batch(8, 256, 0, 1e-10, [0.0] * 12, srcs, P[:12], dfl=True)    # warm-up
+    # warm-up with the shape of a timed batch (work fields of 24 systems,
+    # the two-mass little operators, the captured SAP sequences)
+    qb.dev_gcr_batch(8, 256, 0, 1e-10, [mus[i // 12] for i in range(24)], [srcs[i % 12] for i in range(24)], P,
+                     dfl=True)
     tot, worst, per_mu, batches = 0.0, 0.0, [], []
     for pair in ((0, 1), (2, 3)):
         E = [srcs[i % 12] for i in range(24)]

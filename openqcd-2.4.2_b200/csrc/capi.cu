@@ -257,7 +257,8 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   }
   // a new geometry invalidates every resident field
   void *bufs[] = {c.ud, c.u32, c.swd, c.swd_inv, c.sw32, c.sw32_inv, c.tmp64, c.tmp32, c.stage,
-                  c.u16, c.sw16, c.sw16_inv, c.u12, c.sap_fld[0], c.sap_fld[1], c.sap_fld[2]};
+                  c.u16, c.sw16, c.sw16_inv, c.u12, c.sap_fld[0], c.sap_fld[1], c.sap_fld[2],
+                  c.sap_mfld[0], c.sap_mfld[1], c.sap_mfld[2]};
   for (void *p : bufs) cudaFree(p);
   for (void *p : c.ws32) cudaFree(p);
   for (void *p : c.ws64) cudaFree(p);
@@ -268,6 +269,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   c.sap_tuned_vbh[0] = c.sap_tuned_vbh[1] = c.sap_tuned_vbh[2] = 0;
   c.u12 = nullptr; c.u12_valid = c.u12_ok = false;
   c.sap_fld[0] = c.sap_fld[1] = c.sap_fld[2] = nullptr;
+  c.sap_mfld[0] = c.sap_mfld[1] = c.sap_mfld[2] = nullptr;
   c.have_ud = c.have_sw = false;
   qcd::dfl_release(c);
   qcd::net_fields_release(c);

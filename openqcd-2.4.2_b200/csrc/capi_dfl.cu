@@ -211,6 +211,8 @@ int b200_release_workspace(void) {
   for (int k = 0; k < 3; k++) {
     cudaFree(c.sap_fld[k]);
     c.sap_fld[k] = nullptr;
+    cudaFree(c.sap_mfld[k]);
+    c.sap_mfld[k] = nullptr;
   }
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : fail("CUDA error");
 }

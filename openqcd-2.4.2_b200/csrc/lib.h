@@ -99,6 +99,8 @@ struct NetState {
   std::vector<void *> f;
 };
 
+constexpr int SAP_MS = 4;   // systems per SAP launch of the batched solvers
+
 // Everything the reference keeps in module-global state for this path:
 // geometry (lattice/geometry.c), the gauge field (uflds/uflds.c udfld/ufld),
 // the SW field (sw_term/swflds.c swdfld/swfld) and the parameter data base
@@ -176,6 +178,8 @@ struct Ctx {
   // on three library-owned FP32 fields (solution, residual, block scratch)
   int use_graphs = 1;
   void *sap_fld[3] = {nullptr, nullptr, nullptr};
+  // the same for SAP_MS systems at once (SAP_MS consecutive fields each)
+  void *sap_mfld[3] = {nullptr, nullptr, nullptr};
   int nthread = 1;              // the caller's NTHREAD, for icom & 0x2 in the BLAS drop-ins
   void *fstage[3] = {nullptr, nullptr, nullptr};   // staging of host operands
   size_t fstage_bytes[3] = {0, 0, 0};
@@ -424,5 +428,14 @@ void *sap_input_field(Ctx &c);
 // psi = ncy cycles on rho = rh, then rho = rh - rho (the sap_gcr preconditioner)
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
             cudaStream_t st, const void *base = nullptr, const void *add = nullptr);
+// the input field of system r (< SAP_MS) of sap_mop_multi (null when CUDA
+// graphs are off or with domain decomposition)
+void *sap_input_field_multi(Ctx &c, int r);
+// sap_mop for ns systems (twisted masses mu[r]) with every SAP launch
+// covering up to SAP_MS of them; base and add may be null (as in sap_mop),
+// or arrays whose entries may be null
+int sap_mop_multi(Ctx &c, int ns, const float *mu, int isolv, int nmr, int ncy, const void *const *rh,
+                  void *const *psi, void *const *rho, void *phi_blk, cudaStream_t st, const void *const *base,
+                  const void *const *add);
 
 }  // namespace qcd

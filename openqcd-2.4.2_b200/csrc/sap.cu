@@ -29,17 +29,39 @@
 
 namespace qcd {
 
+// nsys systems (SAP_MS at most) per launch: their fields psi, rho, phi lie
+// fstride float4 apart, the CTAs of one block are adjacent (CTA x: block
+// x / nsys, system x % nsys), so the block's links and SW matrices are read
+// by all systems while they are in L2.
 struct SapArgs {
   Geom g;
   int colour;
-  float mu;
+  float mu;             // system 0
   int nmr;
   int eoflg;
-  float4 *psi, *rho, *phi;
+  float4 *psi, *rho, *phi;   // system 0
   const void *u;        // links as the block solver's policy reads them
   const void *ub;       // links for the block-boundary hops (as u, but 18-real FP32 in the FP32 mode)
   const void *sw, *swinv;
+  int nsys;
+  size_t fstride;
+  float mus[SAP_MS];
 };
+
+// the fields and twisted mass of system r of a launch
+struct SapSys {
+  float4 *psi, *rho, *phi;
+  float mu;
+};
+__device__ __forceinline__ SapSys sap_sys(const SapArgs &a, int r) {
+  const size_t o = (size_t)r * a.fstride;
+  SapSys y;
+  y.psi = a.psi + o;
+  y.rho = a.rho + o;
+  y.phi = a.phi + o;
+  y.mu = r == 0 ? a.mus[0] : r == 1 ? a.mus[1] : r == 2 ? a.mus[2] : a.mus[3];
+  return y;
+}
 
 // block of the given colour with in-colour index h (block lex index of the
 // pair 2h, 2h+1 that has the requested parity of sum(n))
@@ -244,7 +266,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
   const int ld = g.vbh;
   T *S1 = smem, *W = smem + P::NP * ld, *S0 = smem + 2 * P::NP * ld;
   __shared__ double red[3 * 32];
-  const int blk = block_of_colour(g, blockIdx.x, a.colour);
+  const SapSys y = sap_sys(a, blockIdx.x % a.nsys);
+  const int blk = block_of_colour(g, blockIdx.x / a.nsys, a.colour);
   const int ce = blk, co = g.nbl + blk;
   const int T_ = blockDim.x;
   const int nmr = a.nmr;
@@ -257,35 +280,35 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
       if (s < g.vbh) {
         spinor<float> h;
         if (step == 0) {
-          h = Store<float>::load_spinor_rw(a.rho, co, s, g.vbh);
+          h = Store<float>::load_spinor_rw(y.rho, co, s, g.vbh);
         } else {
           h = block_hop<P>(a, 1, blk, s, last ? S0 : S1, ld);
         }
         spinor<float> t = P::sw(a.swinv, co, s, g.vbh, 0.0f, h);
         if (step == 0) {
-          Store<float>::store_spinor(a.phi, co, s, g.vbh, t);
+          Store<float>::store_spinor(y.phi, co, s, g.vbh, t);
           P::sm_store(W, ld, s, t);
         } else if (!last) {
           P::sm_store(W, ld, s, t);
         } else {
-          spinor<float> ph = Store<float>::load_spinor_rw(a.phi, co, s, g.vbh);
+          spinor<float> ph = Store<float>::load_spinor_rw(y.phi, co, s, g.vbh);
           ssub(ph, t);
-          spinor<float> ps = Store<float>::load_spinor_rw(a.psi, co, s, g.vbh);
+          spinor<float> ps = Store<float>::load_spinor_rw(y.psi, co, s, g.vbh);
           sadd(ps, ph);
-          Store<float>::store_spinor(a.psi, co, s, g.vbh, ps);
-          Store<float>::store_spinor(a.phi, co, s, g.vbh, ph);
+          Store<float>::store_spinor(y.psi, co, s, g.vbh, ps);
+          Store<float>::store_spinor(y.phi, co, s, g.vbh, ph);
           spinor<float> ro;
           if (a.eoflg) {
             szero(ro);
           } else {
 #pragma unroll
             for (int c = 0; c < 4; c++) {
-              const float m = c < 2 ? -a.mu : a.mu;   // rho_o = i m phi_o
+              const float m = c < 2 ? -y.mu : y.mu;   // rho_o = i m phi_o
 #pragma unroll
               for (int j = 0; j < 3; j++) ro.c[c].c[j] = mk<float>(-m * ph.c[c].c[j].im, m * ph.c[c].c[j].re);
             }
           }
-          Store<float>::store_spinor(a.rho, co, s, g.vbh, ro);
+          Store<float>::store_spinor(y.rho, co, s, g.vbh, ro);
         }
       }
     }
@@ -298,11 +321,11 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
         if (s < g.vbh) {
           spinor<float> s0 = P::sm_load(S0, ld, s);
           spinor<float> r1 = P::sm_load(S1, ld, s);
-          spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ce, s, g.vbh);
+          spinor<float> ps = Store<float>::load_spinor_rw(y.psi, ce, s, g.vbh);
           sadd(ps, s0);
-          Store<float>::store_spinor(a.psi, ce, s, g.vbh, ps);
-          Store<float>::store_spinor(a.phi, ce, s, g.vbh, s0);
-          Store<float>::store_spinor(a.rho, ce, s, g.vbh, r1);
+          Store<float>::store_spinor(y.psi, ce, s, g.vbh, ps);
+          Store<float>::store_spinor(y.phi, ce, s, g.vbh, s0);
+          Store<float>::store_spinor(y.rho, ce, s, g.vbh, r1);
         }
       }
       break;
@@ -315,7 +338,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
       if (s < g.vbh) {
         spinor<float> hw = block_hop<P>(a, 0, blk, s, W, ld);
         if (step == 0) {
-          spinor<float> r = Store<float>::load_spinor_rw(a.rho, ce, s, g.vbh);
+          spinor<float> r = Store<float>::load_spinor_rw(y.rho, ce, s, g.vbh);
           ssub(r, hw);
           P::sm_store(S1, ld, s, r);
           spinor<float> z;
@@ -323,7 +346,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
           P::sm_store(S0, ld, s, z);
         } else {
           spinor<float> s1 = P::sm_load(S1, ld, s);
-          s2[k] = P::sw(a.sw, ce, s, g.vbh, a.mu, s1);
+          s2[k] = P::sw(a.sw, ce, s, g.vbh, y.mu, s1);
           ssub(s2[k], hw);
 #pragma unroll
           for (int c = 0; c < 4; c++)
@@ -386,19 +409,20 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
   // planes: S1 even, S1 odd; the solution S0 accumulates in phi
   float *S1[2] = {smem, smem + 24 * ld};
   __shared__ double red[3 * 32];
-  const int blk = block_of_colour(g, blockIdx.x, a.colour);
+  const SapSys y = sap_sys(a, blockIdx.x % a.nsys);
+  const int blk = block_of_colour(g, blockIdx.x / a.nsys, a.colour);
   const int T = blockDim.x;
-  const float muo = a.eoflg ? 0.0f : a.mu;
+  const float muo = a.eoflg ? 0.0f : y.mu;
 
   for (int p = 0; p < 2; p++)
 #pragma unroll
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T;
       if (s < g.vbh) {
-        P::sm_store(S1[p], ld, s, Store<float>::load_spinor_rw(a.rho, p * g.nbl + blk, s, g.vbh));
+        P::sm_store(S1[p], ld, s, Store<float>::load_spinor_rw(y.rho, p * g.nbl + blk, s, g.vbh));
         spinor<float> z;
         szero(z);
-        Store<float>::store_spinor(a.phi, p * g.nbl + blk, s, g.vbh, z);
+        Store<float>::store_spinor(y.phi, p * g.nbl + blk, s, g.vbh, z);
       }
     }
   __syncthreads();
@@ -412,7 +436,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         int s = threadIdx.x + k * T;
         if (s < g.vbh) {
           spinor<float> s1 = P::sm_load(S1[p], ld, s);
-          s2[p][k] = apply_sw_site<float>(a.sw, p * g.nbl + blk, s, g.vbh, p ? muo : a.mu, s1);
+          s2[p][k] = apply_sw_site<float>(a.sw, p * g.nbl + blk, s, g.vbh, p ? muo : y.mu, s1);
           sadd(s2[p][k], block_hop<P>(a, p, blk, s, S1[1 - p], ld));
 #pragma unroll
           for (int c = 0; c < 4; c++)
@@ -435,7 +459,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
         int s = threadIdx.x + k * T;
         if (s < g.vbh) {
           const int ch = p * g.nbl + blk;
-          spinor<float> s1 = P::sm_load(S1[p], ld, s), s0 = Store<float>::load_spinor_rw(a.phi, ch, s, g.vbh);
+          spinor<float> s1 = P::sm_load(S1[p], ld, s), s0 = Store<float>::load_spinor_rw(y.phi, ch, s, g.vbh);
 #pragma unroll
           for (int c = 0; c < 4; c++)
 #pragma unroll
@@ -446,7 +470,7 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
               s1.c[c].c[j].re -= zr * x2.re - zi * x2.im;
               s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
             }
-          Store<float>::store_spinor(a.phi, ch, s, g.vbh, s0);
+          Store<float>::store_spinor(y.phi, ch, s, g.vbh, s0);
           P::sm_store(S1[p], ld, s, s1);
         }
       }
@@ -458,11 +482,11 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
       int s = threadIdx.x + k * T;
       if (s < g.vbh) {
         int ch = p * g.nbl + blk;
-        spinor<float> s0 = Store<float>::load_spinor_rw(a.phi, ch, s, g.vbh);
-        spinor<float> ps = Store<float>::load_spinor_rw(a.psi, ch, s, g.vbh);
+        spinor<float> s0 = Store<float>::load_spinor_rw(y.phi, ch, s, g.vbh);
+        spinor<float> ps = Store<float>::load_spinor_rw(y.psi, ch, s, g.vbh);
         sadd(ps, s0);
-        Store<float>::store_spinor(a.psi, ch, s, g.vbh, ps);
-        Store<float>::store_spinor(a.rho, ch, s, g.vbh, P::sm_load(S1[p], ld, s));
+        Store<float>::store_spinor(y.psi, ch, s, g.vbh, ps);
+        Store<float>::store_spinor(y.rho, ch, s, g.vbh, P::sm_load(S1[p], ld, s));
       }
     }
 }
@@ -479,7 +503,8 @@ __global__ void __launch_bounds__(256) k_sap_blocks_plain(SapArgs a) {
 template <class P, int DD>
 __device__ __forceinline__ void sap_bnd_body(const SapArgs &a, const DDGeom &dg) {
   const Geom &g = a.g;
-  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const SapSys y = sap_sys(a, blockIdx.x % a.nsys);
+  size_t i = (blockIdx.x / a.nsys) * (size_t)blockDim.x + threadIdx.x;
   if (i >= (size_t)(g.nbl / 2) * g.vb) return;
   int h = (int)(i / g.vb), r = (int)(i % g.vb);
   int p = r >= g.vbh, s = r - p * g.vbh;
@@ -508,7 +533,7 @@ __device__ __forceinline__ void sap_bnd_body(const SapArgs &a, const DDGeom &dg)
       } else {
         int c2, s2;
         site_nbr(g, x, mu, +1, c2, s2);
-        spinor<float> sp = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
+        spinor<float> sp = Store<float>::load_spinor(y.phi, c2, s2, g.vbh);
         hop_fwd<float>(mu, uu, sp, hsum);
       }
       any = true;
@@ -521,7 +546,7 @@ __device__ __forceinline__ void sap_bnd_body(const SapArgs &a, const DDGeom &dg)
       } else {
         int c2, s2;
         site_nbr(g, x, mu, -1, c2, s2);
-        spinor<float> sm = Store<float>::load_spinor(a.phi, c2, s2, g.vbh);
+        spinor<float> sm = Store<float>::load_spinor(y.phi, c2, s2, g.vbh);
         su3<float> uu = P::blink(a.ub, c2, mu, s2, g.vbh, mu == 0 && x0 == 0);
         hop_bwd<float>(mu, uu, sm, hsum);
       }
@@ -530,9 +555,9 @@ __device__ __forceinline__ void sap_bnd_body(const SapArgs &a, const DDGeom &dg)
   }
   if (!any) return;
   sscale<float>(hsum, 0.5f);   // rho -= (-1/2) H phi
-  spinor<float> rr = Store<float>::load_spinor_rw(a.rho, chunk, s, g.vbh);
+  spinor<float> rr = Store<float>::load_spinor_rw(y.rho, chunk, s, g.vbh);
   sadd(rr, hsum);
-  Store<float>::store_spinor(a.rho, chunk, s, g.vbh, rr);
+  Store<float>::store_spinor(y.rho, chunk, s, g.vbh, rr);
 }
 
 // the single-GPU kernel keeps its parameter list; the DD twin takes the
@@ -575,7 +600,7 @@ static void sap_bnd_launch(Ctx &c, SapArgs a, cudaStream_t st) {
   const unsigned nbnd = (unsigned)((nb_sites + 127) / 128);
   DDGeom dg = c.ddg;
   if (!dd_on(c)) {
-    k_sap_bnd<P><<<nbnd, 128, 0, st>>>(a);
+    k_sap_bnd<P><<<nbnd * a.nsys, 128, 0, st>>>(a);
     return;
   }
   const int F = c.g.L[1] * c.g.L[2] * c.g.L[3];
@@ -725,14 +750,14 @@ static void launch_blocks(Ctx &c, const SapArgs &a, int isolv, int mode, cudaStr
   if (isolv) {
     const EoVariant &v = kEo[c.sap_variant[mode]];
     const int t = eo_threads(v, c.g.vbh);
-    v.k[mode]<<<nbh, t, eo_smem(c.g.vbh), st>>>(a);
+    v.k[mode]<<<nbh * a.nsys, t, eo_smem(c.g.vbh), st>>>(a);
   } else {
     int ns;
     int t = pick_threads(c.g.vbh, ns);
     const size_t shm = (size_t)48 * c.g.vbh * sizeof(float);
-    if (ns == 1) k_sap_blocks_plain<1><<<nbh, t, shm, st>>>(a);
-    else if (ns == 2) k_sap_blocks_plain<2><<<nbh, t, shm, st>>>(a);
-    else k_sap_blocks_plain<3><<<nbh, t, shm, st>>>(a);
+    if (ns == 1) k_sap_blocks_plain<1><<<nbh * a.nsys, t, shm, st>>>(a);
+    else if (ns == 2) k_sap_blocks_plain<2><<<nbh * a.nsys, t, shm, st>>>(a);
+    else k_sap_blocks_plain<3><<<nbh * a.nsys, t, shm, st>>>(a);
   }
 }
 
@@ -748,6 +773,9 @@ static SapArgs sap_args(Ctx &c, float mu, int nmr, int mode, void *psi, void *rh
   a.psi = (float4 *)psi;
   a.rho = (float4 *)rho;
   a.phi = (float4 *)phi;
+  a.nsys = 1;
+  a.fstride = 0;
+  a.mus[0] = mu;
   a.u = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
   a.ub = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
   a.sw = half ? (const void *)c.sw16 : (const void *)c.sw32;
@@ -967,6 +995,82 @@ int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void 
   k_sap_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, (const float4 *)spsi, (const float4 *)srho,
                                                            (const float4 *)base, (const float4 *)add,
                                                            (float4 *)psi, (float4 *)rho);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+}
+
+// the fields of sap_mop_multi; false (and nothing held) when the device
+// has no room for them, in which case the systems run one at a time
+static bool sap_multi_fields(Ctx &c) {
+  for (int k = 0; k < 3; k++)
+    if (!c.sap_mfld[k] && cudaMalloc(&c.sap_mfld[k], SAP_MS * spinor_bytes(c, 32)) != cudaSuccess) {
+      cudaGetLastError();
+      for (int j = 0; j < 3; j++) {
+        cudaFree(c.sap_mfld[j]);
+        c.sap_mfld[j] = nullptr;
+      }
+      return false;
+    }
+  return true;
+}
+
+void *sap_input_field_multi(Ctx &c, int r) {
+  if (!c.use_graphs || dd_on(c) || r < 0 || r >= SAP_MS || !sap_multi_fields(c)) return nullptr;
+  return (char *)c.sap_mfld[1] + (size_t)r * spinor_bytes(c, 32);
+}
+
+// Several systems: the SAP sequence of sap_mop captured once for up to
+// SAP_MS systems on library-owned fields, every block-solver and boundary
+// launch covering all of them.  Without graphs, or with domain
+// decomposition, the systems run one after the other through sap_mop.
+int sap_mop_multi(Ctx &c, int ns, const float *mu, int isolv, int nmr, int ncy, const void *const *rh,
+                  void *const *psi, void *const *rho, void *phi_blk, cudaStream_t st, const void *const *base,
+                  const void *const *add) {
+  if (!c.use_graphs || dd_on(c) || ns == 1 || !sap_multi_fields(c)) {
+    for (int r = 0; r < ns; r++)
+      if (sap_mop(c, mu[r], isolv, nmr, ncy, rh[r], psi[r], rho[r], phi_blk, st, base ? base[r] : nullptr,
+                  add ? add[r] : nullptr))
+        return -1;
+    return 0;
+  }
+  const size_t fb = spinor_bytes(c, 32);
+  const int mode = sap_ready(c, isolv, st);
+  if (mode < 0) return -1;
+  const size_t n = (size_t)c.g.vol * 6;   // float4 of a field
+  for (int r0 = 0; r0 < ns; r0 += SAP_MS) {
+    const int m = ns - r0 < SAP_MS ? ns - r0 : SAP_MS;
+    SapKey key;
+    std::memset(&key, 0, sizeof(key));
+    key.tag = 0x5aa;
+    key.isolv = isolv;
+    key.mode = mode;
+    key.variant = c.sap_variant[mode];
+    key.ncy = ncy;
+    key.a = sap_args(c, mu[r0], nmr, mode, c.sap_mfld[0], c.sap_mfld[1], c.sap_mfld[2]);
+    key.a.nsys = m;
+    key.a.fstride = n;
+    for (int r = 0; r < m; r++) key.a.mus[r] = mu[r0 + r];
+    for (int r = 0; r < m; r++) {
+      void *in = (char *)c.sap_mfld[1] + (size_t)r * fb;
+      const void *b = base && base[r0 + r] ? base[r0 + r] : rh[r0 + r];
+      if (b == in) return fail("sap_mop_multi: an input in the SAP input field needs a separate base");
+      if (rh[r0 + r] != in) la_copy(c, 32, rh[r0 + r], 32, in, PAR_ALL, st);
+    }
+    const int rc = graph_run(c, &key, sizeof(key), st, [&]() {
+      cudaMemsetAsync(c.sap_mfld[0], 0, (size_t)m * fb, st);
+      for (int k = 0; k < ncy; k++) sap_cycle_launch(c, key.a, isolv, mode, st);
+      return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+    });
+    if (rc) return -1;
+    for (int r = 0; r < m; r++) {
+      const float4 *spsi = (const float4 *)((char *)c.sap_mfld[0] + (size_t)r * fb);
+      const float4 *srho = (const float4 *)((char *)c.sap_mfld[1] + (size_t)r * fb);
+      const void *b = base && base[r0 + r] ? base[r0 + r] : rh[r0 + r];
+      k_sap_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, spsi, srho, (const float4 *)b,
+                                                               (const float4 *)(add ? add[r0 + r] : nullptr),
+                                                               (float4 *)psi[r0 + r], (float4 *)rho[r0 + r]);
+    }
+  }
+  (void)phi_blk;
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
 }
 

@@ -792,26 +792,47 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       }
       dfl_prolong_b(c, na, (const double2 *const *)v.data(), w0.data(), st);
       dfl_mark(c, 3);
-      for (int i = 0; i < na; i++) {
-        SysState &y = S[A[i]];
-        void *ph = y.phi[y.k], *ch = y.chi[y.k];
-        // rho - D ws0, written where the SAP sequence reads its input
-        void *in = sap_input_field(c);
-        if (!in) in = ch;
-        void *const rv[1] = {in}, *const bv[1] = {y.rho};
-        dirac_multi32(c, 1, (float)y.mu, &w0[i], rv, bv, st);
+      // SAP_MS systems per SAP launch
+      for (int i0 = 0; i0 < na; i0 += SAP_MS) {
+        const int m = na - i0 < SAP_MS ? na - i0 : SAP_MS;
+        const void *rh[SAP_MS], *base[SAP_MS], *add[SAP_MS];
+        void *ph[SAP_MS], *ch[SAP_MS];
+        float mus[SAP_MS];
+        for (int q = 0; q < m; q++) {
+          SysState &y = S[A[i0 + q]];
+          ph[q] = y.phi[y.k];
+          ch[q] = y.chi[y.k];
+          // rho - D ws0, written where the SAP sequence reads its input
+          void *in = sap_input_field_multi(c, q);
+          if (!in) in = ch[q];
+          void *const rv[1] = {in}, *const bv[1] = {y.rho};
+          dirac_multi32(c, 1, (float)y.mu, &w0[i0 + q], rv, bv, st);
+          rh[q] = in;
+          base[q] = y.rho;
+          add[q] = y.ws0;
+          mus[q] = (float)y.mu;
+          y.lstat += ls[i0 + q];
+        }
         dfl_mark(c, 3);
-        // SAP on it, then ch = rho - (final residual), ph += ws0
-        sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, in, ph, ch, phib, st, y.rho, y.ws0);
+        // SAP on them, then ch = rho - (final residual), ph += ws0
+        if (sap_mop_multi(c, m, mus, c.isolv, c.nmr, c.ncy, rh, ph, ch, phib, st, base, add)) return -1;
         dfl_mark(c, 4);
-        y.lstat += ls[i];
       }
     } else {
-      for (int r : A) {
-        SysState &y = S[r];
-        void *ph = y.phi[y.k], *ch = y.chi[y.k];
+      for (int i0 = 0; i0 < na; i0 += SAP_MS) {
+        const int m = na - i0 < SAP_MS ? na - i0 : SAP_MS;
+        const void *rh[SAP_MS];
+        void *ph[SAP_MS], *ch[SAP_MS];
+        float mus[SAP_MS];
+        for (int q = 0; q < m; q++) {
+          SysState &y = S[A[i0 + q]];
+          rh[q] = y.rho;
+          ph[q] = y.phi[y.k];
+          ch[q] = y.chi[y.k];
+          mus[q] = (float)y.mu;
+        }
         dfl_mark(c, 2);
-        sap_mop(c, (float)y.mu, c.isolv, c.nmr, c.ncy, y.rho, ph, ch, phib, st);
+        if (sap_mop_multi(c, m, mus, c.isolv, c.nmr, c.ncy, rh, ph, ch, phib, st, nullptr, nullptr)) return -1;
         dfl_mark(c, 4);
       }
     }
