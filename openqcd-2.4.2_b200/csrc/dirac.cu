@@ -114,11 +114,10 @@ constexpr int kDwUnroll = DW_UNROLL;
 // L12 = 1 (FP32 only): the links are read as 12 reals (load_link12), the
 // time links at x0 = N0-1 with the boundary sign.
 template <typename R, int OPS, int PAR, int RHALF, int THALF, int L12, int DD>
-__device__ __forceinline__ void dirac_body(const Geom &g, const DDGeom &dg, const void *__restrict__ s,
+__device__ __forceinline__ void dirac_body(const Geom &g, const DDGeom &dg, int i, const void *__restrict__ s,
                                            const void *__restrict__ t, void *r, const void *__restrict__ u,
                                            const void *__restrict__ sw, const void *__restrict__ swinv, R mu_e,
                                            R mu_o, const int *__restrict__ sched, const void *__restrict__ sub) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
   int p, blk, si;
   if (PAR == 2) {
     if (i >= g.vol) return;
@@ -235,7 +234,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32)
     dirac_kernel(Geom g, const void *__restrict__ s, const void *__restrict__ t, void *r, const void *__restrict__ u,
                  const void *__restrict__ sw, const void *__restrict__ swinv, R mu_e, R mu_o,
                  const int *__restrict__ sched, const void *__restrict__ sub) {
-  dirac_body<R, OPS, PAR, RHALF, THALF, L12, 0>(g, DDGeom{0, 0, nullptr, nullptr}, s, t, r, u, sw, swinv, mu_e, mu_o,
+  dirac_body<R, OPS, PAR, RHALF, THALF, L12, 0>(g, DDGeom{0, 0, nullptr, nullptr}, blockIdx.x * blockDim.x + threadIdx.x,
+                                                s, t, r, u, sw, swinv, mu_e, mu_o,
                                                 sched, sub);
 }
 template <typename R, int OPS, int PAR, int L12>
@@ -243,7 +243,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 8 ? DW_MINB64 : DW_MINB32)
     dirac_dd_kernel(Geom g, DDGeom dg, const void *__restrict__ s, const void *__restrict__ t, void *r,
                     const void *__restrict__ u, const void *__restrict__ sw, const void *__restrict__ swinv, R mu_e,
                     R mu_o, const int *__restrict__ sched) {
-  dirac_body<R, OPS, PAR, 0, 0, L12, 1>(g, dg, s, t, r, u, sw, swinv, mu_e, mu_o, sched, nullptr);
+  dirac_body<R, OPS, PAR, 0, 0, L12, 1>(g, dg, blockIdx.x * blockDim.x + threadIdx.x, s, t, r, u, sw, swinv, mu_e,
+                                        mu_o, sched, nullptr);
 }
 
 // ------------------------------------------------------------------------
@@ -323,6 +324,29 @@ __device__ __forceinline__ void staged_tile(const Geom &g, int PAR_, int t, int 
 // with bulk prefetches while the current tile was computed: 0.90 ms against
 // 0.69 ms at 32^3x64, DRAM reads 4.35 GB against 3.36 GB per launch (the
 // prefetched lines were partly evicted before use).
+// Several systems of the batched solvers (SAP_MS at most): r_j = sub_j -
+// Dw(mu_j) s_j, FP32, in one launch whose CTAs of one tile of 128 sites
+// are adjacent (CTA x: tile x / n, system x % n), so the links and SW
+// matrices of a tile serve every system while they are in L2.
+struct DwSys {
+  const void *s[SAP_MS];
+  void *r[SAP_MS];
+  const void *sub[SAP_MS];
+  float mu[SAP_MS];
+};
+template <int L12>
+__global__ void __launch_bounds__(128, DW_MINB32)
+    dirac_sys_kernel(Geom g, DwSys f, int n, const void *__restrict__ u, const void *__restrict__ sw, int eoflg,
+                     const int *__restrict__ sched) {
+  const int j = blockIdx.x % n, i = (blockIdx.x / n) * blockDim.x + threadIdx.x;
+  const void *s = j == 0 ? f.s[0] : j == 1 ? f.s[1] : j == 2 ? f.s[2] : f.s[3];
+  void *r = j == 0 ? f.r[0] : j == 1 ? f.r[1] : j == 2 ? f.r[2] : f.r[3];
+  const void *sb = j == 0 ? f.sub[0] : j == 1 ? f.sub[1] : j == 2 ? f.sub[2] : f.sub[3];
+  const float mu = j == 0 ? f.mu[0] : j == 1 ? f.mu[1] : j == 2 ? f.mu[2] : f.mu[3];
+  dirac_body<float, OP_SW | OP_HOP | OP_SUB, 2, 0, 0, L12, 0>(g, DDGeom{0, 0, nullptr, nullptr}, i, s, s, r, u, sw,
+                                                               nullptr, mu, eoflg ? 0.0f : mu, sched, sb);
+}
+
 template <int OPS, int PAR, int DD>
 __device__ __forceinline__ void staged_body(const Geom &g, const DDGeom &dg, const double2 *__restrict__ s,
                                             const double2 *__restrict__ t, double2 *r, const double2 *__restrict__ u,
@@ -613,6 +637,26 @@ int dirac_multi32(const Ctx &c, int n, float mu, void *const *sv, void *const *r
       dirac_kernel<float, OP_SW | OP_HOP, 2><<<nb, threads, 0, st>>>(c.g, sv[j], sv[j], rv[j], c.u32, c.sw32, nullptr,
                                                                     mu, muo, c.sched, nullptr);
   }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// r_j = sub_j - Dw(mu_j) s_j for n <= SAP_MS systems in one launch (FP32)
+int dirac_sys32(const Ctx &c, int n, const float *mu, void *const *sv, void *const *rv, void *const *subv,
+                cudaStream_t st) {
+  if (n < 1 || n > SAP_MS) return -2;
+  DwSys f;
+  for (int j = 0; j < SAP_MS; j++) {
+    const int k = j < n ? j : 0;
+    f.s[j] = sv[k];
+    f.r[j] = rv[k];
+    f.sub[j] = subv[k];
+    f.mu[j] = mu[k];
+  }
+  const int threads = 128;
+  const unsigned nb = (unsigned)((c.g.vol + threads - 1) / threads) * n;
+  const void *u12 = links12(const_cast<Ctx &>(c), st);
+  if (u12) dirac_sys_kernel<1><<<nb, threads, 0, st>>>(c.g, f, n, u12, c.sw32, c.eoflg, c.sched);
+  else dirac_sys_kernel<0><<<nb, threads, 0, st>>>(c.g, f, n, c.u32, c.sw32, c.eoflg, c.sched);
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 

@@ -377,6 +377,9 @@ void net_fields_release(Ctx &c);
 int dfl_batch_alloc(Ctx &c);
 int dirac_multi32(const Ctx &c, int n, float mu, void *const *sv, void *const *rv, void *const *subv,
                   cudaStream_t st);
+// r_j = sub_j - Dw(mu_j) s_j for n <= SAP_MS systems in one launch (FP32)
+int dirac_sys32(const Ctx &c, int n, const float *mu, void *const *sv, void *const *rv, void *const *subv,
+                cudaStream_t st);
 void dfl_mark(Ctx &c, int k);
 int ensure_lvd_n(Ctx &c, int n);
 int dfl_batch_check(Ctx &c);

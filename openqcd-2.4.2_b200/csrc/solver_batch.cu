@@ -796,23 +796,23 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
       for (int i0 = 0; i0 < na; i0 += SAP_MS) {
         const int m = na - i0 < SAP_MS ? na - i0 : SAP_MS;
         const void *rh[SAP_MS], *base[SAP_MS], *add[SAP_MS];
-        void *ph[SAP_MS], *ch[SAP_MS];
+        void *ph[SAP_MS], *ch[SAP_MS], *in[SAP_MS], *rv[SAP_MS];
         float mus[SAP_MS];
         for (int q = 0; q < m; q++) {
           SysState &y = S[A[i0 + q]];
           ph[q] = y.phi[y.k];
           ch[q] = y.chi[y.k];
           // rho - D ws0, written where the SAP sequence reads its input
-          void *in = sap_input_field_multi(c, q);
-          if (!in) in = ch[q];
-          void *const rv[1] = {in}, *const bv[1] = {y.rho};
-          dirac_multi32(c, 1, (float)y.mu, &w0[i0 + q], rv, bv, st);
-          rh[q] = in;
+          in[q] = sap_input_field_multi(c, q);
+          if (!in[q]) in[q] = ch[q];
+          rv[q] = y.rho;
+          rh[q] = in[q];
           base[q] = y.rho;
           add[q] = y.ws0;
           mus[q] = (float)y.mu;
           y.lstat += ls[i0 + q];
         }
+        if (dirac_sys32(c, m, mus, &w0[i0], in, rv, st)) return fail("gcr_batch: Dirac launch failed");
         dfl_mark(c, 3);
         // SAP on them, then ch = rho - (final residual), ph += ws0
         if (sap_mop_multi(c, m, mus, c.isolv, c.nmr, c.ncy, rh, ph, ch, phib, st, base, add)) return -1;
