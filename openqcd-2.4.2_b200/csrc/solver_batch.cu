@@ -342,9 +342,6 @@ constexpr int OG = 1184, OK_ = 32;
 struct F2Ptrs {
   const float4 *p[OK_];
 };
-struct F2Coef {
-  float2 c[OK_];
-};
 
 // products summed in FP32 over runs of 16 grid-stride steps, the runs in
 // double (FP64 adds per element halved the speed of these kernels)
@@ -448,10 +445,22 @@ __device__ __forceinline__ void block_sum2(double a0, double a1, double a2, doub
   }
 }
 
-// chi_k -= sum_l c_l chi_l ; partial |chi_k|^2 and (chi_k, rho)
+// The same three passes with the coefficients kept on the device: the
+// products of pass (1) and the two sums of pass (2) are written to the
+// system's record dsum (OK_ + 3 entries: a_lk, |chi_k|^2, (chi_k, rho),
+// |rho|^2), pass (2) reads its coefficients there and pass (3) derives its
+// scale and coefficient there exactly as the host does (float(sqrt(double
+// (float |chi_k|^2))), 1.0f / b), so the host reads one record per system
+// per step instead of waiting three times per system.
+constexpr int DS = OK_ + 3;
+
 template <int KM>
-__global__ void __launch_bounds__(256) k_fgs(F2Ptrs q, int k, F2Coef c, float4 *chik, const float4 *__restrict__ rho,
-                                             size_t n, double2 *part) {
+__global__ void __launch_bounds__(256) k_fgs_d(F2Ptrs q, int k, const double2 *__restrict__ coef, float4 *chik,
+                                               const float4 *__restrict__ rho, size_t n, double2 *part) {
+  float2 cz[KM];
+#pragma unroll
+  for (int j = 0; j < KM; j++)
+    cz[j] = j < k ? make_float2((float)coef[j].x, (float)coef[j].y) : make_float2(0.0f, 0.0f);
   double nn = 0.0, dr = 0.0, di = 0.0;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -463,7 +472,7 @@ __global__ void __launch_bounds__(256) k_fgs(F2Ptrs q, int k, F2Coef c, float4 *
       for (int j = 0; j < KM; j++)
         if (j < k) {
           const float4 a = __ldg(q.p[j] + i);
-          const float2 z = c.c[j];
+          const float2 z = cz[j];
           x.x -= z.x * a.x - z.y * a.y;
           x.y -= z.x * a.y + z.y * a.x;
           x.z -= z.x * a.z - z.y * a.w;
@@ -482,8 +491,11 @@ __global__ void __launch_bounds__(256) k_fgs(F2Ptrs q, int k, F2Coef c, float4 *
   block_sum2(nn, dr, di, part);
 }
 
-// chi_k *= s ; rho -= c chi_k ; partial |rho|^2
-__global__ void __launch_bounds__(256) k_fupd(float4 *chik, float4 *rho, float s, float2 c, size_t n, double2 *part) {
+__global__ void __launch_bounds__(256) k_fupd_d(float4 *chik, float4 *rho, const double2 *__restrict__ sums, size_t n,
+                                                double2 *part) {
+  const float bn = (float)sqrt((double)(float)sums[0].x);
+  const float s = bn != 0.0f ? 1.0f / bn : 0.0f;
+  const float2 c = make_float2((float)sums[1].x * s, (float)sums[1].y * s);
   double nn = 0.0;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -509,57 +521,63 @@ __global__ void __launch_bounds__(256) k_fupd(float4 *chik, float4 *rho, float s
 }
 
 struct OrthoBufs {
-  double2 *part = nullptr, *out = nullptr, *h = nullptr;
+  double2 *part = nullptr;
+  double2 *dsum = nullptr, *h_dsum = nullptr;   // DS entries per system
+  int nsys = 0;
 };
 static OrthoBufs g_ob;
 
 static int ortho_alloc() {
   if (g_ob.part) return 0;
-  if (cudaMalloc(&g_ob.part, (size_t)OG * OK_ * sizeof(double2)) != cudaSuccess ||
-      cudaMalloc(&g_ob.out, OK_ * sizeof(double2)) != cudaSuccess ||
-      cudaMallocHost(&g_ob.h, OK_ * sizeof(double2)) != cudaSuccess)
+  if (cudaMalloc(&g_ob.part, (size_t)OG * OK_ * sizeof(double2)) != cudaSuccess)
     return fail("out of memory (orthogonalisation buffers)");
   return 0;
 }
 
-static void ortho_read(cudaStream_t st, int k) {
-  k_fsum<<<k, 256, 0, st>>>(g_ob.part, g_ob.out);
-  cudaMemcpyAsync(g_ob.h, g_ob.out, k * sizeof(double2), cudaMemcpyDeviceToHost, st);
-  cudaStreamSynchronize(st);
+static int dsum_alloc(int nr) {
+  if (g_ob.nsys >= nr) return 0;
+  cudaFree(g_ob.dsum);
+  cudaFreeHost(g_ob.h_dsum);
+  g_ob.dsum = g_ob.h_dsum = nullptr;
+  g_ob.nsys = 0;
+  if (cudaMalloc(&g_ob.dsum, (size_t)nr * DS * sizeof(double2)) != cudaSuccess ||
+      cudaMallocHost(&g_ob.h_dsum, (size_t)nr * DS * sizeof(double2)) != cudaSuccess)
+    return fail("out of memory (orthogonalisation buffers)");
+  g_ob.nsys = nr;
+  return 0;
 }
 
-// gcr_step for one system with the fused passes (istop = 0): returns rn
-static double gcr_step_fused(const Ctx &c, int nkv, int k, const std::vector<void *> &chi, void *rho,
-                             std::vector<cplxf> &a, std::vector<float> &b, std::vector<cplxf> &cc,
-                             cudaStream_t st) {
-  const size_t n = (size_t)c.g.vol * 6;   // float4 elements of an FP32 field
+// the passes of gcr_step_fused for one system, its record at dsum
+static void gcr_step_dev(const Ctx &c, int k, const std::vector<void *> &chi, void *rho, double2 *dsum,
+                         cudaStream_t st) {
+  const size_t n = (size_t)c.g.vol * 6;
   F2Ptrs q;
   for (int j = 0; j < OK_; j++) q.p[j] = j < k ? (const float4 *)chi[j] : nullptr;
-  F2Coef co;
-  for (int j = 0; j < OK_; j++) co.c[j] = make_float2(0.0f, 0.0f);
   if (k > 0) {
     if (k <= 8) k_fmdot<8><<<OG, 256, 0, st>>>(q, k, (const float4 *)chi[k], n, g_ob.part);
     else if (k <= 16) k_fmdot<16><<<OG, 256, 0, st>>>(q, k, (const float4 *)chi[k], n, g_ob.part);
     else k_fmdot<32><<<OG, 256, 0, st>>>(q, k, (const float4 *)chi[k], n, g_ob.part);
-    ortho_read(st, k);
-    for (int l = 0; l < k; l++) {
-      const cplxf z = {(float)g_ob.h[l].x, (float)g_ob.h[l].y};
-      a[(size_t)nkv * l + k] = z;
-      co.c[l] = make_float2(z.re, z.im);
-    }
+    k_fsum<<<k, 256, 0, st>>>(g_ob.part, dsum);
   }
-  if (k <= 8) k_fgs<8><<<OG, 256, 0, st>>>(q, k, co, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
-  else if (k <= 16) k_fgs<16><<<OG, 256, 0, st>>>(q, k, co, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
-  else k_fgs<32><<<OG, 256, 0, st>>>(q, k, co, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
-  ortho_read(st, 2);
-  const float bn = (float)sqrt((double)(float)g_ob.h[0].x);
+  if (k <= 8) k_fgs_d<8><<<OG, 256, 0, st>>>(q, k, dsum, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
+  else if (k <= 16) k_fgs_d<16><<<OG, 256, 0, st>>>(q, k, dsum, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
+  else k_fgs_d<32><<<OG, 256, 0, st>>>(q, k, dsum, (float4 *)chi[k], (const float4 *)rho, n, g_ob.part);
+  k_fsum<<<2, 256, 0, st>>>(g_ob.part, dsum + OK_);
+  k_fupd_d<<<OG, 256, 0, st>>>((float4 *)chi[k], (float4 *)rho, dsum + OK_, n, g_ob.part);
+  k_fsum<<<1, 256, 0, st>>>(g_ob.part, dsum + OK_ + 2);
+}
+
+// a_lk, b_k, c_k and rn of a system from its record, as gcr_step_fused sets them
+static double gcr_step_coefs(int nkv, int k, const double2 *h, std::vector<cplxf> &a, std::vector<float> &b,
+                             std::vector<cplxf> &cc) {
+  for (int l = 0; l < k; l++) a[(size_t)nkv * l + k] = {(float)h[l].x, (float)h[l].y};
+  const float bn = (float)sqrt((double)(float)h[OK_].x);
   b[k] = bn;
   const float s = bn != 0.0f ? 1.0f / bn : 0.0f;
-  cc[k] = {(float)g_ob.h[1].x * s, (float)g_ob.h[1].y * s};
-  k_fupd<<<OG, 256, 0, st>>>((float4 *)chi[k], (float4 *)rho, s, make_float2(cc[k].re, cc[k].im), n, g_ob.part);
-  ortho_read(st, 1);
-  return sqrt((double)(float)g_ob.h[0].x);
+  cc[k] = {(float)h[OK_ + 1].x * s, (float)h[OK_ + 1].y * s};
+  return sqrt((double)(float)h[OK_ + 2].x);
 }
+
 
 // ------------------------------------------------------------- outer solver
 struct SysState {
@@ -682,7 +700,7 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
     if (!d.ready || !d.have_basis) return fail("gcr_batch: the deflation subspace is not set");
     if (dfl_batch_alloc(c)) return -1;
   }
-  if (sap_prepare(c, st) || ortho_alloc()) return -1;
+  if (sap_prepare(c, st) || ortho_alloc() || dsum_alloc(nr)) return -1;
   const int per32 = 2 * nkv + 1 + (dfl ? 1 : 0);
   if (bw_reserve(c, g_bw.f32, (size_t)nr * per32 + 1, 32) || bw_reserve(c, g_bw.f64, (size_t)nr + 1, 64)) return -1;
   if (!c.tmp32 && cudaMalloc(&c.tmp32, spinor_bytes(c, 32)) != cudaSuccess) return fail("out of device memory");
@@ -836,12 +854,35 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
         dfl_mark(c, 4);
       }
     }
-    // --- the rest of gcr_step, and restarts, per system (fgcr.c:157-299)
-    for (int r : A) {
+    // --- the rest of gcr_step, and restarts, per system (fgcr.c:157-299):
+    // with the fused passes, every system's passes first, then one read of
+    // all their records
+    const bool fused = istop == 0 && nkv <= OK_;
+    if (fused) {
+      // captured as one CUDA graph per step shape (the systems' k and
+      // fields), replayed by later steps and solves of the same shape
+      std::vector<uint64_t> key = {0x0e7a0ull, (uint64_t)na, (uint64_t)(size_t)c.g.vol};
+      for (int i = 0; i < na; i++) {
+        const SysState &y = S[A[i]];
+        key.push_back((uint64_t)y.k);
+        key.push_back((uint64_t)(uintptr_t)y.rho);
+        for (int l = 0; l <= y.k; l++) key.push_back((uint64_t)(uintptr_t)y.chi[l]);
+      }
+      const int rc = graph_run(c, key.data(), key.size() * sizeof(uint64_t), st, [&]() {
+        for (int i = 0; i < na; i++)
+          gcr_step_dev(c, S[A[i]].k, S[A[i]].chi, S[A[i]].rho, g_ob.dsum + (size_t)i * DS, st);
+        return cudaGetLastError() == cudaSuccess ? 0 : fail("gcr_batch: launch failed");
+      });
+      if (rc) return -1;
+      cudaMemcpyAsync(g_ob.h_dsum, g_ob.dsum, (size_t)na * DS * sizeof(double2), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) return fail("gcr_batch: CUDA error");
+    }
+    for (int ia = 0; ia < na; ia++) {
+      const int r = A[ia];
       SysState &y = S[r];
       const int k = y.k;
-      if (istop == 0 && nkv <= OK_) {
-        y.rn = gcr_step_fused(c, nkv, k, y.chi, y.rho, y.a, y.b, y.cc, st);
+      if (fused) {
+        y.rn = gcr_step_coefs(nkv, k, g_ob.h_dsum + (size_t)ia * DS, y.a, y.b, y.cc);
       } else {
         for (int l = 0; l < k; l++) {
           cplxf z = o.dot32(y.chi[l], y.chi[k]);
