@@ -192,18 +192,16 @@ struct SapF32R {
   }
 };
 
-// -1/2 * H restricted to the block (Dirichlet exterior): hop terms of the
+// h += H restricted to the block (Dirichlet exterior): hop terms of the
 // field in shared memory (parity 1-p) around site (p, s) of block blk.
 template <class P>
-__device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int blk, int s,
-                                                   const typename P::T *src, int ld) {
+__device__ __forceinline__ void block_hop_acc(const SapArgs &a, int p, int blk, int s, const typename P::T *src,
+                                              int ld, spinor<float> &h) {
   const Geom &g = a.g;
   int y[4];
   unpack4(__ldg(g.lcoord + p * g.vbh + s), y);
   int l = y[0] * g.lstr[0] + y[1] * g.lstr[1] + y[2] * g.lstr[2] + y[3] * g.lstr[3];
   const int chunk = p * g.nbl + blk, ochunk = (1 - p) * g.nbl + blk;
-  spinor<float> h;
-  szero(h);
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
     if (y[mu] + 1 < g.bs[mu]) {
@@ -219,6 +217,15 @@ __device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int 
       hop_bwd<float>(mu, uu, sm, h);
     }
   }
+}
+
+// -1/2 * H restricted to the block
+template <class P>
+__device__ __forceinline__ spinor<float> block_hop(const SapArgs &a, int p, int blk, int s,
+                                                   const typename P::T *src, int ld) {
+  spinor<float> h;
+  szero(h);
+  block_hop_acc<P>(a, p, blk, s, src, ld, h);
   sscale<float>(h, -0.5f);
   return h;
 }
@@ -291,12 +298,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
         } else if (!last) {
           P::sm_store(W, ld, s, t);
         } else {
+          // one field at a time, so that few spinors are live at once
           spinor<float> ph = Store<float>::load_spinor_rw(y.phi, co, s, g.vbh);
           ssub(ph, t);
-          spinor<float> ps = Store<float>::load_spinor_rw(y.psi, co, s, g.vbh);
-          sadd(ps, ph);
-          Store<float>::store_spinor(y.psi, co, s, g.vbh, ps);
           Store<float>::store_spinor(y.phi, co, s, g.vbh, ph);
+          {
+            spinor<float> ps = Store<float>::load_spinor_rw(y.psi, co, s, g.vbh);
+            sadd(ps, ph);
+            Store<float>::store_spinor(y.psi, co, s, g.vbh, ps);
+          }
           spinor<float> ro;
           if (a.eoflg) {
             szero(ro);
@@ -319,13 +329,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
       for (int k = 0; k < NS; k++) {
         int s = threadIdx.x + k * T_;
         if (s < g.vbh) {
-          spinor<float> s0 = P::sm_load(S0, ld, s);
-          spinor<float> r1 = P::sm_load(S1, ld, s);
-          spinor<float> ps = Store<float>::load_spinor_rw(y.psi, ce, s, g.vbh);
-          sadd(ps, s0);
-          Store<float>::store_spinor(y.psi, ce, s, g.vbh, ps);
+          const spinor<float> s0 = P::sm_load(S0, ld, s);
           Store<float>::store_spinor(y.phi, ce, s, g.vbh, s0);
-          Store<float>::store_spinor(y.rho, ce, s, g.vbh, r1);
+          {
+            spinor<float> ps = Store<float>::load_spinor_rw(y.psi, ce, s, g.vbh);
+            sadd(ps, s0);
+            Store<float>::store_spinor(y.psi, ce, s, g.vbh, ps);
+          }
+          Store<float>::store_spinor(y.rho, ce, s, g.vbh, P::sm_load(S1, ld, s));
         }
       }
       break;
@@ -336,18 +347,23 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T_;
       if (s < g.vbh) {
-        spinor<float> hw = block_hop<P>(a, 0, blk, s, W, ld);
+        // base - (-1/2) H W as (2 base + H W) / 2 (exact scalings), with
+        // base = rho_e (step 0) or (A_e + i mu g5) S1: the hop accumulates
+        // straight into it, so no second spinor is live across the hop
+        spinor<float> b2;
+        if (step == 0) b2 = Store<float>::load_spinor_rw(y.rho, ce, s, g.vbh);
+        else b2 = P::sw(a.sw, ce, s, g.vbh, y.mu, P::sm_load(S1, ld, s));
+        sscale<float>(b2, 2.0f);
+        block_hop_acc<P>(a, 0, blk, s, W, ld, b2);
+        sscale<float>(b2, 0.5f);
         if (step == 0) {
-          spinor<float> r = Store<float>::load_spinor_rw(y.rho, ce, s, g.vbh);
-          ssub(r, hw);
-          P::sm_store(S1, ld, s, r);
+          P::sm_store(S1, ld, s, b2);
           spinor<float> z;
           szero(z);
           P::sm_store(S0, ld, s, z);
         } else {
-          spinor<float> s1 = P::sm_load(S1, ld, s);
-          s2[k] = P::sw(a.sw, ce, s, g.vbh, y.mu, s1);
-          ssub(s2[k], hw);
+          const spinor<float> s1 = P::sm_load(S1, ld, s);
+          s2[k] = b2;
 #pragma unroll
           for (int c = 0; c < 4; c++)
 #pragma unroll
@@ -377,19 +393,25 @@ __global__ void __launch_bounds__(MAXT, MINB) k_sap_blocks_eo(SapArgs a) {
     for (int k = 0; k < NS; k++) {
       int s = threadIdx.x + k * T_;
       if (s < g.vbh) {
-        spinor<float> s1 = P::sm_load(S1, ld, s), s0 = P::sm_load(S0, ld, s);
+        // plane by plane (two complex components), so that only s2 stays
+        // live across the update
+        float4 *v1 = reinterpret_cast<float4 *>(S1), *v0 = reinterpret_cast<float4 *>(S0);
 #pragma unroll
-        for (int c = 0; c < 4; c++)
-#pragma unroll
-          for (int j = 0; j < 3; j++) {
-            cpx<float> x1 = s1.c[c].c[j], x2 = s2[k].c[c].c[j];
-            s0.c[c].c[j].re += zr * x1.re - zi * x1.im;
-            s0.c[c].c[j].im += zr * x1.im + zi * x1.re;
-            s1.c[c].c[j].re -= zr * x2.re - zi * x2.im;
-            s1.c[c].c[j].im -= zr * x2.im + zi * x2.re;
-          }
-        P::sm_store(S0, ld, s, s0);
-        P::sm_store(S1, ld, s, s1);
+        for (int jp = 0; jp < 6; jp++) {
+          float4 a1 = v1[jp * ld + s], a0 = v0[jp * ld + s];
+          const cpx<float> x2 = s2[k].c[(2 * jp) / 3].c[(2 * jp) % 3];
+          const cpx<float> y2 = s2[k].c[(2 * jp + 1) / 3].c[(2 * jp + 1) % 3];
+          a0.x += zr * a1.x - zi * a1.y;
+          a0.y += zr * a1.y + zi * a1.x;
+          a0.z += zr * a1.z - zi * a1.w;
+          a0.w += zr * a1.w + zi * a1.z;
+          a1.x -= zr * x2.re - zi * x2.im;
+          a1.y -= zr * x2.im + zi * x2.re;
+          a1.z -= zr * y2.re - zi * y2.im;
+          a1.w -= zr * y2.im + zi * y2.re;
+          v0[jp * ld + s] = a0;
+          v1[jp * ld + s] = a1;
+        }
       }
     }
     __syncthreads();
