@@ -270,6 +270,7 @@ int b200_geometry(const int L[4], const int bs[4], const int *ipt) {
   c.u12 = nullptr; c.u12_valid = c.u12_ok = false;
   c.sap_fld[0] = c.sap_fld[1] = c.sap_fld[2] = nullptr;
   c.sap_mfld[0] = c.sap_mfld[1] = c.sap_mfld[2] = nullptr;
+  c.sap_mfld_n = 0;
   c.have_ud = c.have_sw = false;
   qcd::dfl_release(c);
   qcd::net_fields_release(c);

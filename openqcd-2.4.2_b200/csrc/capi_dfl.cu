@@ -214,6 +214,7 @@ int b200_release_workspace(void) {
     cudaFree(c.sap_mfld[k]);
     c.sap_mfld[k] = nullptr;
   }
+  c.sap_mfld_n = 0;
   return cudaDeviceSynchronize() == cudaSuccess ? 0 : fail("CUDA error");
 }
 

@@ -339,10 +339,19 @@ __global__ void __launch_bounds__(128, DW_MINB32)
     dirac_sys_kernel(Geom g, DwSys f, int n, const void *__restrict__ u, const void *__restrict__ sw, int eoflg,
                      const int *__restrict__ sched) {
   const int j = blockIdx.x % n, i = (blockIdx.x / n) * blockDim.x + threadIdx.x;
-  const void *s = j == 0 ? f.s[0] : j == 1 ? f.s[1] : j == 2 ? f.s[2] : f.s[3];
-  void *r = j == 0 ? f.r[0] : j == 1 ? f.r[1] : j == 2 ? f.r[2] : f.r[3];
-  const void *sb = j == 0 ? f.sub[0] : j == 1 ? f.sub[1] : j == 2 ? f.sub[2] : f.sub[3];
-  const float mu = j == 0 ? f.mu[0] : j == 1 ? f.mu[1] : j == 2 ? f.mu[2] : f.mu[3];
+  // selected without indexing the parameter arrays by a variable (which
+  // would copy them to local memory)
+  const void *s = f.s[0], *sb = f.sub[0];
+  void *r = f.r[0];
+  float mu = f.mu[0];
+#pragma unroll
+  for (int q = 1; q < SAP_MS; q++)
+    if (j == q) {
+      s = f.s[q];
+      r = f.r[q];
+      sb = f.sub[q];
+      mu = f.mu[q];
+    }
   dirac_body<float, OP_SW | OP_HOP | OP_SUB, 2, 0, 0, L12, 0>(g, DDGeom{0, 0, nullptr, nullptr}, i, s, s, r, u, sw,
                                                                nullptr, mu, eoflg ? 0.0f : mu, sched, sb);
 }

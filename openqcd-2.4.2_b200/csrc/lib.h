@@ -99,7 +99,7 @@ struct NetState {
   std::vector<void *> f;
 };
 
-constexpr int SAP_MS = 4;   // systems per SAP launch of the batched solvers
+constexpr int SAP_MS = 8;   // systems per SAP launch of the batched solvers
 
 // Everything the reference keeps in module-global state for this path:
 // geometry (lattice/geometry.c), the gauge field (uflds/uflds.c udfld/ufld),
@@ -178,8 +178,10 @@ struct Ctx {
   // on three library-owned FP32 fields (solution, residual, block scratch)
   int use_graphs = 1;
   void *sap_fld[3] = {nullptr, nullptr, nullptr};
-  // the same for SAP_MS systems at once (SAP_MS consecutive fields each)
+  // the same for up to SAP_MS systems at once (sap_mfld_n consecutive
+  // fields each)
   void *sap_mfld[3] = {nullptr, nullptr, nullptr};
+  int sap_mfld_n = 0;
   int nthread = 1;              // the caller's NTHREAD, for icom & 0x2 in the BLAS drop-ins
   void *fstage[3] = {nullptr, nullptr, nullptr};   // staging of host operands
   size_t fstage_bytes[3] = {0, 0, 0};
@@ -431,9 +433,10 @@ void *sap_input_field(Ctx &c);
 // psi = ncy cycles on rho = rh, then rho = rh - rho (the sap_gcr preconditioner)
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
             cudaStream_t st, const void *base = nullptr, const void *add = nullptr);
-// the input field of system r (< SAP_MS) of sap_mop_multi (null when CUDA
-// graphs are off or with domain decomposition)
-void *sap_input_field_multi(Ctx &c, int r);
+// the input field of system r (< n <= SAP_MS) of an sap_mop_multi call on
+// n systems (null when CUDA graphs are off, with domain decomposition, or
+// when the fields do not fit)
+void *sap_input_field_multi(Ctx &c, int r, int n);
 // sap_mop for ns systems (twisted masses mu[r]) with every SAP launch
 // covering up to SAP_MS of them; base and add may be null (as in sap_mop),
 // or arrays whose entries may be null

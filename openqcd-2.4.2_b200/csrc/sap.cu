@@ -59,7 +59,10 @@ __device__ __forceinline__ SapSys sap_sys(const SapArgs &a, int r) {
   y.psi = a.psi + o;
   y.rho = a.rho + o;
   y.phi = a.phi + o;
-  y.mu = r == 0 ? a.mus[0] : r == 1 ? a.mus[1] : r == 2 ? a.mus[2] : a.mus[3];
+  y.mu = a.mus[0];
+#pragma unroll
+  for (int q = 1; q < SAP_MS; q++)
+    if (r == q) y.mu = a.mus[q];
   return y;
 }
 
@@ -1020,11 +1023,18 @@ int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void 
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
 }
 
-// the fields of sap_mop_multi; false (and nothing held) when the device
-// has no room for them, in which case the systems run one at a time
-static bool sap_multi_fields(Ctx &c) {
+// the fields of sap_mop_multi for n systems; false (and nothing held) when
+// the device has no room for them, in which case the systems run one at a
+// time
+static bool sap_multi_fields(Ctx &c, int n) {
+  if (c.sap_mfld_n >= n) return true;
+  for (int k = 0; k < 3; k++) {
+    cudaFree(c.sap_mfld[k]);
+    c.sap_mfld[k] = nullptr;
+  }
+  c.sap_mfld_n = 0;
   for (int k = 0; k < 3; k++)
-    if (!c.sap_mfld[k] && cudaMalloc(&c.sap_mfld[k], SAP_MS * spinor_bytes(c, 32)) != cudaSuccess) {
+    if (cudaMalloc(&c.sap_mfld[k], (size_t)n * spinor_bytes(c, 32)) != cudaSuccess) {
       cudaGetLastError();
       for (int j = 0; j < 3; j++) {
         cudaFree(c.sap_mfld[j]);
@@ -1032,11 +1042,12 @@ static bool sap_multi_fields(Ctx &c) {
       }
       return false;
     }
+  c.sap_mfld_n = n;
   return true;
 }
 
-void *sap_input_field_multi(Ctx &c, int r) {
-  if (!c.use_graphs || dd_on(c) || r < 0 || r >= SAP_MS || !sap_multi_fields(c)) return nullptr;
+void *sap_input_field_multi(Ctx &c, int r, int n) {
+  if (!c.use_graphs || dd_on(c) || r < 0 || r >= n || n > SAP_MS || !sap_multi_fields(c, n)) return nullptr;
   return (char *)c.sap_mfld[1] + (size_t)r * spinor_bytes(c, 32);
 }
 
@@ -1047,7 +1058,7 @@ void *sap_input_field_multi(Ctx &c, int r) {
 int sap_mop_multi(Ctx &c, int ns, const float *mu, int isolv, int nmr, int ncy, const void *const *rh,
                   void *const *psi, void *const *rho, void *phi_blk, cudaStream_t st, const void *const *base,
                   const void *const *add) {
-  if (!c.use_graphs || dd_on(c) || ns == 1 || !sap_multi_fields(c)) {
+  if (!c.use_graphs || dd_on(c) || ns == 1 || !sap_multi_fields(c, ns < SAP_MS ? ns : SAP_MS)) {
     for (int r = 0; r < ns; r++)
       if (sap_mop(c, mu[r], isolv, nmr, ncy, rh[r], psi[r], rho[r], phi_blk, st, base ? base[r] : nullptr,
                   add ? add[r] : nullptr))

@@ -821,7 +821,7 @@ int gcr_batch(Ctx &c, int nr, int dfl, int nkv, int nmx, int istop, double res, 
           ph[q] = y.phi[y.k];
           ch[q] = y.chi[y.k];
           // rho - D ws0, written where the SAP sequence reads its input
-          in[q] = sap_input_field_multi(c, q);
+          in[q] = sap_input_field_multi(c, q, m);
           if (!in[q]) in[q] = ch[q];
           rv[q] = y.rho;
           rh[q] = in[q];
