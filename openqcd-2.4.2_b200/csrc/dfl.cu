@@ -1272,7 +1272,7 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   if (d.gen_kappa == 0.0) return fail("dfl_modes: kappa = 0 (infinite generation mass) is not supported");
   if (!c.sap_set) return fail("dfl_modes: SAP parameters are not set");
   cudaStream_t st = c.stream;
-  if (sap_prepare(c, st) || ensure_lvd(c) || reserve32(c, d.modes, d.Ns) || reserve32(c, c.ws32, 9) ||
+  if (sap_prepare(c, st) || ensure_lvd(c) || reserve32(c, d.modes, d.Ns) || reserve32(c, c.ws32, 9 + 2 * SAP_MS) ||
       dfl_batch_alloc(c) || ensure_lvd_n(c, 4))
     return -1;
   // device table of the mode fields (for the Cholesky QR kernels)
@@ -1293,7 +1293,10 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   }
   c.eoflg = 1;
   if (c.sw_inv_fail & 2) ifail[0] = -3;
-  void *ws0 = c.ws32[0], *phib = c.ws32[8];
+  // SAP runs on up to SAP_MS modes per launch: ws32[9 ..] holds their
+  // residuals in the smoothing rounds, ws32[9 + SAP_MS ..] their block
+  // scratch
+  void *const *rs = c.ws32.data() + 9, *const *phib = c.ws32.data() + 9 + SAP_MS;
   const float mug = (float)d.gen_mu;
   if (d.use_start) {
     // the caller's start fields (e.g. the reference's ranlxs fields)
@@ -1306,10 +1309,13 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
   if (ifail[0] == 0) {
     int n;
     for (n = 0; n < 3; n++) {
-      for (int l = 0; l < d.Ns; l++) {
-        la_copy(c, 32, d.modes[l], 32, ws0, PAR_ALL, st);
-        la_zero(c, 32, d.modes[l], PAR_ALL, st);
-        sap_cycles(c, mug, 1, d.gen_nmr, n + 1, d.modes[l], ws0, phib, st);
+      for (int l0 = 0; l0 < d.Ns; l0 += SAP_MS) {
+        const int m = std::min(SAP_MS, d.Ns - l0);
+        for (int i = 0; i < m; i++) {
+          la_copy(c, 32, d.modes[l0 + i], 32, rs[i], PAR_ALL, st);
+          la_zero(c, 32, d.modes[l0 + i], PAR_ALL, st);
+        }
+        if (sap_cycles_multi(c, m, mug, 1, d.gen_nmr, n + 1, d.modes.data() + l0, rs, phib, st)) return -1;
       }
     }
     dfl_mark(c, 0);
@@ -1344,9 +1350,9 @@ int dfl_modes_dev(Ctx &c, uint64_t seed, int *ifail, int *status) {
         dfl_mark(c, 3);
         dirac_multi32(c, na, mug, w1, w0, md, st);          // w0 = mode - D w1
         dfl_mark(c, 5);
+        for (int i = 0; i < na; i++) la_zero(c, 32, d.modes[l0 + i], PAR_ALL, st);
+        if (sap_cycles_multi(c, na, mug, 1, d.gen_nmr, d.gen_ncy, d.modes.data() + l0, w0, phib, st)) return -1;
         for (int i = 0; i < na; i++) {
-          la_zero(c, 32, d.modes[l0 + i], PAR_ALL, st);
-          sap_cycles(c, mug, 1, d.gen_nmr, d.gen_ncy, d.modes[l0 + i], w0[i], phib, st);
           la_axpy(c, 32, d.modes[l0 + i], 1.0, 0.0, w1[i], PAR_ALL, st);
           status[0] += ls[i];
         }

@@ -433,6 +433,9 @@ void *sap_input_field(Ctx &c);
 // psi = ncy cycles on rho = rh, then rho = rh - rho (the sap_gcr preconditioner)
 int sap_mop(Ctx &c, float mu, int isolv, int nmr, int ncy, const void *rh, void *psi, void *rho, void *phi_blk,
             cudaStream_t st, const void *base = nullptr, const void *add = nullptr);
+// ncy SAP cycles for n systems of one twisted mass on their own fields
+int sap_cycles_multi(Ctx &c, int n, float mu, int isolv, int nmr, int ncy, void *const *psi, void *const *rho,
+                     void *const *phi_blk, cudaStream_t st);
 // the input field of system r (< n <= SAP_MS) of an sap_mop_multi call on
 // n systems (null when CUDA graphs are off, with domain decomposition, or
 // when the fields do not fit)

@@ -29,22 +29,21 @@
 
 namespace qcd {
 
-// nsys systems (SAP_MS at most) per launch: their fields psi, rho, phi lie
-// fstride float4 apart, the CTAs of one block are adjacent (CTA x: block
-// x / nsys, system x % nsys), so the block's links and SW matrices are read
-// by all systems while they are in L2.
+// nsys systems (SAP_MS at most) per launch, with their own fields psi,
+// rho, phi and twisted masses; the CTAs of one block are adjacent (CTA x:
+// block x / nsys, system x % nsys), so the block's links and SW matrices
+// are read by all systems while they are in L2.
 struct SapArgs {
   Geom g;
   int colour;
   float mu;             // system 0
   int nmr;
   int eoflg;
-  float4 *psi, *rho, *phi;   // system 0
+  float4 *psi[SAP_MS], *rho[SAP_MS], *phi[SAP_MS];
   const void *u;        // links as the block solver's policy reads them
   const void *ub;       // links for the block-boundary hops (as u, but 18-real FP32 in the FP32 mode)
   const void *sw, *swinv;
   int nsys;
-  size_t fstride;
   float mus[SAP_MS];
 };
 
@@ -54,15 +53,21 @@ struct SapSys {
   float mu;
 };
 __device__ __forceinline__ SapSys sap_sys(const SapArgs &a, int r) {
-  const size_t o = (size_t)r * a.fstride;
+  // selected without indexing the parameter arrays by a variable (which
+  // would copy them to local memory)
   SapSys y;
-  y.psi = a.psi + o;
-  y.rho = a.rho + o;
-  y.phi = a.phi + o;
+  y.psi = a.psi[0];
+  y.rho = a.rho[0];
+  y.phi = a.phi[0];
   y.mu = a.mus[0];
 #pragma unroll
   for (int q = 1; q < SAP_MS; q++)
-    if (r == q) y.mu = a.mus[q];
+    if (r == q) {
+      y.psi = a.psi[q];
+      y.rho = a.rho[q];
+      y.phi = a.phi[q];
+      y.mu = a.mus[q];
+    }
   return y;
 }
 
@@ -607,7 +612,7 @@ __global__ void k_sap_dd_pack(SapArgs a, DDGeom dg, void *dn, void *up) {
   const int side = i >= F, f = i - side * F;
   int chunk, s, n[4], y[4];
   face_site(g, side, f, chunk, s, n, y);
-  const spinor<float> v = Store<float>::load_spinor(a.phi, chunk, s, g.vbh);
+  const spinor<float> v = Store<float>::load_spinor(a.phi[0], chunk, s, g.vbh);
   vec3<float> h0, h1;
   if (side == 0) {
     dd_proj_fwd<float>(v, h0, h1);
@@ -795,11 +800,10 @@ static SapArgs sap_args(Ctx &c, float mu, int nmr, int mode, void *psi, void *rh
   a.mu = mu;
   a.nmr = nmr;
   a.eoflg = c.eoflg;
-  a.psi = (float4 *)psi;
-  a.rho = (float4 *)rho;
-  a.phi = (float4 *)phi;
+  a.psi[0] = (float4 *)psi;
+  a.rho[0] = (float4 *)rho;
+  a.phi[0] = (float4 *)phi;
   a.nsys = 1;
-  a.fstride = 0;
   a.mus[0] = mu;
   a.u = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
   a.ub = half ? (const void *)c.u16 : (mode == 2 ? (const void *)c.u12 : (const void *)c.u32);
@@ -962,6 +966,33 @@ int sap_cycles(Ctx &c, float mu, int isolv, int nmr, int ncy, void *psi, void *r
   return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
 }
 
+// ncy cycles for n systems with the same twisted mass on their own fields
+// (psi[r], rho[r] in and out, phi_blk[r] scratch), up to SAP_MS systems per
+// launch; with domain decomposition one system after the other
+int sap_cycles_multi(Ctx &c, int n, float mu, int isolv, int nmr, int ncy, void *const *psi, void *const *rho,
+                     void *const *phi_blk, cudaStream_t st) {
+  if (dd_on(c)) {
+    for (int r = 0; r < n; r++)
+      if (sap_cycles(c, mu, isolv, nmr, ncy, psi[r], rho[r], phi_blk[r], st)) return -1;
+    return 0;
+  }
+  const int mode = sap_ready(c, isolv, st);
+  if (mode < 0) return -1;
+  for (int r0 = 0; r0 < n; r0 += SAP_MS) {
+    const int m = n - r0 < SAP_MS ? n - r0 : SAP_MS;
+    SapArgs a = sap_args(c, mu, nmr, mode, psi[r0], rho[r0], phi_blk[r0]);
+    a.nsys = m;
+    for (int r = 0; r < m; r++) {
+      a.psi[r] = (float4 *)psi[r0 + r];
+      a.rho[r] = (float4 *)rho[r0 + r];
+      a.phi[r] = (float4 *)phi_blk[r0 + r];
+      a.mus[r] = mu;
+    }
+    for (int k = 0; k < ncy; k++) sap_cycle_launch(c, a, isolv, mode, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("sap: launch failed");
+}
+
 // The preconditioner of sap_gcr (sap_gcr.c:126-134): psi = ncy SAP cycles
 // from psi = 0 on rho = rh, then rho = rh - rho (= D psi); with base given,
 // rho = base - (final residual), and psi += add (the deflated
@@ -1080,8 +1111,12 @@ int sap_mop_multi(Ctx &c, int ns, const float *mu, int isolv, int nmr, int ncy, 
     key.ncy = ncy;
     key.a = sap_args(c, mu[r0], nmr, mode, c.sap_mfld[0], c.sap_mfld[1], c.sap_mfld[2]);
     key.a.nsys = m;
-    key.a.fstride = n;
-    for (int r = 0; r < m; r++) key.a.mus[r] = mu[r0 + r];
+    for (int r = 0; r < m; r++) {
+      key.a.psi[r] = (float4 *)c.sap_mfld[0] + (size_t)r * n;
+      key.a.rho[r] = (float4 *)c.sap_mfld[1] + (size_t)r * n;
+      key.a.phi[r] = (float4 *)c.sap_mfld[2] + (size_t)r * n;
+      key.a.mus[r] = mu[r0 + r];
+    }
     for (int r = 0; r < m; r++) {
       void *in = (char *)c.sap_mfld[1] + (size_t)r * fb;
       const void *b = base && base[r0 + r] ? base[r0 + r] : rh[r0 + r];
