@@ -275,21 +275,34 @@ int ltl_gcr_b(Ctx &c, double mu, int nr, const double2 *const *eta, double2 *con
     for (int k = 0; k < nkv && !act.empty() && it < d.nmx; k++) {
       const int na = (int)act.size();
       set_act(act);
-      k_bcopy<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, JR, JP + k, n, 0);
-      {
-        const std::vector<double2 *> Pk = pick(vecs(JP + k), act), Qk = pick(vecs(JQ + k), act), Ya = pick(Y, act);
-        dfl_Awhat_b(c, na, (const double2 *const *)Pk.data(), Qk.data(), Ya.data(), st);
-      }
-      if (k > 0)
-        for (int pass = 0; pass < 2; pass++) {
-          mdot(na, JQ, k, JQ + k, 0);
-          k_bgs_sub<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, k, B.dots, JQ, JP, n);
+      // the iteration's launches as one CUDA graph per shape (the active
+      // systems, k, the little operator in use); the active list itself
+      // is copied to the device before the replay
+      std::vector<uint64_t> key = {0x17a9ull, (uint64_t)na, (uint64_t)k, (uint64_t)(uintptr_t)B.base, nv,
+                                   (uint64_t)nvec, (uint64_t)(uintptr_t)d.Mhop, (uint64_t)(uintptr_t)d.Mhop32,
+                                   (uint64_t)(uintptr_t)B.act, (uint64_t)(uintptr_t)B.dots,
+                                   (uint64_t)(uintptr_t)B.part, (uint64_t)(uintptr_t)d.nbr, (uint64_t)d.Ns};
+      for (int r : act) key.push_back((uint64_t)r);
+      const int rc = graph_run(c, key.data(), key.size() * sizeof(uint64_t), st, [&]() {
+        k_bcopy<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, JR, JP + k, n, 0);
+        {
+          const std::vector<double2 *> Pk = pick(vecs(JP + k), act), Qk = pick(vecs(JQ + k), act),
+                                       Ya = pick(Y, act);
+          dfl_Awhat_b(c, na, (const double2 *const *)Pk.data(), Qk.data(), Ya.data(), st);
         }
-      mdot(na, JQ + k, 1, JQ + k, 32);
-      k_bnorm<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, B.dots, 32, JQ + k, JP + k, n);
-      mdot(na, JQ + k, 1, JR, 33);
-      k_bxr<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, B.dots, 33, JX, JR, JP + k, JQ + k, n);
-      mdot(na, JR, 1, JR, 34);
+        if (k > 0)
+          for (int pass = 0; pass < 2; pass++) {
+            mdot(na, JQ, k, JQ + k, 0);
+            k_bgs_sub<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, k, B.dots, JQ, JP, n);
+          }
+        mdot(na, JQ + k, 1, JQ + k, 32);
+        k_bnorm<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, B.dots, 32, JQ + k, JP + k, n);
+        mdot(na, JQ + k, 1, JR, 33);
+        k_bxr<<<dim3(gv, na), 256, 0, st>>>(B.base, nvec, nv, B.act, B.dots, 33, JX, JR, JP + k, JQ + k, n);
+        mdot(na, JR, 1, JR, 34);
+        return cudaGetLastError() == cudaSuccess ? 0 : fail("ltl_gcr: launch failed");
+      });
+      if (rc) return -1;
       read_dots();
       it++;
       std::vector<int> keep;
