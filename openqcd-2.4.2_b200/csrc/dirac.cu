@@ -297,6 +297,52 @@ __device__ __forceinline__ spinor<double> apply_sw_smem(const double2 *sm, int t
   return out;
 }
 
+// h += sg (A + i mu g5) in for one Weyl half (half = 0, 1) of the input,
+// with the Pauli entries read from shared memory one at a time and the
+// product folded into the hop sum as it is formed, so that neither the
+// whole input nor the whole product is live beside h.  The products and
+// their order are those of mul_pauli.  With sg = -2 and the sum scaled by
+// -1/2 afterwards (or +2 and +1/2) this equals forming (A + i mu g5) in and
+// -1/2 h apart and adding (subtracting) them, rounding included: the
+// scalings by 2 and 1/2 are exact.
+__device__ __forceinline__ void sw_fold_half(const double2 *sm, int t, double mu, int half, const cpx<double> (&w)[6],
+                                             double sg, spinor<double> &h) {
+  const double m = half == 0 ? mu : -mu;
+  cpx<double> r[6];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const double2 d = sm[(18 * half + i) * DWT_TS + t];
+    r[2 * i] = mk<double>(d.x * w[2 * i].re - m * w[2 * i].im, d.x * w[2 * i].im + m * w[2 * i].re);
+    r[2 * i + 1] = mk<double>(d.y * w[2 * i + 1].re - m * w[2 * i + 1].im, d.y * w[2 * i + 1].im + m * w[2 * i + 1].re);
+  }
+  int e = 0;
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = i + 1; j < 6; j++) {
+      const double2 a = sm[(18 * half + 3 + e) * DWT_TS + t];
+      e++;
+      r[i].re += a.x * w[j].re - a.y * w[j].im;
+      r[i].im += a.x * w[j].im + a.y * w[j].re;
+      r[j].re += a.x * w[i].re + a.y * w[i].im;
+      r[j].im += a.x * w[i].im - a.y * w[i].re;
+    }
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    cpx<double> &hh = h.c[2 * half + i / 3].c[i % 3];
+    hh.re += sg * r[i].re;
+    hh.im += sg * r[i].im;
+  }
+}
+
+__device__ __forceinline__ void load_weyl(const double2 *p, size_t vbh, int half, cpx<double> (&w)[6]) {
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const double2 v = __ldg(p + (size_t)(6 * half + i) * vbh);
+    w[i] = mk<double>(v.x, v.y);
+  }
+}
+
 // Tile t of a launch: its chunk (parity p, block blk) and first site.
 __device__ __forceinline__ void staged_tile(const Geom &g, int PAR_, int t, int tpc, const int *sched, int &p,
                                            int &blk, int &si0) {
@@ -427,22 +473,36 @@ __device__ __forceinline__ void staged_body(const Geom &g, const DDGeom &dg, con
           hop_bwd<double>(mu, ub, sm, h);
         }
       }
-      sscale<double>(h, -0.5);
       const double mux = p == 0 ? mu_e : mu_o;
-      if (OPS & OP_INV) {
-        ok &= mbar_wait_st(&bar[0], phase, err);
-        h = apply_sw_smem(sw_s, tid, 0.0, h);
-      }
       spinor<double> acc;
-      if (OPS & OP_SW) {
-        const spinor<double> in = Store<double>::load_spinor(s, chunk, si, g.vbh);
+      if constexpr ((OPS & OP_SW) && !(OPS & OP_INV) && (OPS & (OP_HOP | OP_HOPSUB))) {
+        // SW term folded into the hop sum, half by half
+        const double2 *ip = s + (size_t)chunk * 12 * g.vbh + si;
+        const double sg = (OPS & OP_HOP) ? -2.0 : 2.0;
+        cpx<double> w[6];
+        load_weyl(ip, g.vbh, 0, w);
         ok &= mbar_wait_st(&bar[0], phase, err);
-        acc = apply_sw_smem(sw_s, tid, mux, in);
+        sw_fold_half(sw_s, tid, mux, 0, w, sg, h);
+        load_weyl(ip, g.vbh, 1, w);
+        sw_fold_half(sw_s, tid, mux, 1, w, sg, h);
+        sscale<double>(h, (OPS & OP_HOP) ? -0.5 : 0.5);
+        acc = h;
       } else {
-        szero(acc);
+        sscale<double>(h, -0.5);
+        if (OPS & OP_INV) {
+          ok &= mbar_wait_st(&bar[0], phase, err);
+          h = apply_sw_smem(sw_s, tid, 0.0, h);
+        }
+        if (OPS & OP_SW) {
+          const spinor<double> in = Store<double>::load_spinor(s, chunk, si, g.vbh);
+          ok &= mbar_wait_st(&bar[0], phase, err);
+          acc = apply_sw_smem(sw_s, tid, mux, in);
+        } else {
+          szero(acc);
+        }
+        if (OPS & OP_HOP) sadd(acc, h);
+        else if (OPS & OP_HOPSUB) ssub(acc, h);
       }
-      if (OPS & OP_HOP) sadd(acc, h);
-      else if (OPS & OP_HOPSUB) ssub(acc, h);
       // a site whose SW matrices did not arrive keeps its old output (the
       // error flag tells the host the result is invalid)
       if (ok) store_spinor_cs(r, chunk, si, g.vbh, acc);
