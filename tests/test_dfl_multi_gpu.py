@@ -108,3 +108,43 @@ def test_awhat_multi(st, nr):
         print("Ns %d nr %d vector %d: relative error %.2e" % (st.Ns, nr, r, err))
         assert err <= (1e-6 if r < 4 else 1e-12), (r, err)
 
+
+
+@pytest.fixture(scope="module")
+def st6():
+    """6^4 blocks on 12^4, Ns = 28: 648 sites per block parity (81 groups of 8
+    sites over the warps of the tensor-core kernels, 486 prolongation tiles)"""
+    L6, BS6, Ns = (12, 12, 12, 12), (6, 6, 6, 6), 28
+    s = Setup(L6, BS6, eps=0.4, csw=1.5, m0=M0, portable=True, private=True)
+    s.ref.set_sap_parms(BS6, 1, 4, 5)
+    s.nv = s.ref.dfl_init(BS6, Ns, nkv=16, nmx=256, res=1e-2, nmx_gcr=24, res_gcr=1e-2, kappa=KAPPA, mu=0.0,
+                          ninv=5, nmr=4, ncy=4)
+    rng = np.random.default_rng(606)
+    s.ref.dfl_subspace([rng.standard_normal(s.vol * 24).astype(np.float32) for _ in range(Ns)])
+    qb.set_sap_parms(BS6, 1, 4, 5)
+    assert qb.set_dfl_parms(BS6, Ns) == s.nv
+    for l in range(Ns):
+        qb.dfl_set_basis(l, s.ref.dfl_get_basis(l))
+    s.Ns = Ns
+    return s
+
+
+@pytest.mark.parametrize("tile,tc", [(4, True), (4, False)])
+def test_multi_6x6x6x6_blocks(st6, tile, tc):
+    qb.set_rhs_tiles(tile, tile, tc, tc)
+    rng = np.random.default_rng(61 + tile + tc)
+    fields = [rng.standard_normal(st6.vol * 24).astype(np.float32) for _ in range(4)]
+    vds = qb.dfl_s2vd_multi(fields, st6.nv)
+    for f, vd in zip(fields, vds):
+        ref = st6.ref.dfl_s2vd(f)
+        assert np.abs(vd - ref).max() <= 2e-6 * np.abs(ref).max()
+    vin = [rng.standard_normal(2 * st6.nv) for _ in range(4)]
+    fs = qb.dfl_vd2s_multi(vin, st6.vol)
+    for vd, f in zip(vin, fs):
+        ref = st6.ref.dfl_vd2s(vd)
+        assert np.abs(f - ref).max() <= 2e-6 * np.abs(ref).max()
+    qb.little(1, 0.01, vin[0])
+    ws = qb.Awhat_multi(vin)
+    for v, w in zip(vin, ws):
+        ref, f = st6.ref.little(1, 0.01, v)
+        assert f == 0 and rel_norm_err(w, ref) <= 1e-6
