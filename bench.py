@@ -414,6 +414,8 @@ def main():
     ap.add_argument("--profile-solver", action="store_true",
                     help="run only the 48^3x96 solver comparison, with profiler collection around the chosen solve")
     ap.add_argument("--solver-lattice", default=None, help="L0,L1,L2,L3 for --profile-solver (smaller cases)")
+    ap.add_argument("--sustained", type=int, default=0,
+                    help="run only Dw_dble n times back to back, its time per launch binned by the sampled SM clock")
     ap.add_argument("--scan-block-orders", action="store_true",
                     help="run only Dw_dble under each block traversal order (timings; the first 10 launches "
                          "are the ones an ncu traffic capture takes)")
@@ -426,6 +428,11 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference(args, d)
+        if args.sustained:
+            import openqcd_b200 as qb
+            qb.set_device(d.local)
+            print(json.dumps(sustained_dw(qb, args.sustained)))
+            return 0
         if args.scan_block_orders:
             import openqcd_b200 as qb
             qb.set_device(d.local)
@@ -526,6 +533,76 @@ def solver_c3(qb, profile=False, lattice=None):
         fld.free()
     psi.free()
     qb.release_workspace()
+    return out
+
+
+def sustained_dw(qb, n, chunk=20):
+    """Dw_dble on the bench's 32^3x64 field, n launches back to back in
+    chunks of `chunk` (CUDA events per chunk, wall-clock stamps around it),
+    with nvidia-smi sampling the SM clock and power every 20 ms: each
+    chunk's time per launch paired with the median clock sampled during it,
+    then binned by clock (100 MHz bins).  For the record of how the kernel
+    behaves once the power cap pulls the clock down; the bench's own timed
+    region is the short burst of --steps launches."""
+    import datetime
+    L = LATTICE
+    qb.geometry(L, BS, qb.even_first_ipt(L))
+    qb.set_parms(CSW, M0, 0)
+    qb.random_ud(EPS, FIELD_SEED)
+    qb.sw_term()
+    s = qb.DevField(64).random(1.0, SOURCE_SEED)
+    r = qb.DevField(64)
+    vol = qb.lib().b200_volume()
+    qb.time_dirac(64, "Dw", MU, s, r, 5)
+    f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    p = subprocess.Popen(["nvidia-smi", "-i", "0", "--query-gpu=timestamp,clocks.sm,power.draw,"
+                          "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "20"],
+                         stdout=f, stderr=subprocess.DEVNULL)
+    time.sleep(1.0)
+    chunks = []
+    for _ in range(max(1, n // chunk)):
+        t0 = time.time()
+        ms = qb.time_dirac(64, "Dw", MU, s, r, chunk) / chunk
+        chunks.append((t0, time.time(), ms))
+    time.sleep(0.2)
+    p.terminate()
+    p.wait(timeout=5)
+    f.flush()
+    samples = []
+    for line in open(f.name):
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) != 4:
+            continue
+        try:
+            ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            samples.append((ts, float(parts[1]), float(parts[2]), parts[3].lower().startswith("active")))
+        except ValueError:
+            continue
+    os.unlink(f.name)
+    peak = peaks()[0]
+    rows = []
+    for t0, t1, ms in chunks:
+        inside = [x for x in samples if t0 <= x[0] <= t1]
+        if not inside:   # a chunk shorter than the sampling interval: the nearest sample
+            inside = [min(samples, key=lambda x: abs(x[0] - 0.5 * (t0 + t1)))] if samples else []
+        if inside:
+            rows.append((statistics.median(x[1] for x in inside), ms, max(x[2] for x in inside),
+                         any(x[3] for x in inside)))
+    bins = {}
+    for mhz, ms, w, cap in rows:
+        b = int(mhz // 100) * 100
+        bins.setdefault(b, []).append((ms, w, cap))
+    out = {"lattice": list(L), "launches": len(chunks) * chunk, "chunk": chunk,
+           "ms_first_chunk": chunks[0][2], "ms_last_chunk": chunks[-1][2],
+           "ms_mean": statistics.mean(c[2] for c in chunks), "bins": []}
+    for b in sorted(bins):
+        v = bins[b]
+        msm = statistics.mean(x[0] for x in v)
+        out["bins"].append({"sm_mhz": [b, b + 100], "chunks": len(v), "ms_per_launch": msm,
+                            "frac_of_measured": BYTES_PER_SITE[64] * vol / (msm / 1e3) / 1e9 / peak,
+                            "max_power_w": max(x[1] for x in v), "sw_power_cap": any(x[2] for x in v)})
+    s.free()
+    r.free()
     return out
 
 
