@@ -253,8 +253,8 @@ __global__ void __launch_bounds__(BSPLIT_T) k_dfl_stream(Geom g, const int *__re
 // ------------------------------------- tensor-core restriction / prolongation
 // Four fields at a time as real matrix products on the tensor cores
 // (mma.sync m16n8k8, TF32 head/tail operands; mma.cuh).  Each lane copies
-// the operand values it will use (the fields, the basis and, for the
-// prolongation, nothing else) from global memory into its own slots of a
+// the operand values it will use (the basis, and for the restriction the
+// fields) from global memory into its own slots of a
 // per-warp shared-memory ring with cp.async, RD - 1 stages ahead of the
 // arithmetic: no registers are tied up by loads in flight and no barrier is
 // needed, since every lane reads only what it copied itself.
