@@ -122,6 +122,10 @@ static int dfl_alloc(Ctx &c) {
   }
   cudaFree(d.Mhop32);
   if (cudaMalloc(&d.Mhop32, 4 * m) != cudaSuccess) return fail("out of device memory (little operator)");
+  // the further masses' arrays have the old sizes
+  for (auto &x : d.xsets)
+    for (void *p : x) cudaFree(p);
+  d.xsets.clear();
   d.aw_valid = d.awhat_valid = false;
   d.have_basis = false;
   d.ready = true;
@@ -815,6 +819,8 @@ void dfl_release(Ctx &c) {
   for (void *p : d.basis) cudaFree(p);
   for (void *p : d.modes) cudaFree(p);
   for (void *p : d.start) cudaFree(p);
+  for (auto &x : d.xsets)
+    for (void *p : x) cudaFree(p);
   for (double2 *p : d.lv) cudaFree(p);
   for (double2 *p : d.lvd) cudaFree(p);
   void *bufs[] = {d.vd2lex, d.nbr, d.faces, d.nfc, d.d_basis, d.Ablk, d.Ainv, d.Ahop, d.Mhop, d.Mhop32,
@@ -912,15 +918,17 @@ int dfl_subspace_dev(Ctx &c, const std::vector<void *> &modes, cudaStream_t st, 
 }
 
 // Little operator for twisted mass mu (set_Aw); returns 0
-int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st) {
+// diag_only: the diagonal blocks alone (the twisted mass enters only
+// there; the hop matrices d.Ahop are those of any mass)
+int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st, bool diag_only) {
   DflState &d = c.dfl;
   if (!d.have_basis) return fail("set_Aw: the deflation subspace is not set");
-  if (d.aw_valid && d.aw_mu == mu && d.aw_eo == c.eoflg) return 0;
+  if (!diag_only && d.aw_valid && d.aw_mu == mu && d.aw_eo == c.eoflg) return 0;
   const double muo = c.eoflg ? 0.0 : mu;
   constexpr int TS = 8, LD = TS * 12 + 1;
   const int NT = d.Ns / 2, ntile = NT * NT;
   const size_t shm = (size_t)NT * LD * (2 * sizeof(double2) + sizeof(float4));
-  const dim3 grid(d.nb, 9);
+  const dim3 grid(d.nb, diag_only ? 1 : 9);
   const float4 *const *bas = (const float4 *const *)d.d_basis;
   if (ntile <= 256) {
     cudaFuncSetAttribute(k_aw_tiles<TS, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -941,10 +949,10 @@ int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st) {
 
 // Even-odd preconditioned little operator (set_Awhat): inverses of the
 // diagonal blocks and H = Ablk^-1 Ahop.  Returns 1 if an inversion was unsafe.
-int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st) {
+int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st, bool diag_only) {
   DflState &d = c.dfl;
-  if (dfl_set_Aw(c, mu, st)) return -1;
-  if (d.awhat_valid) return d.awhat_fail;
+  if (dfl_set_Aw(c, mu, st, diag_only)) return -1;
+  if (d.awhat_valid && !diag_only) return d.awhat_fail;
   int *dfail = nullptr;
   cudaMallocAsync(&dfail, sizeof(int), st);
   cudaMemsetAsync(dfail, 0, sizeof(int), st);

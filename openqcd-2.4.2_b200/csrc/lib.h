@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <functional>
 #include <string>
+#include <array>
 #include <vector>
 #include "qcd.cuh"
 
@@ -62,6 +63,10 @@ struct DflState {
   void **d_basis = nullptr;
   double2 *Ablk = nullptr, *Ainv = nullptr, *Ahop = nullptr, *Mhop = nullptr;
   float2 *Mhop32 = nullptr;     // FP32 copy of Mhop (the batched little hops on the tensor cores)
+  // Ablk, Ainv, Mhop, Mhop32 of the further masses of a batched solve
+  // (kept between calls, so that their addresses, part of the keys of the
+  // captured little-solver iterations, repeat)
+  std::vector<std::array<void *, 4>> xsets;
   bool aw_valid = false, awhat_valid = false;
   int awhat_fail = 0, aw_eo = 0;
   double aw_mu = 0.0;
@@ -407,8 +412,10 @@ void dfl_Aweeinv(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
 void dfl_Awooinv(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
 void dfl_Awoe(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
 void dfl_Aweo(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
-int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st);
-int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st);
+// diag_only: recompute the diagonal blocks only (keeping d.Ahop, which
+// does not depend on the twisted mass)
+int dfl_set_Aw(Ctx &c, double mu, cudaStream_t st, bool diag_only = false);
+int dfl_set_Awhat(Ctx &c, double mu, cudaStream_t st, bool diag_only = false);
 void dfl_Aw(Ctx &c, const double2 *v, double2 *w, cudaStream_t st);
 void dfl_Awhat(Ctx &c, const double2 *v, double2 *w, double2 *t, cudaStream_t st);
 double dfl_ltl_gcr(Ctx &c, double mu, const double2 *eta, double2 *psi, int *ifail, int *status, cudaStream_t st);

@@ -634,6 +634,10 @@ struct LittleSets {
   std::vector<std::array<void *, 5>> set;
   std::vector<double> mu;
   std::vector<int> fail;
+  // The first mass in the library's own arrays (recomputed only if they
+  // hold another mass); every further mass gets its own diagonal blocks,
+  // inverses and preconditioned hops, and shares the hop matrices Ahop,
+  // which do not depend on the mass.
   int build(Ctx &cc, const std::vector<double> &umu, cudaStream_t st) {
     c = &cc;
     DflState &d = cc.dfl;
@@ -644,16 +648,28 @@ struct LittleSets {
     set.assign(umu.size(), {nullptr, nullptr, nullptr, nullptr, nullptr});
     fail.assign(umu.size(), 0);
     for (size_t j = 0; j < umu.size(); j++) {
+      if (j > 0 && d.xsets.size() < j) {
+        std::array<void *, 4> x = {nullptr, nullptr, nullptr, nullptr};
+        const int ks[4] = {0, 1, 3, 4};
+        for (int q = 0; q < 4; q++)
+          if (cudaMalloc(&x[q], sz[ks[q]]) != cudaSuccess) {
+            for (void *p : x) cudaFree(p);
+            return qcd::fail("gcr_batch: out of device memory (little operators)");
+          }
+        d.xsets.push_back(x);
+      }
       for (int k = 0; k < 5; k++) {
-        if (j == 0) set[j][k] = own[k];
-        else if (cudaMalloc(&set[j][k], sz[k]) != cudaSuccess) return qcd::fail("gcr_batch: out of device memory (little operators)");
+        if (j == 0 || k == 2) set[j][k] = own[k];
+        else set[j][k] = d.xsets[j - 1][k < 2 ? k : k - 1];
       }
       point(j);
-      if (umu.size() > 1) d.aw_valid = d.awhat_valid = false;
-      const int f = dfl_set_Awhat(cc, umu[j], st);
+      // set 0: the operator of umu[0] if the arrays do not hold it yet
+      // (with the hop matrices); sets j > 0: their diagonal part
+      const int f = j == 0 ? dfl_set_Awhat(cc, umu[0], st) : dfl_set_Awhat(cc, umu[j], st, true);
       if (f < 0) return -1;
       fail[j] = f;
     }
+    if (umu.size() > 1) point(0);
     return 0;
   }
   void point(size_t j) {
@@ -675,11 +691,13 @@ struct LittleSets {
     if (!c || set.size() <= 1) return;
     DflState &d = c->dfl;
     cudaStreamSynchronize(c->stream);
-    for (size_t j = 1; j < set.size(); j++)
-      for (int k = 0; k < 5; k++) cudaFree(set[j][k]);
     d.Ablk = (double2 *)own[0]; d.Ainv = (double2 *)own[1]; d.Ahop = (double2 *)own[2];
     d.Mhop = (double2 *)own[3]; d.Mhop32 = (float2 *)own[4];
-    d.aw_valid = d.awhat_valid = false;   // set 0's arrays hold the first mass; recompute on demand
+    // the own arrays hold the operator of the first mass
+    d.aw_valid = d.awhat_valid = true;
+    d.aw_mu = mu[0];
+    d.aw_eo = c->eoflg;
+    d.awhat_fail = fail[0];
     d.awhat_ver++;
   }
 };
