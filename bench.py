@@ -915,10 +915,18 @@ def run_b200(args, d):
     b32 = 672 if qb.links12_active() else BYTES_PER_SITE[32]
     extra["dw_f32"] = {"ms": ms32, "GBs": b32 * vol / (ms32 / 1e3) / 1e9, "bytes_per_site": b32,
                        "frac_of_peak": b32 * vol / (ms32 / 1e3) / 1e9 / peak}
-    for op, bps in (("Dwhat", 1344), ):
+    # Dwhat_dble: 1344 algorithmic bytes per site (s_e in and r_e out, links
+    # and both parities' SW matrices once); its two launches (odd sites:
+    # A_oo^-1 D_oe s_e into a scratch field, even sites: the SW term minus
+    # D_eo of the scratch) read every link twice, s_e twice and move the
+    # scratch field out and in: 2208 bytes per site at the least
+    for op, bps, moved in (("Dwhat", 1344, 2208), ):
         qb.time_dirac(64, op, MU, s, r, 3)
         m = qb.time_dirac(64, op, MU, s, r, args.steps) / args.steps
-        extra["dwhat_f64"] = {"ms": m, "GBs": bps * vol / (m / 1e3) / 1e9}
+        extra["dwhat_f64"] = {"ms": m, "GBs": bps * vol / (m / 1e3) / 1e9, "bytes_per_site": bps,
+                              "frac_of_peak": bps * vol / (m / 1e3) / 1e9 / peak,
+                              "two_launch_bytes_per_site": moved,
+                              "two_launch_frac_of_peak": moved * vol / (m / 1e3) / 1e9 / peak}
     s32.free(); r32.free()
 
     e2e = None

@@ -299,15 +299,22 @@ int b200_tune_block_order(float *ms);
  * counterpart). */
 int b200_set_cuda_graphs(int on);
 /* on != 0 (default): Dw_dble and Dw on page-locked host arrays run as a
- * pipeline over x0-slabs (copy in, operator, copy out of different slabs
- * overlap) when every slab of whole block rows is a contiguous range of
- * each parity half of the caller's storage order, as openQCD's ipt[] makes
- * slabs of L0_TRD planes; otherwise, or with 0, the fields are copied
- * whole.  Returns the previous setting.  b200_pipeline_slabs: the number of
- * slabs of the current geometry (0: no pipeline).  No reference
- * counterpart. */
+ * pipeline (copy in, operator, copy out of different parts of the lattice
+ * overlap) when the lattice has at least three block rows along x0 and can
+ * be cut into at least three x0-slabs ("pieces", as thin as possible, at
+ * least 65536 sites or a sixteenth of the lattice) that are contiguous
+ * ranges of each parity half of the caller's storage order: planes for a
+ * lexicographic order with x0 slowest, multiples of L0_TRD planes for
+ * openQCD's ipt[].  The pieces are copied in and converted one by one; the operator
+ * runs on a block row once the pieces holding it and its two neighbouring
+ * planes are in; a piece is copied out once its rows are done.  Otherwise,
+ * or with 0, the fields are copied whole.  Returns the previous setting.
+ * b200_pipeline_slabs: the number of block rows of the pipeline,
+ * b200_pipeline_pieces: the number of pieces (0: no pipeline).  No
+ * reference counterpart. */
 int b200_set_pipeline(int on);
 int b200_pipeline_slabs(void);
+int b200_pipeline_pieces(void);
 int b200_graphs_cached(void);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32, 16, or 12 for the 12-real links): index,

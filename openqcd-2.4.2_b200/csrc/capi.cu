@@ -3,11 +3,13 @@
 #include "lib.h"
 #include <cuda_profiler_api.h>
 #include "../../include/openqcd_b200.h"
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 
 namespace qcd {
 
@@ -69,46 +71,75 @@ static bool pinned_host(const void *p) {
   return a.type == cudaMemoryTypeHost;
 }
 
-// Dw on page-locked host arrays, pipelined over the x0-slabs of the slab
-// plan: the input slabs are copied and converted on one stream in the order
-// R-1, 0, 1, ..., R-2; as soon as a slab's neighbours are in, its Dw runs
-// on the library stream and its result is converted and copied back on a
-// third stream, so host-to-device and device-to-host transfers overlap.
+// Dw on page-locked host arrays, pipelined: the input pieces are copied
+// back to back on one stream in the order np-1, 0, 1, ..., np-2 and each is
+// converted to the device layout on a second; the operator runs on a block
+// row (a slab) on the library stream as soon as the pieces holding its
+// planes and the two neighbouring planes are in; its result is converted
+// back there, and every piece whose rows are all done is copied out on a
+// third stream (adjacent ranges in one copy), so that the two transfer
+// directions overlap.  The output
+// of a piece is written only after its own input was copied, so s and r may
+// be the same array.
 template <typename R>
 static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr, char *st_in, char *st_out) {
   const int prec = sizeof(R) == 8 ? 64 : 32;
   const size_t site = 24 * sizeof(R);
-  const int nsl = (int)c.slab.size();
+  const int np = (int)c.piece.size(), nr = (int)c.slab.size(), L0 = c.g.L[0];
   if ((!c.st_in && cudaStreamCreateWithFlags(&c.st_in, cudaStreamNonBlocking) != cudaSuccess) ||
       (!c.st_out && cudaStreamCreateWithFlags(&c.st_out, cudaStreamNonBlocking) != cudaSuccess) ||
       (!c.st_cv && cudaStreamCreateWithFlags(&c.st_cv, cudaStreamNonBlocking) != cudaSuccess))
     return fail("no CUDA stream for the pipelined transfers");
-  while ((int)c.slab_ev.size() < 3 * nsl + 1) {
+  while ((int)c.slab_ev.size() < 2 * np + nr + 1) {
     cudaEvent_t e;
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return fail("no CUDA event");
     c.slab_ev.push_back(e);
   }
-  cudaEvent_t *ev_in = c.slab_ev.data(), *ev_out = ev_in + nsl, *ev_cp = ev_in + 2 * nsl, ev0 = ev_in[3 * nsl];
+  cudaEvent_t *ev_cp = c.slab_ev.data(), *ev_in = ev_cp + np, *ev_out = ev_in + np, ev0 = ev_out[nr];
+  // the transfer position of each piece; a row can run once the last of
+  // the pieces holding its planes and its two neighbouring planes is in
+  const int P = c.piece[0].t1 - c.piece[0].t0;
+  auto pos = [&](int i) { return i == np - 1 ? 0 : i + 1; };
+  std::vector<int> need(nr, 0), rows_left(np, 0);
+  for (int k = 0; k < nr; k++) {
+    const Slab &sb = c.slab[k];
+    for (int t = sb.t0 - 1; t <= sb.t1; t++) need[k] = std::max(need[k], pos(((t + L0) % L0) / P));
+    for (int i = sb.t0 / P; i <= (sb.t1 - 1) / P; i++) rows_left[i]++;
+  }
   cudaEventRecord(ev0, c.stream);
   cudaStreamWaitEvent(c.st_in, ev0, 0);
   cudaStreamWaitEvent(c.st_cv, ev0, 0);
   cudaStreamWaitEvent(c.st_out, ev0, 0);
-  // the host-to-device copies run back to back on st_in; each slab's
-  // conversion to the device layout follows on st_cv
-  auto h2d = [&](int k) {
-    const Slab &sb = c.slab[k];
+  auto h2d = [&](int i) {
+    const Piece &pc = c.piece[i];
     for (int p = 0; p < 2; p++) {
-      const size_t o = (size_t)sb.q0[p] * site, n = (size_t)(sb.q1[p] - sb.q0[p]) * site;
+      const size_t o = (size_t)pc.q0[p] * site, n = (size_t)(pc.q1[p] - pc.q0[p]) * site;
       cudaMemcpyAsync(st_in + o, (const char *)s + o, n, cudaMemcpyHostToDevice, c.st_in);
     }
-    cudaEventRecord(ev_cp[k], c.st_in);
-    cudaStreamWaitEvent(c.st_cv, ev_cp[k], 0);
-    for (int p = 0; p < 2; p++) {
-      const int d0 = (p * c.g.nbl + sb.b0) * c.g.vbh, nd = (sb.b1 - sb.b0) * c.g.vbh;
-      spinor_from_ref_range(c, prec, st_in, fs, d0, nd, c.st_cv);
-    }
-    cudaEventRecord(ev_in[k], c.st_cv);
+    cudaEventRecord(ev_cp[i], c.st_in);
+    cudaStreamWaitEvent(c.st_cv, ev_cp[i], 0);
+    spinor_from_ref_piece(c, prec, st_in, fs, pc, c.st_cv);
+    cudaEventRecord(ev_in[i], c.st_cv);
   };
+  // the pieces a row completes go out together: per parity half, their
+  // storage ranges sorted and the adjacent ones joined into one copy
+  auto d2h = [&](const std::vector<int> &done) {
+    for (int p = 0; p < 2; p++) {
+      std::vector<std::pair<int, int>> rg;
+      for (int i : done) rg.push_back({c.piece[i].q0[p], c.piece[i].q1[p]});
+      std::sort(rg.begin(), rg.end());
+      for (size_t a = 0; a < rg.size();) {
+        size_t b = a + 1;
+        int q1 = rg[a].second;
+        while (b < rg.size() && rg[b].first == q1) q1 = rg[b++].second;
+        const size_t o = (size_t)rg[a].first * site, n = (size_t)(q1 - rg[a].first) * site;
+        cudaMemcpyAsync((char *)r + o, st_out + o, n, cudaMemcpyDeviceToHost, c.st_out);
+        a = b;
+      }
+    }
+  };
+  // row k after the conversion of piece `after` (the conversions run in
+  // order on one stream, so the earlier ones are done too)
   auto comp = [&](int k, int after) {
     const Slab &sb = c.slab[k];
     cudaStreamWaitEvent(c.stream, ev_in[after], 0);
@@ -118,21 +149,20 @@ static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr
       spinor_to_ref_range(c, prec, fr, st_out, d0, nd, c.stream);
     }
     cudaEventRecord(ev_out[k], c.stream);
-    cudaStreamWaitEvent(c.st_out, ev_out[k], 0);
-    for (int p = 0; p < 2; p++) {
-      const size_t o = (size_t)sb.q0[p] * site, n = (size_t)(sb.q1[p] - sb.q0[p]) * site;
-      cudaMemcpyAsync((char *)r + o, st_out + o, n, cudaMemcpyDeviceToHost, c.st_out);
+    std::vector<int> done;
+    for (int i = sb.t0 / P; i <= (sb.t1 - 1) / P; i++)
+      if (--rows_left[i] == 0) done.push_back(i);
+    if (!done.empty()) {
+      cudaStreamWaitEvent(c.st_out, ev_out[k], 0);
+      d2h(done);
     }
   };
-  // slab j-1 has its neighbours j-2 (or nsl-1), j-1, j once slab j is in
-  h2d(nsl - 1);
-  h2d(0);
-  for (int j = 1; j <= nsl - 2; j++) {
-    h2d(j);
-    comp(j - 1, j);
+  for (int j = 0; j < np; j++) {
+    const int i = j == 0 ? np - 1 : j - 1;
+    h2d(i);
+    for (int k = 0; k < nr; k++)
+      if (need[k] == j) comp(k, i);
   }
-  comp(nsl - 2, nsl - 2);
-  comp(nsl - 1, nsl - 2);
   const cudaError_t e1 = cudaStreamSynchronize(c.st_out), e2 = cudaStreamSynchronize(c.stream),
                     e3 = cudaStreamSynchronize(c.st_in), e4 = cudaStreamSynchronize(c.st_cv);
   if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess || e4 != cudaSuccess)
@@ -157,7 +187,8 @@ static void ref_layout_op(int op, R mu, const void *s, void *r) {
   void *fr = prec == 64 ? c.ws64[1] : c.ws32[1];
   char *st_in = (char *)c.stage, *st_out = (char *)c.stage + nb;
   cudaStream_t st = c.stream;
-  if (op == 0 && c.pipeline && !qcd::dd_on(c) && c.slab.size() >= 3 && pinned_host(s) && pinned_host(r)) {
+  if (op == 0 && c.pipeline && !qcd::dd_on(c) && c.slab.size() >= 3 && c.piece.size() >= 3 && pinned_host(s) &&
+      pinned_host(r)) {
     dw_pipelined<R>(c, mu, s, r, fs, fr, st_in, st_out);
     return;
   }
@@ -459,6 +490,7 @@ int b200_set_pipeline(int on) {
 }
 
 int b200_pipeline_slabs(void) { return (int)ctx().slab.size(); }
+int b200_pipeline_pieces(void) { return (int)ctx().piece.size(); }
 
 int b200_set_dw_staged(int mode) {
   Ctx &c = ctx();

@@ -17,6 +17,16 @@
 
 namespace qcd {
 
+// the pieces of the host pipeline hold at least this many sites (or a
+// sixteenth of the lattice, if less): 12.6 MB of FP64 spinors, copied in as
+// two ranges of 6.3 MB.  At 32^3x64 (lexicographic order) a Dw_dble call
+// took 10.43 ms with pieces of two planes, 11.17 ms with single planes
+// (twice the copies and conversions) and 10.86 ms with whole block rows
+#ifndef PIPE_PIECE_SITES
+#define PIPE_PIECE_SITES 65536
+#endif
+static const size_t kPieceSites = PIPE_PIECE_SITES;
+
 static int pack4(const int a[4]) { return a[0] | (a[1] << 8) | (a[2] << 16) | (a[3] << 24); }
 
 static uint64_t interleave(const int *n, int dims, int first) {
@@ -107,8 +117,8 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
   g.bcoord = c.d_bcoord;
   g.lcoord = c.d_lcoord;
 
-  cudaFree(c.d_dev2q); cudaFree(c.d_link2q);
-  c.d_dev2q = c.d_link2q = nullptr;
+  cudaFree(c.d_dev2q); cudaFree(c.d_link2q); cudaFree(c.d_q2dev);
+  c.d_dev2q = c.d_link2q = c.d_q2dev = nullptr;
   c.have_ipt = false;
   if (ipt) {
     std::vector<int> d2q(g.vol), l2q(4 * (size_t)g.vol), seen(g.vol, 0);
@@ -143,42 +153,64 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
         cudaMalloc(&c.d_link2q, 4 * (size_t)g.vol * sizeof(int)) != cudaSuccess)
       return fail("geometry: device allocation failed");
     cudaMemcpy(c.d_dev2q, d2q.data(), g.vol * sizeof(int), cudaMemcpyHostToDevice);
+    {
+      std::vector<int> q2d(g.vol);
+      for (int d = 0; d < g.vol; d++) q2d[d2q[d]] = d;
+      if (cudaMalloc(&c.d_q2dev, g.vol * sizeof(int)) != cudaSuccess) return fail("geometry: device allocation failed");
+      cudaMemcpy(c.d_q2dev, q2d.data(), g.vol * sizeof(int), cudaMemcpyHostToDevice);
+    }
     cudaMemcpy(c.d_link2q, l2q.data(), 4 * (size_t)g.vol * sizeof(int), cudaMemcpyHostToDevice);
     c.h_dev2q = d2q;
     c.h_ipt.assign(ipt, ipt + g.vol);
     c.have_ipt = true;
   }
-  // x0-slab plan: the thinnest slabs (a whole number of block rows, at least
-  // three slabs) whose sites are contiguous in each parity half of the
-  // storage order.  openQCD's ipt orders the sites by the thread-local
-  // sub-lattices with x0 slowest (modules/lattice/geometry.c:200-240), so
-  // slabs of L0_TRD planes qualify.
+  // Plans of the host pipeline (Dw / Dw_dble on page-locked host arrays):
+  // the slabs are the block rows along x0 (at least three); the pieces are
+  // the thinnest x0-slabs of at least kPieceSites sites (or a sixteenth of
+  // the lattice; at least three pieces) whose sites are a contiguous range
+  // of each parity half of the storage order.  Lexicographic orders with x0
+  // slowest qualify plane by plane; openQCD's ipt orders the sites by the
+  // thread-local sub-lattices with x0 slowest (modules/lattice/
+  // geometry.c:200-240), so pieces of L0_TRD planes qualify.
   c.slab.clear();
-  if (ipt) {
-    const int nb0 = g.nb[0], bs0 = g.bstr[0];
-    for (int rows = 1; rows <= nb0 / 3 && c.slab.empty(); rows++) {
-      if (nb0 % rows) continue;
-      const int R = nb0 / rows;
-      std::vector<Slab> sl(R);
-      bool ok = true;
-      for (int k = 0; k < R && ok; k++) {
-        Slab &sb = sl[k];
-        sb.b0 = k * rows * bs0;
-        sb.b1 = (k + 1) * rows * bs0;
-        for (int p = 0; p < 2 && ok; p++) {
-          const size_t d0 = (size_t)(p * g.nbl + sb.b0) * g.vbh, d1 = (size_t)(p * g.nbl + sb.b1) * g.vbh;
-          int lo = g.vol, hi = -1;
-          for (size_t d = d0; d < d1; d++) {
-            lo = std::min(lo, c.h_dev2q[d]);
-            hi = std::max(hi, c.h_dev2q[d]);
+  c.piece.clear();
+  if (ipt && g.nb[0] >= 3) {
+    const int L0 = L[0], ps = g.vol / L0;
+    std::vector<int> lo(2 * L0, g.vol), hi(2 * L0, -1);
+    int x[4];
+    for (x[0] = 0; x[0] < L0; x[0]++)
+      for (x[1] = 0; x[1] < L[1]; x[1]++)
+        for (x[2] = 0; x[2] < L[2]; x[2]++)
+          for (x[3] = 0; x[3] < L[3]; x[3]++) {
+            const int q = ipt[x[3] + L[3] * (x[2] + L[2] * (x[1] + L[1] * x[0]))];
+            const int k = 2 * x[0] + ((x[0] + x[1] + x[2] + x[3]) & 1);
+            lo[k] = std::min(lo[k], q);
+            hi[k] = std::max(hi[k], q);
           }
-          ok = (size_t)(hi - lo + 1) == d1 - d0;
-          sb.q0[p] = lo;
-          sb.q1[p] = hi + 1;
+    for (int P = 1; P <= L0 / 3 && c.piece.empty(); P++) {
+      if (L0 % P || (size_t)P * ps < std::min(kPieceSites, (size_t)g.vol / 16)) continue;
+      std::vector<Piece> pcs(L0 / P);
+      bool ok = true;
+      for (int i = 0; i < L0 / P && ok; i++) {
+        Piece &pc = pcs[i];
+        pc.t0 = i * P;
+        pc.t1 = (i + 1) * P;
+        for (int p = 0; p < 2 && ok; p++) {
+          int a = g.vol, b = -1;
+          for (int t = pc.t0; t < pc.t1; t++) {
+            a = std::min(a, lo[2 * t + p]);
+            b = std::max(b, hi[2 * t + p]);
+          }
+          ok = b - a + 1 == P * ps / 2;   // a plane holds ps/2 sites of each parity
+          pc.q0[p] = a;
+          pc.q1[p] = b + 1;
         }
       }
-      if (ok) c.slab = sl;
+      if (ok) c.piece = pcs;
     }
+    if (!c.piece.empty())
+      for (int k = 0; k < g.nb[0]; k++)
+        c.slab.push_back(Slab{k * g.bstr[0], (k + 1) * g.bstr[0], k * bs[0], (k + 1) * bs[0]});
   }
   cudaFree(c.d_ident);
   c.d_ident = nullptr;
@@ -216,6 +248,37 @@ __global__ void k_spinor_to_ref(Geom g, const int *__restrict__ d2q, const void 
   spinor<R> v = Store<R>::load_spinor_rw(dev, chunk, s, g.vbh);
 #pragma unroll
   for (int k = 0; k < 12; k++) { dst[2 * k] = v.c[k / 3].c[k % 3].re; dst[2 * k + 1] = v.c[k / 3].c[k % 3].im; }
+}
+
+// the sites of a piece, both parity halves in one launch: thread i takes
+// storage index q0[0] + i or q0[1] + (i - n0), reads it (contiguous) and
+// stores it at its device site
+template <typename R>
+__global__ void k_spinor_from_ref_piece(Geom g, const int *__restrict__ q2d, const R *__restrict__ q, void *dev,
+                                        int qa, int na, int qb, int nb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na + nb) return;
+  const int iq = i < na ? qa + i : qb + (i - na);
+  const int d = __ldg(q2d + iq);
+  const int chunk = d / g.vbh, s = d - chunk * g.vbh;
+  const R *src = q + (size_t)iq * 24;
+  spinor<R> v;
+#pragma unroll
+  for (int k = 0; k < 12; k++) v.c[k / 3].c[k % 3] = mk<R>(src[2 * k], src[2 * k + 1]);
+  Store<R>::store_spinor(dev, chunk, s, g.vbh, v);
+}
+
+int spinor_from_ref_piece(const Ctx &c, int prec, const void *q, void *dev, const Piece &pc, cudaStream_t st) {
+  if (!c.d_q2dev) return fail("no reference site order: pass ipt[] to the geometry call");
+  const int t = 128, na = pc.q1[0] - pc.q0[0], nb = pc.q1[1] - pc.q0[1];
+  const unsigned grid = (unsigned)((na + nb + t - 1) / t);
+  if (prec == 64)
+    k_spinor_from_ref_piece<double><<<grid, t, 0, st>>>(c.g, c.d_q2dev, (const double *)q, dev, pc.q0[0], na,
+                                                        pc.q0[1], nb);
+  else
+    k_spinor_from_ref_piece<float><<<grid, t, 0, st>>>(c.g, c.d_q2dev, (const float *)q, dev, pc.q0[0], na,
+                                                       pc.q0[1], nb);
+  return cudaGetLastError() == cudaSuccess ? 0 : fail("spinor_from_ref: launch failed");
 }
 
 int spinor_from_ref_range(const Ctx &c, int prec, const void *q, void *dev, int d0, int n, cudaStream_t st) {

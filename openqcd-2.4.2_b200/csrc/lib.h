@@ -33,11 +33,18 @@ struct DDState {
   long long nxchg = 0;
 };
 
-// An x0-slab of the lattice whose sites are contiguous ranges of the
-// reference's storage order in each parity half: device blocks [b0, b1)
-// (lexicographic block order, x0 slowest) and storage indices [q0[p], q1[p]).
+// The host pipeline of Dw / Dw_dble works on two plans of x0-slabs.  A
+// Slab is one block row, the unit of the operator launches: device blocks
+// [b0, b1) (lexicographic block order, x0 slowest), planes [t0, t1).  A
+// Piece is the unit of the transfers and layout conversions: planes
+// [t0, t1) whose sites are the storage indices [q0[p], q1[p]) of each
+// parity half of the caller's storage order.
 struct Slab {
   int b0, b1;
+  int t0, t1;
+};
+struct Piece {
+  int t0, t1;
   int q0[2], q1[2];
 };
 
@@ -120,12 +127,15 @@ struct Ctx {
   // reference (openQCD) storage order, when the caller supplied its ipt[]
   bool have_ipt = false;
   int *d_dev2q = nullptr;       // [vol] device site (chunk*vbh+s) -> reference index ix
+  int *d_q2dev = nullptr;       // [vol] its inverse
   int *d_link2q = nullptr;      // [4*vol] (device site, mu) -> slot in the reference ud[4V]
   std::vector<int> h_dev2q;
   std::vector<int> h_ipt;       // the caller's ipt[] (for a change of block shape)
-  // x0-slab plan for pipelined host transfers (empty if the storage order
-  // has no contiguous slabs), the identity block list, the copy streams
+  // slab and piece plans for pipelined host transfers (both empty if the
+  // storage order has no contiguous pieces), the identity block list, the
+  // copy streams
   std::vector<Slab> slab;
+  std::vector<Piece> piece;
   int *d_ident = nullptr;
   cudaStream_t st_in = nullptr, st_out = nullptr, st_cv = nullptr;
   std::vector<cudaEvent_t> slab_ev;
@@ -241,6 +251,7 @@ int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream
 // the same for the device sites [d0, d0 + n) only
 int spinor_from_ref_range(const Ctx &c, int prec, const void *q, void *dev, int d0, int n, cudaStream_t st);
 int spinor_to_ref_range(const Ctx &c, int prec, const void *dev, void *q, int d0, int n, cudaStream_t st);
+int spinor_from_ref_piece(const Ctx &c, int prec, const void *q, void *dev, const Piece &pc, cudaStream_t st);
 int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st);
 int links_from_ref(Ctx &c, const void *qud, cudaStream_t st);                           // qud on device
 int links_to_ref(const Ctx &c, void *qud, cudaStream_t st);

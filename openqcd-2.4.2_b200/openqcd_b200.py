@@ -132,6 +132,7 @@ _SIGS = {
     "b200_set_cuda_graphs": (C.c_int, [C.c_int]),
     "b200_set_pipeline": (C.c_int, [C.c_int]),
     "b200_pipeline_slabs": (C.c_int, []),
+    "b200_pipeline_pieces": (C.c_int, []),
     "b200_graphs_cached": (C.c_int, []),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_void_p]),
@@ -326,7 +327,13 @@ def set_pipeline(on):
 
 
 def pipeline_slabs():
+    """block rows of the host pipeline (0: no pipeline)"""
     return lib().b200_pipeline_slabs()
+
+
+def pipeline_pieces():
+    """transfer pieces of the host pipeline (0: no pipeline)"""
+    return lib().b200_pipeline_pieces()
 
 
 def graphs_cached():
