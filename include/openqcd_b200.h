@@ -310,11 +310,14 @@ int b200_set_cuda_graphs(int on);
  * planes are in; a piece is copied out once its rows are done.  Otherwise,
  * or with 0, the fields are copied whole.  Returns the previous setting.
  * b200_pipeline_slabs: the number of block rows of the pipeline,
- * b200_pipeline_pieces: the number of pieces (0: no pipeline).  No
- * reference counterpart. */
+ * b200_pipeline_pieces: the number of pieces (0: no pipeline);
+ * b200_pipeline_used: 1 if the last Dw_dble or Dw call on host arrays ran
+ * the pipeline, 0 if it copied the fields whole.  No reference
+ * counterpart. */
 int b200_set_pipeline(int on);
 int b200_pipeline_slabs(void);
 int b200_pipeline_pieces(void);
+int b200_pipeline_used(void);
 int b200_graphs_cached(void);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32, 16, or 12 for the 12-real links): index,

@@ -189,9 +189,11 @@ static void ref_layout_op(int op, R mu, const void *s, void *r) {
   cudaStream_t st = c.stream;
   if (op == 0 && c.pipeline && !qcd::dd_on(c) && c.slab.size() >= 3 && c.piece.size() >= 3 && pinned_host(s) &&
       pinned_host(r)) {
+    c.pipeline_used = 1;
     dw_pipelined<R>(c, mu, s, r, fs, fr, st_in, st_out);
     return;
   }
+  if (op == 0) c.pipeline_used = 0;
   cudaMemcpyAsync(st_in, s, nb, cudaMemcpyDefault, st);
   spinor_from_ref(c, prec, st_in, fs, st);
   if (op != 0) {
@@ -491,6 +493,7 @@ int b200_set_pipeline(int on) {
 
 int b200_pipeline_slabs(void) { return (int)ctx().slab.size(); }
 int b200_pipeline_pieces(void) { return (int)ctx().piece.size(); }
+int b200_pipeline_used(void) { return ctx().pipeline_used; }
 
 int b200_set_dw_staged(int mode) {
   Ctx &c = ctx();

@@ -140,6 +140,7 @@ struct Ctx {
   cudaStream_t st_in = nullptr, st_out = nullptr, st_cv = nullptr;
   std::vector<cudaEvent_t> slab_ev;
   int pipeline = 1;             // pipelined host transfers of Dw / Dw_dble when possible
+  int pipeline_used = 0;        // whether the last host Dw / Dw_dble call ran the pipeline
 
   // parameters
   double csw = 0.0, m0 = 0.0;

@@ -133,6 +133,7 @@ _SIGS = {
     "b200_set_pipeline": (C.c_int, [C.c_int]),
     "b200_pipeline_slabs": (C.c_int, []),
     "b200_pipeline_pieces": (C.c_int, []),
+    "b200_pipeline_used": (C.c_int, []),
     "b200_graphs_cached": (C.c_int, []),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_void_p]),
@@ -334,6 +335,12 @@ def pipeline_slabs():
 def pipeline_pieces():
     """transfer pieces of the host pipeline (0: no pipeline)"""
     return lib().b200_pipeline_pieces()
+
+
+def pipeline_used():
+    """1 if the last host Dw / Dw_dble call ran the pipeline, 0 if it copied
+    the fields whole"""
+    return lib().b200_pipeline_used()
 
 
 def graphs_cached():

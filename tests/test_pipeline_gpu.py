@@ -66,16 +66,19 @@ def _piped_whole_inplace(prec, mu, s):
     try:
         hs.a[:] = s
         f(mu, hs.ptr, hr.ptr)
+        assert qb.pipeline_used() == 1
         piped = hr.a.copy()
         prev = qb.set_pipeline(False)
         try:
             hr.a[:] = 0
             f(mu, hs.ptr, hr.ptr)
+            assert qb.pipeline_used() == 0
             whole = hr.a.copy()
         finally:
             qb.set_pipeline(prev)
         hx.a[:] = s
         f(mu, hx.ptr, hx.ptr)
+        assert qb.pipeline_used() == 1
         inplace = hx.a.copy()
     finally:
         for h in (hs, hr, hx):
