@@ -20,7 +20,10 @@ struct GraphEntry {
 };
 std::vector<GraphEntry> g_graphs;
 unsigned long long g_tick = 0;
-const size_t kMaxGraphs = 96;
+// the batched deflated solver with two masses per batch keeps about 80
+// graphs alive (SAP sequences, orthogonalisation passes, little-solver
+// iterations); two alternating mass pairs need about twice that
+const size_t kMaxGraphs = 256;
 }  // namespace
 
 void graphs_release() {
