@@ -81,6 +81,20 @@ static bool pinned_host(const void *p) {
 // directions overlap.  The output
 // of a piece is written only after its own input was copied, so s and r may
 // be the same array.
+// The two parity ranges of a piece (or of the pieces a row completes), at
+// offsets o[0] < o[1] of both arrays, as one copy of two rows (pitch o[1] -
+// o[0]) when they are equally long; otherwise, or if the pitch is refused,
+// as two copies.
+static void copy_pair(char *dst, const char *src, const size_t o[2], const size_t n[2], cudaMemcpyKind kind,
+                      cudaStream_t st) {
+  if (n[0] == n[1] && n[0] > 0 && o[1] >= o[0] + n[0] &&
+      cudaMemcpy2DAsync(dst + o[0], o[1] - o[0], src + o[0], o[1] - o[0], n[0], 2, kind, st) == cudaSuccess)
+    return;
+  cudaGetLastError();
+  for (int p = 0; p < 2; p++)
+    if (n[p]) cudaMemcpyAsync(dst + o[p], src + o[p], n[p], kind, st);
+}
+
 template <typename R>
 static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr, char *st_in, char *st_out) {
   const int prec = sizeof(R) == 8 ? 64 : 32;
@@ -112,10 +126,9 @@ static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr
   cudaStreamWaitEvent(c.st_out, ev0, 0);
   auto h2d = [&](int i) {
     const Piece &pc = c.piece[i];
-    for (int p = 0; p < 2; p++) {
-      const size_t o = (size_t)pc.q0[p] * site, n = (size_t)(pc.q1[p] - pc.q0[p]) * site;
-      cudaMemcpyAsync(st_in + o, (const char *)s + o, n, cudaMemcpyHostToDevice, c.st_in);
-    }
+    const size_t o[2] = {(size_t)pc.q0[0] * site, (size_t)pc.q0[1] * site};
+    const size_t n[2] = {(size_t)(pc.q1[0] - pc.q0[0]) * site, (size_t)(pc.q1[1] - pc.q0[1]) * site};
+    copy_pair(st_in, (const char *)s, o, n, cudaMemcpyHostToDevice, c.st_in);
     cudaEventRecord(ev_cp[i], c.st_in);
     cudaStreamWaitEvent(c.st_cv, ev_cp[i], 0);
     spinor_from_ref_piece(c, prec, st_in, fs, pc, c.st_cv);
@@ -124,19 +137,31 @@ static int dw_pipelined(Ctx &c, R mu, const void *s, void *r, void *fs, void *fr
   // the pieces a row completes go out together: per parity half, their
   // storage ranges sorted and the adjacent ones joined into one copy
   auto d2h = [&](const std::vector<int> &done) {
+    std::vector<std::pair<int, int>> rg[2];
     for (int p = 0; p < 2; p++) {
-      std::vector<std::pair<int, int>> rg;
-      for (int i : done) rg.push_back({c.piece[i].q0[p], c.piece[i].q1[p]});
-      std::sort(rg.begin(), rg.end());
-      for (size_t a = 0; a < rg.size();) {
+      std::vector<std::pair<int, int>> in;
+      for (int i : done) in.push_back({c.piece[i].q0[p], c.piece[i].q1[p]});
+      std::sort(in.begin(), in.end());
+      for (size_t a = 0; a < in.size();) {
         size_t b = a + 1;
-        int q1 = rg[a].second;
-        while (b < rg.size() && rg[b].first == q1) q1 = rg[b++].second;
-        const size_t o = (size_t)rg[a].first * site, n = (size_t)(q1 - rg[a].first) * site;
-        cudaMemcpyAsync((char *)r + o, st_out + o, n, cudaMemcpyDeviceToHost, c.st_out);
+        int q1 = in[a].second;
+        while (b < in.size() && in[b].first == q1) q1 = in[b++].second;
+        rg[p].push_back({in[a].first, q1});
         a = b;
       }
     }
+    if (rg[0].size() == 1 && rg[1].size() == 1) {
+      const size_t o[2] = {(size_t)rg[0][0].first * site, (size_t)rg[1][0].first * site};
+      const size_t n[2] = {(size_t)(rg[0][0].second - rg[0][0].first) * site,
+                           (size_t)(rg[1][0].second - rg[1][0].first) * site};
+      copy_pair((char *)r, st_out, o, n, cudaMemcpyDeviceToHost, c.st_out);
+      return;
+    }
+    for (int p = 0; p < 2; p++)
+      for (const auto &q : rg[p]) {
+        const size_t o = (size_t)q.first * site, n = (size_t)(q.second - q.first) * site;
+        cudaMemcpyAsync((char *)r + o, st_out + o, n, cudaMemcpyDeviceToHost, c.st_out);
+      }
   };
   // row k after the conversion of piece `after` (the conversions run in
   // order on one stream, so the earlier ones are done too)
