@@ -302,7 +302,7 @@ int b200_set_cuda_graphs(int on);
  * pipeline (copy in, operator, copy out of different parts of the lattice
  * overlap) when the lattice has at least three block rows along x0 and can
  * be cut into at least three x0-slabs ("pieces", as thin as possible, at
- * least 65536 sites or a sixteenth of the lattice) that are contiguous
+ * least 131072 sites or a sixteenth of the lattice) that are contiguous
  * ranges of each parity half of the caller's storage order: planes for a
  * lexicographic order with x0 slowest, multiples of L0_TRD planes for
  * openQCD's ipt[].  The pieces are copied in and converted one by one; the operator

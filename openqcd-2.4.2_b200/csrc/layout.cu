@@ -18,12 +18,13 @@
 namespace qcd {
 
 // the pieces of the host pipeline hold at least this many sites (or a
-// sixteenth of the lattice, if less): 12.6 MB of FP64 spinors, copied in as
-// two ranges of 6.3 MB.  At 32^3x64 (lexicographic order) a Dw_dble call
-// took 10.43 ms with pieces of two planes, 11.17 ms with single planes
-// (twice the copies and conversions) and 10.86 ms with whole block rows
+// sixteenth of the lattice, if less): 25 MB of FP64 spinors.  At 32^3x64
+// (lexicographic order, pieces of 1, 2 or 4 planes) a Dw_dble call took
+// 11.0, 10.5-10.8 and 10.2-10.3 ms on one box, 16.4, 15.5 and 15.2 ms on
+// another, and on a third 11.2 and 10.4 ms for 1 and 2 planes against
+// 10.9 ms with the earlier pipeline of block rows
 #ifndef PIPE_PIECE_SITES
-#define PIPE_PIECE_SITES 65536
+#define PIPE_PIECE_SITES 131072
 #endif
 static const size_t kPieceSites = PIPE_PIECE_SITES;
 
