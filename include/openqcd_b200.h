@@ -318,6 +318,10 @@ int b200_set_pipeline(int on);
 int b200_pipeline_slabs(void);
 int b200_pipeline_pieces(void);
 int b200_pipeline_used(void);
+/* The numbers of pieces and block rows the pipeline would have for lattice
+ * L, blocks bs and storage order ipt (host code only; needs no device and
+ * no geometry call).  No reference counterpart. */
+int b200_pipeline_plan(const int L[4], const int bs[4], const int *ipt, int *npieces, int *nslabs);
 int b200_graphs_cached(void);
 /* Launch variant of the SAP block kernel picked by the autotuner for the
  * current block size (prec 32, 16, or 12 for the 12-real links): index,

@@ -520,6 +520,19 @@ int b200_pipeline_slabs(void) { return (int)ctx().slab.size(); }
 int b200_pipeline_pieces(void) { return (int)ctx().piece.size(); }
 int b200_pipeline_used(void) { return ctx().pipeline_used; }
 
+int b200_pipeline_plan(const int L[4], const int bs[4], const int *ipt, int *npieces, int *nslabs) {
+  if (!L || !bs || !ipt || !npieces || !nslabs) return fail("pipeline_plan: null argument");
+  for (int mu = 0; mu < 4; mu++)
+    if (L[mu] < 2 || bs[mu] < 2 || L[mu] % bs[mu] || L[mu] > 4096)
+      return fail("pipeline_plan: block sizes must divide the lattice sizes");
+  std::vector<qcd::Piece> pc;
+  std::vector<qcd::Slab> sl;
+  qcd::pipeline_plan(L, bs, ipt, pc, sl);
+  *npieces = (int)pc.size();
+  *nslabs = (int)sl.size();
+  return 0;
+}
+
 int b200_set_dw_staged(int mode) {
   Ctx &c = ctx();
   const int prev = c.dw_staged;

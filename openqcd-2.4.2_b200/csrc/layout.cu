@@ -74,6 +74,59 @@ int set_block_order(Ctx &c, int kind) {
   return 0;
 }
 
+// Plans of the host pipeline (Dw / Dw_dble on page-locked host arrays):
+// the slabs are the block rows along x0 (at least three); the pieces are
+// the thinnest x0-slabs of at least kPieceSites sites (or a sixteenth of
+// the lattice; at least three pieces) whose sites are a contiguous range of
+// each parity half of the storage order.  Lexicographic orders with x0
+// slowest qualify plane by plane; openQCD's ipt orders the sites by the
+// thread-local sub-lattices with x0 slowest (modules/lattice/
+// geometry.c:200-240), so pieces of L0_TRD planes qualify.  Host code only
+// (the values of ipt are compared, never used as addresses).
+void pipeline_plan(const int L[4], const int bs[4], const int *ipt, std::vector<Piece> &piece,
+                   std::vector<Slab> &slab) {
+  slab.clear();
+  piece.clear();
+  const int nb0 = L[0] / bs[0], bstr0 = (L[1] / bs[1]) * (L[2] / bs[2]) * (L[3] / bs[3]);
+  const int vol = L[0] * L[1] * L[2] * L[3];
+  if (!ipt || nb0 < 3) return;
+  const int L0 = L[0], ps = vol / L0;
+  std::vector<int> lo(2 * L0, vol), hi(2 * L0, -1);
+  int x[4];
+  for (x[0] = 0; x[0] < L0; x[0]++)
+    for (x[1] = 0; x[1] < L[1]; x[1]++)
+      for (x[2] = 0; x[2] < L[2]; x[2]++)
+        for (x[3] = 0; x[3] < L[3]; x[3]++) {
+          const int q = ipt[x[3] + L[3] * (x[2] + L[2] * (x[1] + L[1] * x[0]))];
+          const int k = 2 * x[0] + ((x[0] + x[1] + x[2] + x[3]) & 1);
+          lo[k] = std::min(lo[k], q);
+          hi[k] = std::max(hi[k], q);
+        }
+  for (int P = 1; P <= L0 / 3 && piece.empty(); P++) {
+    if (L0 % P || (size_t)P * ps < std::min(kPieceSites, (size_t)vol / 16)) continue;
+    std::vector<Piece> pcs(L0 / P);
+    bool ok = true;
+    for (int i = 0; i < L0 / P && ok; i++) {
+      Piece &pc = pcs[i];
+      pc.t0 = i * P;
+      pc.t1 = (i + 1) * P;
+      for (int p = 0; p < 2 && ok; p++) {
+        int a = vol, b = -1;
+        for (int t = pc.t0; t < pc.t1; t++) {
+          a = std::min(a, lo[2 * t + p]);
+          b = std::max(b, hi[2 * t + p]);
+        }
+        ok = b - a + 1 == P * ps / 2;   // a plane holds ps/2 sites of each parity
+        pc.q0[p] = a;
+        pc.q1[p] = b + 1;
+      }
+    }
+    if (ok) piece = pcs;
+  }
+  if (!piece.empty())
+    for (int k = 0; k < nb0; k++) slab.push_back(Slab{k * bstr0, (k + 1) * bstr0, k * bs[0], (k + 1) * bs[0]});
+}
+
 int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
   Geom &g = c.g;
   for (int mu = 0; mu < 4; mu++) {
@@ -165,54 +218,7 @@ int geometry_init(Ctx &c, const int L[4], const int bs[4], const int *ipt) {
     c.h_ipt.assign(ipt, ipt + g.vol);
     c.have_ipt = true;
   }
-  // Plans of the host pipeline (Dw / Dw_dble on page-locked host arrays):
-  // the slabs are the block rows along x0 (at least three); the pieces are
-  // the thinnest x0-slabs of at least kPieceSites sites (or a sixteenth of
-  // the lattice; at least three pieces) whose sites are a contiguous range
-  // of each parity half of the storage order.  Lexicographic orders with x0
-  // slowest qualify plane by plane; openQCD's ipt orders the sites by the
-  // thread-local sub-lattices with x0 slowest (modules/lattice/
-  // geometry.c:200-240), so pieces of L0_TRD planes qualify.
-  c.slab.clear();
-  c.piece.clear();
-  if (ipt && g.nb[0] >= 3) {
-    const int L0 = L[0], ps = g.vol / L0;
-    std::vector<int> lo(2 * L0, g.vol), hi(2 * L0, -1);
-    int x[4];
-    for (x[0] = 0; x[0] < L0; x[0]++)
-      for (x[1] = 0; x[1] < L[1]; x[1]++)
-        for (x[2] = 0; x[2] < L[2]; x[2]++)
-          for (x[3] = 0; x[3] < L[3]; x[3]++) {
-            const int q = ipt[x[3] + L[3] * (x[2] + L[2] * (x[1] + L[1] * x[0]))];
-            const int k = 2 * x[0] + ((x[0] + x[1] + x[2] + x[3]) & 1);
-            lo[k] = std::min(lo[k], q);
-            hi[k] = std::max(hi[k], q);
-          }
-    for (int P = 1; P <= L0 / 3 && c.piece.empty(); P++) {
-      if (L0 % P || (size_t)P * ps < std::min(kPieceSites, (size_t)g.vol / 16)) continue;
-      std::vector<Piece> pcs(L0 / P);
-      bool ok = true;
-      for (int i = 0; i < L0 / P && ok; i++) {
-        Piece &pc = pcs[i];
-        pc.t0 = i * P;
-        pc.t1 = (i + 1) * P;
-        for (int p = 0; p < 2 && ok; p++) {
-          int a = g.vol, b = -1;
-          for (int t = pc.t0; t < pc.t1; t++) {
-            a = std::min(a, lo[2 * t + p]);
-            b = std::max(b, hi[2 * t + p]);
-          }
-          ok = b - a + 1 == P * ps / 2;   // a plane holds ps/2 sites of each parity
-          pc.q0[p] = a;
-          pc.q1[p] = b + 1;
-        }
-      }
-      if (ok) c.piece = pcs;
-    }
-    if (!c.piece.empty())
-      for (int k = 0; k < g.nb[0]; k++)
-        c.slab.push_back(Slab{k * g.bstr[0], (k + 1) * g.bstr[0], k * bs[0], (k + 1) * bs[0]});
-  }
+  pipeline_plan(L, bs, ipt, c.piece, c.slab);
   cudaFree(c.d_ident);
   c.d_ident = nullptr;
   {

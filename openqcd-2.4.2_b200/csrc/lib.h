@@ -253,6 +253,8 @@ int spinor_from_ref(const Ctx &c, int prec, const void *q, void *dev, cudaStream
 int spinor_from_ref_range(const Ctx &c, int prec, const void *q, void *dev, int d0, int n, cudaStream_t st);
 int spinor_to_ref_range(const Ctx &c, int prec, const void *dev, void *q, int d0, int n, cudaStream_t st);
 int spinor_from_ref_piece(const Ctx &c, int prec, const void *q, void *dev, const Piece &pc, cudaStream_t st);
+void pipeline_plan(const int L[4], const int bs[4], const int *ipt, std::vector<Piece> &piece,
+                   std::vector<Slab> &slab);
 int spinor_to_ref(const Ctx &c, int prec, const void *dev, void *q, cudaStream_t st);
 int links_from_ref(Ctx &c, const void *qud, cudaStream_t st);                           // qud on device
 int links_to_ref(const Ctx &c, void *qud, cudaStream_t st);

@@ -134,6 +134,7 @@ _SIGS = {
     "b200_pipeline_slabs": (C.c_int, []),
     "b200_pipeline_pieces": (C.c_int, []),
     "b200_pipeline_used": (C.c_int, []),
+    "b200_pipeline_plan": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "b200_graphs_cached": (C.c_int, []),
     "tmcg": (C.c_double, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                           C.c_void_p]),
@@ -335,6 +336,17 @@ def pipeline_slabs():
 def pipeline_pieces():
     """transfer pieces of the host pipeline (0: no pipeline)"""
     return lib().b200_pipeline_pieces()
+
+
+def pipeline_plan(L, bs, ipt):
+    """(pieces, block rows) of the host pipeline for lattice L, blocks bs and
+    storage order ipt (host code; no device needed)"""
+    Lc = np.ascontiguousarray(L, dtype=np.int32)
+    bc = np.ascontiguousarray(bs, dtype=np.int32)
+    ip = np.ascontiguousarray(ipt, dtype=np.int32)
+    npc, nsl = C.c_int(0), C.c_int(0)
+    check(lib().b200_pipeline_plan(_ptr(Lc), _ptr(bc), _ptr(ip), C.byref(npc), C.byref(nsl)))
+    return npc.value, nsl.value
 
 
 def pipeline_used():
